@@ -1,0 +1,226 @@
+/*
+ * tensum_gpu.h -- C ABI of the B200 residual/update path for TENSUM's 2D
+ * vertex-centred median-dual finite-volume solver.
+ *
+ * Drop-in boundary.  In the reference the hot path is reached through private
+ * members of FiniteVolume (src/fv.h:351-403) called from FiniteVolume::solve
+ * (src/fv.cc:2273-2305), operating on the member arrays primitive,
+ * conserved_old, entropy_var, residual, dE, dE_cell, dt (src/fv.h:137-164) and
+ * on the public Grid data (src/grid.h:141-229).  Each entry point below
+ * replaces one of those calls; the caller keeps the reference's parameter
+ * reader, part-file reader, Grid::preproc and writers unchanged and hands the
+ * resulting arrays across this ABI.
+ *
+ * Conventions
+ *  - Plain C types only; every pointer is a HOST pointer unless the name ends
+ *    in _dev.  Arrays use the reference's local vertex/cell/face numbering.
+ *  - Every call returns tg_status; nothing throws across the ABI.  After a
+ *    failure tg_last_error(h) returns a message (thread-local when h is NULL).
+ *  - One host thread per handle.  Calls are ordered on the handle's CUDA
+ *    stream and return after the work is complete unless documented otherwise.
+ *  - The device path has no CPU fallback: without a usable CUDA device
+ *    tg_create returns TG_NO_DEVICE.
+ */
+#ifndef TENSUM_GPU_H
+#define TENSUM_GPU_H
+
+#ifdef __cplusplus
+extern "C" {
+#endif
+
+#define TG_ABI_VERSION 1
+
+typedef enum {
+  TG_OK = 0,
+  TG_BAD_STATE = 1,     /* non-finite value or p <= 0 / rho <= 0 seen in an update   */
+  TG_TIMEOUT = 2,       /* a bounded device wait ran out                            */
+  TG_CUDA_ERROR = 3,    /* a CUDA runtime call failed                               */
+  TG_INVALID_ARG = 4,   /* malformed mesh / option / size                           */
+  TG_NOT_SUPPORTED = 5, /* option the device path does not implement               */
+  TG_NO_DEVICE = 6      /* no CUDA device visible                                   */
+} tg_status;
+
+/* Material::FluxScheme, src/material.h:78-91 (same order). */
+typedef enum {
+  TG_FLUX_KEPES_TECNO_ROE = 0,
+  TG_FLUX_KEPES_TECNO_RUSANOV = 1,
+  TG_FLUX_KEPEC = 2,
+  TG_FLUX_ROE_EC = 3,
+  TG_FLUX_KEP = 4,
+  TG_FLUX_AVG = 5
+} tg_flux_scheme;
+
+/* Material::ReconstructScheme, src/material.h:97-106 (same order). */
+typedef enum {
+  TG_RECON_FIRST = 0,
+  TG_RECON_SECOND = 1,
+  TG_RECON_SECOND_MUSCL = 2,
+  TG_RECON_VAN_ALBADA = 3,
+  TG_RECON_TVD_MINMOD = 4,
+  TG_RECON_TVB_MINMOD = 5,
+  TG_RECON_ENO2 = 6
+} tg_reconstruct_scheme;
+
+/* Material::MuModel, src/material.h:92-95. */
+typedef enum { TG_MU_CONSTANT = 0, TG_MU_SUTHERLAND = 1, TG_MU_POWER = 2 } tg_mu_model;
+
+/* BC::BCType, src/bc.h:16-25 (same order). */
+typedef enum {
+  TG_BC_NONE = 0,
+  TG_BC_SLIP = 1,
+  TG_BC_NOSLIP = 2,
+  TG_BC_FARFIELD = 3,
+  TG_BC_INLET = 4,
+  TG_BC_OUTLET = 5,
+  TG_BC_PRESSURE = 6,
+  TG_BC_PERIODIC = 7
+} tg_bc_kind;
+
+/*
+ * Mesh after Grid::preproc (src/grid_preproc.cc:1147-1194), one partition,
+ * 2D (radius 1), median dual.  Field-by-field the members of Grid:
+ *   coords        vertex[i].coord.{x,y}                      2*n_vertex
+ *   dcarea/mcarea dual / median areas, periodic-summed        n_vertex
+ *   cell_vertex   cell[c].vertex[0..2]                        3*n_cell
+ *   cell_normal   cell[c].normal[k].{x,y} (P1 normals)        6*n_cell
+ *   cell_area     cell[c].area                                n_cell
+ *   face_*        face[f]: vertex[0..1], type (-1 interior, else boundary tag),
+ *                 normal.{x,y} (dual-face normal), lcell, rcell (-1 if none).
+ *                 Boundary faces come first, face[i] <-> bface[i].
+ *   bface_*       bface[b]: vertex[0..1], type, normal.{x,y} (outward),
+ *                 lcell, periodic flag.
+ *   periodic_*    periodic_lists[i].P_ij as CSR (offsets n_periodic+1).
+ */
+typedef struct {
+  int n_vertex;
+  const double* coords;
+  const double* dcarea;
+  const double* mcarea;
+  int n_cell;
+  const int* cell_vertex;
+  const double* cell_normal;
+  const double* cell_area;
+  int n_face;
+  const int* face_vertex;
+  const int* face_type;
+  const double* face_normal;
+  const int* face_lcell;
+  const int* face_rcell;
+  int n_bface;
+  const int* bface_vertex;
+  const int* bface_type;
+  const double* bface_normal;
+  const int* bface_lcell;
+  const unsigned char* bface_periodic;
+  int n_periodic;
+  const int* periodic_offsets;
+  const int* periodic_members;
+} tg_mesh;
+
+/* class Material, src/material.h:54-420 (data members). */
+typedef struct {
+  double gamma;
+  double gas_const;
+  double prandtl;
+  double mu_ref;
+  double T_0;
+  double T_ref;
+  double omega;
+  double ev_mod_alpha;
+  double ev_mod_beta;
+  double tvb_minmod_coef;
+  int model;               /* 0 = euler, 1 = ns (Material::FlowModel) */
+  int flux_scheme;         /* tg_flux_scheme */
+  int mu_model;            /* tg_mu_model */
+  int reconstruct_scheme;  /* tg_reconstruct_scheme */
+  int nd_active;
+  int visc_active;
+  int heat_active;
+} tg_material;
+
+/*
+ * Boundary conditions.  The reference evaluates fparser expressions of (x,y,t)
+ * per boundary vertex inside BoundaryCondition::apply (src/bc.h:568-654); for
+ * SSP-RK3 the time argument is never advanced, so the caller evaluates them
+ * once and passes the values per boundary-face vertex:
+ *   bface_values[(2*b + k)*5 + {0..4}] = (T, u, v, w, p) at bface[b].vertex[k].
+ * Components a kind does not use are ignored; bface_values may be NULL when
+ * every kind is periodic/slip/outlet.
+ */
+typedef struct {
+  int n_types;
+  const int* type_tag;             /* boundary tag (face type)                   */
+  const int* kind;                 /* tg_bc_kind per tag                         */
+  const unsigned char* adiabatic;  /* BoundaryCondition::adiabatic per tag        */
+  const double* bface_values;      /* n_bface*2*5 or NULL                         */
+} tg_bc_table;
+
+typedef enum { TG_TIME_SSPRK3 = 0, TG_TIME_RK4 = 1, TG_TIME_HEUNS = 2 } tg_time_scheme;
+typedef enum { TG_STEADY = 0, TG_UNSTEADY = 1 } tg_time_mode;
+
+/* Parameter members of the numeric/output sections, src/parameter.h. */
+typedef struct {
+  int time_scheme;      /* tg_time_scheme                                         */
+  int time_mode;        /* tg_time_mode                                           */
+  double time_step;     /* > 0: fixed global step (src/fv.cc:1503-1509)           */
+  double cfl;
+  double final_time;
+  int n_time_stamps;    /* unsteady output instances: t_i = i*final_time/n        */
+  long max_iter;
+  double min_residue;
+  int bad_state_check;  /* nonzero: flag non-finite / p<=0 / rho<=0 in updates  */
+} tg_options;
+
+typedef struct tg_handle tg_handle;
+
+/* ---- lifetime ---------------------------------------------------------- */
+
+/* Replaces FiniteVolume::initialize (src/fv.cc:25-197) for the hot path:
+ * validates the mesh, builds the device layout, allocates all device memory. */
+tg_status tg_create(const tg_mesh* mesh, const tg_material* mat, const tg_bc_table* bc,
+                    const tg_options* opt, tg_handle** out);
+tg_status tg_destroy(tg_handle* h);
+const char* tg_last_error(const tg_handle* h);
+int tg_abi_version(void);
+
+/* ---- state ------------------------------------------------------------- */
+
+/* primitive[] <- prim_aos (T,u,v,w,p per vertex, PrimVar layout, src/primvar.h:17-18),
+ * then entropy_var = prim2ent(primitive) (src/fv.cc:392-393).  Resets time to t0. */
+tg_status tg_set_state(tg_handle* h, const double* prim_aos, int n_vertex, double t0);
+/* prim_aos <- primitive[] (periodic copies receive their set's value). */
+tg_status tg_get_state(tg_handle* h, double* prim_aos, int n_vertex);
+
+/* ---- hot path, one call per reference member function ----------------- */
+
+/* store_conserved_old (src/fv.cc:1626-1630). */
+tg_status tg_store_conserved_old(tg_handle* h);
+/* compute_dt (src/fv.cc:1499-1621): local dt, periodic sum, global min and the
+ * unsteady clamp to the next output time.  dt_out (n_vertex) may be NULL. */
+tg_status tg_compute_dt(tg_handle* h, double* dt_global_out, double* dt_out);
+/* compute_gradients (src/fv.cc:699-1059): dE_out is n_vertex*5*3 in the
+ * reference layout dE[v][var][xyz] (var order V1,V2,V3,V4,V5; z = 0). May be NULL. */
+tg_status tg_gradients(tg_handle* h, double* dE_out);
+/* compute_residual (src/fv.cc:1467-1494): gradients + inviscid + viscous +
+ * periodic sum.  res_out is n_vertex*5 in Flux layout (mass, mx, my, mz, energy). */
+tg_status tg_residual(tg_handle* h, double* res_out);
+/* update_solution(r) for SSP-RK3 (src/fv.cc:1635-1658). */
+tg_status tg_update(tg_handle* h, int r);
+/* compute_residual_norm (src/fv.cc:1801-1879) on the current residual.
+ * out[0..5] = mass, mx, my, energy norms, total (normalised), total0. */
+tg_status tg_residual_norm(tg_handle* h, long iter, double* out6);
+
+/* One or more complete time steps of FiniteVolume::solve's loop
+ * (src/fv.cc:2273-2316): store_conserved_old, compute_dt, n_rks x
+ * (compute_residual, [norm at last stage], update_solution), t += dt.
+ * Steps after final_time is reached are no-ops.  info (may be NULL) receives
+ * {elapsed_time, dt_global, residual_norm_total, iterations_done}. */
+tg_status tg_step(tg_handle* h, int n_steps, double* info4);
+
+/* Global kinetic energy and entropy integrals, compute_global (src/fv.cc:2175-2225). */
+tg_status tg_global(tg_handle* h, double* ke_out, double* entropy_out);
+
+#ifdef __cplusplus
+}
+#endif
+#endif /* TENSUM_GPU_H */

@@ -1,0 +1,252 @@
+// Dump harness around the unmodified TENSUM reference sources.
+//
+// Test infrastructure only: it is compiled together with the reference's own
+// src/*.cc (minus src/main.cc) by oracle/Makefile into oracle/_ref/, and run in
+// this container to produce golden fixtures (tests/golden/) and, on a host
+// without the reference tree, as the timed CPU arm of bench.py.  Nothing in the
+// product links or calls it.
+//
+// It drives FiniteVolume exactly like FiniteVolume::solve (src/fv.cc:2273-2305)
+// but exposes the per-stage arrays: the class members are private in
+// src/fv.h:119-404, so this translation unit opens them with a preprocessor
+// override before including the header (the reference files are untouched).
+//
+// Usage:
+//   tensum_harness <param.in> <case_dir> <ic.bin|-> <n_steps> <n_dump_steps> <out.bin>
+//
+// case_dir holds PARTITION/part_file_0.dat.  ic.bin (optional, "-" to use the
+// parameter file's initial condition) is n_vertex x 5 doubles in the reference
+// PrimVar order (T, u, v, w, p), indexed like the part file's active vertices.
+// Full per-stage arrays are dumped for the first n_dump_steps steps; the state
+// after the last step is always dumped.  The wall time of the stepping loop is
+// written as record "wall_s" so the harness doubles as the reference CPU timer.
+
+#include <cmath>
+#include <cstdio>
+#include <cstdlib>
+#include <cstring>
+#include <fstream>
+#include <iostream>
+#include <map>
+#include <set>
+#include <sstream>
+#include <string>
+#include <vector>
+#include <chrono>
+#include <algorithm>
+#include <complex>
+#include <limits>
+#include <iomanip>
+#include <stdint.h>
+#include <dlfcn.h>
+#include <mpi.h>
+
+// Every system header the reference pulls in is included above, so the
+// override below only reaches the reference's own class definitions.
+#define private public
+#include "fv.h"
+#undef private
+
+// Globals normally defined in src/main.cc:10-31.
+Dimension dim;
+bool debug;
+bool restart;
+bool preprocess;
+bool bounds;
+bool verbose;
+bool PERIODIC;
+std::map<std::string, double> constants;
+unsigned int NPART;
+unsigned int N_MC_GROUPS;
+std::vector<double> rnd_nos;
+
+namespace {
+
+struct Dump {
+  FILE* f = nullptr;
+  explicit Dump(const char* path) { f = std::fopen(path, "wb"); if (!f) { std::perror(path); std::exit(2); } }
+  ~Dump() { if (f) std::fclose(f); }
+  void rec(const std::string& tag, const std::vector<double>& v) {
+    char name[32];
+    std::memset(name, 0, sizeof(name));
+    std::strncpy(name, tag.c_str(), sizeof(name) - 1);
+    long long n = (long long)v.size();
+    std::fwrite(name, 1, sizeof(name), f);
+    std::fwrite(&n, sizeof(n), 1, f);
+    if (n) std::fwrite(v.data(), sizeof(double), (size_t)n, f);
+  }
+};
+
+std::vector<double> prim_vec(const std::vector<PrimVar>& p) {
+  std::vector<double> out;
+  out.reserve(p.size() * 5);
+  for (const auto& q : p) {
+    out.push_back(q.temperature);
+    out.push_back(q.velocity.x);
+    out.push_back(q.velocity.y);
+    out.push_back(q.velocity.z);
+    out.push_back(q.pressure);
+  }
+  return out;
+}
+
+std::vector<double> flux_vec(const std::vector<Flux>& r) {
+  std::vector<double> out;
+  out.reserve(r.size() * 5);
+  for (const auto& q : r) {
+    out.push_back(q.mass_flux);
+    out.push_back(q.momentum_flux.x);
+    out.push_back(q.momentum_flux.y);
+    out.push_back(q.momentum_flux.z);
+    out.push_back(q.energy_flux);
+  }
+  return out;
+}
+
+std::vector<double> grad_vec(const std::vector<std::vector<Vector> >& g) {
+  std::vector<double> out;
+  out.reserve(g.size() * 15);
+  for (const auto& v : g)
+    for (unsigned int k = 0; k < NVAR; ++k) {
+      out.push_back(v[k].x);
+      out.push_back(v[k].y);
+      out.push_back(v[k].z);
+    }
+  return out;
+}
+
+void dump_geometry(Dump& d, const Grid& g) {
+  std::vector<double> coords, cells, cnormal, carea, faces, bfaces, nbr;
+  for (const auto& v : g.vertex) { coords.push_back(v.coord.x); coords.push_back(v.coord.y); }
+  for (const auto& c : g.cell) {
+    for (int k = 0; k < 3; ++k) cells.push_back(c.vertex[k]);
+    for (int k = 0; k < 3; ++k) { cnormal.push_back(c.normal[k].x); cnormal.push_back(c.normal[k].y); }
+    carea.push_back(c.area);
+    nbr.push_back((double)c.nbr_bface.size());
+  }
+  for (const auto& f : g.face) {
+    faces.push_back(f.vertex[0]); faces.push_back(f.vertex[1]); faces.push_back(f.type);
+    faces.push_back(f.normal.x); faces.push_back(f.normal.y); faces.push_back(f.measure);
+    faces.push_back(f.lcell); faces.push_back(f.rcell);
+  }
+  for (const auto& f : g.bface) {
+    bfaces.push_back(f.vertex[0]); bfaces.push_back(f.vertex[1]); bfaces.push_back(f.type);
+    bfaces.push_back(f.normal.x); bfaces.push_back(f.normal.y); bfaces.push_back(f.measure);
+    bfaces.push_back(f.lcell); bfaces.push_back(f.periodic ? 1.0 : 0.0);
+  }
+  std::vector<double> periodic;  // flattened: count, members...
+  for (const auto& p : g.periodic_lists) {
+    periodic.push_back((double)p.P_ij.size());
+    for (int v : p.P_ij) periodic.push_back(v);
+  }
+  d.rec("coords", coords);
+  d.rec("cells", cells);
+  d.rec("cell_normal", cnormal);
+  d.rec("cell_area", carea);
+  d.rec("cell_nbr_bface", nbr);
+  d.rec("faces", faces);
+  d.rec("bfaces", bfaces);
+  d.rec("dcarea", g.dcarea);
+  d.rec("mcarea", g.mcarea);
+  d.rec("periodic", periodic);
+}
+
+}  // namespace
+
+int main(int argc, char* argv[]) {
+  if (argc < 7) {
+    std::fprintf(stderr, "usage: %s <param.in> <case_dir> <ic.bin|-> <n_steps> <n_dump_steps> <out.bin>\n", argv[0]);
+    return 2;
+  }
+  mpi_init(argc, argv);
+  NPART = 1;
+  N_MC_GROUPS = 1;
+  PERIODIC = false;
+  dim = two;
+  debug = restart = preprocess = bounds = verbose = false;
+
+  const long n_steps = std::atol(argv[4]);
+  const long n_dump = std::atol(argv[5]);
+  Dump dump(argv[6]);
+
+  FiniteVolume fv(argv[1], argv[2]);
+  fv.grid.read(fv.param);
+  fv.create_force_face_list();
+  fv.initialize();
+  fv.counter = 0;
+  fv.initialize_sample_run(fv.param.sample_start_ind);
+
+  if (std::strcmp(argv[3], "-") != 0) {
+    std::ifstream ic(argv[3], std::ios::binary);
+    if (!ic) { std::fprintf(stderr, "cannot open %s\n", argv[3]); return 2; }
+    std::vector<double> buf(fv.grid.n_vertex * 5);
+    ic.read(reinterpret_cast<char*>(buf.data()), (std::streamsize)(buf.size() * sizeof(double)));
+    if (!ic) { std::fprintf(stderr, "short initial-condition file %s\n", argv[3]); return 2; }
+    for (unsigned int i = 0; i < fv.grid.n_vertex; ++i) {
+      fv.primitive[i].temperature = buf[5 * i + 0];
+      fv.primitive[i].velocity.x = buf[5 * i + 1];
+      fv.primitive[i].velocity.y = buf[5 * i + 2];
+      fv.primitive[i].velocity.z = buf[5 * i + 3];
+      fv.primitive[i].pressure = buf[5 * i + 4];
+      fv.entropy_var[i] = fv.param.material.prim2ent(fv.primitive[i]);
+    }
+  }
+
+  dump_geometry(dump, fv.grid);
+  dump.rec("prim0", prim_vec(fv.primitive));
+
+  // Mirrors FiniteVolume::solve (src/fv.cc:2273-2343) without file output.
+  if (fv.counter == 0) fv.counter++;
+  unsigned long iter = 0;
+  fv.residual_norm_total = 1.0e20;
+  auto t0 = std::chrono::steady_clock::now();
+  for (long step = 0; step < n_steps; ++step) {
+    const bool full = step < n_dump;
+    fv.store_conserved_old();
+    fv.compute_dt();
+    if (full) {
+      std::ostringstream tg;
+      tg << "s" << step << "_dt";
+      dump.rec(tg.str(), fv.dt);
+      dump.rec(tg.str() + "g", std::vector<double>(1, fv.dt_global));
+    }
+    if (fv.param.liou_fix) fv.compute_ssw();
+    for (unsigned int r = 0; r < fv.param.n_rks; ++r) {
+      fv.compute_residual();
+      if (r == fv.param.n_rks - 1) fv.compute_residual_norm(iter);
+      if (full) {
+        std::ostringstream tg;
+        tg << "s" << step << "r" << r << "_";
+        dump.rec(tg.str() + "grad", grad_vec(fv.dE));
+        dump.rec(tg.str() + "res", flux_vec(fv.residual));
+      }
+      fv.update_solution(r);
+      if (full) {
+        std::ostringstream tg;
+        tg << "s" << step << "r" << r << "_prim";
+        dump.rec(tg.str(), prim_vec(fv.primitive));
+      }
+    }
+    if (full) {
+      std::ostringstream tg;
+      tg << "s" << step << "_norm";
+      dump.rec(tg.str(), std::vector<double>{fv.residual_norm.mass_flux, fv.residual_norm.momentum_flux.x,
+                                             fv.residual_norm.momentum_flux.y, fv.residual_norm.energy_flux,
+                                             fv.residual_norm_total, fv.residual_norm_total0});
+    }
+    ++iter;
+    fv.elapsed_time += fv.dt_global;
+    if (fv.time_instance_reached && fv.param.time_mode == "unsteady") {
+      fv.counter++;
+      fv.time_instance_reached = false;
+    }
+    if (fv.elapsed_time >= fv.param.final_time) { ++step; dump.rec("steps_run", std::vector<double>(1, (double)step)); break; }
+  }
+  auto t1 = std::chrono::steady_clock::now();
+  dump.rec("wall_s", std::vector<double>(1, std::chrono::duration<double>(t1 - t0).count()));
+  dump.rec("iters", std::vector<double>(1, (double)iter));
+  dump.rec("elapsed", std::vector<double>(1, fv.elapsed_time));
+  dump.rec("prim_final", prim_vec(fv.primitive));
+  mpi_finalize();
+  return 0;
+}

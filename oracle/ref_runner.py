@@ -1,0 +1,202 @@
+"""Drive the compiled TENSUM reference (oracle/_ref) on a synthetic case.
+
+Test infrastructure only (the oracle is the checker, never the product):
+used to generate golden fixtures in a container that has the reference
+sources, and by the reference arm of bench.py to time the reference's own CPU
+code.  It writes a ``param.in`` in the reference's section format
+(src/parameter.cc:16-33, readme/README.md "Description of param.in"), a
+single-partition part file, an optional initial-condition file, runs
+``oracle/_ref/tensum_harness`` and parses its dump.
+"""
+from __future__ import annotations
+
+import os
+import struct
+import subprocess
+import tempfile
+
+import numpy as np
+
+HERE = os.path.dirname(os.path.abspath(__file__))
+HARNESS = os.path.join(HERE, "_ref", "tensum_harness")
+
+RECON_NAMES = {"first", "second", "minmod", "tvb_minmod", "eno2", "van_albada"}
+FLUX_NAMES = {"kepes_tecno_roe", "kepes_tecno_rusanov", "kepec", "kep", "roe_ec", "simple_avg"}
+
+
+def harness_available() -> bool:
+    return os.access(HARNESS, os.X_OK)
+
+
+def param_text(cfg: dict) -> str:
+    """Render a param.in for the reference from a flat config dict.
+
+    Keys: flux, reconstruct, tvb_M, model ('euler'|'ns'), mu_ref, prandtl,
+    gamma, gas_const, cfl, time_mode, time_step, final_time, max_iter,
+    time_stamps, ev_alpha, ev_beta, boundary: {tag: (type, {var: expr})}.
+    """
+    flux = cfg.get("flux", "kepes_tecno_roe")
+    recon = cfg.get("reconstruct", "minmod")
+    assert flux in FLUX_NAMES and recon in RECON_NAMES
+    rec = f"      method   {recon}\n"
+    if recon == "tvb_minmod":
+        rec += f"      M_value  {cfg.get('tvb_M', 1.0):.17g}\n"
+    model = cfg.get("model", "euler")
+    bnd = []
+    for tag, (btype, vals) in sorted(cfg["boundary"].items()):
+        body = "\n".join(f"      {k}   {v}" for k, v in vals.items())
+        bnd.append(f"   {tag}\n   {{\n      type   {btype}\n{body}\n   }}")
+    bnd_text = "\n".join(bnd)
+    return f"""grid
+{{
+   cell      median
+}}
+
+numeric
+{{
+   time_mode    {cfg.get('time_mode', 'unsteady')}
+   time_scheme  {cfg.get('time_scheme', 'ssprk3')}
+   time_step    {cfg.get('time_step', 0.0):.17g}
+   cfl          {cfg.get('cfl', 0.8):.17g}
+   max_iter     {cfg.get('max_iter', 1000000000)}
+   final_time   {cfg.get('final_time', 10.0):.17g}
+   min_residue  0.0
+   reconstruct
+   {{
+{rec}   }}
+   bc_scheme    weak
+   liou_fix     no
+   sample_list
+   {{
+      groups
+      {{
+      }}
+      free_list
+      {{
+      }}
+   }}
+   rnd_file_loc    rnd_nos.dat
+   rnd_per_sample  0
+}}
+
+material
+{{
+   gamma       {cfg.get('gamma', 1.4):.17g}
+   gas_const   {cfg.get('gas_const', 1.0):.17g}
+   model       {model}
+   viscosity
+   {{
+      model    constant
+      mu_ref   {cfg.get('mu_ref', 0.0):.17g}
+   }}
+   prandtl     {cfg.get('prandtl', 0.72):.17g}
+   flux        {flux}
+   flux_par
+   {{
+      alpha      {cfg.get('ev_alpha', 0.0):.17g}
+      beta       {cfg.get('ev_beta', 0.0):.17g}
+   }}
+   balance
+   {{
+       switch_active  no
+       ND             yes
+       HEAT           yes
+       VISC           yes
+   }}
+}}
+
+constants
+{{
+   dummy 0.0
+}}
+
+initial_condition
+{{
+   temperature  1.0
+   xvelocity    0.0
+   yvelocity    0.0
+   zvelocity    0.0
+   pressure     1.0
+}}
+
+boundary
+{{
+{bnd_text}
+}}
+
+exact_soln
+{{
+   available    no
+}}
+
+integrals
+{{
+}}
+
+output
+{{
+   format                vtk
+   frequency             100000000
+   time_stamps           {cfg.get('time_stamps', 1)}
+   use_online_stat_tool  no
+   variables
+   {{
+   }}
+   surfaces
+   {{
+   }}
+   restart               no
+   restart_frequency     100
+   log_output            no
+   soln_output           no
+   save_global           no
+   find_error            no
+}}
+"""
+
+
+def read_dump(path: str) -> dict:
+    """Parse the harness dump: records of (32-byte tag, int64 n, n doubles)."""
+    out = {}
+    with open(path, "rb") as fh:
+        data = fh.read()
+    p = 0
+    while p < len(data):
+        tag = data[p:p + 32].split(b"\0", 1)[0].decode()
+        (n,) = struct.unpack_from("<q", data, p + 32)
+        p += 40
+        out[tag] = np.frombuffer(data, dtype="<f8", count=n, offset=p).copy()
+        p += 8 * n
+    return out
+
+
+def run_case(mesh, cfg: dict, prim0: np.ndarray | None, n_steps: int, n_dump: int,
+             workdir: str | None = None, timeout: float = 3600.0) -> dict:
+    """Write the case, run the harness, return the parsed dump."""
+    from tensum_b200.mesh import write_part_file  # local import: tests put repo on sys.path
+
+    if not harness_available():
+        raise RuntimeError("oracle/_ref/tensum_harness is not built (make -C oracle ref)")
+    own = workdir is None
+    wd = workdir or tempfile.mkdtemp(prefix="tensum_ref_")
+    try:
+        write_part_file(mesh, wd)
+        with open(os.path.join(wd, "param.in"), "w") as fh:
+            fh.write(param_text(cfg))
+        ic = "-"
+        if prim0 is not None:
+            ic = os.path.join(wd, "ic.bin")
+            np.ascontiguousarray(prim0, dtype="<f8").tofile(ic)
+        out = os.path.join(wd, "dump.bin")
+        r = subprocess.run([HARNESS, "param.in", ".", ic, str(n_steps), str(n_dump), out],
+                           cwd=wd, capture_output=True, text=True, timeout=timeout)
+        if r.returncode != 0 or not os.path.exists(out):
+            raise RuntimeError(f"reference harness failed ({r.returncode}):\n{r.stdout[-2000:]}\n{r.stderr[-2000:]}")
+        if "ERROR" in r.stdout or "assertion failed" in r.stdout:
+            # the reference reports configuration errors on stdout and may exit 0
+            raise RuntimeError("reference harness reported an error:\n" + r.stdout[-2000:])
+        return read_dump(out)
+    finally:
+        if own:
+            import shutil
+            shutil.rmtree(wd, ignore_errors=True)

@@ -1,0 +1,86 @@
+"""Synthetic workloads: meshes, initial conditions and boundary conditions.
+
+Each case is a seeded stand-in for one of the reference's benchmark setups;
+initial conditions are returned in the reference's PrimVar order
+(T, u, v, w, p) per vertex (src/primvar.h:17-18), i.e. exactly the array a
+reference caller hands to ``tg_set_state``.
+"""
+from __future__ import annotations
+
+import numpy as np
+
+from . import mesh as _mesh
+
+GAMMA = 1.4
+
+
+def vortex_mesh(n: int = 65, seed: int = 0) -> _mesh.TriMesh:
+    """Isentropic-vortex mesh: [-5,5]^2 periodic, n x n vertices."""
+    return _mesh.periodic_square(n, -5.0, 5.0, -5.0, 5.0, seed, name=f"vortex{n}")
+
+
+def vortex_ic(coords: np.ndarray, beta: float = 5.0, gamma: float = GAMMA,
+              u_inf: float = 1.0, v_inf: float = 1.0, gas_const: float = 1.0) -> np.ndarray:
+    """Isentropic vortex (strength beta) centred at the origin in a (1,1,1,1) stream."""
+    x, y = coords[:, 0], coords[:, 1]
+    r2 = x * x + y * y
+    T = 1.0 - (gamma - 1.0) * beta * beta / (8.0 * gamma * np.pi * np.pi) * np.exp(1.0 - r2)
+    e = np.exp(0.5 * (1.0 - r2))
+    u = u_inf - beta / (2.0 * np.pi) * y * e
+    v = v_inf + beta / (2.0 * np.pi) * x * e
+    p = T ** (gamma / (gamma - 1.0))
+    rho = p / (gas_const * T)
+    T = p / (gas_const * rho)
+    return np.stack([T, u, v, np.zeros_like(T), p], axis=1)
+
+
+def kh_mesh(n: int = 1025, seed: int = 0) -> _mesh.TriMesh:
+    """Kelvin-Helmholtz mesh: [0,1]^2 periodic, n x n vertices."""
+    return _mesh.periodic_square(n, 0.0, 1.0, 0.0, 1.0, seed, name=f"kh{n}")
+
+
+def kh_coefficients(seed: int, n_modes: int = 10):
+    """Perturbation amplitudes a_k ~ U[0,1] and phases phi_k ~ U[0, 2 pi)."""
+    rng = np.random.default_rng(seed)
+    a = rng.uniform(0.0, 1.0, n_modes)
+    phi = rng.uniform(0.0, 2.0 * np.pi, n_modes)
+    return a, phi
+
+
+def kh_ic(coords: np.ndarray, a: np.ndarray, phi: np.ndarray, gas_const: float = 1.0) -> np.ndarray:
+    """Kelvin-Helmholtz shear layer with a multimodal vertical-velocity perturbation."""
+    x, y = coords[:, 0], coords[:, 1]
+    inside = np.abs(y - 0.5) < 0.25
+    rho = np.where(inside, 2.0, 1.0)
+    u = np.where(inside, 0.5, -0.5)
+    k = np.arange(1, a.size + 1)
+    v = 0.01 * np.sum(a[None, :] * np.sin(2.0 * np.pi * k[None, :] * x[:, None] + phi[None, :]), axis=1)
+    p = np.full_like(x, 2.5)
+    T = p / (gas_const * rho)
+    return np.stack([T, u, v, np.zeros_like(T), p], axis=1)
+
+
+def cylinder_mesh(n_r: int = 256, n_t: int = 512, seed: int = 0) -> _mesh.TriMesh:
+    """O-mesh around a unit-diameter cylinder out to radius 20."""
+    return _mesh.annulus(n_r, n_t, 0.5, 20.0, 2.0e-3, seed, name=f"cyl{n_r}x{n_t}")
+
+
+def cylinder_freestream(mach: float = 0.2, angle_deg: float = 0.0, gamma: float = GAMMA,
+                        gas_const: float = 1.0):
+    """Free stream with rho = 1, p = 1/gamma (sound speed 1), speed = Mach."""
+    p = 1.0 / gamma
+    rho = 1.0
+    T = p / (gas_const * rho)
+    th = np.deg2rad(angle_deg)
+    return T, mach * np.cos(th), mach * np.sin(th), p
+
+
+def cylinder_ic(coords: np.ndarray, mach: float = 0.2, angle_deg: float = 0.0) -> np.ndarray:
+    T, u, v, p = cylinder_freestream(mach, angle_deg)
+    n = coords.shape[0]
+    return np.stack([np.full(n, T), np.full(n, u), np.full(n, v), np.zeros(n), np.full(n, p)], axis=1)
+
+
+def cylinder_viscosity(mach: float = 0.2, reynolds: float = 100.0, diameter: float = 1.0) -> float:
+    """Constant viscosity giving Re = rho U D / mu with rho = 1."""
+    return mach * diameter / reynolds
