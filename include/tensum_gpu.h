@@ -210,6 +210,12 @@ tg_status tg_update(tg_handle* h, int r);
  * out[0..5] = mass, mx, my, energy norms, total (normalised), total0. */
 tg_status tg_residual_norm(tg_handle* h, long iter, double* out6);
 
+/* Tail of one solve-loop iteration (src/fv.cc:2307-2343): iteration count +1,
+ * elapsed_time += dt_global, advance the output-time counter when reached.
+ * Used with the single-phase calls above; tg_step does it itself.
+ * info4 as for tg_step (may be NULL). */
+tg_status tg_end_step(tg_handle* h, double* info4);
+
 /* One or more complete time steps of FiniteVolume::solve's loop
  * (src/fv.cc:2273-2316): store_conserved_old, compute_dt, n_rks x
  * (compute_residual, [norm at last stage], update_solution), t += dt.
@@ -219,6 +225,35 @@ tg_status tg_step(tg_handle* h, int n_steps, double* info4);
 
 /* Global kinetic energy and entropy integrals, compute_global (src/fv.cc:2175-2225). */
 tg_status tg_global(tg_handle* h, double* ke_out, double* entropy_out);
+
+/* ---- measurement (no counterpart in the reference, whose Timer class,
+ *      src/timer.h:8-72, wraps MPI_Wtime around each phase) -------------- */
+
+/* The CUDA stream (cudaStream_t) every call of this handle is ordered on, so a
+ * caller can bracket calls with its own CUDA events. */
+tg_status tg_stream(tg_handle* h, void** stream_out);
+
+typedef enum {
+  TG_PHASE_GRADIENT = 0,   /* compute_gradients                                   */
+  TG_PHASE_FLUX = 1,       /* inviscid + viscous fluxes and residual assembly     */
+  TG_PHASE_UPDATE = 2,     /* update_solution (changes the state)                 */
+  TG_PHASE_DT = 3,         /* compute_dt                                          */
+  TG_PHASE_STEP = 4        /* one full time step (graph replay)                   */
+} tg_phase;
+
+/* Average device time of one phase over `reps` back-to-back launches, measured
+ * with CUDA events on the handle's stream after one untimed launch. */
+tg_status tg_time_phase(tg_handle* h, int phase, int reps, double* ms_per_launch);
+
+typedef enum {
+  TG_Q_N_VERTEX = 0,
+  TG_Q_N_EDGE = 1,
+  TG_Q_N_BFACE = 2,
+  TG_Q_KERNELS_PER_STEP = 3,   /* kernel launches in one tg_step step        */
+  TG_Q_DEVICE_BYTES = 4,       /* device memory owned by the handle          */
+  TG_Q_KERNELS_PER_PHASE = 5   /* launches of one TG_PHASE_FLUX call         */
+} tg_query_key;
+tg_status tg_query(tg_handle* h, int key, double* out);
 
 #ifdef __cplusplus
 }

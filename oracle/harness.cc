@@ -200,8 +200,10 @@ int main(int argc, char* argv[]) {
   unsigned long iter = 0;
   fv.residual_norm_total = 1.0e20;
   auto t0 = std::chrono::steady_clock::now();
+  std::vector<double> step_s;
   for (long step = 0; step < n_steps; ++step) {
     const bool full = step < n_dump;
+    auto ts = std::chrono::steady_clock::now();
     fv.store_conserved_old();
     fv.compute_dt();
     if (full) {
@@ -235,6 +237,7 @@ int main(int argc, char* argv[]) {
                                              fv.residual_norm_total, fv.residual_norm_total0});
     }
     ++iter;
+    step_s.push_back(std::chrono::duration<double>(std::chrono::steady_clock::now() - ts).count());
     fv.elapsed_time += fv.dt_global;
     if (fv.time_instance_reached && fv.param.time_mode == "unsteady") {
       fv.counter++;
@@ -244,6 +247,7 @@ int main(int argc, char* argv[]) {
   }
   auto t1 = std::chrono::steady_clock::now();
   dump.rec("wall_s", std::vector<double>(1, std::chrono::duration<double>(t1 - t0).count()));
+  dump.rec("step_s", step_s);
   dump.rec("iters", std::vector<double>(1, (double)iter));
   dump.rec("elapsed", std::vector<double>(1, fv.elapsed_time));
   dump.rec("prim_final", prim_vec(fv.primitive));

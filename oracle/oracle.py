@@ -43,6 +43,7 @@ def lib():
         L.tor_compute_residual.argtypes = [vp, dp, dp]
         L.tor_update.argtypes = [vp, C.c_int]
         L.tor_residual_norm.argtypes = [vp, C.c_long, dp]
+        L.tor_end_step.argtypes = [vp]
         L.tor_step.argtypes = [vp, C.c_long, dp]
         L.tor_step.restype = C.c_long
         L.tor_global.argtypes = [vp, dp, dp]
@@ -110,6 +111,9 @@ class Oracle:
         out = np.empty(6)
         self.L.tor_residual_norm(self.h, it, _d(out))
         return out
+
+    def end_step(self):
+        self.L.tor_end_step(self.h)
 
     def step(self, n):
         info = np.empty(4)

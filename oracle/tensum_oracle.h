@@ -38,6 +38,7 @@ void tor_compute_gradients(tor_state* s, double* dE_out);
 void tor_compute_residual(tor_state* s, double* res_out, double* dE_out);
 void tor_update(tor_state* s, int r);
 void tor_residual_norm(tor_state* s, long iter, double* out6);
+void tor_end_step(tor_state* s);
 /* Runs n_steps of the solve loop; returns the number of steps actually taken
  * (stops at final_time).  info4 = {elapsed, dt_global, residual_total, iter}. */
 long tor_step(tor_state* s, long n_steps, double* info4);

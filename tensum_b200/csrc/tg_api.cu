@@ -1,0 +1,566 @@
+// tg_api.cu -- the C ABI of include/tensum_gpu.h over the device kernels.
+//
+// Each entry point replaces one FiniteVolume member call of the reference (see
+// the header for the mapping).  The handle owns all device memory and one
+// stream; whole time steps are captured once into a CUDA graph and replayed.
+#include <cuda_runtime.h>
+
+#include <cstdio>
+#include <cstdlib>
+#include <cstring>
+#include <new>
+#include <string>
+#include <vector>
+
+#include "../../include/tensum_gpu.h"
+#include "tg_kernels.cuh"
+#include "tg_mesh.h"
+
+using namespace tg;
+
+namespace {
+
+thread_local std::string g_last_error;
+
+}  // namespace
+
+struct tg_handle {
+  int device = 0;
+  cudaStream_t stream = nullptr;
+  HostLayout L;
+  Params prm{};
+  Control ctl{};
+  MeshView mv{};
+  StateView sv{};
+  Scalars* sc = nullptr;       // device
+  int* done = nullptr;         // device flag written by k_step_begin
+  int* never = nullptr;        // device zero, used by single-phase calls
+  double* tinst = nullptr;
+  std::vector<void*> allocs;
+  std::string err;
+  int nblocks_v = 0;
+  bool viscous = false;
+  bool grads_needed = false;
+  cudaGraph_t graph = nullptr;
+  cudaGraphExec_t graph_exec = nullptr;
+  // pinned host staging for state transfers (4*nv doubles)
+  double* hP = nullptr;
+  size_t device_bytes = 0;
+  int kernels_per_step = 0;
+  int kernels_per_flux = 0;
+};
+
+namespace {
+
+tg_status fail(tg_handle* h, tg_status st, const std::string& msg) {
+  if (h) h->err = msg;
+  g_last_error = msg;
+  return st;
+}
+
+#define TG_CUDA(h, call)                                                                             \
+  do {                                                                                               \
+    cudaError_t e_ = (call);                                                                         \
+    if (e_ != cudaSuccess)                                                                           \
+      return fail((h), TG_CUDA_ERROR, std::string(#call " failed: ") + cudaGetErrorString(e_));     \
+  } while (0)
+
+template <class T>
+tg_status dev_upload(tg_handle* h, const std::vector<T>& v, const T** out) {
+  void* p = nullptr;
+  size_t bytes = std::max<size_t>(1, v.size()) * sizeof(T);
+  cudaError_t e = cudaMalloc(&p, bytes);
+  if (e != cudaSuccess) return fail(h, TG_CUDA_ERROR, std::string("cudaMalloc: ") + cudaGetErrorString(e));
+  h->allocs.push_back(p);
+  h->device_bytes += bytes;
+  if (!v.empty()) {
+    e = cudaMemcpy(p, v.data(), v.size() * sizeof(T), cudaMemcpyHostToDevice);
+    if (e != cudaSuccess) return fail(h, TG_CUDA_ERROR, std::string("cudaMemcpy: ") + cudaGetErrorString(e));
+  }
+  *out = (const T*)p;
+  return TG_OK;
+}
+
+template <class T>
+tg_status dev_alloc(tg_handle* h, size_t n, T** out) {
+  void* p = nullptr;
+  cudaError_t e = cudaMalloc(&p, std::max<size_t>(1, n) * sizeof(T));
+  if (e != cudaSuccess) return fail(h, TG_CUDA_ERROR, std::string("cudaMalloc: ") + cudaGetErrorString(e));
+  h->allocs.push_back(p);
+  h->device_bytes += std::max<size_t>(1, n) * sizeof(T);
+  cudaMemset(p, 0, std::max<size_t>(1, n) * sizeof(T));
+  *out = (T*)p;
+  return TG_OK;
+}
+
+inline int nblk(int n) { return (n + kBlock - 1) / kBlock; }
+
+// ---- kernel dispatch over (flux, reconstruction)
+typedef void (*EdgeKernel)(Params, MeshView, StateView, const int*);
+
+template <int F>
+EdgeKernel pick_edge(int recon) {
+  switch (recon) {
+    case RECON_FIRST: return k_edge_flux<F, RECON_FIRST>;
+    case RECON_SECOND: return k_edge_flux<F, RECON_SECOND>;
+    case RECON_SECOND_MUSCL: return k_edge_flux<F, RECON_SECOND_MUSCL>;
+    case RECON_VAN_ALBADA: return k_edge_flux<F, RECON_VAN_ALBADA>;
+    case RECON_TVD_MINMOD: return k_edge_flux<F, RECON_TVD_MINMOD>;
+    case RECON_TVB_MINMOD: return k_edge_flux<F, RECON_TVB_MINMOD>;
+    default: return k_edge_flux<F, RECON_ENO2>;
+  }
+}
+template <int F>
+EdgeKernel pick_bflux(int recon) {
+  switch (recon) {
+    case RECON_FIRST: return k_bflux<F, RECON_FIRST>;
+    case RECON_SECOND: return k_bflux<F, RECON_SECOND>;
+    case RECON_SECOND_MUSCL: return k_bflux<F, RECON_SECOND_MUSCL>;
+    case RECON_VAN_ALBADA: return k_bflux<F, RECON_VAN_ALBADA>;
+    case RECON_TVD_MINMOD: return k_bflux<F, RECON_TVD_MINMOD>;
+    case RECON_TVB_MINMOD: return k_bflux<F, RECON_TVB_MINMOD>;
+    default: return k_bflux<F, RECON_ENO2>;
+  }
+}
+
+EdgeKernel edge_kernel(int flux, int recon) {
+  switch (flux) {
+    case FLUX_TECNO_ROE: return pick_edge<FLUX_TECNO_ROE>(recon);
+    case FLUX_TECNO_RUSANOV: return pick_edge<FLUX_TECNO_RUSANOV>(recon);
+    case FLUX_KEPEC: return k_edge_flux<FLUX_KEPEC, RECON_FIRST>;
+    case FLUX_KEP: return k_edge_flux<FLUX_KEP, RECON_FIRST>;
+    case FLUX_ROE_EC: return k_edge_flux<FLUX_ROE_EC, RECON_FIRST>;
+    default: return k_edge_flux<FLUX_AVG, RECON_FIRST>;
+  }
+}
+EdgeKernel bflux_kernel(int flux, int recon) {
+  switch (flux) {
+    case FLUX_TECNO_ROE: return pick_bflux<FLUX_TECNO_ROE>(recon);
+    case FLUX_TECNO_RUSANOV: return pick_bflux<FLUX_TECNO_RUSANOV>(recon);
+    case FLUX_KEPEC: return k_bflux<FLUX_KEPEC, RECON_FIRST>;
+    case FLUX_KEP: return k_bflux<FLUX_KEP, RECON_FIRST>;
+    case FLUX_ROE_EC: return k_bflux<FLUX_ROE_EC, RECON_FIRST>;
+    default: return k_bflux<FLUX_AVG, RECON_FIRST>;
+  }
+}
+
+// ---- phases (all enqueue on h->stream; `done` gates work inside graphs)
+void enqueue_gradient(tg_handle* h, const int* done) {
+  k_gradient<<<nblk(h->mv.nv), kBlock, 0, h->stream>>>(h->prm, h->mv, h->sv, done);
+}
+
+int residual_kernels(const tg_handle* h, bool force_gradient) {
+  return ((h->grads_needed || force_gradient) ? 1 : 0) + 1 + (h->mv.nb > 0 ? 1 : 0) + (h->viscous ? 1 : 0) + 1;
+}
+
+void enqueue_residual(tg_handle* h, const int* done, bool force_gradient) {
+  if (h->grads_needed || force_gradient) enqueue_gradient(h, done);
+  edge_kernel(h->prm.flux, h->prm.recon)<<<nblk(h->mv.ne), kBlock, 0, h->stream>>>(h->prm, h->mv, h->sv, done);
+  if (h->mv.nb > 0)
+    bflux_kernel(h->prm.flux, h->prm.recon)<<<nblk(2 * h->mv.nb), kBlock, 0, h->stream>>>(h->prm, h->mv, h->sv, done);
+  if (h->viscous) k_viscous<<<nblk(h->mv.nvu), kBlock, 0, h->stream>>>(h->prm, h->mv, h->sv, done);
+  k_assemble<<<nblk(h->mv.nv), kBlock, 0, h->stream>>>(h->mv, h->sv, h->viscous ? 1 : 0, done);
+}
+
+void enqueue_dt(tg_handle* h, const int* done) {
+  if (h->ctl.time_step <= 0.0)
+    k_dt<<<nblk(h->mv.nv), kBlock, 0, h->stream>>>(h->prm, h->mv, h->sv, h->sc, done);
+  k_dt_final<<<1, 1, 0, h->stream>>>(h->ctl, h->sc, done);
+}
+
+void enqueue_update(tg_handle* h, int r, bool norm, const int* done) {
+  k_update<<<nblk(h->mv.nv), kBlock, 0, h->stream>>>(h->prm, h->mv, h->sv, h->ctl, h->sc, r, norm ? 1 : 0, done);
+}
+
+void enqueue_norm_final(tg_handle* h, bool use_sc_iter, long long iter, const int* done) {
+  k_norm_final<<<1, kBlock, 0, h->stream>>>(h->sv, h->nblocks_v, h->mv.nv, h->sc, use_sc_iter ? 1 : 0, iter, done);
+}
+
+void enqueue_step(tg_handle* h) {
+  k_step_begin<<<1, 1, 0, h->stream>>>(h->ctl, h->sc, h->done);
+  k_store_old<<<nblk(h->mv.nv), kBlock, 0, h->stream>>>(h->prm, h->mv, h->sv, h->done);
+  // dtmin reset happens in k_step_begin
+  enqueue_dt(h, h->done);
+  for (int r = 0; r < h->ctl.n_rks; ++r) {
+    enqueue_residual(h, h->done, false);
+    bool last = (r == h->ctl.n_rks - 1);
+    enqueue_update(h, r, last, h->done);
+    if (last) enqueue_norm_final(h, true, 0, h->done);
+  }
+  k_step_end<<<1, 1, 0, h->stream>>>(h->ctl, h->sc, h->done);
+}
+
+tg_status sync(tg_handle* h) {
+  TG_CUDA(h, cudaGetLastError());
+  TG_CUDA(h, cudaStreamSynchronize(h->stream));
+  return TG_OK;
+}
+
+tg_status read_scalars(tg_handle* h, Scalars* out) {
+  TG_CUDA(h, cudaMemcpyAsync(out, h->sc, sizeof(Scalars), cudaMemcpyDeviceToHost, h->stream));
+  return sync(h);
+}
+
+tg_status check_bad(tg_handle* h) {
+  Scalars s;
+  tg_status st = read_scalars(h, &s);
+  if (st != TG_OK) return st;
+  if (s.bad) return fail(h, TG_BAD_STATE, "non-finite or non-positive state produced by an update");
+  return TG_OK;
+}
+
+}  // namespace
+
+tg_status capture_step_graph(tg_handle* h) {
+  if (h->graph_exec) return TG_OK;
+  TG_CUDA(h, cudaStreamBeginCapture(h->stream, cudaStreamCaptureModeThreadLocal));
+  enqueue_step(h);
+  cudaError_t e = cudaStreamEndCapture(h->stream, &h->graph);
+  if (e != cudaSuccess) return fail(h, TG_CUDA_ERROR, std::string("graph capture: ") + cudaGetErrorString(e));
+  TG_CUDA(h, cudaGraphInstantiate(&h->graph_exec, h->graph, 0));
+  return TG_OK;
+}
+
+void enqueue_phase(tg_handle* h, int phase) {
+  switch (phase) {
+    case TG_PHASE_GRADIENT: enqueue_gradient(h, h->never); break;
+    case TG_PHASE_FLUX: {
+      edge_kernel(h->prm.flux, h->prm.recon)<<<nblk(h->mv.ne), kBlock, 0, h->stream>>>(h->prm, h->mv, h->sv, h->never);
+      if (h->mv.nb > 0)
+        bflux_kernel(h->prm.flux, h->prm.recon)<<<nblk(2 * h->mv.nb), kBlock, 0, h->stream>>>(h->prm, h->mv, h->sv, h->never);
+      if (h->viscous) k_viscous<<<nblk(h->mv.nvu), kBlock, 0, h->stream>>>(h->prm, h->mv, h->sv, h->never);
+      k_assemble<<<nblk(h->mv.nv), kBlock, 0, h->stream>>>(h->mv, h->sv, h->viscous ? 1 : 0, h->never);
+      break;
+    }
+    case TG_PHASE_UPDATE: enqueue_update(h, 1, false, h->never); break;
+    case TG_PHASE_DT: enqueue_dt(h, h->never); break;
+    default: cudaGraphLaunch(h->graph_exec, h->stream); break;
+  }
+}
+
+extern "C" {
+
+int tg_abi_version(void) { return TG_ABI_VERSION; }
+
+const char* tg_last_error(const tg_handle* h) {
+  if (h && !h->err.empty()) return h->err.c_str();
+  return g_last_error.c_str();
+}
+
+tg_status tg_create(const tg_mesh* mesh, const tg_material* mat, const tg_bc_table* bc, const tg_options* opt,
+                    tg_handle** out) {
+  if (!out) return fail(nullptr, TG_INVALID_ARG, "out is NULL");
+  *out = nullptr;
+  if (!mesh || !mat || !opt) return fail(nullptr, TG_INVALID_ARG, "mesh, material or options is NULL");
+  int ndev = 0;
+  if (cudaGetDeviceCount(&ndev) != cudaSuccess || ndev == 0)
+    return fail(nullptr, TG_NO_DEVICE, "no CUDA device visible; the GPU path has no CPU fallback");
+  if (opt->time_scheme != TG_TIME_SSPRK3)
+    return fail(nullptr, TG_NOT_SUPPORTED, "only the ssprk3 time scheme is implemented on the device");
+  if (mat->flux_scheme < 0 || mat->flux_scheme > 5 || mat->reconstruct_scheme < 0 || mat->reconstruct_scheme > 6)
+    return fail(nullptr, TG_INVALID_ARG, "unknown flux or reconstruction scheme");
+  if (!(mat->gamma > 1.0) || !(mat->gas_const > 0.0)) return fail(nullptr, TG_INVALID_ARG, "gamma must be > 1, gas_const > 0");
+  if (opt->time_mode == TG_UNSTEADY && opt->n_time_stamps <= 0)
+    return fail(nullptr, TG_INVALID_ARG, "unsteady runs need n_time_stamps > 0");
+  if (!(opt->cfl > 0.0) && !(opt->time_step > 0.0)) return fail(nullptr, TG_INVALID_ARG, "cfl or time_step must be > 0");
+
+  tg_handle* h = new (std::nothrow) tg_handle();
+  if (!h) return fail(nullptr, TG_INVALID_ARG, "out of host memory");
+  cudaGetDevice(&h->device);
+  h->viscous = mat->model == 1;
+  std::string msg = build_layout(*mesh, bc, h->viscous, h->L);
+  if (!msg.empty()) {
+    delete h;
+    return fail(nullptr, TG_INVALID_ARG, msg);
+  }
+  const HostLayout& L = h->L;
+  h->grads_needed = h->viscous || ((mat->flux_scheme == FLUX_TECNO_ROE || mat->flux_scheme == FLUX_TECNO_RUSANOV) &&
+                                   mat->reconstruct_scheme != RECON_FIRST);
+
+  Params& k = h->prm;
+  k.gamma = mat->gamma; k.R = mat->gas_const; k.Cp = mat->gamma * mat->gas_const / (mat->gamma - 1.0);
+  k.prandtl = mat->prandtl; k.mu_ref = mat->mu_ref; k.T0 = mat->T_0; k.Tref = mat->T_ref; k.omega = mat->omega;
+  k.ev_alpha = mat->ev_mod_alpha; k.ev_beta = mat->ev_mod_beta; k.tvbM = mat->tvb_minmod_coef; k.cfl = opt->cfl;
+  k.model = mat->model; k.flux = mat->flux_scheme; k.mu_model = mat->mu_model; k.recon = mat->reconstruct_scheme;
+  k.nd = mat->nd_active; k.visc = mat->visc_active; k.heat = mat->heat_active;
+
+  tg_status st;
+#define UP(vec, field) \
+  if ((st = dev_upload(h, L.vec, &h->mv.field)) != TG_OK) { tg_destroy(h); return st; }
+  h->mv.nv = L.nv; h->mv.ne = L.ne; h->mv.nb = L.nb; h->mv.nvu = L.nvu; h->mv.n_int_cells = L.n_int_cells;
+  UP(dcarea, dcarea) UP(inv6mc, inv6mc) UP(pweight, pweight)
+  UP(e_a, e_a) UP(e_b, e_b) UP(e_nx, e_nx) UP(e_ny, e_ny) UP(e_dx, e_dx) UP(e_dy, e_dy)
+  UP(e_g0x, e_g0x) UP(e_g0y, e_g0y) UP(e_g1x, e_g1x) UP(e_g1y, e_g1y)
+  UP(ce_off, ce_off) UP(ce_ent, ce_ent) UP(cb_off, cb_off) UP(cb_ent, cb_ent)
+  UP(b_v0, b_v0) UP(b_v1, b_v1) UP(b_kind, b_kind) UP(b_adiab, b_adiab) UP(b_cell, b_cell)
+  UP(b_nx, b_nx) UP(b_ny, b_ny) UP(b_val, b_val)
+  UP(bf_face_nx, bf_face_nx) UP(bf_face_ny, bf_face_ny) UP(bf_face_v0, bf_face_v0) UP(bf_face_v1, bf_face_v1)
+  UP(u_cell, u_cell) UP(c_v, c_v) UP(c_n, c_n) UP(c_inv2a, c_inv2a)
+  UP(c_bf_off, c_bf_off) UP(c_bf, c_bf) UP(c_nbr_off, c_nbr_off) UP(c_nbr, c_nbr)
+#undef UP
+  const size_t nv = L.nv;
+  h->nblocks_v = nblk(L.nv);
+#define AL(field, n) \
+  if ((st = dev_alloc(h, (n), &h->sv.field)) != TG_OK) { tg_destroy(h); return st; }
+  AL(P, 4 * nv) AL(W, 4 * nv) AL(G, 8 * nv) AL(R, 4 * nv) AL(Uold, 4 * nv) AL(dt, nv)
+  AL(Fe, 4 * (size_t)L.ne) AL(Fb, 8 * (size_t)L.nb) AL(Fv, 9 * (size_t)L.nvu) AL(Fvb, 3 * (size_t)L.nb)
+  AL(part, 4 * (size_t)h->nblocks_v)
+#undef AL
+  if ((st = dev_alloc(h, 1, &h->sc)) != TG_OK) { tg_destroy(h); return st; }
+  if ((st = dev_alloc(h, 1, &h->done)) != TG_OK) { tg_destroy(h); return st; }
+  if ((st = dev_alloc(h, 1, &h->never)) != TG_OK) { tg_destroy(h); return st; }
+
+  // output time instances (src/fv.cc:52-62)
+  std::vector<double> ti;
+  if (opt->time_mode == TG_UNSTEADY) {
+    double dti = opt->final_time / opt->n_time_stamps;
+    for (int i = 0; i <= opt->n_time_stamps; ++i) ti.push_back(i * dti);
+  } else {
+    ti.assign(2, 0.0);
+  }
+  const double* tip = nullptr;
+  if ((st = dev_upload(h, ti, &tip)) != TG_OK) { tg_destroy(h); return st; }
+  Control& c = h->ctl;
+  c.time_mode = opt->time_mode; c.n_rks = 3; c.ntinst = (int)ti.size(); c.time_step = opt->time_step;
+  c.min_residue = opt->min_residue; c.max_iter = opt->max_iter; c.final_time = opt->final_time; c.tinst = tip;
+
+  h->kernels_per_flux = residual_kernels(h, false) - (h->grads_needed ? 1 : 0);
+  h->kernels_per_step = 2 + (c.time_step > 0.0 ? 1 : 2) + 3 * (residual_kernels(h, false) + 1) + 1 + 1;
+  {
+    cudaError_t ep = cudaMallocHost((void**)&h->hP, 4 * nv * sizeof(double));
+    if (ep != cudaSuccess) { tg_destroy(h); return fail(nullptr, TG_CUDA_ERROR, cudaGetErrorString(ep)); }
+  }
+  cudaError_t e = cudaStreamCreateWithFlags(&h->stream, cudaStreamNonBlocking);
+  if (e != cudaSuccess) { tg_destroy(h); return fail(nullptr, TG_CUDA_ERROR, cudaGetErrorString(e)); }
+  e = cudaDeviceSynchronize();
+  if (e != cudaSuccess) { tg_destroy(h); return fail(nullptr, TG_CUDA_ERROR, cudaGetErrorString(e)); }
+  *out = h;
+  return TG_OK;
+}
+
+tg_status tg_destroy(tg_handle* h) {
+  if (!h) return TG_OK;
+  if (h->graph_exec) cudaGraphExecDestroy(h->graph_exec);
+  if (h->graph) cudaGraphDestroy(h->graph);
+  if (h->stream) cudaStreamSynchronize(h->stream);
+  for (void* p : h->allocs) cudaFree(p);
+  if (h->hP) cudaFreeHost(h->hP);
+  if (h->stream) cudaStreamDestroy(h->stream);
+  delete h;
+  return TG_OK;
+}
+
+tg_status tg_set_state(tg_handle* h, const double* prim, int n_vertex, double t0) {
+  if (!h || !prim) return fail(h, TG_INVALID_ARG, "NULL argument");
+  if (n_vertex != h->L.nv) return fail(h, TG_INVALID_ARG, "n_vertex does not match the mesh");
+  const int nv = h->L.nv;
+  for (int i = 0; i < nv; ++i) {
+    const double* q = prim + 5 * (size_t)h->L.old_of_new[i];
+    if (!(q[0] > 0.0) || !(q[4] > 0.0)) return fail(h, TG_INVALID_ARG, "state needs T > 0 and p > 0 (src/fv.cc:388-389)");
+    h->hP[i] = q[0]; h->hP[nv + i] = q[1]; h->hP[2 * (size_t)nv + i] = q[2]; h->hP[3 * (size_t)nv + i] = q[4];
+  }
+  TG_CUDA(h, cudaMemcpyAsync(h->sv.P, h->hP, 4 * (size_t)nv * sizeof(double), cudaMemcpyHostToDevice, h->stream));
+  k_prim2ent<<<nblk(nv), kBlock, 0, h->stream>>>(h->prm, nv, h->sv.P, h->sv.W);
+  Scalars s;
+  std::memset(&s, 0, sizeof(s));
+  s.elapsed = t0;
+  s.rtotal = 1.0e20;
+  s.rtotal0 = 1.0;
+  s.counter = 1;
+  if (h->ctl.time_mode == 1) {
+    double dti = h->ctl.final_time / (h->ctl.ntinst - 1);
+    while (s.counter < h->ctl.ntinst - 1 && s.counter * dti <= t0) s.counter++;
+  }
+  s.dtmin_bits = 0x7ff0000000000000ull;
+  TG_CUDA(h, cudaMemcpyAsync(h->sc, &s, sizeof(s), cudaMemcpyHostToDevice, h->stream));
+  return sync(h);
+}
+
+tg_status tg_get_state(tg_handle* h, double* prim, int n_vertex) {
+  if (!h || !prim) return fail(h, TG_INVALID_ARG, "NULL argument");
+  if (n_vertex != h->L.nv) return fail(h, TG_INVALID_ARG, "n_vertex does not match the mesh");
+  const int nv = h->L.nv;
+  TG_CUDA(h, cudaMemcpyAsync(h->hP, h->sv.P, 4 * (size_t)nv * sizeof(double), cudaMemcpyDeviceToHost, h->stream));
+  tg_status st = sync(h);
+  if (st != TG_OK) return st;
+  for (int i = 0; i < nv; ++i) {
+    double* q = prim + 5 * (size_t)h->L.old_of_new[i];
+    q[0] = h->hP[i]; q[1] = h->hP[nv + i]; q[2] = h->hP[2 * (size_t)nv + i]; q[3] = 0.0; q[4] = h->hP[3 * (size_t)nv + i];
+  }
+  return TG_OK;
+}
+
+tg_status tg_store_conserved_old(tg_handle* h) {
+  if (!h) return fail(h, TG_INVALID_ARG, "NULL handle");
+  k_store_old<<<nblk(h->mv.nv), kBlock, 0, h->stream>>>(h->prm, h->mv, h->sv, h->never);
+  return sync(h);
+}
+
+tg_status tg_compute_dt(tg_handle* h, double* dt_global_out, double* dt_out) {
+  if (!h) return fail(h, TG_INVALID_ARG, "NULL handle");
+  unsigned long long inf = 0x7ff0000000000000ull;
+  TG_CUDA(h, cudaMemcpyAsync(&h->sc->dtmin_bits, &inf, sizeof(inf), cudaMemcpyHostToDevice, h->stream));
+  enqueue_dt(h, h->never);
+  Scalars s;
+  tg_status st = read_scalars(h, &s);
+  if (st != TG_OK) return st;
+  if (dt_global_out) *dt_global_out = s.dt_global;
+  if (dt_out) {
+    const int nv = h->L.nv;
+    std::vector<double> d(nv);
+    if (h->ctl.time_mode == 1 || h->ctl.time_step > 0.0) {
+      for (int i = 0; i < nv; ++i) dt_out[i] = s.dt_global;
+    } else {
+      TG_CUDA(h, cudaMemcpy(d.data(), h->sv.dt, nv * sizeof(double), cudaMemcpyDeviceToHost));
+      for (int i = 0; i < nv; ++i) dt_out[h->L.old_of_new[i]] = d[i];
+    }
+  }
+  return TG_OK;
+}
+
+static tg_status copy_grad_out(tg_handle* h, double* dE_out) {
+  const int nv = h->L.nv;
+  std::vector<double> g(8 * (size_t)nv);
+  TG_CUDA(h, cudaMemcpy(g.data(), h->sv.G, g.size() * sizeof(double), cudaMemcpyDeviceToHost));
+  static const int var_of[4] = {0, 1, 2, 4};
+  for (int i = 0; i < nv; ++i) {
+    double* d = dE_out + 15 * (size_t)h->L.old_of_new[i];
+    for (int q = 0; q < 15; ++q) d[q] = 0.0;
+    for (int c = 0; c < 4; ++c) {
+      d[3 * var_of[c]] = g[(2 * c) * (size_t)nv + i];
+      d[3 * var_of[c] + 1] = g[(2 * c + 1) * (size_t)nv + i];
+    }
+  }
+  return TG_OK;
+}
+
+tg_status tg_gradients(tg_handle* h, double* dE_out) {
+  if (!h) return fail(h, TG_INVALID_ARG, "NULL handle");
+  enqueue_gradient(h, h->never);
+  tg_status st = sync(h);
+  if (st != TG_OK || !dE_out) return st;
+  return copy_grad_out(h, dE_out);
+}
+
+tg_status tg_residual(tg_handle* h, double* res_out) {
+  if (!h) return fail(h, TG_INVALID_ARG, "NULL handle");
+  enqueue_residual(h, h->never, true);
+  tg_status st = sync(h);
+  if (st != TG_OK || !res_out) return st;
+  const int nv = h->L.nv;
+  std::vector<double> r(4 * (size_t)nv);
+  TG_CUDA(h, cudaMemcpy(r.data(), h->sv.R, r.size() * sizeof(double), cudaMemcpyDeviceToHost));
+  for (int i = 0; i < nv; ++i) {
+    double* d = res_out + 5 * (size_t)h->L.old_of_new[i];
+    d[0] = r[i]; d[1] = r[nv + i]; d[2] = r[2 * (size_t)nv + i]; d[3] = 0.0; d[4] = r[3 * (size_t)nv + i];
+  }
+  return TG_OK;
+}
+
+tg_status tg_update(tg_handle* h, int r) {
+  if (!h) return fail(h, TG_INVALID_ARG, "NULL handle");
+  if (r < 0 || r > 2) return fail(h, TG_INVALID_ARG, "stage index must be 0..2 for ssprk3");
+  enqueue_update(h, r, false, h->never);
+  tg_status st = sync(h);
+  if (st != TG_OK) return st;
+  return check_bad(h);
+}
+
+tg_status tg_residual_norm(tg_handle* h, long iter, double* out6) {
+  if (!h) return fail(h, TG_INVALID_ARG, "NULL handle");
+  k_norm_part<<<h->nblocks_v, kBlock, 0, h->stream>>>(h->mv, h->sv, h->never);
+  enqueue_norm_final(h, false, iter, h->never);
+  Scalars s;
+  tg_status st = read_scalars(h, &s);
+  if (st != TG_OK) return st;
+  if (out6) {
+    out6[0] = s.rnorm[0]; out6[1] = s.rnorm[1]; out6[2] = s.rnorm[2]; out6[3] = s.rnorm[3];
+    out6[4] = s.rtotal; out6[5] = s.rtotal0;
+  }
+  return TG_OK;
+}
+
+tg_status tg_end_step(tg_handle* h, double* info4) {
+  if (!h) return fail(h, TG_INVALID_ARG, "NULL handle");
+  k_step_end<<<1, 1, 0, h->stream>>>(h->ctl, h->sc, h->never);
+  Scalars s;
+  tg_status st = read_scalars(h, &s);
+  if (st != TG_OK) return st;
+  if (info4) { info4[0] = s.elapsed; info4[1] = s.dt_global; info4[2] = s.rtotal; info4[3] = (double)s.iter; }
+  return TG_OK;
+}
+
+tg_status tg_step(tg_handle* h, int n_steps, double* info4) {
+  if (!h) return fail(h, TG_INVALID_ARG, "NULL handle");
+  if (n_steps < 0) return fail(h, TG_INVALID_ARG, "n_steps < 0");
+  tg_status st = capture_step_graph(h);
+  if (st != TG_OK) return st;
+  for (int i = 0; i < n_steps; ++i) TG_CUDA(h, cudaGraphLaunch(h->graph_exec, h->stream));
+  Scalars s;
+  st = read_scalars(h, &s);
+  if (st != TG_OK) return st;
+  if (info4) { info4[0] = s.elapsed; info4[1] = s.dt_global; info4[2] = s.rtotal; info4[3] = (double)s.iter; }
+  if (s.bad) return fail(h, TG_BAD_STATE, "non-finite or non-positive state produced by an update");
+  return TG_OK;
+}
+
+tg_status tg_global(tg_handle* h, double* ke, double* ent) {
+  if (!h) return fail(h, TG_INVALID_ARG, "NULL handle");
+  k_global<<<h->nblocks_v, kBlock, 0, h->stream>>>(h->prm, h->mv, h->sv);
+  std::vector<double> part(4 * (size_t)h->nblocks_v);
+  TG_CUDA(h, cudaMemcpyAsync(part.data(), h->sv.part, part.size() * sizeof(double), cudaMemcpyDeviceToHost, h->stream));
+  tg_status st = sync(h);
+  if (st != TG_OK) return st;
+  double a = 0.0, b = 0.0;
+  for (int i = 0; i < h->nblocks_v; ++i) { a += part[4 * (size_t)i]; b += part[4 * (size_t)i + 1]; }
+  if (ke) *ke = a;
+  if (ent) *ent = b;
+  return TG_OK;
+}
+
+tg_status tg_stream(tg_handle* h, void** out) {
+  if (!h || !out) return fail(h, TG_INVALID_ARG, "NULL argument");
+  *out = (void*)h->stream;
+  return TG_OK;
+}
+
+tg_status tg_time_phase(tg_handle* h, int phase, int reps, double* ms) {
+  if (!h || !ms || reps <= 0 || phase < 0 || phase > 4) return fail(h, TG_INVALID_ARG, "bad argument");
+  if (phase == TG_PHASE_STEP) {
+    tg_status st = capture_step_graph(h);
+    if (st != TG_OK) return st;
+  }
+  cudaEvent_t a, b;
+  TG_CUDA(h, cudaEventCreate(&a));
+  TG_CUDA(h, cudaEventCreate(&b));
+  enqueue_phase(h, phase);
+  TG_CUDA(h, cudaEventRecord(a, h->stream));
+  for (int i = 0; i < reps; ++i) enqueue_phase(h, phase);
+  TG_CUDA(h, cudaEventRecord(b, h->stream));
+  tg_status st = sync(h);
+  float t = 0.0f;
+  if (st == TG_OK) {
+    cudaError_t e = cudaEventElapsedTime(&t, a, b);
+    if (e != cudaSuccess) st = fail(h, TG_CUDA_ERROR, cudaGetErrorString(e));
+  }
+  cudaEventDestroy(a);
+  cudaEventDestroy(b);
+  *ms = (double)t / reps;
+  return st;
+}
+
+tg_status tg_query(tg_handle* h, int key, double* out) {
+  if (!h || !out) return fail(h, TG_INVALID_ARG, "NULL argument");
+  switch (key) {
+    case TG_Q_N_VERTEX: *out = h->mv.nv; break;
+    case TG_Q_N_EDGE: *out = h->mv.ne; break;
+    case TG_Q_N_BFACE: *out = h->mv.nb; break;
+    case TG_Q_KERNELS_PER_STEP: *out = h->kernels_per_step; break;
+    case TG_Q_DEVICE_BYTES: *out = (double)h->device_bytes; break;
+    case TG_Q_KERNELS_PER_PHASE: *out = h->kernels_per_flux; break;
+    default: return fail(h, TG_INVALID_ARG, "unknown query key");
+  }
+  return TG_OK;
+}
+
+}  // extern "C"

@@ -1,0 +1,550 @@
+// tg_kernels.cuh -- device kernels of the FP64 single-solve path.
+//
+// One launch per reference phase; every accumulation is a fixed-order gather
+// over per-vertex lists built on the host (tg_mesh.cc), so results are
+// bitwise reproducible from run to run.
+#pragma once
+
+#include <cstdint>
+
+#include "tg_physics.cuh"
+
+namespace tg {
+
+constexpr int kBlock = 256;
+
+struct MeshView {
+  int nv, ne, nb, nvu, n_int_cells;
+  const double *dcarea, *inv6mc, *pweight;
+  const int *e_a, *e_b;
+  const double *e_nx, *e_ny, *e_dx, *e_dy, *e_g0x, *e_g0y, *e_g1x, *e_g1y;
+  const int *ce_off, *ce_ent;
+  const int *cb_off, *cb_ent;
+  const int *b_v0, *b_v1, *b_kind, *b_adiab, *b_cell;
+  const double *b_nx, *b_ny, *b_val;
+  const double *bf_face_nx, *bf_face_ny;
+  const int *bf_face_v0, *bf_face_v1;
+  const int* u_cell;
+  const int* c_v;
+  const double *c_n, *c_inv2a;
+  const int *c_bf_off, *c_bf, *c_nbr_off, *c_nbr;
+};
+
+// Device state, structure-of-arrays with component stride nv (or ne, nb ...).
+struct StateView {
+  double* P;      // 4*nv  T,u,v,p
+  double* W;      // 4*nv  V1,V2,V3,V5
+  double* G;      // 8*nv  dV1/dx, dV1/dy, dV2/dx, ..., dV5/dy
+  double* R;      // 4*nv
+  double* Uold;   // 4*nv
+  double* dt;     // nv
+  double* Fe;     // 4*ne
+  double* Fb;     // 4*2*nb
+  double* Fv;     // 3*3*nvu  (x-mom, y-mom, energy)
+  double* Fvb;    // 3*nb
+  double* part;   // block partial sums
+};
+
+// Step bookkeeping kept on the device so that whole steps replay from a CUDA graph.
+struct Scalars {
+  double dt_global;
+  double elapsed;
+  double rtotal;
+  double rtotal0;
+  double rnorm[4];
+  long long iter;
+  int counter;
+  int reached;
+  int done;
+  int bad;
+  unsigned long long dtmin_bits;
+};
+
+struct Control {
+  int time_mode;       // 0 steady, 1 unsteady
+  int n_rks;
+  int ntinst;
+  double time_step;
+  double min_residue;
+  long long max_iter;
+  double final_time;
+  const double* tinst;
+};
+
+__device__ __forceinline__ Prim load_prim(const double* P, int nv, int i) {
+  Prim q;
+  q.T = P[i]; q.u = P[nv + i]; q.v = P[2 * nv + i]; q.p = P[3 * nv + i];
+  return q;
+}
+
+// Boundary correction n_b * (W_b0 + W_b1 - W_0 - W_1)/2 of one boundary face
+// (src/fv.cc:926-966): states after the single-state BC at each face vertex.
+__device__ __forceinline__ void bface_grad_corr(const Params& k, const MeshView& m, const StateView& s, int d,
+                                                double* dW /*4*/) {
+  int v0 = m.b_v0[d], v1 = m.b_v1[d];
+  Prim s0 = load_prim(s.P, m.nv, v0), s1 = load_prim(s.P, m.nv, v1);
+  double nx = m.b_nx[d], ny = m.b_ny[d];
+  bc_apply1(m.b_kind[d], m.b_adiab[d], m.b_val + (size_t)d * 10, nx, ny, s0);
+  bc_apply1(m.b_kind[d], m.b_adiab[d], m.b_val + (size_t)d * 10 + 5, nx, ny, s1);
+  Ent e0 = prim2ent(k, s0), e1 = prim2ent(k, s1);
+  const double* W = s.W;
+  const int nv = m.nv;
+  dW[0] = (e0.f + e1.f - W[v0] - W[v1]) / 2.0;
+  dW[1] = (e0.vx + e1.vx - W[nv + v0] - W[nv + v1]) / 2.0;
+  dW[2] = (e0.vy + e1.vy - W[2 * nv + v0] - W[2 * nv + v1]) / 2.0;
+  dW[3] = (e0.l + e1.l - W[3 * nv + v0] - W[3 * nv + v1]) / 2.0;
+}
+
+// ------------------------------------------------------------------ kernels
+
+__global__ void k_prim2ent(Params k, int nv, const double* __restrict__ P, double* __restrict__ W) {
+  int i = blockIdx.x * blockDim.x + threadIdx.x;
+  if (i >= nv) return;
+  Ent e = prim2ent(k, load_prim(P, nv, i));
+  W[i] = e.f; W[nv + i] = e.vx; W[2 * nv + i] = e.vy; W[3 * nv + i] = e.l;
+}
+
+// store_conserved_old (src/fv.cc:1626-1630)
+__global__ void k_store_old(Params k, MeshView m, StateView s, const int* __restrict__ done) {
+  if (*done) return;
+  int i = blockIdx.x * blockDim.x + threadIdx.x;
+  if (i >= m.nv) return;
+  Cons c = prim2con(k, load_prim(s.P, m.nv, i));
+  s.Uold[i] = c.r; s.Uold[m.nv + i] = c.mx; s.Uold[2 * m.nv + i] = c.my; s.Uold[3 * m.nv + i] = c.E;
+}
+
+// Vertex gradients of the entropy variables (src/fv.cc:699-1059), as a gather:
+// sum over incident edges of g_side (W_other - W_self) plus the boundary
+// corrections of the incident boundary cells, times 1/(6 mcarea).
+__global__ void k_gradient(Params k, MeshView m, StateView s, const int* __restrict__ done) {
+  if (*done) return;
+  int v = blockIdx.x * blockDim.x + threadIdx.x;
+  if (v >= m.nv) return;
+  const int nv = m.nv;
+  double acc[8];
+#pragma unroll
+  for (int c = 0; c < 8; ++c) acc[c] = 0.0;
+  const double* W = s.W;
+  for (int j = m.ce_off[v]; j < m.ce_off[v + 1]; ++j) {
+    int ent = m.ce_ent[j];
+    int e = ent >> 1, side = ent & 1;
+    int a = m.e_a[e], b = m.e_b[e];
+    int self = side ? b : a, other = side ? a : b;
+    double gx = side ? m.e_g1x[e] : m.e_g0x[e];
+    double gy = side ? m.e_g1y[e] : m.e_g0y[e];
+#pragma unroll
+    for (int c = 0; c < 4; ++c) {
+      double dW = W[c * nv + other] - W[c * nv + self];
+      acc[2 * c] += gx * dW;
+      acc[2 * c + 1] += gy * dW;
+    }
+  }
+  for (int j = m.cb_off[v]; j < m.cb_off[v + 1]; ++j) {
+    int ent = m.cb_ent[j];
+    if ((ent & 3) != 1) continue;
+    int d = ent >> 2;
+    double dW[4];
+    bface_grad_corr(k, m, s, d, dW);
+#pragma unroll
+    for (int c = 0; c < 4; ++c) {
+      acc[2 * c] += m.b_nx[d] * dW[c];
+      acc[2 * c + 1] += m.b_ny[d] * dW[c];
+    }
+  }
+  double f = m.inv6mc[v];
+#pragma unroll
+  for (int c = 0; c < 8; ++c) s.G[c * nv + v] = acc[c] * f;
+}
+
+// Interior/boundary edge fluxes (src/fv.cc:1071-1097) into the edge buffer.
+template <int FLUX, int RECON>
+__global__ void k_edge_flux(Params k, MeshView m, StateView s, const int* __restrict__ done) {
+  if (*done) return;
+  int e = blockIdx.x * blockDim.x + threadIdx.x;
+  if (e >= m.ne) return;
+  const int nv = m.nv;
+  int a = m.e_a[e], b = m.e_b[e];
+  Prim L = load_prim(s.P, nv, a), R = load_prim(s.P, nv, b);
+  double gl[8], gr[8];
+  const bool needs_grad = (FLUX == FLUX_TECNO_ROE || FLUX == FLUX_TECNO_RUSANOV) && RECON != RECON_FIRST;
+  if (needs_grad) {
+#pragma unroll
+    for (int c = 0; c < 8; ++c) { gl[c] = s.G[c * nv + a]; gr[c] = s.G[c * nv + b]; }
+  } else {
+#pragma unroll
+    for (int c = 0; c < 8; ++c) { gl[c] = 0.0; gr[c] = 0.0; }
+  }
+  Flx F = num_flux<FLUX, RECON>(k, L, R, m.e_nx[e], m.e_ny[e], m.e_dx[e], m.e_dy[e], gl, gr);
+  const int ne = m.ne;
+  s.Fe[e] = F.m; s.Fe[ne + e] = F.x; s.Fe[2 * ne + e] = F.y; s.Fe[3 * ne + e] = F.e;
+}
+
+// Boundary-face inviscid fluxes (src/fv.cc:1100-1188): one thread per (face, vertex).
+template <int FLUX, int RECON>
+__global__ void k_bflux(Params k, MeshView m, StateView s, const int* __restrict__ done) {
+  if (*done) return;
+  int t = blockIdx.x * blockDim.x + threadIdx.x;
+  if (t >= 2 * m.nb) return;
+  int d = t >> 1, q = t & 1;
+  int c = q ? m.b_v1[d] : m.b_v0[d];
+  Prim s0 = load_prim(s.P, m.nv, c), s1 = s0;
+  double nx = m.b_nx[d], ny = m.b_ny[d];
+  int kind = m.b_kind[d];
+  bc_apply2(kind, m.b_adiab[d], m.b_val + (size_t)d * 10 + 5 * q, nx, ny, s0, s1);
+  Flx F;
+  if (kind == BC_FARFIELD) {
+    double z[8] = {0, 0, 0, 0, 0, 0, 0, 0};
+    F = num_flux<FLUX, RECON>(k, s0, s1, nx, ny, 0.0, 0.0, z, z);
+  } else {
+    F = inviscid_bflux(k, s0, s1, nx, ny);
+  }
+  const int n2 = 2 * m.nb;
+  s.Fb[t] = F.m; s.Fb[n2 + t] = F.x; s.Fb[2 * n2 + t] = F.y; s.Fb[3 * n2 + t] = F.e;
+}
+
+// Viscous residual units (src/fv.cc:1197-1320): interior cells and boundary faces.
+__global__ void k_viscous(Params k, MeshView m, StateView s, const int* __restrict__ done) {
+  if (*done) return;
+  int u = blockIdx.x * blockDim.x + threadIdx.x;
+  if (u >= m.nvu) return;
+  const int nv = m.nv;
+  int c = m.u_cell[u];
+  int v[3] = {m.c_v[3 * c], m.c_v[3 * c + 1], m.c_v[3 * c + 2]};
+  const double* n = m.c_n + 6 * (size_t)c;
+  // cell gradient: P1 sum, boundary corrections in face order, / (2 area)
+  double dE[8];
+#pragma unroll
+  for (int q = 0; q < 4; ++q) {
+    double w0 = s.W[q * nv + v[0]], w1 = s.W[q * nv + v[1]], w2 = s.W[q * nv + v[2]];
+    dE[2 * q] = n[0] * w0 + n[2] * w1 + n[4] * w2;
+    dE[2 * q + 1] = n[1] * w0 + n[3] * w1 + n[5] * w2;
+  }
+  for (int j = m.c_bf_off[c]; j < m.c_bf_off[c + 1]; ++j) {
+    int d = m.c_bf[j];
+    double dW[4];
+    bface_grad_corr(k, m, s, d, dW);
+#pragma unroll
+    for (int q = 0; q < 4; ++q) {
+      dE[2 * q] += m.b_nx[d] * dW[q];
+      dE[2 * q + 1] += m.b_ny[d] * dW[q];
+    }
+  }
+  double f = m.c_inv2a[c];
+#pragma unroll
+  for (int q = 0; q < 8; ++q) dE[q] *= f;
+
+  Ent avg;
+  if (u < m.n_int_cells) {
+    const double t3 = 1.0 / 3.0;
+    avg.f = s.W[v[0]] * t3 + s.W[v[1]] * t3 + s.W[v[2]] * t3;
+    avg.vx = s.W[nv + v[0]] * t3 + s.W[nv + v[1]] * t3 + s.W[nv + v[2]] * t3;
+    avg.vy = s.W[2 * nv + v[0]] * t3 + s.W[2 * nv + v[1]] * t3 + s.W[2 * nv + v[2]] * t3;
+    avg.l = s.W[3 * nv + v[0]] * t3 + s.W[3 * nv + v[1]] * t3 + s.W[3 * nv + v[2]] * t3;
+  } else {
+    avg.f = avg.vx = avg.vy = avg.l = 0.0;
+    int cnt = m.c_nbr_off[c + 1] - m.c_nbr_off[c];
+    for (int j = m.c_nbr_off[c]; j < m.c_nbr_off[c + 1]; ++j) {
+      int d = m.c_nbr[j];
+      for (int q = 0; q < 2; ++q) {
+        int vb = q ? m.bf_face_v1[d] : m.bf_face_v0[d];
+        Prim st = load_prim(s.P, nv, vb);
+        const double* val = m.b_val + (size_t)d * 10 + (vb == m.b_v0[d] ? 0 : 5);
+        bc_apply1(m.b_kind[d], m.b_adiab[d], val, m.bf_face_nx[d], m.bf_face_ny[d], st);
+        Ent e = prim2ent(k, st);
+        avg.f += e.f; avg.vx += e.vx; avg.vy += e.vy; avg.l += e.l;
+      }
+    }
+    double sc = (0.5 * 1.0 / cnt);
+    avg.f *= sc; avg.vx *= sc; avg.vy *= sc; avg.l *= sc;
+  }
+  ViscK K = viscous_K(k, avg, dE);
+  const int n3 = 3 * m.nvu;
+#pragma unroll
+  for (int q = 0; q < 3; ++q) {
+    Flx F = viscous_apply(K, n[2 * q], n[2 * q + 1]);
+    s.Fv[3 * u + q] = F.x; s.Fv[n3 + 3 * u + q] = F.y; s.Fv[2 * n3 + 3 * u + q] = F.e;
+  }
+  if (u >= m.n_int_cells) {
+    int d = u - m.n_int_cells;
+    double nbx = m.b_nx[d], nby = m.b_ny[d];
+    double Cor = m.b_adiab[d] ? -1.0 * (0.0 + K.c2 * K.e4 * K.e4 * (dE[6] * nbx + dE[7] * nby)) : 0.0;
+    Flx F = viscous_apply(K, nbx, nby);
+    s.Fvb[d] = F.x; s.Fvb[m.nb + d] = F.y; s.Fvb[2 * m.nb + d] = F.e - Cor;
+  }
+}
+
+// Residual assembly: fixed-order gather of every contribution to a vertex.
+__global__ void k_assemble(MeshView m, StateView s, int viscous, const int* __restrict__ done) {
+  if (*done) return;
+  int v = blockIdx.x * blockDim.x + threadIdx.x;
+  if (v >= m.nv) return;
+  const int ne = m.ne;
+  double r0 = 0.0, r1 = 0.0, r2 = 0.0, r3 = 0.0;
+  for (int j = m.ce_off[v]; j < m.ce_off[v + 1]; ++j) {
+    int ent = m.ce_ent[j];
+    int e = ent >> 1;
+    double sg = (ent & 1) ? -1.0 : 1.0;
+    r0 += s.Fe[e] * sg; r1 += s.Fe[ne + e] * sg; r2 += s.Fe[2 * ne + e] * sg; r3 += s.Fe[3 * ne + e] * sg;
+  }
+  const int n2 = 2 * m.nb, n3 = 3 * m.nvu;
+  for (int j = m.cb_off[v]; j < m.cb_off[v + 1]; ++j) {
+    int ent = m.cb_ent[j];
+    int type = ent & 3, idx = ent >> 2;
+    if (type == 0) {
+      r0 += s.Fb[idx] * 0.5; r1 += s.Fb[n2 + idx] * 0.5; r2 += s.Fb[2 * n2 + idx] * 0.5; r3 += s.Fb[3 * n2 + idx] * 0.5;
+    } else if (type == 2 && viscous) {
+      r1 += s.Fv[idx] * -(0.5 * 1.0); r2 += s.Fv[n3 + idx] * -(0.5 * 1.0); r3 += s.Fv[2 * n3 + idx] * -(0.5 * 1.0);
+    } else if (type == 3 && viscous) {
+      r1 += s.Fvb[idx] * 0.5; r2 += s.Fvb[m.nb + idx] * 0.5; r3 += s.Fvb[2 * m.nb + idx] * 0.5;
+    }
+  }
+  const int nv = m.nv;
+  s.R[v] = r0; s.R[nv + v] = r1; s.R[2 * nv + v] = r2; s.R[3 * nv + v] = r3;
+}
+
+__device__ __forceinline__ unsigned long long warp_min_u64(unsigned long long x) {
+#pragma unroll
+  for (int o = 16; o > 0; o >>= 1) {
+    unsigned long long y = __shfl_xor_sync(0xffffffffu, x, o);
+    x = y < x ? y : x;
+  }
+  return x;
+}
+
+// Local time step (src/fv.cc:1499-1598): spectral-radius gather, dt = cfl A / sum,
+// block minimum by warp shuffles, then one atomicMin on the (positive) bit pattern.
+__global__ void k_dt(Params k, MeshView m, StateView s, Scalars* sc, const int* __restrict__ done) {
+  if (*done) return;
+  int v = blockIdx.x * blockDim.x + threadIdx.x;
+  unsigned long long bits = 0x7ff0000000000000ull;  // +inf
+  if (v < m.nv) {
+    const int nv = m.nv;
+    double lam = 0.0;
+    for (int j = m.ce_off[v]; j < m.ce_off[v + 1]; ++j) {
+      int ent = m.ce_ent[j];
+      int e = ent >> 1;
+      int self = (ent & 1) ? m.e_b[e] : m.e_a[e];
+      Prim q = load_prim(s.P, nv, self);
+      double nx = m.e_nx[e], ny = m.e_ny[e];
+      double area = sqrt(nx * nx + ny * ny);
+      lam += (fabs(q.u * nx + q.v * ny) + sound_speed(k, q) * area) * 1.0;
+    }
+    for (int j = m.cb_off[v]; j < m.cb_off[v + 1]; ++j) {
+      int ent = m.cb_ent[j];
+      if ((ent & 3) != 0) continue;
+      int idx = ent >> 2, d = idx >> 1;
+      int self = (idx & 1) ? m.b_v1[d] : m.b_v0[d];
+      Prim q = load_prim(s.P, nv, self);
+      double nx = m.b_nx[d], ny = m.b_ny[d];
+      double area = sqrt(nx * nx + ny * ny);
+      lam += 0.5 * (fabs(q.u * nx + q.v * ny) + sound_speed(k, q) * area);
+    }
+    if (k.model == 1) {
+      for (int j = m.ce_off[v]; j < m.ce_off[v + 1]; ++j) {
+        int ent = m.ce_ent[j];
+        int e = ent >> 1;
+        int self = (ent & 1) ? m.e_b[e] : m.e_a[e];
+        Prim q = load_prim(s.P, nv, self);
+        double nx = m.e_nx[e], ny = m.e_ny[e];
+        double area = sqrt(nx * nx + ny * ny);
+        double dl = sqrt(m.e_dx[e] * m.e_dx[e] + m.e_dy[e] * m.e_dy[e]);
+        lam += (viscosity(k, q.T) * area / dl / density(k, q)) * 1.0;
+      }
+    }
+    double dtv = k.cfl * m.dcarea[v] / lam;
+    s.dt[v] = dtv;
+    bits = (unsigned long long)__double_as_longlong(dtv);
+    if (!(dtv > 0.0)) bits = 0x7ff0000000000000ull;  // NaN / non-positive: flagged by the update
+  }
+  bits = warp_min_u64(bits);
+  __shared__ unsigned long long wmin[kBlock / 32];
+  int lane = threadIdx.x & 31, w = threadIdx.x >> 5;
+  if (lane == 0) wmin[w] = bits;
+  __syncthreads();
+  if (w == 0) {
+    bits = lane < (int)(blockDim.x >> 5) ? wmin[lane] : 0x7ff0000000000000ull;
+    bits = warp_min_u64(bits);
+    if (lane == 0) atomicMin(&sc->dtmin_bits, bits);
+  }
+}
+
+// Start of a solve-loop iteration (src/fv.cc:2273-2276): loop condition and dt reset.
+__global__ void k_step_begin(Control ctl, Scalars* sc, int* done) {
+  // unsteady runs never advance the iteration bound (term_iter stays 0, src/fv.cc:2266-2268)
+  bool go = sc->rtotal > ctl.min_residue && (ctl.time_mode == 1 || sc->iter < ctl.max_iter) &&
+            sc->elapsed < ctl.final_time;
+  *done = go ? 0 : 1;
+  sc->dtmin_bits = 0x7ff0000000000000ull;
+}
+
+// Global dt and the unsteady clamp to the next output time (src/fv.cc:1584-1618).
+__global__ void k_dt_final(Control ctl, Scalars* sc, const int* __restrict__ done) {
+  if (*done) return;
+  double dtg;
+  if (ctl.time_step > 0.0) {
+    dtg = ctl.time_step;
+  } else {
+    dtg = 1.0e20;
+    double m = __longlong_as_double((long long)sc->dtmin_bits);
+    dtg = dmin_(dtg, m);
+    if (ctl.time_mode == 1) {
+      int c = sc->counter < ctl.ntinst ? sc->counter : ctl.ntinst - 1;
+      if (sc->elapsed + dtg > ctl.tinst[c]) {
+        dtg = ctl.tinst[c] - sc->elapsed;
+        sc->reached = 1;
+      }
+    }
+  }
+  sc->dt_global = dtg;
+}
+
+// update_solution for SSP-RK3 (src/fv.cc:1641-1652), fused with the residual-norm
+// partial sums of compute_residual_norm (src/fv.cc:1822-1841) at the last stage.
+__global__ void k_update(Params k, MeshView m, StateView s, Control ctl, Scalars* sc, int r, int do_norm,
+                         const int* __restrict__ done) {
+  if (*done) return;
+  int i = blockIdx.x * blockDim.x + threadIdx.x;
+  const int nv = m.nv;
+  double nrm[4] = {0.0, 0.0, 0.0, 0.0};
+  if (i < nv) {
+    const double a_rk[3] = {0.0, 3.0 / 4.0, 1.0 / 3.0};
+    const double b_rk[3] = {1.0, 1.0 / 4.0, 2.0 / 3.0};
+    double R0 = s.R[i], R1 = s.R[nv + i], R2 = s.R[2 * nv + i], R3 = s.R[3 * nv + i];
+    double area = m.dcarea[i];
+    if (do_norm) {
+      double w = m.pweight[i];
+      double q0 = R0 / area, q1 = R1 / area, q2 = R2 / area, q3 = R3 / area;
+      nrm[0] = q0 * q0 * w; nrm[1] = q1 * q1 * w; nrm[2] = q2 * q2 * w; nrm[3] = q3 * q3 * w;
+    }
+    double dtv = (ctl.time_mode == 1 || ctl.time_step > 0.0) ? sc->dt_global : s.dt[i];
+    double factor = dtv / (1.0 * area);
+    Cons c = prim2con(k, load_prim(s.P, nv, i));
+    double br = b_rk[r], ar = a_rk[r], c2 = -factor * br;
+    c.r *= br; c.mx *= br; c.my *= br; c.E *= br;
+    c.r += s.Uold[i] * ar + R0 * c2;
+    c.mx += s.Uold[nv + i] * ar + R1 * c2;
+    c.my += s.Uold[2 * nv + i] * ar + R2 * c2;
+    c.E += s.Uold[3 * nv + i] * ar + R3 * c2;
+    Prim q = con2prim(k, c);
+    Ent e = prim2ent(k, q);
+    s.P[i] = q.T; s.P[nv + i] = q.u; s.P[2 * nv + i] = q.v; s.P[3 * nv + i] = q.p;
+    s.W[i] = e.f; s.W[nv + i] = e.vx; s.W[2 * nv + i] = e.vy; s.W[3 * nv + i] = e.l;
+    bool ok = isfinite(q.T) && isfinite(q.u) && isfinite(q.v) && isfinite(q.p) && q.p > 0.0 && c.r > 0.0;
+    if (!ok) atomicOr(&sc->bad, 1);
+  }
+  if (do_norm) {
+    // fixed-shape block reduction -> per-block partials, summed in block order later
+    __shared__ double red[4][kBlock];
+#pragma unroll
+    for (int c = 0; c < 4; ++c) red[c][threadIdx.x] = nrm[c];
+    __syncthreads();
+    for (int o = kBlock / 2; o > 0; o >>= 1) {
+      if ((int)threadIdx.x < o)
+#pragma unroll
+        for (int c = 0; c < 4; ++c) red[c][threadIdx.x] += red[c][threadIdx.x + o];
+      __syncthreads();
+    }
+    if (threadIdx.x == 0)
+#pragma unroll
+      for (int c = 0; c < 4; ++c) s.part[(size_t)blockIdx.x * 4 + c] = red[c][0];
+  }
+}
+
+// Residual-norm partial sums alone (src/fv.cc:1822-1841), same reduction shape as k_update.
+__global__ void k_norm_part(MeshView m, StateView s, const int* __restrict__ done) {
+  if (*done) return;
+  int i = blockIdx.x * blockDim.x + threadIdx.x;
+  const int nv = m.nv;
+  double nrm[4] = {0.0, 0.0, 0.0, 0.0};
+  if (i < nv) {
+    double area = m.dcarea[i], w = m.pweight[i];
+#pragma unroll
+    for (int c = 0; c < 4; ++c) {
+      double q = s.R[c * nv + i] / area;
+      nrm[c] = q * q * w;
+    }
+  }
+  __shared__ double red[4][kBlock];
+#pragma unroll
+  for (int c = 0; c < 4; ++c) red[c][threadIdx.x] = nrm[c];
+  __syncthreads();
+  for (int o = kBlock / 2; o > 0; o >>= 1) {
+    if ((int)threadIdx.x < o)
+#pragma unroll
+      for (int c = 0; c < 4; ++c) red[c][threadIdx.x] += red[c][threadIdx.x + o];
+    __syncthreads();
+  }
+  if (threadIdx.x == 0)
+#pragma unroll
+    for (int c = 0; c < 4; ++c) s.part[(size_t)blockIdx.x * 4 + c] = red[c][0];
+}
+
+// Norm finalisation (src/fv.cc:1846-1876): one block sums the partials in a fixed order.
+__global__ void k_norm_final(StateView s, int nblocks, int nv_total, Scalars* sc, int use_sc_iter, long long iter,
+                             const int* __restrict__ done) {
+  if (*done) return;
+  __shared__ double red[4][kBlock];
+  double acc[4] = {0.0, 0.0, 0.0, 0.0};
+  for (int b = threadIdx.x; b < nblocks; b += blockDim.x)
+#pragma unroll
+    for (int c = 0; c < 4; ++c) acc[c] += s.part[(size_t)b * 4 + c];
+#pragma unroll
+  for (int c = 0; c < 4; ++c) red[c][threadIdx.x] = acc[c];
+  __syncthreads();
+  for (int o = kBlock / 2; o > 0; o >>= 1) {
+    if ((int)threadIdx.x < o)
+#pragma unroll
+      for (int c = 0; c < 4; ++c) red[c][threadIdx.x] += red[c][threadIdx.x + o];
+    __syncthreads();
+  }
+  if (threadIdx.x == 0) {
+    double n0 = sqrt(red[0][0]) / nv_total, n1 = sqrt(red[1][0]) / nv_total;
+    double n2 = sqrt(red[2][0]) / nv_total, n3 = sqrt(red[3][0]) / nv_total;
+    double total = sqrt(n0 * n0 + (n1 * n1 + n2 * n2 + 0.0) + n3 * n3);
+    long long it = use_sc_iter ? sc->iter : iter;
+    if (it == 0) {
+      sc->rtotal0 = total;
+      if (sc->rtotal0 == 0.0) sc->rtotal0 = 1.0;
+    }
+    sc->rnorm[0] = n0; sc->rnorm[1] = n1; sc->rnorm[2] = n2; sc->rnorm[3] = n3;
+    sc->rtotal = total / sc->rtotal0;
+  }
+}
+
+// End of a solve-loop iteration (src/fv.cc:2307-2343).
+__global__ void k_step_end(Control ctl, Scalars* sc, const int* __restrict__ done) {
+  if (*done) return;
+  sc->iter += 1;
+  sc->elapsed += sc->dt_global;
+  if (sc->reached && ctl.time_mode == 1) {
+    sc->counter += 1;
+    sc->reached = 0;
+  }
+}
+
+// Kinetic-energy and entropy integrals (src/fv.cc:2186-2203), block partials.
+__global__ void k_global(Params k, MeshView m, StateView s) {
+  int i = blockIdx.x * blockDim.x + threadIdx.x;
+  double ke = 0.0, en = 0.0;
+  if (i < m.nv) {
+    Prim q = load_prim(s.P, m.nv, i);
+    double w = m.pweight[i], A = m.dcarea[i];
+    double rho = density(k, q);
+    ke = (0.5 * rho * (q.u * q.u + q.v * q.v) * A) * w;
+    en = (-rho * entropy_fn(k, q) / (k.gamma - 1.0)) * A * w;
+  }
+  __shared__ double red[2][kBlock];
+  red[0][threadIdx.x] = ke;
+  red[1][threadIdx.x] = en;
+  __syncthreads();
+  for (int o = kBlock / 2; o > 0; o >>= 1) {
+    if ((int)threadIdx.x < o) {
+      red[0][threadIdx.x] += red[0][threadIdx.x + o];
+      red[1][threadIdx.x] += red[1][threadIdx.x + o];
+    }
+    __syncthreads();
+  }
+  if (threadIdx.x == 0) { s.part[(size_t)blockIdx.x * 4] = red[0][0]; s.part[(size_t)blockIdx.x * 4 + 1] = red[1][0]; }
+}
+
+}  // namespace tg

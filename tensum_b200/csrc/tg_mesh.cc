@@ -1,0 +1,327 @@
+// tg_mesh.cc -- host construction of the device mesh layout (see tg_mesh.h).
+#include "tg_mesh.h"
+
+#include <algorithm>
+#include <cmath>
+#include <cstdio>
+#include <numeric>
+#include <unordered_map>
+
+namespace tg {
+
+namespace {
+
+// Position along a Hilbert curve on a 2^16 x 2^16 grid.
+uint64_t hilbert_index(uint32_t x, uint32_t y) {
+  const uint32_t n = 1u << 16;
+  uint64_t d = 0;
+  for (uint32_t s = n / 2; s > 0; s /= 2) {
+    uint32_t rx = (x & s) ? 1u : 0u;
+    uint32_t ry = (y & s) ? 1u : 0u;
+    d += (uint64_t)s * (uint64_t)s * (uint64_t)((3u * rx) ^ ry);
+    if (ry == 0) {
+      if (rx == 1) {
+        x = n - 1 - x;
+        y = n - 1 - y;
+      }
+      std::swap(x, y);
+    }
+  }
+  return d;
+}
+
+struct Err {
+  std::string msg;
+  bool bad() const { return !msg.empty(); }
+};
+
+}  // namespace
+
+std::string build_layout(const tg_mesh& m, const tg_bc_table* bc, bool need_viscous, HostLayout& L) {
+  char buf[256];
+  const int nv = m.n_vertex, nc = m.n_cell, nf = m.n_face, nbf = m.n_bface;
+  if (nv <= 0 || nc <= 0 || nf <= 0 || nbf < 0) return "mesh has no vertices, cells or faces";
+  if (!m.coords || !m.dcarea || !m.mcarea || !m.cell_vertex || !m.cell_normal || !m.cell_area ||
+      !m.face_vertex || !m.face_type || !m.face_normal || !m.face_lcell || !m.face_rcell)
+    return "mesh array pointer is NULL";
+  if (nbf > 0 && (!m.bface_vertex || !m.bface_type || !m.bface_normal || !m.bface_lcell || !m.bface_periodic))
+    return "boundary-face array pointer is NULL";
+  if (nbf > nf) return "more boundary faces than faces";
+  for (int i = 0; i < 2 * nf; ++i)
+    if (m.face_vertex[i] < 0 || m.face_vertex[i] >= nv) return "face vertex index out of range";
+  for (int i = 0; i < nf; ++i) {
+    if (m.face_lcell[i] < 0 || m.face_lcell[i] >= nc) return "face left cell out of range";
+    if (m.face_rcell[i] >= nc) return "face right cell out of range";
+    if (m.face_type[i] == -2) return "inter-partition faces (type -2) need more than one partition";
+  }
+  for (int i = 0; i < 3 * nc; ++i)
+    if (m.cell_vertex[i] < 0 || m.cell_vertex[i] >= nv) return "cell vertex index out of range";
+  for (int b = 0; b < nbf; ++b) {
+    if (m.bface_vertex[2 * b] < 0 || m.bface_vertex[2 * b] >= nv || m.bface_vertex[2 * b + 1] < 0 ||
+        m.bface_vertex[2 * b + 1] >= nv)
+      return "boundary-face vertex index out of range";
+    if (m.bface_lcell[b] < 0 || m.bface_lcell[b] >= nc) return "boundary-face cell out of range";
+    // Boundary faces lead the face list: face[b] is bface[b] (src/grid_preproc.cc:530-541).
+    int a0 = m.face_vertex[2 * b], a1 = m.face_vertex[2 * b + 1];
+    int b0 = m.bface_vertex[2 * b], b1 = m.bface_vertex[2 * b + 1];
+    if (m.face_type[b] != m.bface_type[b] || !((a0 == b0 && a1 == b1) || (a0 == b1 && a1 == b0))) {
+      std::snprintf(buf, sizeof(buf), "face %d does not match boundary face %d (boundary faces must lead the face list)", b, b);
+      return buf;
+    }
+  }
+  for (int i = 0; i < nv; ++i)
+    if (!(m.dcarea[i] > 0.0) || !(m.mcarea[i] > 0.0)) return "non-positive dual area";
+
+  // periodic sets -> set id per vertex
+  std::vector<int> set_of(nv, -1);
+  const int np = m.n_periodic;
+  if (np > 0 && (!m.periodic_offsets || !m.periodic_members)) return "periodic list pointer is NULL";
+  for (int s = 0; s < np; ++s) {
+    if (m.periodic_offsets[s + 1] <= m.periodic_offsets[s]) return "empty periodic set";
+    for (int j = m.periodic_offsets[s]; j < m.periodic_offsets[s + 1]; ++j) {
+      int v = m.periodic_members[j];
+      if (v < 0 || v >= nv) return "periodic vertex out of range";
+      if (set_of[v] != -1) return "vertex belongs to two periodic sets";
+      set_of[v] = s;
+    }
+  }
+
+  // boundary-condition lookup
+  auto bc_of = [&](int tag, int& kind, int& adiab) {
+    kind = 0;
+    adiab = 0;
+    if (!bc) return false;
+    for (int i = 0; i < bc->n_types; ++i)
+      if (bc->type_tag[i] == tag) {
+        kind = bc->kind[i];
+        adiab = bc->adiabatic ? bc->adiabatic[i] : 0;
+        return true;
+      }
+    return false;
+  };
+
+  // ---- vertex order: Hilbert curve over the bounding box
+  double xmin = 1e300, xmax = -1e300, ymin = 1e300, ymax = -1e300;
+  for (int i = 0; i < nv; ++i) {
+    xmin = std::min(xmin, m.coords[2 * i]); xmax = std::max(xmax, m.coords[2 * i]);
+    ymin = std::min(ymin, m.coords[2 * i + 1]); ymax = std::max(ymax, m.coords[2 * i + 1]);
+  }
+  double span = std::max(xmax - xmin, ymax - ymin);
+  if (!(span > 0.0)) span = 1.0;
+  std::vector<uint64_t> key(nv);
+  for (int i = 0; i < nv; ++i) {
+    double fx = (m.coords[2 * i] - xmin) / span, fy = (m.coords[2 * i + 1] - ymin) / span;
+    uint32_t ix = (uint32_t)std::min(65535.0, std::max(0.0, std::floor(fx * 65535.0)));
+    uint32_t iy = (uint32_t)std::min(65535.0, std::max(0.0, std::floor(fy * 65535.0)));
+    key[i] = hilbert_index(ix, iy);
+  }
+  L.nv = nv;
+  L.old_of_new.resize(nv);
+  std::iota(L.old_of_new.begin(), L.old_of_new.end(), 0);
+  std::stable_sort(L.old_of_new.begin(), L.old_of_new.end(), [&](int a, int b) { return key[a] < key[b]; });
+  L.new_of_old.assign(nv, 0);
+  for (int i = 0; i < nv; ++i) L.new_of_old[L.old_of_new[i]] = i;
+  const std::vector<int>& N = L.new_of_old;
+
+  L.dcarea.resize(nv); L.inv6mc.resize(nv); L.pweight.resize(nv); L.x.resize(nv); L.y.resize(nv);
+  for (int i = 0; i < nv; ++i) {
+    int o = L.old_of_new[i];
+    L.dcarea[i] = m.dcarea[o];
+    L.inv6mc[i] = 1.0 / (6.0 * m.mcarea[o]);          // src/fv.cc:1040
+    L.x[i] = m.coords[2 * o];
+    L.y[i] = m.coords[2 * o + 1];
+    // weight in norms / integrals: 1/|P_i| for periodic vertices (src/grid_preproc.cc:1037-1052)
+    L.pweight[i] = set_of[o] >= 0 ? 1.0 / ((double)(m.periodic_offsets[set_of[o] + 1] - m.periodic_offsets[set_of[o]]) * 1.0)
+                                  : 1.0 / 1.0;
+  }
+
+  // ---- edges: every reference face, sorted by (lower vertex, upper vertex, face)
+  std::vector<int> eorder(nf);
+  std::iota(eorder.begin(), eorder.end(), 0);
+  auto lo = [&](int f) { return std::min(N[m.face_vertex[2 * f]], N[m.face_vertex[2 * f + 1]]); };
+  auto hi = [&](int f) { return std::max(N[m.face_vertex[2 * f]], N[m.face_vertex[2 * f + 1]]); };
+  std::stable_sort(eorder.begin(), eorder.end(), [&](int a, int b) {
+    int la = lo(a), lb = lo(b);
+    if (la != lb) return la < lb;
+    return hi(a) < hi(b);
+  });
+  L.ne = nf;
+  L.e_a.resize(nf); L.e_b.resize(nf); L.e_face.resize(nf);
+  L.e_nx.resize(nf); L.e_ny.resize(nf); L.e_dx.resize(nf); L.e_dy.resize(nf);
+  L.e_g0x.assign(nf, 0.0); L.e_g0y.assign(nf, 0.0); L.e_g1x.assign(nf, 0.0); L.e_g1y.assign(nf, 0.0);
+  std::vector<int> edge_of_face(nf);
+  for (int e = 0; e < nf; ++e) {
+    int f = eorder[e];
+    edge_of_face[f] = e;
+    int va = m.face_vertex[2 * f], vb = m.face_vertex[2 * f + 1];
+    L.e_face[e] = f;
+    L.e_a[e] = N[va];
+    L.e_b[e] = N[vb];
+    L.e_nx[e] = m.face_normal[2 * f];
+    L.e_ny[e] = m.face_normal[2 * f + 1];
+    L.e_dx[e] = m.coords[2 * vb] - m.coords[2 * va];     // src/kepes_tecno_roe.cc:112
+    L.e_dy[e] = m.coords[2 * vb + 1] - m.coords[2 * va + 1];
+    // gradient weights: sum over the face's cells of the P1 normal of the other endpoint
+    int cells[2] = {m.face_lcell[f], m.face_rcell[f]};
+    for (int q = 0; q < 2; ++q) {
+      int c = cells[q];
+      if (c < 0) continue;
+      int ka = -1, kb = -1;
+      for (int k = 0; k < 3; ++k) {
+        if (m.cell_vertex[3 * c + k] == va) ka = k;
+        if (m.cell_vertex[3 * c + k] == vb) kb = k;
+      }
+      if (ka < 0 || kb < 0) return "face vertices are not vertices of its cell";
+      L.e_g0x[e] += m.cell_normal[6 * c + 2 * kb];
+      L.e_g0y[e] += m.cell_normal[6 * c + 2 * kb + 1];
+      L.e_g1x[e] += m.cell_normal[6 * c + 2 * ka];
+      L.e_g1y[e] += m.cell_normal[6 * c + 2 * ka + 1];
+    }
+  }
+
+  // members of the periodic group of a (reference) vertex, in set order
+  auto group = [&](int o, std::vector<int>& g) {
+    g.clear();
+    if (set_of[o] < 0) { g.push_back(o); return; }
+    for (int j = m.periodic_offsets[set_of[o]]; j < m.periodic_offsets[set_of[o] + 1]; ++j)
+      g.push_back(m.periodic_members[j]);
+  };
+
+  // per reference vertex incident edges (in edge order)
+  std::vector<std::vector<int>> inc(nv);
+  for (int e = 0; e < nf; ++e) {
+    inc[m.face_vertex[2 * L.e_face[e]]].push_back(e << 1);
+    inc[m.face_vertex[2 * L.e_face[e] + 1]].push_back((e << 1) | 1);
+  }
+  L.ce_off.assign(nv + 1, 0);
+  std::vector<int> g;
+  for (int i = 0; i < nv; ++i) {
+    group(L.old_of_new[i], g);
+    size_t cnt = 0;
+    for (int o : g) cnt += inc[o].size();
+    L.ce_off[i + 1] = L.ce_off[i] + (int)cnt;
+  }
+  L.ce_ent.resize(L.ce_off[nv]);
+  for (int i = 0; i < nv; ++i) {
+    group(L.old_of_new[i], g);
+    int p = L.ce_off[i];
+    for (int o : g)
+      for (int x : inc[o]) L.ce_ent[p++] = x;
+  }
+
+  // ---- non-periodic boundary faces
+  std::vector<int> dev_bface(nbf, -1);
+  for (int b = 0; b < nbf; ++b) {
+    int kind, adiab;
+    bc_of(m.bface_type[b], kind, adiab);
+    if (m.bface_periodic[b]) continue;
+    if (kind == 0) {
+      std::snprintf(buf, sizeof(buf), "no boundary condition for boundary tag %d", m.bface_type[b]);
+      return buf;
+    }
+    if (kind == 7) continue;  // periodic tag: treated like the reference (no flux, no correction)
+    dev_bface[b] = L.nb++;
+  }
+  const int nb = L.nb;
+  L.b_v0.resize(nb); L.b_v1.resize(nb); L.b_kind.resize(nb); L.b_adiab.resize(nb); L.b_cell.resize(nb);
+  L.b_nx.resize(nb); L.b_ny.resize(nb); L.b_val.assign((size_t)nb * 10, 0.0);
+  L.bf_face_nx.resize(nb); L.bf_face_ny.resize(nb); L.bf_face_v0.resize(nb); L.bf_face_v1.resize(nb);
+  std::vector<int> ref_bface_of_dev(nb);
+  for (int b = 0; b < nbf; ++b) {
+    int d = dev_bface[b];
+    if (d < 0) continue;
+    ref_bface_of_dev[d] = b;
+    int kind, adiab;
+    bc_of(m.bface_type[b], kind, adiab);
+    L.b_v0[d] = N[m.bface_vertex[2 * b]];
+    L.b_v1[d] = N[m.bface_vertex[2 * b + 1]];
+    L.b_kind[d] = kind;
+    L.b_adiab[d] = adiab;
+    L.b_cell[d] = m.bface_lcell[b];
+    L.b_nx[d] = m.bface_normal[2 * b];
+    L.b_ny[d] = m.bface_normal[2 * b + 1];
+    if (bc && bc->bface_values)
+      for (int q = 0; q < 10; ++q) L.b_val[(size_t)d * 10 + q] = bc->bface_values[(size_t)b * 10 + q];
+    L.bf_face_nx[d] = m.face_normal[2 * b];
+    L.bf_face_ny[d] = m.face_normal[2 * b + 1];
+    L.bf_face_v0[d] = N[m.face_vertex[2 * b]];
+    L.bf_face_v1[d] = N[m.face_vertex[2 * b + 1]];
+  }
+
+  // cells' non-periodic boundary faces (left-cell relation, face order)
+  std::vector<std::vector<int>> cell_bf(nc);
+  for (int d = 0; d < nb; ++d) cell_bf[L.b_cell[d]].push_back(d);
+
+  // ---- viscous units
+  std::vector<std::vector<int>> inc_b(nv);   // per reference vertex: tagged boundary entries
+  for (int d = 0; d < nb; ++d) {
+    int b = ref_bface_of_dev[d];
+    inc_b[m.bface_vertex[2 * b]].push_back(((2 * d + 0) << 2) | 0);
+    inc_b[m.bface_vertex[2 * b + 1]].push_back(((2 * d + 1) << 2) | 0);
+  }
+  for (int c = 0; c < nc; ++c)
+    for (int d : cell_bf[c])
+      for (int k = 0; k < 3; ++k) inc_b[m.cell_vertex[3 * c + k]].push_back((d << 2) | 1);
+  if (need_viscous) {
+    // cell face slots in ascending face order (src/grid_preproc.cc:528-551)
+    std::vector<int> cface(3 * (size_t)nc, -1);
+    for (int f = 0; f < nf; ++f) {
+      int c = m.face_lcell[f], j = 0;
+      while (cface[3 * c + j] != -1) ++j;
+      cface[3 * c + j] = f;
+      c = m.face_rcell[f];
+      if (c >= 0) { j = 0; while (cface[3 * c + j] != -1) ++j; cface[3 * c + j] = f; }
+    }
+    L.c_v.resize(3 * (size_t)nc); L.c_n.resize(6 * (size_t)nc); L.c_inv2a.resize(nc);
+    L.c_bf_off.assign(nc + 1, 0); L.c_nbr_off.assign(nc + 1, 0);
+    for (int c = 0; c < nc; ++c) {
+      for (int k = 0; k < 3; ++k) L.c_v[3 * c + k] = N[m.cell_vertex[3 * c + k]];
+      for (int k = 0; k < 6; ++k) L.c_n[6 * c + k] = m.cell_normal[6 * c + k];
+      L.c_inv2a[c] = 1.0 / (2.0 * m.cell_area[c]);                    // src/fv.cc:1051
+      L.c_bf_off[c + 1] = L.c_bf_off[c] + (int)cell_bf[c].size();
+      for (int d : cell_bf[c]) L.c_bf.push_back(d);
+      int cnt = 0;
+      for (int j = 0; j < 3; ++j) {                                     // nbr_bface (src/grid_preproc.cc:811-832)
+        int f = cface[3 * c + j];
+        if (f >= 0 && f < nbf && dev_bface[f] >= 0) { L.c_nbr.push_back(dev_bface[f]); ++cnt; }
+      }
+      L.c_nbr_off[c + 1] = L.c_nbr_off[c] + cnt;
+    }
+    // units: interior cells first (cell order), then one per boundary face (face order)
+    for (int c = 0; c < nc; ++c)
+      if (L.c_nbr_off[c + 1] == L.c_nbr_off[c]) L.u_cell.push_back(c);
+    L.n_int_cells = (int)L.u_cell.size();
+    for (int d = 0; d < nb; ++d) L.u_cell.push_back(L.b_cell[d]);
+    L.nvu = (int)L.u_cell.size();
+    for (int u = 0; u < L.nvu; ++u) {
+      int c = L.u_cell[u];
+      for (int k = 0; k < 3; ++k) inc_b[m.cell_vertex[3 * c + k]].push_back(((3 * u + k) << 2) | 2);
+      if (u >= L.n_int_cells) {
+        int d = u - L.n_int_cells;
+        int b = ref_bface_of_dev[d];
+        inc_b[m.bface_vertex[2 * b]].push_back((d << 2) | 3);
+        inc_b[m.bface_vertex[2 * b + 1]].push_back((d << 2) | 3);
+      }
+    }
+  }
+  L.cb_off.assign(nv + 1, 0);
+  for (int i = 0; i < nv; ++i) {
+    group(L.old_of_new[i], g);
+    size_t cnt = 0;
+    for (int o : g) cnt += inc_b[o].size();
+    L.cb_off[i + 1] = L.cb_off[i] + (int)cnt;
+  }
+  L.cb_ent.resize(L.cb_off[nv]);
+  for (int i = 0; i < nv; ++i) {
+    group(L.old_of_new[i], g);
+    int p = L.cb_off[i];
+    for (int o : g)
+      for (int x : inc_b[o]) L.cb_ent[p++] = x;
+  }
+  // the fixed-order gather relies on indices fitting the entry encodings
+  if ((long long)nf * 2 >= (1LL << 31) || (long long)L.nvu * 3 >= (1LL << 29) || (long long)nb * 2 >= (1LL << 29))
+    return "mesh too large for 32-bit gather entries";
+  return "";
+}
+
+}  // namespace tg

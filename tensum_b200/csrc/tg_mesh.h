@@ -1,0 +1,60 @@
+// tg_mesh.h -- host-side construction of the device mesh layout.
+//
+// Input: the reference's Grid after preproc (tg_mesh, reference numbering).
+// Output: flat arrays in the device numbering (vertices reordered along a
+// Hilbert curve, edges sorted by their lower vertex) plus the per-vertex
+// gather lists that make every accumulation deterministic.
+//
+// Periodic vertices are kept as separate degrees of freedom, as the reference
+// stores them.  The reference sums residual, gradient and dt contributions
+// over each periodic set and copies the sum back
+// (src/reduce_residual_periodic.cc:18-31,122-130, src/reduce_gradient_periodic.cc,
+// src/reduce_dt_periodic.cc); here every member's gather list is the union of
+// the lists of all members of its set, in a fixed order, so each copy computes
+// that same sum itself in one pass and all copies end bitwise equal.
+#pragma once
+
+#include <cstdint>
+#include <string>
+#include <vector>
+
+#include "../../include/tensum_gpu.h"
+
+namespace tg {
+
+struct HostLayout {
+  int nv = 0;          // vertices (reference n_vertex, periodic copies included)
+  int ne = 0;          // edges    (reference faces, boundary and periodic faces included)
+  int nb = 0;          // non-periodic boundary faces
+  int nvu = 0;         // viscous units: interior cells + one per non-periodic boundary face
+  std::vector<int> new_of_old, old_of_new;
+  // vertices (device order)
+  std::vector<double> dcarea, inv6mc, pweight, x, y;
+  // edges
+  std::vector<int> e_a, e_b, e_face;
+  std::vector<double> e_nx, e_ny, e_dx, e_dy, e_g0x, e_g0y, e_g1x, e_g1y;
+  // per-vertex edge gather: entry = (edge << 1) | side   (side 1 = vertex is endpoint b)
+  std::vector<int> ce_off, ce_ent;
+  // non-periodic boundary faces
+  std::vector<int> b_v0, b_v1, b_kind, b_adiab, b_cell;
+  std::vector<double> b_nx, b_ny, b_val;  // b_val: nb*2*5 (T,u,v,w,p) at vertex 0 / 1
+  // per-vertex boundary / viscous gather: entry = (index << 2) | type
+  //   type 0: inviscid boundary flux (2*b + k)     type 1: gradient boundary correction (b)
+  //   type 2: viscous unit contribution (3*u + k)  type 3: viscous boundary flux (b)
+  std::vector<int> cb_off, cb_ent;
+  // viscous units: u < n_int_cells -> interior cell; else boundary face (u - n_int_cells)
+  int n_int_cells = 0;
+  std::vector<int> u_cell;                 // cell id (device cell numbering) per unit
+  std::vector<int> c_v;                    // 3 per cell (device vertex ids)
+  std::vector<double> c_n;                 // 6 per cell: P1 normals
+  std::vector<double> c_inv2a;             // 1/(2 area)
+  std::vector<int> c_bf_off, c_bf;         // non-periodic boundary faces with this cell on their left, face order
+  std::vector<int> c_nbr_off, c_nbr;       // the cell's non-periodic boundary faces in cell.face slot order
+  std::vector<double> bf_face_nx, bf_face_ny;  // face-list normal of the boundary face (slip in viscous BC states)
+  std::vector<int> bf_face_v0, bf_face_v1;     // face-list vertex order of the boundary face
+};
+
+// Returns "" on success, else an error message.
+std::string build_layout(const tg_mesh& m, const tg_bc_table* bc, bool need_viscous, HostLayout& out);
+
+}  // namespace tg

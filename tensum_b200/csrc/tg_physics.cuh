@@ -1,0 +1,451 @@
+// tg_physics.cuh -- pointwise and edgewise physics of the TENSUM hot path, 2D.
+//
+// Device restatement of Material (src/material.h, src/material.cc) and the
+// numerical fluxes (src/kep*.cc, src/roe_ec.cc, src/simple_avg.cc).  The
+// reference carries z components that are identically zero in 2D
+// (n_z = 0, w = 0); they are dropped here, which leaves every value unchanged
+// (only exact +-0 terms disappear).  Operand order follows the reference so
+// that results differ from it only by FMA contraction and the last-ulp
+// behaviour of log/sqrt.
+//
+// Variable order on the device:
+//   primitive  P = (T, u, v, p)
+//   conserved  U = (rho, rho u, rho v, E)
+//   entropy    W = (V1, V2, V3, V5)  (reference EntVar entf, entv.x, entv.y, entl)
+//   flux / residual = (mass, x-momentum, y-momentum, energy)
+#pragma once
+
+#include <cuda_runtime.h>
+#include <math.h>
+
+namespace tg {
+
+enum : int { FLUX_TECNO_ROE = 0, FLUX_TECNO_RUSANOV = 1, FLUX_KEPEC = 2, FLUX_ROE_EC = 3, FLUX_KEP = 4, FLUX_AVG = 5 };
+enum : int { RECON_FIRST = 0, RECON_SECOND = 1, RECON_SECOND_MUSCL = 2, RECON_VAN_ALBADA = 3,
+             RECON_TVD_MINMOD = 4, RECON_TVB_MINMOD = 5, RECON_ENO2 = 6 };
+enum : int { BC_NONE = 0, BC_SLIP = 1, BC_NOSLIP = 2, BC_FARFIELD = 3, BC_INLET = 4, BC_OUTLET = 5,
+             BC_PRESSURE = 6, BC_PERIODIC = 7 };
+
+struct Params {
+  double gamma, R, Cp, prandtl;
+  double mu_ref, T0, Tref, omega;
+  double ev_alpha, ev_beta, tvbM;
+  double cfl;
+  int model;      // 0 euler, 1 ns
+  int flux, mu_model, recon;
+  int nd, visc, heat;
+};
+
+struct Prim { double T, u, v, p; };
+struct Cons { double r, mx, my, E; };
+struct Ent { double f, vx, vy, l; };
+struct Flx { double m, x, y, e; };
+
+__device__ __forceinline__ double dmin_(double a, double b) { return (b < a) ? b : a; }  // std::min
+__device__ __forceinline__ double dmax_(double a, double b) { return (a < b) ? b : a; }  // std::max
+
+// src/material.h:24-42
+__device__ __forceinline__ double logavg(double a, double b) {
+  double xi = b / a;
+  double f = (xi - 1.0) / (xi + 1.0);
+  double u = f * f;
+  double F;
+  if (u < 1.0e-2) {
+    double u2 = u * u;
+    double u3 = u2 * u;
+    F = 1.0 + u / 3.0 + u2 / 5.0 + u3 / 7.0;
+  } else {
+    F = log(xi) / 2.0 / f;
+  }
+  return 0.5 * (a + b) / F;
+}
+
+__device__ __forceinline__ double density(const Params& k, const Prim& q) { return q.p / (k.R * q.T); }
+__device__ __forceinline__ double sound_speed(const Params& k, const Prim& q) { return sqrt(k.gamma * k.R * q.T); }
+__device__ __forceinline__ double entropy_fn(const Params& k, const Prim& q) {
+  return log(q.p) - k.gamma * log(density(k, q));
+}
+
+__device__ __forceinline__ double viscosity(const Params& k, double T) {   // src/material.h:551-568
+  if (k.mu_model == 1) return k.mu_ref * pow(T, 1.5) / (T + k.T0);
+  if (k.mu_model == 2) return k.mu_ref * pow(T / k.Tref, k.omega);
+  return k.mu_ref;
+}
+
+__device__ __forceinline__ Cons prim2con(const Params& k, const Prim& q) {   // src/material.h:501-513
+  Cons c;
+  double rho = density(k, q);
+  c.r = rho;
+  c.mx = q.u * rho;
+  c.my = q.v * rho;
+  c.E = q.p / (k.gamma - 1.0) + 0.5 * (q.u * q.u + q.v * q.v) * rho;
+  return c;
+}
+
+__device__ __forceinline__ Prim con2prim(const Params& k, const Cons& c) {   // src/material.h:518-529
+  Prim q;
+  double ir = 1.0 / c.r;
+  q.u = c.mx * ir;
+  q.v = c.my * ir;
+  q.p = (k.gamma - 1.0) * (c.E - 0.5 * (c.mx * c.mx + c.my * c.my) / c.r);
+  q.T = q.p / (k.R * c.r);
+  return q;
+}
+
+__device__ __forceinline__ Ent prim2ent(const Params& k, const Prim& q) {   // src/material.h:534-546
+  Ent e;
+  double rho = density(k, q);
+  double beta = rho / (2 * q.p);
+  double s = entropy_fn(k, q);
+  e.f = (k.gamma - s) / (k.gamma - 1) - (q.u * q.u + q.v * q.v) * beta;
+  e.vx = q.u * (2 * beta);
+  e.vy = q.v * (2 * beta);
+  e.l = -2 * beta;
+  return e;
+}
+
+// ----------------------------------------------------------------- limiters
+__device__ __forceinline__ double minmod_tvd(double a, double b) {          // src/limiter.h:14-27
+  if (a < 0.0 && b < 0.0) return -dmin_(-a, -b);
+  if (a > 0.0 && b > 0.0) return dmin_(a, b);
+  return 0.0;
+}
+
+template <int RECON>
+__device__ __forceinline__ double limited_slope(double ul, double ur, double h, double M) {  // src/reconstruct.cc:101-134
+  if (RECON == RECON_VAN_ALBADA) {
+    double s = dmax_(0.0, (2 * ul * ur + 1.0e-14) / (ul * ul + ur * ur + 1.0e-14));
+    return 0.25 * s * ((1.0 - (1.0 / 3.0) * s) * ul + (1.0 + (1.0 / 3.0) * s) * ur);
+  } else if (RECON == RECON_TVD_MINMOD) {
+    return 0.5 * minmod_tvd(ul, ur);
+  } else if (RECON == RECON_ENO2) {
+    return 0.5 * ((fabs(ul) < fabs(ur)) ? ul : ur);
+  } else {  // TVB minmod, src/limiter.h:66-77
+    double c = 0.5 * (ul + ur);
+    if (fabs(c) < M * (h * h)) return 0.5 * c;
+    return 0.5 * minmod_tvd(ul, ur);
+  }
+}
+
+// Material::reconstruct (src/reconstruct.cc:139-188) for one component.
+template <int RECON>
+__device__ __forceinline__ void reconstruct1(double l, double r, double gl, double gr, double h, double M,
+                                             double& rl, double& rr) {
+  if (RECON == RECON_FIRST) {
+    rl = l; rr = r;
+  } else if (RECON == RECON_SECOND) {
+    rl = l + 0.5 * gl;
+    rr = r - 0.5 * gr;
+  } else if (RECON == RECON_SECOND_MUSCL) {
+    const double K = 1.0 / 3.0;
+    double d = r - l;
+    double dl = 2.0 * gl - d;
+    rl = l + (dl * (1.0 - K) + d * (1.0 + K)) * 0.25;
+    double dr = 2.0 * gr - d;
+    rr = r - (dr * (1.0 - K) + d * (1.0 + K)) * 0.25;
+  } else {
+    double d = r - l;
+    double dl = 2.0 * gl - d;
+    rl = l + limited_slope<RECON>(dl, d, h, M);
+    double dr = 2.0 * gr - d;
+    rr = r - limited_slope<RECON>(dr, d, h, M);
+  }
+}
+
+// ------------------------------------------------------------------- fluxes
+// All take the raw dual normal (nx, ny) and return the flux per unit normal
+// length; the caller multiplies by |n| like Material::num_flux (src/material.cc:69-73).
+
+__device__ __forceinline__ Flx kepec_flux(const Params& k, const Prim& L, const Prim& R, double unx, double uny) {
+  // src/kepec.cc:10-38
+  double rhol = density(k, L), rhor = density(k, R);
+  double rho = logavg(rhol, rhor);
+  double vel2 = 0.5 * ((L.u * L.u + L.v * L.v) + (R.u * R.u + R.v * R.v));
+  double betal = 0.5 / (k.R * L.T);
+  double betar = 0.5 / (k.R * R.T);
+  double beta = logavg(betal, betar);
+  double p = 0.5 * (rhol + rhor) / (betal + betar);
+  double vx = L.u * 0.5 + R.u * 0.5, vy = L.v * 0.5 + R.v * 0.5;
+  double vn = vx * unx + vy * uny;
+  Flx F;
+  F.m = rho * vn;
+  F.x = unx * p + vx * F.m;
+  F.y = uny * p + vy * F.m;
+  F.e = 0.5 * (1.0 / ((k.gamma - 1.0) * beta) - vel2) * F.m + (F.x * vx + F.y * vy);
+  return F;
+}
+
+__device__ __forceinline__ Flx kep_flux(const Params& k, const Prim& L, const Prim& R, double unx, double uny) {
+  // src/kep.cc:10-38
+  double rhol = density(k, L), rhor = density(k, R);
+  double al = sound_speed(k, L), ar = sound_speed(k, R);
+  double Hl = al * al / (k.gamma - 1.0) + 0.5 * (L.u * L.u + L.v * L.v);
+  double Hr = ar * ar / (k.gamma - 1.0) + 0.5 * (R.u * R.u + R.v * R.v);
+  double p = 0.5 * (L.p + R.p);
+  double rho = 0.5 * (rhol + rhor);
+  double H = 0.5 * (Hl + Hr);
+  double vx = L.u * 0.5 + R.u * 0.5, vy = L.v * 0.5 + R.v * 0.5;
+  double vn = vx * unx + vy * uny;
+  Flx F;
+  F.m = rho * vn;
+  F.x = unx * p + vx * F.m;
+  F.y = uny * p + vy * F.m;
+  F.e = rho * H * vn;
+  return F;
+}
+
+__device__ __forceinline__ Flx roe_ec_flux(const Params& k, const Prim& L, const Prim& R, double unx, double uny) {
+  // src/roe_ec.cc:10-44
+  double rhol = density(k, L), rhor = density(k, R);
+  double pl = L.p, pr = R.p;
+  double bl = sqrt(rhol / pl), br = sqrt(rhor / pr);
+  double z1b = 0.5 * (bl + br);
+  double zx = L.u * (0.5 * bl) + R.u * (0.5 * br);
+  double zy = L.v * (0.5 * bl) + R.v * (0.5 * br);
+  double z5b = 0.5 * (bl * pl + br * pr);
+  double zn = zx * unx + zy * uny;
+  double z1l = logavg(bl, br);
+  double z5l = logavg(bl * pl, br * pr);
+  Flx F;
+  F.m = z5l * zn;
+  double c1 = z5b / z1b, c2 = F.m / z1b;
+  F.x = unx * c1 + zx * c2;
+  F.y = uny * c1 + zy * c2;
+  F.e = 0.5 * ((k.gamma + 1.0) / (k.gamma - 1.0) * F.m / z1l + (F.x * zx + F.y * zy)) / z1b;
+  return F;
+}
+
+__device__ __forceinline__ Flx avg_flux(const Params& k, const Prim& L, const Prim& R, double unx, double uny) {
+  // src/simple_avg.cc:10-46
+  double rhol = density(k, L), rhor = density(k, R);
+  double El = 0.5 * rhol * (L.u * L.u + L.v * L.v) + L.p / (k.gamma - 1);
+  double Er = 0.5 * rhor * (R.u * R.u + R.v * R.v) + R.p / (k.gamma - 1);
+  double vnl = L.u * unx + L.v * uny, vnr = R.u * unx + R.v * uny;
+  double ml = rhol * vnl, mr = rhor * vnr;
+  Flx F;
+  F.m = 0.0 + ml * 0.5;
+  F.m += mr * 0.5;
+  F.x = 0.0 + (unx * L.p + L.u * ml) * 0.5;
+  F.x += (unx * R.p + R.u * mr) * 0.5;
+  F.y = 0.0 + (uny * L.p + L.v * ml) * 0.5;
+  F.y += (uny * R.p + R.v * mr) * 0.5;
+  F.e = 0.0 + ((El + L.p) * vnl) * 0.5;
+  F.e += ((Er + R.p) * vnr) * 0.5;
+  return F;
+}
+
+// KEPES-TeCNO (src/kepes_tecno_roe.cc:11-173, src/kepes_tecno_rusanov.cc:11-164):
+// KEPEC central flux minus 0.5 R Lambda (Z_ji - Z_ij), Z = R^T V reconstructed
+// along the edge with the slopes R^T (grad V . dr).  dEl/dEr are the entropy-
+// variable gradients (V1,V2,V3,V5) x (x,y) at the two vertices, (dx,dy) the
+// edge vector x_r - x_l.
+template <int ROE, int RECON>
+__device__ __forceinline__ Flx tecno_flux(const Params& k, const Prim& L, const Prim& Rp, double unx, double uny,
+                                          double dx, double dy, const double* dEl, const double* dEr) {
+  const double g = k.gamma;
+  double rhol = density(k, L), rhor = density(k, Rp);
+  double rho = logavg(rhol, rhor);
+  double betal = 0.5 / (k.R * L.T);
+  double betar = 0.5 / (k.R * Rp.T);
+  double beta = logavg(betal, betar);
+  double a = sqrt(0.5 * g / beta);
+  double p = 0.5 * (rhol + rhor) / (betal + betar);
+  double vx = L.u * 0.5 + Rp.u * 0.5, vy = L.v * 0.5 + Rp.v * 0.5;
+  double vn = vx * unx + vy * uny;
+  Flx F = kepec_flux(k, L, Rp, unx, uny);
+  if (!k.nd) return F;
+
+  double vsq = vx * vx + vy * vy;
+  double H = a * a / (g - 1.0) + 0.5 * vsq;
+  double v1 = vx * uny - vy * unx;
+  double const1 = sqrt(rho / g);
+  double psqrt = sqrt(p);
+  double S0 = sqrt(0.5) * const1, S1 = sqrt(g - 1.0) * const1, S2 = psqrt;
+  // scaled eigenvector matrix; rows = (mass, mx, my, energy), cols = waves (u-a, entropy, shear, u+a)
+  double R[4][4] = {{1 * S0, 1 * S1, 0 * S2, 1 * S0},
+                    {(vx - a * unx) * S0, vx * S1, uny * S2, (vx + a * unx) * S0},
+                    {(vy - a * uny) * S0, vy * S1, -unx * S2, (vy + a * uny) * S0},
+                    {(H - a * vn) * S0, (0.5 * vsq) * S1, v1 * S2, (H + a * vn) * S0}};
+  double Lam[4];
+  if (ROE) {
+    double vnl = L.u * unx + L.v * uny, vnr = Rp.u * unx + Rp.v * uny;
+    double al = sound_speed(k, L), ar = sound_speed(k, Rp);
+    double l2 = fabs(vn);
+    Lam[0] = (1 + k.ev_beta) * fabs(vn - a) + k.ev_alpha * fabs((vnl - al) - (vnr - ar));
+    Lam[1] = l2;
+    Lam[2] = l2;
+    Lam[3] = (1 + k.ev_beta) * fabs(vn + a) + k.ev_alpha * fabs((vnl + al) - (vnr + ar));
+  } else {
+    double lr = fabs(vn) + fabs(a);
+    Lam[0] = Lam[1] = Lam[2] = Lam[3] = lr;
+  }
+  double sl = entropy_fn(k, L), sr = entropy_fn(k, Rp);
+  double Vl[4] = {(g - sl) / (g - 1.0) - betal * (L.u * L.u + L.v * L.v), 2 * L.u * betal, 2 * L.v * betal, -2 * betal};
+  double Vr[4] = {(g - sr) / (g - 1.0) - betar * (Rp.u * Rp.u + Rp.v * Rp.v), 2 * Rp.u * betar, 2 * Rp.v * betar,
+                  -2 * betar};
+  double h = sqrt(dx * dx + dy * dy);
+  double gl[4], gr[4];
+#pragma unroll
+  for (int i = 0; i < 4; ++i) {
+    gl[i] = dEl[2 * i] * dx + dEl[2 * i + 1] * dy;
+    gr[i] = dEr[2 * i] * dx + dEr[2 * i + 1] * dy;
+  }
+  double dZ[4];
+#pragma unroll
+  for (int i = 0; i < 4; ++i) {
+    double Zl = 0.0, Zr = 0.0, sgl = 0.0, sgr = 0.0;
+#pragma unroll
+    for (int j = 0; j < 4; ++j) {
+      Zl += R[j][i] * Vl[j];
+      Zr += R[j][i] * Vr[j];
+      sgl += R[j][i] * gl[j];
+      sgr += R[j][i] * gr[j];
+    }
+    double zij, zji;
+    reconstruct1<RECON>(Zl, Zr, sgl, sgr, h, k.tvbM, zij, zji);
+    dZ[i] = zji - zij;
+  }
+  double Diff[4];
+#pragma unroll
+  for (int i = 0; i < 4; ++i) {
+    double d = 0.0;
+#pragma unroll
+    for (int j = 0; j < 4; ++j) d += R[i][j] * Lam[j] * dZ[j];
+    Diff[i] = d;
+  }
+  F.m -= 0.5 * Diff[0];
+  F.x -= 0.5 * Diff[1];
+  F.y -= 0.5 * Diff[2];
+  F.e -= 0.5 * Diff[3];
+  return F;
+}
+
+// Material::num_flux (src/material.cc:27-74): flux times |n|.
+template <int FLUX, int RECON>
+__device__ __forceinline__ Flx num_flux(const Params& k, const Prim& L, const Prim& R, double nx, double ny, double dx,
+                                        double dy, const double* dEl, const double* dEr) {
+  double area = sqrt(nx * nx + ny * ny);
+  double ia = 1.0 / area;
+  double unx = nx * ia, uny = ny * ia;
+  Flx F;
+  if (FLUX == FLUX_TECNO_ROE) F = tecno_flux<1, RECON>(k, L, R, unx, uny, dx, dy, dEl, dEr);
+  else if (FLUX == FLUX_TECNO_RUSANOV) F = tecno_flux<0, RECON>(k, L, R, unx, uny, dx, dy, dEl, dEr);
+  else if (FLUX == FLUX_KEPEC) F = kepec_flux(k, L, R, unx, uny);
+  else if (FLUX == FLUX_KEP) F = kep_flux(k, L, R, unx, uny);
+  else if (FLUX == FLUX_ROE_EC) F = roe_ec_flux(k, L, R, unx, uny);
+  else F = avg_flux(k, L, R, unx, uny);
+  F.m *= area; F.x *= area; F.y *= area; F.e *= area;
+  return F;
+}
+
+// Material::inviscid_bflux (src/material.cc:110-127).
+__device__ __forceinline__ Flx inviscid_bflux(const Params& k, const Prim& q, const Prim& qb, double nx, double ny) {
+  double vnb = qb.u * nx + qb.v * ny;
+  double vn = q.u * nx + q.v * ny;
+  double rho = density(k, q);
+  Flx F;
+  F.m = rho * vnb;
+  F.x = nx * qb.p + q.u * F.m;
+  F.y = ny * qb.p + q.v * F.m;
+  F.e = (0.5 * rho * (q.u * q.u + q.v * q.v) + k.gamma * q.p / (k.gamma - 1.0)) * vnb + (qb.p - q.p) * vn;
+  return F;
+}
+
+// Viscous matrices K_ij dV_j (src/material.cc:158-230); dE is the cell
+// gradient (V1,V2,V3,V5) x (x,y).  Returns the four (x,y) flux-direction
+// products needed for any normal, and e4 = 1/V5, c2 = k/R.
+struct ViscK { double a1, a2, a4, b1, b2, b4, e4, c2; };
+
+__device__ __forceinline__ ViscK viscous_K(const Params& k, const Ent& st, const double* dE) {
+  double mu = viscosity(k, -1 / (k.R * st.l));
+  double kk = mu * k.Cp / k.prandtl;
+  if (!k.visc) mu = 0.0;
+  if (!k.heat) kk = 0.0;
+  double e1 = st.vx / st.l, e2 = st.vy / st.l, e4 = 1.0 / st.l;
+  double c1 = 4.0 * mu / 3.0, c2 = kk / k.R, c3 = 2 * mu / 3.0;
+  // dE index: V1:(0,1) V2:(2,3) V3:(4,5) V5:(6,7)
+  double d1x = dE[2], d1y = dE[3], d2x = dE[4], d2y = dE[5], d4x = dE[6], d4y = dE[7];
+  double K11_1 = c1 * (-d1x + e1 * d4x);
+  double K11_2 = mu * (-d2x + e2 * d4x);
+  double K11_4 = c1 * e1 * d1x + mu * (e2 * d2x) + (-c1 * e1 * e1 - mu * (e2 * e2) + c2 * e4) * d4x;
+  double K12_1 = c3 * (d2y - e2 * d4y);
+  double K12_2 = mu * (-d1y + e1 * d4y);
+  double K12_4 = mu * e2 * d1y - c3 * e1 * d2y - (mu - c3) * e1 * e2 * d4y;
+  double K21_1 = mu * (-d2x + e2 * d4x);
+  double K21_2 = c3 * (d1x - e1 * d4x);
+  double K21_4 = -c3 * e2 * d1x + mu * e1 * d2x - (mu - c3) * e1 * e2 * d4x;
+  double K22_1 = mu * (-d1y + e1 * d4y);
+  double K22_2 = c1 * (-d2y + e2 * d4y);
+  double K22_4 = mu * (e1 * d1y) + c1 * e2 * d2y + (-mu * (e1 * e1) - c1 * e2 * e2 + c2 * e4) * d4y;
+  ViscK r;
+  r.a1 = K11_1 + K12_1; r.a2 = K11_2 + K12_2; r.a4 = K11_4 + K12_4;
+  r.b1 = K21_1 + K22_1; r.b2 = K21_2 + K22_2; r.b4 = K21_4 + K22_4;
+  r.e4 = e4;
+  r.c2 = c2;
+  return r;
+}
+
+__device__ __forceinline__ Flx viscous_apply(const ViscK& K, double nx, double ny) {
+  Flx F;
+  F.m = 0.0;
+  F.x = -(K.a1 * nx + K.b1 * ny) * K.e4;
+  F.y = -(K.a2 * nx + K.b2 * ny) * K.e4;
+  F.e = -(K.a4 * nx + K.b4 * ny) * K.e4;
+  return F;
+}
+
+// BoundaryCondition::apply, two-state form (src/bc.h:568-610).
+__device__ __forceinline__ void bc_apply2(int kind, int adiabatic, const double* val, double nx, double ny,
+                                          Prim& s0, Prim& s1) {
+  switch (kind) {
+    case BC_SLIP: {
+      double meas = sqrt(nx * nx + ny * ny);
+      double ux = nx * (1.0 / meas), uy = ny * (1.0 / meas);
+      double fact = s0.u * ux + s0.v * uy;
+      s0.u += ux * -fact;
+      s0.v += uy * -fact;
+      s1 = s0;
+      break;
+    }
+    case BC_NOSLIP:
+      s0.u = val[1]; s0.v = val[2];
+      s1.u = s0.u; s1.v = s0.v;
+      s1.p = s0.p;
+      if (adiabatic) s1.T = s0.T;
+      else { s0.T = val[0]; s1.T = val[0]; }
+      break;
+    case BC_PRESSURE: s1.p = val[4]; break;
+    case BC_INLET:
+      s0.T = val[0]; s0.u = val[1]; s0.v = val[2]; s0.p = val[4];
+      s1 = s0;
+      break;
+    case BC_OUTLET: s1 = s0; break;
+    case BC_FARFIELD:
+      s1.T = val[0]; s1.u = val[1]; s1.v = val[2]; s1.p = val[4];
+      break;
+    default: break;
+  }
+}
+
+// BoundaryCondition::apply, single-state form (src/bc.h:615-654).
+__device__ __forceinline__ void bc_apply1(int kind, int adiabatic, const double* val, double nx, double ny, Prim& s) {
+  switch (kind) {
+    case BC_SLIP: {
+      double meas = sqrt(nx * nx + ny * ny);
+      double ux = nx * (1.0 / meas), uy = ny * (1.0 / meas);
+      double fact = s.u * ux + s.v * uy;
+      s.u += ux * -fact;
+      s.v += uy * -fact;
+      break;
+    }
+    case BC_NOSLIP:
+      s.u = val[1]; s.v = val[2];
+      if (!adiabatic) s.T = val[0];
+      break;
+    case BC_PRESSURE: s.p = val[4]; break;
+    case BC_INLET: s.T = val[0]; s.u = val[1]; s.v = val[2]; s.p = val[4]; break;
+    default: break;
+  }
+}
+
+}  // namespace tg

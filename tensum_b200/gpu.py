@@ -1,0 +1,169 @@
+"""Python binding of the C ABI (include/tensum_gpu.h) via ctypes.
+
+The device library is mandatory: loading fails loudly if it is missing, and
+:class:`Solver` raises if ``tg_create`` reports no CUDA device.  There is no
+CPU fallback anywhere on this path.
+"""
+from __future__ import annotations
+
+import ctypes as C
+import os
+
+import numpy as np
+
+from . import abi
+
+HERE = os.path.dirname(os.path.abspath(__file__))
+LIB_PATH = os.path.join(HERE, "libtensum_b200.so")
+
+EXPORTS = ["tg_create", "tg_destroy", "tg_last_error", "tg_abi_version", "tg_set_state", "tg_get_state",
+           "tg_store_conserved_old", "tg_compute_dt", "tg_gradients", "tg_residual", "tg_update",
+           "tg_residual_norm", "tg_end_step", "tg_step", "tg_global", "tg_stream", "tg_time_phase", "tg_query"]
+
+PHASE = {"gradient": 0, "flux": 1, "update": 2, "dt": 3, "step": 4}
+QUERY = {"n_vertex": 0, "n_edge": 1, "n_bface": 2, "kernels_per_step": 3, "device_bytes": 4, "kernels_per_flux": 5}
+
+_lib = None
+
+
+class TensumError(RuntimeError):
+    def __init__(self, status: int, msg: str):
+        super().__init__(f"{abi.STATUS.get(status, status)}: {msg}")
+        self.status = status
+
+
+def load():
+    """Load libtensum_b200.so (raises OSError when it has not been built)."""
+    global _lib
+    if _lib is not None:
+        return _lib
+    if not os.path.exists(LIB_PATH):
+        raise OSError(f"{LIB_PATH} is missing; build it with `python -m tensum_b200.build`")
+    L = C.CDLL(LIB_PATH)
+    vp, dp, i = C.c_void_p, C.POINTER(C.c_double), C.c_int
+    L.tg_create.argtypes = [vp, vp, vp, vp, C.POINTER(vp)]
+    L.tg_destroy.argtypes = [vp]
+    L.tg_last_error.argtypes = [vp]
+    L.tg_last_error.restype = C.c_char_p
+    L.tg_abi_version.restype = i
+    L.tg_set_state.argtypes = [vp, dp, i, C.c_double]
+    L.tg_get_state.argtypes = [vp, dp, i]
+    L.tg_store_conserved_old.argtypes = [vp]
+    L.tg_compute_dt.argtypes = [vp, dp, dp]
+    L.tg_gradients.argtypes = [vp, dp]
+    L.tg_residual.argtypes = [vp, dp]
+    L.tg_update.argtypes = [vp, i]
+    L.tg_residual_norm.argtypes = [vp, C.c_long, dp]
+    L.tg_end_step.argtypes = [vp, dp]
+    L.tg_step.argtypes = [vp, i, dp]
+    L.tg_global.argtypes = [vp, dp, dp]
+    L.tg_stream.argtypes = [vp, C.POINTER(vp)]
+    L.tg_time_phase.argtypes = [vp, i, i, dp]
+    L.tg_query.argtypes = [vp, i, dp]
+    for name in EXPORTS:
+        f = getattr(L, name)
+        if name not in ("tg_last_error", "tg_abi_version"):
+            f.restype = i
+    _lib = L
+    return L
+
+
+def _d(a: np.ndarray):
+    return a.ctypes.data_as(C.POINTER(C.c_double))
+
+
+class Solver:
+    """One device solver instance (mirrors the FiniteVolume hot-path members)."""
+
+    def __init__(self, problem: abi.Problem):
+        self.L = load()
+        self.problem = problem
+        self.nv = problem.geom.n_vertex
+        h = C.c_void_p()
+        st = self.L.tg_create(C.byref(problem.mesh), C.byref(problem.material), C.byref(problem.bc),
+                              C.byref(problem.options), C.byref(h))
+        if st != 0:
+            raise TensumError(st, self.L.tg_last_error(None).decode())
+        self.h = h
+
+    def _chk(self, st):
+        if st != 0:
+            raise TensumError(st, self.L.tg_last_error(self.h).decode())
+
+    def close(self):
+        if getattr(self, "h", None):
+            self.L.tg_destroy(self.h)
+            self.h = None
+
+    def __del__(self):
+        try:
+            self.close()
+        except Exception:
+            pass
+
+    def set_state(self, prim: np.ndarray, t0: float = 0.0):
+        prim = np.ascontiguousarray(prim, np.float64)
+        self._chk(self.L.tg_set_state(self.h, _d(prim), self.nv, t0))
+
+    def get_state(self) -> np.ndarray:
+        out = np.empty((self.nv, 5))
+        self._chk(self.L.tg_get_state(self.h, _d(out), self.nv))
+        return out
+
+    def store_conserved_old(self):
+        self._chk(self.L.tg_store_conserved_old(self.h))
+
+    def compute_dt(self):
+        g = C.c_double()
+        dt = np.empty(self.nv)
+        self._chk(self.L.tg_compute_dt(self.h, C.byref(g), _d(dt)))
+        return g.value, dt
+
+    def gradients(self) -> np.ndarray:
+        out = np.empty((self.nv, 5, 3))
+        self._chk(self.L.tg_gradients(self.h, _d(out)))
+        return out
+
+    def residual(self) -> np.ndarray:
+        out = np.empty((self.nv, 5))
+        self._chk(self.L.tg_residual(self.h, _d(out)))
+        return out
+
+    def update(self, r: int):
+        self._chk(self.L.tg_update(self.h, r))
+
+    def residual_norm(self, it: int) -> np.ndarray:
+        out = np.empty(6)
+        self._chk(self.L.tg_residual_norm(self.h, it, _d(out)))
+        return out
+
+    def end_step(self) -> np.ndarray:
+        info = np.empty(4)
+        self._chk(self.L.tg_end_step(self.h, _d(info)))
+        return info
+
+    def step(self, n: int) -> np.ndarray:
+        info = np.empty(4)
+        self._chk(self.L.tg_step(self.h, n, _d(info)))
+        return info
+
+    def global_integrals(self):
+        a, b = C.c_double(), C.c_double()
+        self._chk(self.L.tg_global(self.h, C.byref(a), C.byref(b)))
+        return a.value, b.value
+
+    def stream_ptr(self) -> int:
+        """cudaStream_t of this handle (for torch.cuda.ExternalStream / CUDA events)."""
+        p = C.c_void_p()
+        self._chk(self.L.tg_stream(self.h, C.byref(p)))
+        return int(p.value or 0)
+
+    def time_phase(self, phase: str, reps: int) -> float:
+        ms = C.c_double()
+        self._chk(self.L.tg_time_phase(self.h, PHASE[phase], reps, C.byref(ms)))
+        return ms.value
+
+    def query(self, key: str) -> float:
+        out = C.c_double()
+        self._chk(self.L.tg_query(self.h, QUERY[key], C.byref(out)))
+        return out.value

@@ -171,7 +171,9 @@ def write_part_file(mesh: TriMesh, case_dir: str) -> str:
     lines = ["DIMENSION 2", "PARTITIONS 1", f"NODES {V} OF {V}"]
     xy = mesh.coords
     ob = mesh.on_boundary.astype(int)
-    lines.extend(f"{v} {xy[v, 0]:.17g} {xy[v, 1]:.17g} 0 1 0 {ob[v]}" for v in range(V))
+    xs = [repr(float(a)) for a in xy[:, 0]]   # shortest round-trip decimal: exact when read back
+    ys = [repr(float(a)) for a in xy[:, 1]]
+    lines.extend(f"{v} {xs[v]} {ys[v]} 0 1 0 {ob[v]}" for v in range(V))
     lines.append(f"PERIODIC {len(mesh.periodic_sets)}")
     for k, s in enumerate(mesh.periodic_sets):
         lines.append(f"{k} {len(s)} " + " ".join(str(v) for v in s) + " 1 0")

@@ -1,0 +1,77 @@
+"""Recipes of the golden-fixture cases (shared by the generator and the tests)."""
+from __future__ import annotations
+
+import numpy as np
+
+from tensum_b200 import cases, mesh as M
+
+WALL = {"xvelocity": 0.0, "yvelocity": 0.0, "zvelocity": 0.0}
+FAR = {"temperature": 1.0 / 1.4, "xvelocity": 0.2, "yvelocity": 0.0, "zvelocity": 0.0, "pressure": 1.0 / 1.4}
+PERIODIC4 = {t: ("periodic", {}) for t in (1, 2, 3, 4)}
+
+
+def _sq(flux, recon, n=9, seed=3, steps=2, dump=2, ic="vortex", **kw):
+    return dict(mesh="square", n=n, seed=seed, flux=flux, reconstruct=recon, ic=ic, steps=steps,
+                dump_steps=dump, **kw)
+
+
+def _cyl(flux, recon, model, steps=2, dump=2, bc="noslip", **kw):
+    return dict(mesh="annulus", nr=6, nt=12, seed=1, flux=flux, reconstruct=recon, model=model, ic="cylinder",
+                steps=steps, dump_steps=dump, wall=bc, **kw)
+
+
+CASES = {
+    "sq_roe_minmod": _sq("kepes_tecno_roe", "minmod"),
+    "sq_rusanov_minmod": _sq("kepes_tecno_rusanov", "minmod"),
+    "sq_kepec": _sq("kepec", "first"),
+    "sq_kep": _sq("kep", "first"),
+    "sq_roe_ec": _sq("roe_ec", "first"),
+    "sq_avg": _sq("simple_avg", "first"),
+    "sq_roe_first": _sq("kepes_tecno_roe", "first"),
+    "sq_roe_second": _sq("kepes_tecno_roe", "second"),
+    "sq_roe_vanalbada": _sq("kepes_tecno_roe", "van_albada"),
+    "sq_roe_tvb": _sq("kepes_tecno_roe", "tvb_minmod", tvb_M=1.0),
+    "sq_roe_eno2": _sq("kepes_tecno_roe", "eno2"),
+    "sq_roe_evmod": _sq("kepes_tecno_roe", "minmod", ev_alpha=0.3, ev_beta=0.2),
+    "sq_kh_rusanov": _sq("kepes_tecno_rusanov", "minmod", n=11, seed=5, ic="kh"),
+    "vortex17_long": _sq("kepes_tecno_roe", "minmod", n=17, seed=7, steps=60, dump=0),
+    "cyl_euler": _cyl("kepes_tecno_roe", "minmod", "euler"),
+    "cyl_ns": _cyl("kepes_tecno_roe", "minmod", "ns"),
+    "cyl_ns_rusanov_va": _cyl("kepes_tecno_rusanov", "van_albada", "ns"),
+    "cyl_ns_isothermal": _cyl("kepes_tecno_roe", "minmod", "ns", bc="isothermal"),
+    "cyl_slip": _cyl("kepes_tecno_roe", "minmod", "euler", bc="slip"),
+    "cyl_inlet_outlet": _cyl("kepes_tecno_roe", "minmod", "euler", bc="inlet_outlet"),
+}
+
+
+def build_case(spec: dict):
+    """Mesh, configuration dict and initial primitive state of one recipe."""
+    if spec["mesh"] == "square":
+        if spec["ic"] == "kh":
+            m = M.periodic_square(spec["n"], 0.0, 1.0, 0.0, 1.0, spec["seed"])
+            a, phi = cases.kh_coefficients(spec["seed"])
+            prim0 = cases.kh_ic(m.coords, a, phi)
+        else:
+            m = cases.vortex_mesh(spec["n"], spec["seed"])
+            prim0 = cases.vortex_ic(m.coords)
+        bnd = dict(PERIODIC4)
+    else:
+        m = M.annulus(spec["nr"], spec["nt"], 0.5, 20.0, 0.3, spec["seed"])
+        prim0 = cases.cylinder_ic(m.coords)
+        # perturb so that gradients and viscous terms are non-trivial
+        prim0[:, 1] += 0.05 * np.sin(m.coords[:, 1])
+        prim0[:, 4] *= 1.0 + 0.01 * np.cos(m.coords[:, 0])
+        wall = spec.get("wall", "noslip")
+        if wall == "noslip":
+            bnd = {1: ("noslip", WALL), 2: ("farfield", FAR)}
+        elif wall == "isothermal":
+            bnd = {1: ("noslip", dict(WALL, temperature=0.8)), 2: ("farfield", FAR)}
+        elif wall == "slip":
+            bnd = {1: ("slip", {}), 2: ("farfield", FAR)}
+        else:
+            bnd = {1: ("inlet", FAR), 2: ("outlet", {})}
+    cfg = dict(flux=spec["flux"], reconstruct=spec["reconstruct"], boundary=bnd, final_time=100.0,
+               model=spec.get("model", "euler"), mu_ref=0.002 if spec.get("model") == "ns" else 0.0,
+               tvb_M=spec.get("tvb_M", 1.0), ev_alpha=spec.get("ev_alpha", 0.0), ev_beta=spec.get("ev_beta", 0.0),
+               time_stamps=1, cfl=0.8)
+    return m, cfg, prim0

@@ -1,0 +1,45 @@
+"""Generate golden fixtures by running the TENSUM reference itself.
+
+Needs the reference tree and a built oracle/_ref/tensum_harness (``make -C
+oracle ref``); run from the repository root:
+
+    python tests/golden/make_golden.py
+
+Every fixture records the case recipe (mesh generator + seed, boundary and
+scheme configuration), the initial state handed to the reference, and the
+reference's per-stage arrays dumped at full precision.  Tests rebuild the mesh
+from the recipe (the generators are deterministic) and compare against these
+arrays, so the checks run on machines without the reference.
+"""
+from __future__ import annotations
+
+import json
+import os
+import sys
+
+import numpy as np
+
+ROOT = os.path.dirname(os.path.dirname(os.path.dirname(os.path.abspath(__file__))))
+sys.path.insert(0, ROOT)
+sys.path.insert(0, os.path.join(ROOT, "oracle"))
+
+from tests.golden.cases_spec import CASES, build_case  # noqa: E402
+import ref_runner  # noqa: E402
+
+OUT = os.path.dirname(os.path.abspath(__file__))
+
+
+def main():
+    if not ref_runner.harness_available():
+        raise SystemExit("oracle/_ref/tensum_harness missing: run `make -C oracle ref` first")
+    for name, spec in CASES.items():
+        mesh, cfg, prim0 = build_case(spec)
+        d = ref_runner.run_case(mesh, cfg, prim0, spec["steps"], spec["dump_steps"])
+        keep = {k: v for k, v in d.items() if k not in ("wall_s",)}
+        keep["prim_in"] = prim0.ravel()
+        np.savez_compressed(os.path.join(OUT, f"{name}.npz"), spec=np.array(json.dumps(spec)), **keep)
+        print(name, "vertices", mesh.n_vertex, "records", len(keep))
+
+
+if __name__ == "__main__":
+    main()
