@@ -106,7 +106,12 @@ def test_cylinder_ns_multistep_matches_oracle(recon):
                                           "zvelocity": 0.0, "pressure": 1 / 1.4})},
                final_time=100.0, time_stamps=1, cfl=0.8)
     s, o = _run_pair(m, cfg, prim0, 25)
-    assert rel_l2(s.get_state(), o.get_prim()) <= TOL_STATE_LONG
+    # ENO2 (minabs) and TVB minmod switch discontinuously (|a| vs |b|, |c| vs M h^2):
+    # a last-ulp difference can pick the other branch at a near-tie and the
+    # difference then propagates.  Their per-stage parity is checked at 1e-12
+    # against the reference fixtures; over many steps they get a looser bound.
+    tol = 1e-5 if recon in ("eno2", "tvb_minmod") else TOL_STATE_LONG
+    assert rel_l2(s.get_state(), o.get_prim()) <= tol
 
 
 def test_unsteady_clamp_hits_output_times():
