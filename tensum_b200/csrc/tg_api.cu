@@ -5,6 +5,7 @@
 // stream; whole time steps are captured once into a CUDA graph and replayed.
 #include <cuda_runtime.h>
 
+#include <cmath>
 #include <cstdio>
 #include <cstdlib>
 #include <cstring>
@@ -14,6 +15,7 @@
 
 #include "../../include/tensum_gpu.h"
 #include "tg_kernels.cuh"
+#include "tg_tiles.cuh"
 #include "tg_mesh.h"
 
 using namespace tg;
@@ -32,6 +34,10 @@ struct tg_handle {
   Control ctl{};
   MeshView mv{};
   StateView sv{};
+  TileView tv{};
+  double* Pb[3] = {nullptr, nullptr, nullptr};   // rotating state buffers (buffer 0 = current state)
+  double* Wb[3] = {nullptr, nullptr, nullptr};
+  size_t smem_grad0 = 0, smem_grad1 = 0, smem_flux = 0;
   Scalars* sc = nullptr;       // device
   int* done = nullptr;         // device flag written by k_step_begin
   int* never = nullptr;        // device zero, used by single-phase calls
@@ -96,22 +102,12 @@ tg_status dev_alloc(tg_handle* h, size_t n, T** out) {
 inline int nblk(int n) { return (n + kBlock - 1) / kBlock; }
 
 // ---- kernel dispatch over (flux, reconstruction)
-typedef void (*EdgeKernel)(Params, MeshView, StateView, const int*);
+typedef void (*BfluxKernel)(Params, MeshView, StateView, const int*);
+typedef void (*TileFluxKernel)(Params, MeshView, TileView, StateView, Control, Scalars*, int, int, double*, double*,
+                               const int*);
 
 template <int F>
-EdgeKernel pick_edge(int recon) {
-  switch (recon) {
-    case RECON_FIRST: return k_edge_flux<F, RECON_FIRST>;
-    case RECON_SECOND: return k_edge_flux<F, RECON_SECOND>;
-    case RECON_SECOND_MUSCL: return k_edge_flux<F, RECON_SECOND_MUSCL>;
-    case RECON_VAN_ALBADA: return k_edge_flux<F, RECON_VAN_ALBADA>;
-    case RECON_TVD_MINMOD: return k_edge_flux<F, RECON_TVD_MINMOD>;
-    case RECON_TVB_MINMOD: return k_edge_flux<F, RECON_TVB_MINMOD>;
-    default: return k_edge_flux<F, RECON_ENO2>;
-  }
-}
-template <int F>
-EdgeKernel pick_bflux(int recon) {
+BfluxKernel pick_bflux(int recon) {
   switch (recon) {
     case RECON_FIRST: return k_bflux<F, RECON_FIRST>;
     case RECON_SECOND: return k_bflux<F, RECON_SECOND>;
@@ -122,18 +118,7 @@ EdgeKernel pick_bflux(int recon) {
     default: return k_bflux<F, RECON_ENO2>;
   }
 }
-
-EdgeKernel edge_kernel(int flux, int recon) {
-  switch (flux) {
-    case FLUX_TECNO_ROE: return pick_edge<FLUX_TECNO_ROE>(recon);
-    case FLUX_TECNO_RUSANOV: return pick_edge<FLUX_TECNO_RUSANOV>(recon);
-    case FLUX_KEPEC: return k_edge_flux<FLUX_KEPEC, RECON_FIRST>;
-    case FLUX_KEP: return k_edge_flux<FLUX_KEP, RECON_FIRST>;
-    case FLUX_ROE_EC: return k_edge_flux<FLUX_ROE_EC, RECON_FIRST>;
-    default: return k_edge_flux<FLUX_AVG, RECON_FIRST>;
-  }
-}
-EdgeKernel bflux_kernel(int flux, int recon) {
+BfluxKernel bflux_kernel(int flux, int recon) {
   switch (flux) {
     case FLUX_TECNO_ROE: return pick_bflux<FLUX_TECNO_ROE>(recon);
     case FLUX_TECNO_RUSANOV: return pick_bflux<FLUX_TECNO_RUSANOV>(recon);
@@ -144,48 +129,105 @@ EdgeKernel bflux_kernel(int flux, int recon) {
   }
 }
 
+template <int F, int M>
+TileFluxKernel pick_tile(int recon) {
+  switch (recon) {
+    case RECON_FIRST: return k_tile_flux<F, RECON_FIRST, M>;
+    case RECON_SECOND: return k_tile_flux<F, RECON_SECOND, M>;
+    case RECON_SECOND_MUSCL: return k_tile_flux<F, RECON_SECOND_MUSCL, M>;
+    case RECON_VAN_ALBADA: return k_tile_flux<F, RECON_VAN_ALBADA, M>;
+    case RECON_TVD_MINMOD: return k_tile_flux<F, RECON_TVD_MINMOD, M>;
+    case RECON_TVB_MINMOD: return k_tile_flux<F, RECON_TVB_MINMOD, M>;
+    default: return k_tile_flux<F, RECON_ENO2, M>;
+  }
+}
+template <int M>
+TileFluxKernel tile_kernel_m(int flux, int recon) {
+  switch (flux) {
+    case FLUX_TECNO_ROE: return pick_tile<FLUX_TECNO_ROE, M>(recon);
+    case FLUX_TECNO_RUSANOV: return pick_tile<FLUX_TECNO_RUSANOV, M>(recon);
+    case FLUX_KEPEC: return k_tile_flux<FLUX_KEPEC, RECON_FIRST, M>;
+    case FLUX_KEP: return k_tile_flux<FLUX_KEP, RECON_FIRST, M>;
+    case FLUX_ROE_EC: return k_tile_flux<FLUX_ROE_EC, RECON_FIRST, M>;
+    default: return k_tile_flux<FLUX_AVG, RECON_FIRST, M>;
+  }
+}
+TileFluxKernel tile_kernel(int flux, int recon, int mode) {
+  return mode == MODE_UPDATE ? tile_kernel_m<MODE_UPDATE>(flux, recon) : tile_kernel_m<MODE_RESIDUAL>(flux, recon);
+}
+
+// state view of buffer b (the three P/W buffers rotate through the stages)
+StateView view(const tg_handle* h, int b) {
+  StateView v = h->sv;
+  v.P = h->Pb[b];
+  v.W = h->Wb[b];
+  return v;
+}
+
 // ---- phases (all enqueue on h->stream; `done` gates work inside graphs)
-void enqueue_gradient(tg_handle* h, const int* done) {
-  k_gradient<<<nblk(h->mv.nv), kBlock, 0, h->stream>>>(h->prm, h->mv, h->sv, done);
+void enqueue_gradient(tg_handle* h, int b, bool first, const int* done) {
+  if (first)
+    k_tile_grad<true><<<h->L.ntiles, kTileThreads, h->smem_grad1, h->stream>>>(h->prm, h->mv, h->tv, view(h, b), h->sc,
+                                                                              done);
+  else
+    k_tile_grad<false><<<h->L.ntiles, kTileThreads, h->smem_grad0, h->stream>>>(h->prm, h->mv, h->tv, view(h, b),
+                                                                               h->sc, done);
 }
 
-int residual_kernels(const tg_handle* h, bool force_gradient) {
-  return ((h->grads_needed || force_gradient) ? 1 : 0) + 1 + (h->mv.nb > 0 ? 1 : 0) + (h->viscous ? 1 : 0) + 1;
-}
-
-void enqueue_residual(tg_handle* h, const int* done, bool force_gradient) {
-  if (h->grads_needed || force_gradient) enqueue_gradient(h, done);
-  edge_kernel(h->prm.flux, h->prm.recon)<<<nblk(h->mv.ne), kBlock, 0, h->stream>>>(h->prm, h->mv, h->sv, done);
+// boundary-face and viscous contributions, gathered by the tiled flux kernel
+void enqueue_boundary(tg_handle* h, int b, const int* done) {
   if (h->mv.nb > 0)
-    bflux_kernel(h->prm.flux, h->prm.recon)<<<nblk(2 * h->mv.nb), kBlock, 0, h->stream>>>(h->prm, h->mv, h->sv, done);
-  if (h->viscous) k_viscous<<<nblk(h->mv.nvu), kBlock, 0, h->stream>>>(h->prm, h->mv, h->sv, done);
-  k_assemble<<<nblk(h->mv.nv), kBlock, 0, h->stream>>>(h->mv, h->sv, h->viscous ? 1 : 0, done);
+    bflux_kernel(h->prm.flux, h->prm.recon)<<<nblk(2 * h->mv.nb), kBlock, 0, h->stream>>>(h->prm, h->mv, view(h, b),
+                                                                                            done);
+  if (h->viscous) k_viscous<<<nblk(h->mv.nvu), kBlock, 0, h->stream>>>(h->prm, h->mv, view(h, b), done);
+}
+
+void enqueue_tile_flux(tg_handle* h, int b, int mode, int r, bool norm, int bout, const int* done) {
+  tile_kernel(h->prm.flux, h->prm.recon, mode)<<<h->L.ntiles, kTileThreads, h->smem_flux, h->stream>>>(
+      h->prm, h->mv, h->tv, view(h, b), h->ctl, h->sc, r, norm ? 1 : 0, h->Pb[bout], h->Wb[bout], done);
+}
+
+int residual_kernels(const tg_handle* h) {
+  return (h->mv.nb > 0 ? 1 : 0) + (h->viscous ? 1 : 0) + 1;
+}
+
+// compute_residual on buffer 0 (gradient, boundary/viscous terms, tiled fluxes -> R)
+void enqueue_residual(tg_handle* h, const int* done) {
+  enqueue_gradient(h, 0, false, done);
+  enqueue_boundary(h, 0, done);
+  enqueue_tile_flux(h, 0, MODE_RESIDUAL, 0, false, 0, done);
 }
 
 void enqueue_dt(tg_handle* h, const int* done) {
   if (h->ctl.time_step <= 0.0)
-    k_dt<<<nblk(h->mv.nv), kBlock, 0, h->stream>>>(h->prm, h->mv, h->sv, h->sc, done);
+    k_dt<<<nblk(h->mv.nv), kBlock, 0, h->stream>>>(h->prm, h->mv, view(h, 0), h->sc, done);
   k_dt_final<<<1, 1, 0, h->stream>>>(h->ctl, h->sc, done);
 }
 
 void enqueue_update(tg_handle* h, int r, bool norm, const int* done) {
-  k_update<<<nblk(h->mv.nv), kBlock, 0, h->stream>>>(h->prm, h->mv, h->sv, h->ctl, h->sc, r, norm ? 1 : 0, done);
+  k_update<<<nblk(h->mv.nv), kBlock, 0, h->stream>>>(h->prm, h->mv, view(h, 0), h->ctl, h->sc, r, norm ? 1 : 0, done);
 }
 
-void enqueue_norm_final(tg_handle* h, bool use_sc_iter, long long iter, const int* done) {
-  k_norm_final<<<1, kBlock, 0, h->stream>>>(h->sv, h->nblocks_v, h->mv.nv, h->sc, use_sc_iter ? 1 : 0, iter, done);
+void enqueue_norm_final(tg_handle* h, int nblocks, bool use_sc_iter, long long iter, const int* done) {
+  k_norm_final<<<1, kBlock, 0, h->stream>>>(h->sv, nblocks, h->mv.nv, h->sc, use_sc_iter ? 1 : 0, iter, done);
 }
 
+// One iteration of FiniteVolume::solve's loop on the rotating buffers:
+// stage r reads buffer r and writes buffer (r+1)%3, so the step ends in buffer 0.
 void enqueue_step(tg_handle* h) {
   k_step_begin<<<1, 1, 0, h->stream>>>(h->ctl, h->sc, h->done);
-  k_store_old<<<nblk(h->mv.nv), kBlock, 0, h->stream>>>(h->prm, h->mv, h->sv, h->done);
-  // dtmin reset happens in k_step_begin
-  enqueue_dt(h, h->done);
-  for (int r = 0; r < h->ctl.n_rks; ++r) {
-    enqueue_residual(h, h->done, false);
-    bool last = (r == h->ctl.n_rks - 1);
-    enqueue_update(h, r, last, h->done);
-    if (last) enqueue_norm_final(h, true, 0, h->done);
+  for (int r = 0; r < 3; ++r) {
+    const bool first = (r == 0), last = (r == 2);
+    if (first && h->ctl.time_step > 0.0) {
+      k_store_old<<<nblk(h->mv.nv), kBlock, 0, h->stream>>>(h->prm, h->mv, view(h, 0), h->done);
+      enqueue_gradient(h, r, false, h->done);
+    } else {
+      enqueue_gradient(h, r, first, h->done);   // first stage: + dt, U_old
+    }
+    if (first) k_dt_final<<<1, 1, 0, h->stream>>>(h->ctl, h->sc, h->done);
+    enqueue_boundary(h, r, h->done);
+    enqueue_tile_flux(h, r, MODE_UPDATE, r, last, (r + 1) % 3, h->done);
+    if (last) enqueue_norm_final(h, h->L.ntiles, true, 0, h->done);
   }
   k_step_end<<<1, 1, 0, h->stream>>>(h->ctl, h->sc, h->done);
 }
@@ -223,15 +265,11 @@ tg_status capture_step_graph(tg_handle* h) {
 
 void enqueue_phase(tg_handle* h, int phase) {
   switch (phase) {
-    case TG_PHASE_GRADIENT: enqueue_gradient(h, h->never); break;
-    case TG_PHASE_FLUX: {
-      edge_kernel(h->prm.flux, h->prm.recon)<<<nblk(h->mv.ne), kBlock, 0, h->stream>>>(h->prm, h->mv, h->sv, h->never);
-      if (h->mv.nb > 0)
-        bflux_kernel(h->prm.flux, h->prm.recon)<<<nblk(2 * h->mv.nb), kBlock, 0, h->stream>>>(h->prm, h->mv, h->sv, h->never);
-      if (h->viscous) k_viscous<<<nblk(h->mv.nvu), kBlock, 0, h->stream>>>(h->prm, h->mv, h->sv, h->never);
-      k_assemble<<<nblk(h->mv.nv), kBlock, 0, h->stream>>>(h->mv, h->sv, h->viscous ? 1 : 0, h->never);
+    case TG_PHASE_GRADIENT: enqueue_gradient(h, 0, false, h->never); break;
+    case TG_PHASE_FLUX:
+      enqueue_boundary(h, 0, h->never);
+      enqueue_tile_flux(h, 0, MODE_RESIDUAL, 0, false, 0, h->never);
       break;
-    }
     case TG_PHASE_UPDATE: enqueue_update(h, 1, false, h->never); break;
     case TG_PHASE_DT: enqueue_dt(h, h->never); break;
     default: cudaGraphLaunch(h->graph_exec, h->stream); break;
@@ -273,12 +311,19 @@ tg_status tg_create(const tg_mesh* mesh, const tg_material* mat, const tg_bc_tab
     delete h;
     return fail(nullptr, TG_INVALID_ARG, msg);
   }
+  msg = build_tiles(h->L, kTileThreads, 448, 1152);
+  if (!msg.empty()) {
+    delete h;
+    return fail(nullptr, TG_INVALID_ARG, msg);
+  }
   const HostLayout& L = h->L;
   h->grads_needed = h->viscous || ((mat->flux_scheme == FLUX_TECNO_ROE || mat->flux_scheme == FLUX_TECNO_RUSANOV) &&
                                    mat->reconstruct_scheme != RECON_FIRST);
 
   Params& k = h->prm;
   k.gamma = mat->gamma; k.R = mat->gas_const; k.Cp = mat->gamma * mat->gas_const / (mat->gamma - 1.0);
+  k.sqrt_gm1 = std::sqrt(mat->gamma - 1.0);
+  k.inv_gamma = 1.0 / mat->gamma;
   k.prandtl = mat->prandtl; k.mu_ref = mat->mu_ref; k.T0 = mat->T_0; k.Tref = mat->T_ref; k.omega = mat->omega;
   k.ev_alpha = mat->ev_mod_alpha; k.ev_beta = mat->ev_mod_beta; k.tvbM = mat->tvb_minmod_coef; k.cfl = opt->cfl;
   k.model = mat->model; k.flux = mat->flux_scheme; k.mu_model = mat->mu_model; k.recon = mat->reconstruct_scheme;
@@ -298,14 +343,41 @@ tg_status tg_create(const tg_mesh* mesh, const tg_material* mat, const tg_bc_tab
   UP(u_cell, u_cell) UP(c_v, c_v) UP(c_n, c_n) UP(c_inv2a, c_inv2a)
   UP(c_bf_off, c_bf_off) UP(c_bf, c_bf) UP(c_nbr_off, c_nbr_off) UP(c_nbr, c_nbr)
 #undef UP
+#define UPT(vec, field) \
+  if ((st = dev_upload(h, L.vec, &h->tv.field)) != TG_OK) { tg_destroy(h); return st; }
+  UPT(t_vbeg, vbeg) UPT(t_loff, loff) UPT(t_eoff, eoff) UPT(lv, lv) UPT(te_ab, ab)
+  UPT(te_nx, nx) UPT(te_ny, ny) UPT(te_g0x, g0x) UPT(te_g0y, g0y) UPT(te_g1x, g1x) UPT(te_g1y, g1y)
+  UPT(cv_off, cv_off) UPT(cv_ent, cv_ent) UPT(x, x) UPT(y, y) UPT(te_ux, ux) UPT(te_uy, uy) UPT(te_ar, ar)
+#undef UPT
   const size_t nv = L.nv;
   h->nblocks_v = nblk(L.nv);
 #define AL(field, n) \
   if ((st = dev_alloc(h, (n), &h->sv.field)) != TG_OK) { tg_destroy(h); return st; }
   AL(P, 4 * nv) AL(W, 4 * nv) AL(G, 8 * nv) AL(R, 4 * nv) AL(Uold, 4 * nv) AL(dt, nv)
-  AL(Fe, 4 * (size_t)L.ne) AL(Fb, 8 * (size_t)L.nb) AL(Fv, 9 * (size_t)L.nvu) AL(Fvb, 3 * (size_t)L.nb)
-  AL(part, 4 * (size_t)h->nblocks_v)
+  AL(Fb, 8 * (size_t)L.nb) AL(Fv, 9 * (size_t)L.nvu) AL(Fvb, 3 * (size_t)L.nb)
+  AL(part, 4 * (size_t)std::max(h->nblocks_v, L.ntiles))
 #undef AL
+  h->Pb[0] = h->sv.P;
+  h->Wb[0] = h->sv.W;
+  for (int b = 1; b < 3; ++b) {
+    if ((st = dev_alloc(h, 4 * nv, &h->Pb[b])) != TG_OK) { tg_destroy(h); return st; }
+    if ((st = dev_alloc(h, 4 * nv, &h->Wb[b])) != TG_OK) { tg_destroy(h); return st; }
+  }
+  h->smem_grad0 = tile_grad_smem(L.lmax, false);
+  h->smem_grad1 = tile_grad_smem(L.lmax, true);
+  h->smem_flux = tile_flux_smem(L.lmax, L.emax);
+  {
+    cudaError_t ea = cudaFuncSetAttribute(k_tile_grad<true>, cudaFuncAttributeMaxDynamicSharedMemorySize, (int)h->smem_grad1);
+    cudaError_t eb = cudaFuncSetAttribute(k_tile_grad<false>, cudaFuncAttributeMaxDynamicSharedMemorySize, (int)h->smem_grad0);
+    cudaError_t ec = cudaFuncSetAttribute(tile_kernel(mat->flux_scheme, mat->reconstruct_scheme, MODE_UPDATE),
+                                          cudaFuncAttributeMaxDynamicSharedMemorySize, (int)h->smem_flux);
+    cudaError_t ed = cudaFuncSetAttribute(tile_kernel(mat->flux_scheme, mat->reconstruct_scheme, MODE_RESIDUAL),
+                                          cudaFuncAttributeMaxDynamicSharedMemorySize, (int)h->smem_flux);
+    if (ea != cudaSuccess || eb != cudaSuccess || ec != cudaSuccess || ed != cudaSuccess) {
+      tg_destroy(h);
+      return fail(nullptr, TG_CUDA_ERROR, "tile kernels need more shared memory than the device allows");
+    }
+  }
   if ((st = dev_alloc(h, 1, &h->sc)) != TG_OK) { tg_destroy(h); return st; }
   if ((st = dev_alloc(h, 1, &h->done)) != TG_OK) { tg_destroy(h); return st; }
   if ((st = dev_alloc(h, 1, &h->never)) != TG_OK) { tg_destroy(h); return st; }
@@ -324,8 +396,8 @@ tg_status tg_create(const tg_mesh* mesh, const tg_material* mat, const tg_bc_tab
   c.time_mode = opt->time_mode; c.n_rks = 3; c.ntinst = (int)ti.size(); c.time_step = opt->time_step;
   c.min_residue = opt->min_residue; c.max_iter = opt->max_iter; c.final_time = opt->final_time; c.tinst = tip;
 
-  h->kernels_per_flux = residual_kernels(h, false) - (h->grads_needed ? 1 : 0);
-  h->kernels_per_step = 2 + (c.time_step > 0.0 ? 1 : 2) + 3 * (residual_kernels(h, false) + 1) + 1 + 1;
+  h->kernels_per_flux = residual_kernels(h);
+  h->kernels_per_step = 1 + 3 * (1 + residual_kernels(h)) + (c.time_step > 0.0 ? 1 : 0) + 1 + 1 + 1;
   {
     cudaError_t ep = cudaMallocHost((void**)&h->hP, 4 * nv * sizeof(double));
     if (ep != cudaSuccess) { tg_destroy(h); return fail(nullptr, TG_CUDA_ERROR, cudaGetErrorString(ep)); }
@@ -392,7 +464,7 @@ tg_status tg_get_state(tg_handle* h, double* prim, int n_vertex) {
 
 tg_status tg_store_conserved_old(tg_handle* h) {
   if (!h) return fail(h, TG_INVALID_ARG, "NULL handle");
-  k_store_old<<<nblk(h->mv.nv), kBlock, 0, h->stream>>>(h->prm, h->mv, h->sv, h->never);
+  k_store_old<<<nblk(h->mv.nv), kBlock, 0, h->stream>>>(h->prm, h->mv, view(h, 0), h->never);
   return sync(h);
 }
 
@@ -436,7 +508,7 @@ static tg_status copy_grad_out(tg_handle* h, double* dE_out) {
 
 tg_status tg_gradients(tg_handle* h, double* dE_out) {
   if (!h) return fail(h, TG_INVALID_ARG, "NULL handle");
-  enqueue_gradient(h, h->never);
+  enqueue_gradient(h, 0, false, h->never);
   tg_status st = sync(h);
   if (st != TG_OK || !dE_out) return st;
   return copy_grad_out(h, dE_out);
@@ -444,7 +516,7 @@ tg_status tg_gradients(tg_handle* h, double* dE_out) {
 
 tg_status tg_residual(tg_handle* h, double* res_out) {
   if (!h) return fail(h, TG_INVALID_ARG, "NULL handle");
-  enqueue_residual(h, h->never, true);
+  enqueue_residual(h, h->never);
   tg_status st = sync(h);
   if (st != TG_OK || !res_out) return st;
   const int nv = h->L.nv;
@@ -469,7 +541,7 @@ tg_status tg_update(tg_handle* h, int r) {
 tg_status tg_residual_norm(tg_handle* h, long iter, double* out6) {
   if (!h) return fail(h, TG_INVALID_ARG, "NULL handle");
   k_norm_part<<<h->nblocks_v, kBlock, 0, h->stream>>>(h->mv, h->sv, h->never);
-  enqueue_norm_final(h, false, iter, h->never);
+  enqueue_norm_final(h, h->nblocks_v, false, iter, h->never);
   Scalars s;
   tg_status st = read_scalars(h, &s);
   if (st != TG_OK) return st;
@@ -506,7 +578,7 @@ tg_status tg_step(tg_handle* h, int n_steps, double* info4) {
 
 tg_status tg_global(tg_handle* h, double* ke, double* ent) {
   if (!h) return fail(h, TG_INVALID_ARG, "NULL handle");
-  k_global<<<h->nblocks_v, kBlock, 0, h->stream>>>(h->prm, h->mv, h->sv);
+  k_global<<<h->nblocks_v, kBlock, 0, h->stream>>>(h->prm, h->mv, view(h, 0));
   std::vector<double> part(4 * (size_t)h->nblocks_v);
   TG_CUDA(h, cudaMemcpyAsync(part.data(), h->sv.part, part.size() * sizeof(double), cudaMemcpyDeviceToHost, h->stream));
   tg_status st = sync(h);

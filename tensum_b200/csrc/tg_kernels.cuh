@@ -113,72 +113,6 @@ __global__ void k_store_old(Params k, MeshView m, StateView s, const int* __rest
   s.Uold[i] = c.r; s.Uold[m.nv + i] = c.mx; s.Uold[2 * m.nv + i] = c.my; s.Uold[3 * m.nv + i] = c.E;
 }
 
-// Vertex gradients of the entropy variables (src/fv.cc:699-1059), as a gather:
-// sum over incident edges of g_side (W_other - W_self) plus the boundary
-// corrections of the incident boundary cells, times 1/(6 mcarea).
-__global__ void k_gradient(Params k, MeshView m, StateView s, const int* __restrict__ done) {
-  if (*done) return;
-  int v = blockIdx.x * blockDim.x + threadIdx.x;
-  if (v >= m.nv) return;
-  const int nv = m.nv;
-  double acc[8];
-#pragma unroll
-  for (int c = 0; c < 8; ++c) acc[c] = 0.0;
-  const double* W = s.W;
-  for (int j = m.ce_off[v]; j < m.ce_off[v + 1]; ++j) {
-    int ent = m.ce_ent[j];
-    int e = ent >> 1, side = ent & 1;
-    int a = m.e_a[e], b = m.e_b[e];
-    int self = side ? b : a, other = side ? a : b;
-    double gx = side ? m.e_g1x[e] : m.e_g0x[e];
-    double gy = side ? m.e_g1y[e] : m.e_g0y[e];
-#pragma unroll
-    for (int c = 0; c < 4; ++c) {
-      double dW = W[c * nv + other] - W[c * nv + self];
-      acc[2 * c] += gx * dW;
-      acc[2 * c + 1] += gy * dW;
-    }
-  }
-  for (int j = m.cb_off[v]; j < m.cb_off[v + 1]; ++j) {
-    int ent = m.cb_ent[j];
-    if ((ent & 3) != 1) continue;
-    int d = ent >> 2;
-    double dW[4];
-    bface_grad_corr(k, m, s, d, dW);
-#pragma unroll
-    for (int c = 0; c < 4; ++c) {
-      acc[2 * c] += m.b_nx[d] * dW[c];
-      acc[2 * c + 1] += m.b_ny[d] * dW[c];
-    }
-  }
-  double f = m.inv6mc[v];
-#pragma unroll
-  for (int c = 0; c < 8; ++c) s.G[c * nv + v] = acc[c] * f;
-}
-
-// Interior/boundary edge fluxes (src/fv.cc:1071-1097) into the edge buffer.
-template <int FLUX, int RECON>
-__global__ void k_edge_flux(Params k, MeshView m, StateView s, const int* __restrict__ done) {
-  if (*done) return;
-  int e = blockIdx.x * blockDim.x + threadIdx.x;
-  if (e >= m.ne) return;
-  const int nv = m.nv;
-  int a = m.e_a[e], b = m.e_b[e];
-  Prim L = load_prim(s.P, nv, a), R = load_prim(s.P, nv, b);
-  double gl[8], gr[8];
-  const bool needs_grad = (FLUX == FLUX_TECNO_ROE || FLUX == FLUX_TECNO_RUSANOV) && RECON != RECON_FIRST;
-  if (needs_grad) {
-#pragma unroll
-    for (int c = 0; c < 8; ++c) { gl[c] = s.G[c * nv + a]; gr[c] = s.G[c * nv + b]; }
-  } else {
-#pragma unroll
-    for (int c = 0; c < 8; ++c) { gl[c] = 0.0; gr[c] = 0.0; }
-  }
-  Flx F = num_flux<FLUX, RECON>(k, L, R, m.e_nx[e], m.e_ny[e], m.e_dx[e], m.e_dy[e], gl, gr);
-  const int ne = m.ne;
-  s.Fe[e] = F.m; s.Fe[ne + e] = F.x; s.Fe[2 * ne + e] = F.y; s.Fe[3 * ne + e] = F.e;
-}
-
 // Boundary-face inviscid fluxes (src/fv.cc:1100-1188): one thread per (face, vertex).
 template <int FLUX, int RECON>
 __global__ void k_bflux(Params k, MeshView m, StateView s, const int* __restrict__ done) {
@@ -194,7 +128,7 @@ __global__ void k_bflux(Params k, MeshView m, StateView s, const int* __restrict
   Flx F;
   if (kind == BC_FARFIELD) {
     double z[8] = {0, 0, 0, 0, 0, 0, 0, 0};
-    F = num_flux<FLUX, RECON>(k, s0, s1, nx, ny, 0.0, 0.0, z, z);
+    F = num_flux<FLUX, RECON>(k, make_vrec<FLUX>(k, s0), make_vrec<FLUX>(k, s1), nx, ny, 0.0, 0.0, z, z);
   } else {
     F = inviscid_bflux(k, s0, s1, nx, ny);
   }
@@ -271,35 +205,6 @@ __global__ void k_viscous(Params k, MeshView m, StateView s, const int* __restri
     Flx F = viscous_apply(K, nbx, nby);
     s.Fvb[d] = F.x; s.Fvb[m.nb + d] = F.y; s.Fvb[2 * m.nb + d] = F.e - Cor;
   }
-}
-
-// Residual assembly: fixed-order gather of every contribution to a vertex.
-__global__ void k_assemble(MeshView m, StateView s, int viscous, const int* __restrict__ done) {
-  if (*done) return;
-  int v = blockIdx.x * blockDim.x + threadIdx.x;
-  if (v >= m.nv) return;
-  const int ne = m.ne;
-  double r0 = 0.0, r1 = 0.0, r2 = 0.0, r3 = 0.0;
-  for (int j = m.ce_off[v]; j < m.ce_off[v + 1]; ++j) {
-    int ent = m.ce_ent[j];
-    int e = ent >> 1;
-    double sg = (ent & 1) ? -1.0 : 1.0;
-    r0 += s.Fe[e] * sg; r1 += s.Fe[ne + e] * sg; r2 += s.Fe[2 * ne + e] * sg; r3 += s.Fe[3 * ne + e] * sg;
-  }
-  const int n2 = 2 * m.nb, n3 = 3 * m.nvu;
-  for (int j = m.cb_off[v]; j < m.cb_off[v + 1]; ++j) {
-    int ent = m.cb_ent[j];
-    int type = ent & 3, idx = ent >> 2;
-    if (type == 0) {
-      r0 += s.Fb[idx] * 0.5; r1 += s.Fb[n2 + idx] * 0.5; r2 += s.Fb[2 * n2 + idx] * 0.5; r3 += s.Fb[3 * n2 + idx] * 0.5;
-    } else if (type == 2 && viscous) {
-      r1 += s.Fv[idx] * -(0.5 * 1.0); r2 += s.Fv[n3 + idx] * -(0.5 * 1.0); r3 += s.Fv[2 * n3 + idx] * -(0.5 * 1.0);
-    } else if (type == 3 && viscous) {
-      r1 += s.Fvb[idx] * 0.5; r2 += s.Fvb[m.nb + idx] * 0.5; r3 += s.Fvb[2 * m.nb + idx] * 0.5;
-    }
-  }
-  const int nv = m.nv;
-  s.R[v] = r0; s.R[nv + v] = r1; s.R[2 * nv + v] = r2; s.R[3 * nv + v] = r3;
 }
 
 __device__ __forceinline__ unsigned long long warp_min_u64(unsigned long long x) {

@@ -324,4 +324,96 @@ std::string build_layout(const tg_mesh& m, const tg_bc_table* bc, bool need_visc
   return "";
 }
 
+std::string build_tiles(HostLayout& L, int max_owned, int max_local, int max_edges) {
+  const int nv = L.nv;
+  if (max_owned <= 0 || max_local > 65535 || max_edges > 32767) return "bad tile limits";
+  L.t_vbeg.clear(); L.t_loff.assign(1, 0); L.t_eoff.assign(1, 0); L.lv.clear();
+  L.te_ab.clear(); L.te_nx.clear(); L.te_ny.clear();
+  L.te_g0x.clear(); L.te_g0y.clear(); L.te_g1x.clear(); L.te_g1y.clear();
+  L.te_ux.clear(); L.te_uy.clear(); L.te_ar.clear();
+  L.cv_off.assign(nv + 1, 0);
+  L.cv_ent.clear();
+  L.lmax = L.emax = L.tmax = 0;
+  // scratch maps global id -> tile-local id, reset per tile
+  std::vector<int> vloc(nv, -1), eloc(L.ne, -1);
+  std::vector<int> tv, te;  // current tile's local vertices / edges (global ids)
+  int v = 0;
+  while (v < nv) {
+    int vb = v;
+    tv.clear();
+    te.clear();
+    // greedily add owned vertices while the neighbourhood fits
+    int nown = 0;
+    while (v < nv && nown < max_owned) {
+      // tentative: count new edges and new local vertices of vertex v
+      int add_e = 0, add_v = (vloc[v] < 0) ? 1 : 0;
+      std::vector<int> new_halo;
+      for (int j = L.ce_off[v]; j < L.ce_off[v + 1]; ++j) {
+        int e = L.ce_ent[j] >> 1;
+        if (eloc[e] >= 0) continue;
+        ++add_e;
+        for (int x : {L.e_a[e], L.e_b[e]})
+          if (vloc[x] < 0 && x != v) {
+            bool seen = false;
+            for (int y : new_halo) seen |= (y == x);
+            if (!seen) { new_halo.push_back(x); ++add_v; }
+          }
+      }
+      if (nown > 0 && ((int)tv.size() + add_v > max_local || (int)te.size() + add_e > max_edges)) break;
+      // commit: owned vertices must occupy local ids 0..nown-1, so an owned
+      // vertex that is already a halo entry of this tile is moved to the front later
+      if (vloc[v] < 0) { vloc[v] = (int)tv.size(); tv.push_back(v); }
+      for (int j = L.ce_off[v]; j < L.ce_off[v + 1]; ++j) {
+        int e = L.ce_ent[j] >> 1;
+        if (eloc[e] >= 0) continue;
+        eloc[e] = (int)te.size();
+        te.push_back(e);
+        for (int x : {L.e_a[e], L.e_b[e]})
+          if (vloc[x] < 0) { vloc[x] = (int)tv.size(); tv.push_back(x); }
+      }
+      ++nown;
+      ++v;
+    }
+    // reorder local vertices: owned [vb, v) first, in order, then the halo in first-seen order
+    std::vector<int> order;
+    order.reserve(tv.size());
+    for (int x = vb; x < v; ++x) order.push_back(x);
+    for (int x : tv)
+      if (x < vb || x >= v) order.push_back(x);
+    for (size_t i = 0; i < order.size(); ++i) vloc[order[i]] = (int)i;
+    if ((int)order.size() > 65535 || (int)te.size() > 32767) return "tile neighbourhood too large";
+    L.t_vbeg.push_back(vb);
+    for (int x : order) L.lv.push_back(x);
+    L.t_loff.push_back((int)L.lv.size());
+    for (int e : te) {
+      L.te_ab.push_back((uint32_t)vloc[L.e_a[e]] | ((uint32_t)vloc[L.e_b[e]] << 16));
+      L.te_nx.push_back(L.e_nx[e]); L.te_ny.push_back(L.e_ny[e]);
+      L.te_g0x.push_back(L.e_g0x[e]); L.te_g0y.push_back(L.e_g0y[e]);
+      L.te_g1x.push_back(L.e_g1x[e]); L.te_g1y.push_back(L.e_g1y[e]);
+      // src/material.cc:69 area = normal.norm(); src/kepec.cc:18 unit = normal * (1/area)
+      double area = std::sqrt(L.e_nx[e] * L.e_nx[e] + L.e_ny[e] * L.e_ny[e] + 0.0 * 0.0);
+      double ia = 1.0 / area;
+      L.te_ux.push_back(L.e_nx[e] * ia);
+      L.te_uy.push_back(L.e_ny[e] * ia);
+      L.te_ar.push_back(area);
+    }
+    L.t_eoff.push_back((int)L.te_ab.size());
+    for (int x = vb; x < v; ++x) {
+      for (int j = L.ce_off[x]; j < L.ce_off[x + 1]; ++j) {
+        int ent = L.ce_ent[j];
+        L.cv_ent.push_back((uint16_t)((eloc[ent >> 1] << 1) | (ent & 1)));
+      }
+      L.cv_off[x + 1] = (int)L.cv_ent.size();
+    }
+    L.lmax = std::max(L.lmax, (int)order.size());
+    L.emax = std::max(L.emax, (int)te.size());
+    L.tmax = std::max(L.tmax, v - vb);
+    for (int x : order) vloc[x] = -1;
+    for (int e : te) eloc[e] = -1;
+  }
+  L.t_vbeg.push_back(nv);
+  L.ntiles = (int)L.t_vbeg.size() - 1;
+  return "";
+}
+
 }  // namespace tg

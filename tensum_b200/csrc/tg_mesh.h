@@ -52,9 +52,29 @@ struct HostLayout {
   std::vector<int> c_nbr_off, c_nbr;       // the cell's non-periodic boundary faces in cell.face slot order
   std::vector<double> bf_face_nx, bf_face_ny;  // face-list normal of the boundary face (slip in viscous BC states)
   std::vector<int> bf_face_v0, bf_face_v1;     // face-list vertex order of the boundary face
+
+  // ---- tiles: contiguous ranges of owned vertices with their edge neighbourhood
+  // Tile t owns vertices [t_vbeg[t], t_vbeg[t+1]).  Its local vertex table
+  // lv[t_loff[t] .. t_loff[t+1]) lists the owned vertices first, then every
+  // other endpoint of the tile's edges.  Its edge list (te_*, t_eoff) holds
+  // every edge incident to an owned vertex or to a periodic copy of one, with
+  // endpoints as local indices (la | lb << 16).  cv_off/cv_ent is the owned
+  // vertices' gather list in tile-local edge indices, (local_edge << 1) | side,
+  // in exactly the order of ce_ent, so the tiled kernels sum in the same order.
+  int ntiles = 0, lmax = 0, emax = 0, tmax = 0;
+  std::vector<int> t_vbeg, t_loff, t_eoff, lv;
+  std::vector<uint32_t> te_ab;
+  std::vector<double> te_nx, te_ny, te_g0x, te_g0y, te_g1x, te_g1y;
+  std::vector<double> te_ux, te_uy, te_ar;   // n/|n| and |n|, as Material::num_flux forms them
+  std::vector<int> cv_off;
+  std::vector<uint16_t> cv_ent;
 };
 
 // Returns "" on success, else an error message.
 std::string build_layout(const tg_mesh& m, const tg_bc_table* bc, bool need_viscous, HostLayout& out);
+
+// Splits the (already built) layout into tiles of at most max_owned owned
+// vertices, max_local local vertices and max_edges edges each.
+std::string build_tiles(HostLayout& L, int max_owned, int max_local, int max_edges);
 
 }  // namespace tg

@@ -28,6 +28,7 @@ enum : int { BC_NONE = 0, BC_SLIP = 1, BC_NOSLIP = 2, BC_FARFIELD = 3, BC_INLET 
 
 struct Params {
   double gamma, R, Cp, prandtl;
+  double sqrt_gm1, inv_gamma;   // sqrt(gamma - 1), 1/gamma
   double mu_ref, T0, Tref, omega;
   double ev_alpha, ev_beta, tvbM;
   double cfl;
@@ -51,9 +52,11 @@ __device__ __forceinline__ double logavg(double a, double b) {
   double u = f * f;
   double F;
   if (u < 1.0e-2) {
+    // the reference divides by 3, 5, 7; multiplying by the rounded reciprocals
+    // differs by at most an ulp per term and saves three FP64 divisions
     double u2 = u * u;
     double u3 = u2 * u;
-    F = 1.0 + u / 3.0 + u2 / 5.0 + u3 / 7.0;
+    F = 1.0 + u * (1.0 / 3.0) + u2 * (1.0 / 5.0) + u3 * (1.0 / 7.0);
   } else {
     F = log(xi) / 2.0 / f;
   }
@@ -153,18 +156,45 @@ __device__ __forceinline__ void reconstruct1(double l, double r, double gl, doub
 }
 
 // ------------------------------------------------------------------- fluxes
-// All take the raw dual normal (nx, ny) and return the flux per unit normal
-// length; the caller multiplies by |n| like Material::num_flux (src/material.cc:69-73).
+// Per-vertex quantities every flux reads.  The reference recomputes them for
+// each edge from the primitive state (Density, beta = 0.5/(R T), Entropy,
+// sound_speed ...); evaluating them once per vertex with the same expressions
+// gives the same values.
+struct VRec {
+  double rho;   // p / (R T)                                    src/material.h:596
+  double u, v, p;
+  double beta;  // 0.5 / (R T)                                  src/kepec.cc:23
+  double V1;    // (gamma - s)/(gamma - 1) - beta |u|^2, s = ln p - gamma ln rho   src/kepes_tecno_roe.cc:100-104
+  double a;     // sqrt(gamma R T)                              src/material.h:587
+  double b;     // sqrt(rho / p)                                src/roe_ec.cc:22
+};
 
-__device__ __forceinline__ Flx kepec_flux(const Params& k, const Prim& L, const Prim& R, double unx, double uny) {
+template <int FLUX>
+__device__ __forceinline__ VRec make_vrec(const Params& k, const Prim& q) {
+  VRec r;
+  r.rho = q.p / (k.R * q.T);
+  r.u = q.u;
+  r.v = q.v;
+  r.p = q.p;
+  r.beta = 0.5 / (k.R * q.T);
+  r.V1 = 0.0;
+  r.a = 0.0;
+  r.b = 0.0;
+  if (FLUX == FLUX_TECNO_ROE || FLUX == FLUX_TECNO_RUSANOV) {
+    double s = log(q.p) - k.gamma * log(r.rho);
+    r.V1 = (k.gamma - s) / (k.gamma - 1.0) - r.beta * (q.u * q.u + q.v * q.v);
+  }
+  if (FLUX == FLUX_TECNO_ROE || FLUX == FLUX_KEP) r.a = sqrt(k.gamma * k.R * q.T);
+  if (FLUX == FLUX_ROE_EC) r.b = sqrt(r.rho / q.p);
+  return r;
+}
+
+__device__ __forceinline__ Flx kepec_flux(const Params& k, const VRec& L, const VRec& R, double unx, double uny) {
   // src/kepec.cc:10-38
-  double rhol = density(k, L), rhor = density(k, R);
-  double rho = logavg(rhol, rhor);
+  double rho = logavg(L.rho, R.rho);
   double vel2 = 0.5 * ((L.u * L.u + L.v * L.v) + (R.u * R.u + R.v * R.v));
-  double betal = 0.5 / (k.R * L.T);
-  double betar = 0.5 / (k.R * R.T);
-  double beta = logavg(betal, betar);
-  double p = 0.5 * (rhol + rhor) / (betal + betar);
+  double beta = logavg(L.beta, R.beta);
+  double p = 0.5 * (L.rho + R.rho) / (L.beta + R.beta);
   double vx = L.u * 0.5 + R.u * 0.5, vy = L.v * 0.5 + R.v * 0.5;
   double vn = vx * unx + vy * uny;
   Flx F;
@@ -175,14 +205,12 @@ __device__ __forceinline__ Flx kepec_flux(const Params& k, const Prim& L, const 
   return F;
 }
 
-__device__ __forceinline__ Flx kep_flux(const Params& k, const Prim& L, const Prim& R, double unx, double uny) {
-  // src/kep.cc:10-38
-  double rhol = density(k, L), rhor = density(k, R);
-  double al = sound_speed(k, L), ar = sound_speed(k, R);
-  double Hl = al * al / (k.gamma - 1.0) + 0.5 * (L.u * L.u + L.v * L.v);
-  double Hr = ar * ar / (k.gamma - 1.0) + 0.5 * (R.u * R.u + R.v * R.v);
+__device__ __forceinline__ Flx kep_flux(const Params& k, const VRec& L, const VRec& R, double unx, double uny) {
+  // src/kep.cc:10-38 (pow(a, 2.0) is the square a*a)
+  double Hl = L.a * L.a / (k.gamma - 1.0) + 0.5 * (L.u * L.u + L.v * L.v);
+  double Hr = R.a * R.a / (k.gamma - 1.0) + 0.5 * (R.u * R.u + R.v * R.v);
   double p = 0.5 * (L.p + R.p);
-  double rho = 0.5 * (rhol + rhor);
+  double rho = 0.5 * (L.rho + R.rho);
   double H = 0.5 * (Hl + Hr);
   double vx = L.u * 0.5 + R.u * 0.5, vy = L.v * 0.5 + R.v * 0.5;
   double vn = vx * unx + vy * uny;
@@ -194,11 +222,10 @@ __device__ __forceinline__ Flx kep_flux(const Params& k, const Prim& L, const Pr
   return F;
 }
 
-__device__ __forceinline__ Flx roe_ec_flux(const Params& k, const Prim& L, const Prim& R, double unx, double uny) {
+__device__ __forceinline__ Flx roe_ec_flux(const Params& k, const VRec& L, const VRec& R, double unx, double uny) {
   // src/roe_ec.cc:10-44
-  double rhol = density(k, L), rhor = density(k, R);
   double pl = L.p, pr = R.p;
-  double bl = sqrt(rhol / pl), br = sqrt(rhor / pr);
+  double bl = L.b, br = R.b;
   double z1b = 0.5 * (bl + br);
   double zx = L.u * (0.5 * bl) + R.u * (0.5 * br);
   double zy = L.v * (0.5 * bl) + R.v * (0.5 * br);
@@ -215,13 +242,12 @@ __device__ __forceinline__ Flx roe_ec_flux(const Params& k, const Prim& L, const
   return F;
 }
 
-__device__ __forceinline__ Flx avg_flux(const Params& k, const Prim& L, const Prim& R, double unx, double uny) {
+__device__ __forceinline__ Flx avg_flux(const Params& k, const VRec& L, const VRec& R, double unx, double uny) {
   // src/simple_avg.cc:10-46
-  double rhol = density(k, L), rhor = density(k, R);
-  double El = 0.5 * rhol * (L.u * L.u + L.v * L.v) + L.p / (k.gamma - 1);
-  double Er = 0.5 * rhor * (R.u * R.u + R.v * R.v) + R.p / (k.gamma - 1);
+  double El = 0.5 * L.rho * (L.u * L.u + L.v * L.v) + L.p / (k.gamma - 1);
+  double Er = 0.5 * R.rho * (R.u * R.u + R.v * R.v) + R.p / (k.gamma - 1);
   double vnl = L.u * unx + L.v * uny, vnr = R.u * unx + R.v * uny;
-  double ml = rhol * vnl, mr = rhor * vnr;
+  double ml = L.rho * vnl, mr = R.rho * vnr;
   Flx F;
   F.m = 0.0 + ml * 0.5;
   F.m += mr * 0.5;
@@ -240,27 +266,32 @@ __device__ __forceinline__ Flx avg_flux(const Params& k, const Prim& L, const Pr
 // variable gradients (V1,V2,V3,V5) x (x,y) at the two vertices, (dx,dy) the
 // edge vector x_r - x_l.
 template <int ROE, int RECON>
-__device__ __forceinline__ Flx tecno_flux(const Params& k, const Prim& L, const Prim& Rp, double unx, double uny,
+__device__ __forceinline__ Flx tecno_flux(const Params& k, const VRec& L, const VRec& Rp, double unx, double uny,
                                           double dx, double dy, const double* dEl, const double* dEr) {
   const double g = k.gamma;
-  double rhol = density(k, L), rhor = density(k, Rp);
-  double rho = logavg(rhol, rhor);
-  double betal = 0.5 / (k.R * L.T);
-  double betar = 0.5 / (k.R * Rp.T);
-  double beta = logavg(betal, betar);
+  double rho = logavg(L.rho, Rp.rho);
+  double beta = logavg(L.beta, Rp.beta);
   double a = sqrt(0.5 * g / beta);
-  double p = 0.5 * (rhol + rhor) / (betal + betar);
+  double p = 0.5 * (L.rho + Rp.rho) / (L.beta + Rp.beta);
   double vx = L.u * 0.5 + Rp.u * 0.5, vy = L.v * 0.5 + Rp.v * 0.5;
   double vn = vx * unx + vy * uny;
-  Flx F = kepec_flux(k, L, Rp, unx, uny);
+  // central KEPEC part (src/kepec.cc:25-34) from the log means computed above
+  Flx F;
+  {
+    double vel2 = 0.5 * ((L.u * L.u + L.v * L.v) + (Rp.u * Rp.u + Rp.v * Rp.v));
+    F.m = rho * vn;
+    F.x = unx * p + vx * F.m;
+    F.y = uny * p + vy * F.m;
+    F.e = 0.5 * (1.0 / ((g - 1.0) * beta) - vel2) * F.m + (F.x * vx + F.y * vy);
+  }
   if (!k.nd) return F;
 
   double vsq = vx * vx + vy * vy;
   double H = a * a / (g - 1.0) + 0.5 * vsq;
   double v1 = vx * uny - vy * unx;
-  double const1 = sqrt(rho / g);
+  double const1 = sqrt(rho * k.inv_gamma);
   double psqrt = sqrt(p);
-  double S0 = sqrt(0.5) * const1, S1 = sqrt(g - 1.0) * const1, S2 = psqrt;
+  double S0 = sqrt(0.5) * const1, S1 = k.sqrt_gm1 * const1, S2 = psqrt;
   // scaled eigenvector matrix; rows = (mass, mx, my, energy), cols = waves (u-a, entropy, shear, u+a)
   double R[4][4] = {{1 * S0, 1 * S1, 0 * S2, 1 * S0},
                     {(vx - a * unx) * S0, vx * S1, uny * S2, (vx + a * unx) * S0},
@@ -269,21 +300,18 @@ __device__ __forceinline__ Flx tecno_flux(const Params& k, const Prim& L, const 
   double Lam[4];
   if (ROE) {
     double vnl = L.u * unx + L.v * uny, vnr = Rp.u * unx + Rp.v * uny;
-    double al = sound_speed(k, L), ar = sound_speed(k, Rp);
     double l2 = fabs(vn);
-    Lam[0] = (1 + k.ev_beta) * fabs(vn - a) + k.ev_alpha * fabs((vnl - al) - (vnr - ar));
+    Lam[0] = (1 + k.ev_beta) * fabs(vn - a) + k.ev_alpha * fabs((vnl - L.a) - (vnr - Rp.a));
     Lam[1] = l2;
     Lam[2] = l2;
-    Lam[3] = (1 + k.ev_beta) * fabs(vn + a) + k.ev_alpha * fabs((vnl + al) - (vnr + ar));
+    Lam[3] = (1 + k.ev_beta) * fabs(vn + a) + k.ev_alpha * fabs((vnl + L.a) - (vnr + Rp.a));
   } else {
     double lr = fabs(vn) + fabs(a);
     Lam[0] = Lam[1] = Lam[2] = Lam[3] = lr;
   }
-  double sl = entropy_fn(k, L), sr = entropy_fn(k, Rp);
-  double Vl[4] = {(g - sl) / (g - 1.0) - betal * (L.u * L.u + L.v * L.v), 2 * L.u * betal, 2 * L.v * betal, -2 * betal};
-  double Vr[4] = {(g - sr) / (g - 1.0) - betar * (Rp.u * Rp.u + Rp.v * Rp.v), 2 * Rp.u * betar, 2 * Rp.v * betar,
-                  -2 * betar};
-  double h = sqrt(dx * dx + dy * dy);
+  double Vl[4] = {L.V1, 2 * L.u * L.beta, 2 * L.v * L.beta, -2 * L.beta};
+  double Vr[4] = {Rp.V1, 2 * Rp.u * Rp.beta, 2 * Rp.v * Rp.beta, -2 * Rp.beta};
+  double h = (RECON == RECON_TVB_MINMOD) ? sqrt(dx * dx + dy * dy) : 0.0;
   double gl[4], gr[4];
 #pragma unroll
   for (int i = 0; i < 4; ++i) {
@@ -320,13 +348,11 @@ __device__ __forceinline__ Flx tecno_flux(const Params& k, const Prim& L, const 
   return F;
 }
 
-// Material::num_flux (src/material.cc:27-74): flux times |n|.
+// Material::num_flux (src/material.cc:27-74) given the unit normal and |n|
+// (area = |n|, unit normal = n * (1/area), as the fluxes compute them).
 template <int FLUX, int RECON>
-__device__ __forceinline__ Flx num_flux(const Params& k, const Prim& L, const Prim& R, double nx, double ny, double dx,
-                                        double dy, const double* dEl, const double* dEr) {
-  double area = sqrt(nx * nx + ny * ny);
-  double ia = 1.0 / area;
-  double unx = nx * ia, uny = ny * ia;
+__device__ __forceinline__ Flx num_flux_unit(const Params& k, const VRec& L, const VRec& R, double unx, double uny,
+                                             double area, double dx, double dy, const double* dEl, const double* dEr) {
   Flx F;
   if (FLUX == FLUX_TECNO_ROE) F = tecno_flux<1, RECON>(k, L, R, unx, uny, dx, dy, dEl, dEr);
   else if (FLUX == FLUX_TECNO_RUSANOV) F = tecno_flux<0, RECON>(k, L, R, unx, uny, dx, dy, dEl, dEr);
@@ -336,6 +362,14 @@ __device__ __forceinline__ Flx num_flux(const Params& k, const Prim& L, const Pr
   else F = avg_flux(k, L, R, unx, uny);
   F.m *= area; F.x *= area; F.y *= area; F.e *= area;
   return F;
+}
+
+template <int FLUX, int RECON>
+__device__ __forceinline__ Flx num_flux(const Params& k, const VRec& L, const VRec& R, double nx, double ny, double dx,
+                                        double dy, const double* dEl, const double* dEr) {
+  double area = sqrt(nx * nx + ny * ny);
+  double ia = 1.0 / area;
+  return num_flux_unit<FLUX, RECON>(k, L, R, nx * ia, ny * ia, area, dx, dy, dEl, dEr);
 }
 
 // Material::inviscid_bflux (src/material.cc:110-127).
