@@ -180,7 +180,8 @@ def run_case(mesh, cfg: dict, prim0: np.ndarray | None, n_steps: int, n_dump: in
     own = workdir is None
     wd = workdir or tempfile.mkdtemp(prefix="tensum_ref_")
     try:
-        write_part_file(mesh, wd)
+        if own or not os.path.exists(os.path.join(wd, "PARTITION", "part_file_0.dat")):
+            write_part_file(mesh, wd)
         with open(os.path.join(wd, "param.in"), "w") as fh:
             fh.write(param_text(cfg))
         ic = "-"

@@ -104,7 +104,7 @@ inline int nblk(int n) { return (n + kBlock - 1) / kBlock; }
 // ---- kernel dispatch over (flux, reconstruction)
 typedef void (*BfluxKernel)(Params, MeshView, StateView, const int*);
 typedef void (*TileFluxKernel)(Params, MeshView, TileView, StateView, Control, Scalars*, int, int, double*, double*,
-                               const int*);
+                               int, int, const int*);
 
 template <int F>
 BfluxKernel pick_bflux(int recon) {
@@ -152,6 +152,28 @@ TileFluxKernel tile_kernel_m(int flux, int recon) {
     default: return k_tile_flux<FLUX_AVG, RECON_FIRST, M>;
   }
 }
+size_t flux_smem(int flux, int recon, int lmax, int emax, int cmax) {
+  const bool grad = recon != RECON_FIRST;
+  switch (flux) {
+    case FLUX_TECNO_ROE:
+      return grad ? tile_flux_smem_t<FLUX_TECNO_ROE, RECON_TVD_MINMOD>(lmax, emax, cmax)
+                  : tile_flux_smem_t<FLUX_TECNO_ROE, RECON_FIRST>(lmax, emax, cmax);
+    case FLUX_TECNO_RUSANOV:
+      return grad ? tile_flux_smem_t<FLUX_TECNO_RUSANOV, RECON_TVD_MINMOD>(lmax, emax, cmax)
+                  : tile_flux_smem_t<FLUX_TECNO_RUSANOV, RECON_FIRST>(lmax, emax, cmax);
+    case FLUX_KEPEC: return tile_flux_smem_t<FLUX_KEPEC, RECON_FIRST>(lmax, emax, cmax);
+    case FLUX_KEP: return tile_flux_smem_t<FLUX_KEP, RECON_FIRST>(lmax, emax, cmax);
+    case FLUX_ROE_EC: return tile_flux_smem_t<FLUX_ROE_EC, RECON_FIRST>(lmax, emax, cmax);
+    default: return tile_flux_smem_t<FLUX_AVG, RECON_FIRST>(lmax, emax, cmax);
+  }
+}
+
+typedef void (*TileGradKernel)(Params, MeshView, TileView, StateView, Scalars*, int, int, const int*);
+TileGradKernel grad_kernel(bool first, bool grad) {
+  if (first) return grad ? k_tile_grad<true, true> : k_tile_grad<true, false>;
+  return k_tile_grad<false, true>;
+}
+
 TileFluxKernel tile_kernel(int flux, int recon, int mode) {
   return mode == MODE_UPDATE ? tile_kernel_m<MODE_UPDATE>(flux, recon) : tile_kernel_m<MODE_RESIDUAL>(flux, recon);
 }
@@ -165,13 +187,11 @@ StateView view(const tg_handle* h, int b) {
 }
 
 // ---- phases (all enqueue on h->stream; `done` gates work inside graphs)
-void enqueue_gradient(tg_handle* h, int b, bool first, const int* done) {
-  if (first)
-    k_tile_grad<true><<<h->L.ntiles, kTileThreads, h->smem_grad1, h->stream>>>(h->prm, h->mv, h->tv, view(h, b), h->sc,
-                                                                              done);
-  else
-    k_tile_grad<false><<<h->L.ntiles, kTileThreads, h->smem_grad0, h->stream>>>(h->prm, h->mv, h->tv, view(h, b),
-                                                                               h->sc, done);
+// Gradients (when `grad`), plus at the first stage dt and U_old.
+void enqueue_gradient(tg_handle* h, int b, bool first, bool grad, const int* done) {
+  if (!first && !grad) return;
+  grad_kernel(first, grad)<<<h->L.ntiles, kTileThreads, first ? h->smem_grad1 : h->smem_grad0, h->stream>>>(
+      h->prm, h->mv, h->tv, view(h, b), h->sc, h->L.lmax, h->L.emax, done);
 }
 
 // boundary-face and viscous contributions, gathered by the tiled flux kernel
@@ -184,7 +204,8 @@ void enqueue_boundary(tg_handle* h, int b, const int* done) {
 
 void enqueue_tile_flux(tg_handle* h, int b, int mode, int r, bool norm, int bout, const int* done) {
   tile_kernel(h->prm.flux, h->prm.recon, mode)<<<h->L.ntiles, kTileThreads, h->smem_flux, h->stream>>>(
-      h->prm, h->mv, h->tv, view(h, b), h->ctl, h->sc, r, norm ? 1 : 0, h->Pb[bout], h->Wb[bout], done);
+      h->prm, h->mv, h->tv, view(h, b), h->ctl, h->sc, r, norm ? 1 : 0, h->Pb[bout], h->Wb[bout], h->L.lmax,
+      h->L.emax, done);
 }
 
 int residual_kernels(const tg_handle* h) {
@@ -193,7 +214,7 @@ int residual_kernels(const tg_handle* h) {
 
 // compute_residual on buffer 0 (gradient, boundary/viscous terms, tiled fluxes -> R)
 void enqueue_residual(tg_handle* h, const int* done) {
-  enqueue_gradient(h, 0, false, done);
+  enqueue_gradient(h, 0, false, true, done);
   enqueue_boundary(h, 0, done);
   enqueue_tile_flux(h, 0, MODE_RESIDUAL, 0, false, 0, done);
 }
@@ -220,9 +241,9 @@ void enqueue_step(tg_handle* h) {
     const bool first = (r == 0), last = (r == 2);
     if (first && h->ctl.time_step > 0.0) {
       k_store_old<<<nblk(h->mv.nv), kBlock, 0, h->stream>>>(h->prm, h->mv, view(h, 0), h->done);
-      enqueue_gradient(h, r, false, h->done);
+      enqueue_gradient(h, r, false, h->grads_needed, h->done);
     } else {
-      enqueue_gradient(h, r, first, h->done);   // first stage: + dt, U_old
+      enqueue_gradient(h, r, first, h->grads_needed, h->done);   // first stage: + dt, U_old
     }
     if (first) k_dt_final<<<1, 1, 0, h->stream>>>(h->ctl, h->sc, h->done);
     enqueue_boundary(h, r, h->done);
@@ -265,7 +286,7 @@ tg_status capture_step_graph(tg_handle* h) {
 
 void enqueue_phase(tg_handle* h, int phase) {
   switch (phase) {
-    case TG_PHASE_GRADIENT: enqueue_gradient(h, 0, false, h->never); break;
+    case TG_PHASE_GRADIENT: enqueue_gradient(h, 0, false, true, h->never); break;
     case TG_PHASE_FLUX:
       enqueue_boundary(h, 0, h->never);
       enqueue_tile_flux(h, 0, MODE_RESIDUAL, 0, false, 0, h->never);
@@ -311,7 +332,7 @@ tg_status tg_create(const tg_mesh* mesh, const tg_material* mat, const tg_bc_tab
     delete h;
     return fail(nullptr, TG_INVALID_ARG, msg);
   }
-  msg = build_tiles(h->L, kTileThreads, 448, 1152);
+  msg = build_tiles(h->L, TG_TILE_OWNED, TG_TILE_LCAP, TG_TILE_ECAP);
   if (!msg.empty()) {
     delete h;
     return fail(nullptr, TG_INVALID_ARG, msg);
@@ -324,6 +345,7 @@ tg_status tg_create(const tg_mesh* mesh, const tg_material* mat, const tg_bc_tab
   k.gamma = mat->gamma; k.R = mat->gas_const; k.Cp = mat->gamma * mat->gas_const / (mat->gamma - 1.0);
   k.sqrt_gm1 = std::sqrt(mat->gamma - 1.0);
   k.inv_gamma = 1.0 / mat->gamma;
+  k.inv_gm1 = 1.0 / (mat->gamma - 1.0);
   k.prandtl = mat->prandtl; k.mu_ref = mat->mu_ref; k.T0 = mat->T_0; k.Tref = mat->T_ref; k.omega = mat->omega;
   k.ev_alpha = mat->ev_mod_alpha; k.ev_beta = mat->ev_mod_beta; k.tvbM = mat->tvb_minmod_coef; k.cfl = opt->cfl;
   k.model = mat->model; k.flux = mat->flux_scheme; k.mu_model = mat->mu_model; k.recon = mat->reconstruct_scheme;
@@ -363,17 +385,21 @@ tg_status tg_create(const tg_mesh* mesh, const tg_material* mat, const tg_bc_tab
     if ((st = dev_alloc(h, 4 * nv, &h->Pb[b])) != TG_OK) { tg_destroy(h); return st; }
     if ((st = dev_alloc(h, 4 * nv, &h->Wb[b])) != TG_OK) { tg_destroy(h); return st; }
   }
-  h->smem_grad0 = tile_grad_smem(L.lmax, false);
-  h->smem_grad1 = tile_grad_smem(L.lmax, true);
-  h->smem_flux = tile_flux_smem(L.lmax, L.emax);
+  h->smem_grad0 = tile_grad_smem(L.lmax, L.emax, L.cmax, false);
+  h->smem_grad1 = tile_grad_smem(L.lmax, L.emax, L.cmax, true);
+  h->smem_flux = flux_smem(mat->flux_scheme, mat->reconstruct_scheme, L.lmax, L.emax, L.cmax);
   {
-    cudaError_t ea = cudaFuncSetAttribute(k_tile_grad<true>, cudaFuncAttributeMaxDynamicSharedMemorySize, (int)h->smem_grad1);
-    cudaError_t eb = cudaFuncSetAttribute(k_tile_grad<false>, cudaFuncAttributeMaxDynamicSharedMemorySize, (int)h->smem_grad0);
+    cudaError_t ea = cudaFuncSetAttribute(grad_kernel(true, true), cudaFuncAttributeMaxDynamicSharedMemorySize,
+                                          (int)h->smem_grad1);
+    cudaError_t ea2 = cudaFuncSetAttribute(grad_kernel(true, false), cudaFuncAttributeMaxDynamicSharedMemorySize,
+                                           (int)h->smem_grad1);
+    cudaError_t eb = cudaFuncSetAttribute(grad_kernel(false, true), cudaFuncAttributeMaxDynamicSharedMemorySize,
+                                          (int)h->smem_grad0);
     cudaError_t ec = cudaFuncSetAttribute(tile_kernel(mat->flux_scheme, mat->reconstruct_scheme, MODE_UPDATE),
                                           cudaFuncAttributeMaxDynamicSharedMemorySize, (int)h->smem_flux);
     cudaError_t ed = cudaFuncSetAttribute(tile_kernel(mat->flux_scheme, mat->reconstruct_scheme, MODE_RESIDUAL),
                                           cudaFuncAttributeMaxDynamicSharedMemorySize, (int)h->smem_flux);
-    if (ea != cudaSuccess || eb != cudaSuccess || ec != cudaSuccess || ed != cudaSuccess) {
+    if (ea != cudaSuccess || ea2 != cudaSuccess || eb != cudaSuccess || ec != cudaSuccess || ed != cudaSuccess) {
       tg_destroy(h);
       return fail(nullptr, TG_CUDA_ERROR, "tile kernels need more shared memory than the device allows");
     }
@@ -397,7 +423,10 @@ tg_status tg_create(const tg_mesh* mesh, const tg_material* mat, const tg_bc_tab
   c.min_residue = opt->min_residue; c.max_iter = opt->max_iter; c.final_time = opt->final_time; c.tinst = tip;
 
   h->kernels_per_flux = residual_kernels(h);
-  h->kernels_per_step = 1 + 3 * (1 + residual_kernels(h)) + (c.time_step > 0.0 ? 1 : 0) + 1 + 1 + 1;
+  // step_begin + gradient/dt passes + per stage (boundary, viscous, tiled flux) + [store_old] + dt_final
+  // + norm_final + step_end
+  h->kernels_per_step = 1 + (1 + (h->grads_needed ? 2 : 0)) + 3 * residual_kernels(h) + (c.time_step > 0.0 ? 1 : 0) +
+                        1 + 1 + 1;
   {
     cudaError_t ep = cudaMallocHost((void**)&h->hP, 4 * nv * sizeof(double));
     if (ep != cudaSuccess) { tg_destroy(h); return fail(nullptr, TG_CUDA_ERROR, cudaGetErrorString(ep)); }
@@ -508,7 +537,7 @@ static tg_status copy_grad_out(tg_handle* h, double* dE_out) {
 
 tg_status tg_gradients(tg_handle* h, double* dE_out) {
   if (!h) return fail(h, TG_INVALID_ARG, "NULL handle");
-  enqueue_gradient(h, 0, false, h->never);
+  enqueue_gradient(h, 0, false, true, h->never);
   tg_status st = sync(h);
   if (st != TG_OK || !dE_out) return st;
   return copy_grad_out(h, dE_out);

@@ -333,7 +333,7 @@ std::string build_tiles(HostLayout& L, int max_owned, int max_local, int max_edg
   L.te_ux.clear(); L.te_uy.clear(); L.te_ar.clear();
   L.cv_off.assign(nv + 1, 0);
   L.cv_ent.clear();
-  L.lmax = L.emax = L.tmax = 0;
+  L.lmax = L.emax = L.tmax = L.cmax = 0;
   // scratch maps global id -> tile-local id, reset per tile
   std::vector<int> vloc(nv, -1), eloc(L.ne, -1);
   std::vector<int> tv, te;  // current tile's local vertices / edges (global ids)
@@ -405,6 +405,7 @@ std::string build_tiles(HostLayout& L, int max_owned, int max_local, int max_edg
       }
       L.cv_off[x + 1] = (int)L.cv_ent.size();
     }
+    L.cmax = std::max(L.cmax, L.cv_off[v] - L.cv_off[vb] + 1);   // +1: staging starts on an even entry
     L.lmax = std::max(L.lmax, (int)order.size());
     L.emax = std::max(L.emax, (int)te.size());
     L.tmax = std::max(L.tmax, v - vb);
@@ -413,6 +414,7 @@ std::string build_tiles(HostLayout& L, int max_owned, int max_local, int max_edg
   }
   L.t_vbeg.push_back(nv);
   L.ntiles = (int)L.t_vbeg.size() - 1;
+  if (L.cv_ent.size() & 1) L.cv_ent.push_back(0);   // the lists are staged in whole 4-byte words
   return "";
 }
 

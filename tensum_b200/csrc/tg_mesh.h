@@ -61,7 +61,7 @@ struct HostLayout {
   // endpoints as local indices (la | lb << 16).  cv_off/cv_ent is the owned
   // vertices' gather list in tile-local edge indices, (local_edge << 1) | side,
   // in exactly the order of ce_ent, so the tiled kernels sum in the same order.
-  int ntiles = 0, lmax = 0, emax = 0, tmax = 0;
+  int ntiles = 0, lmax = 0, emax = 0, tmax = 0, cmax = 0;  // cmax: gather entries per tile
   std::vector<int> t_vbeg, t_loff, t_eoff, lv;
   std::vector<uint32_t> te_ab;
   std::vector<double> te_nx, te_ny, te_g0x, te_g0y, te_g1x, te_g1y;

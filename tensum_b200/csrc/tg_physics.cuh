@@ -28,7 +28,7 @@ enum : int { BC_NONE = 0, BC_SLIP = 1, BC_NOSLIP = 2, BC_FARFIELD = 3, BC_INLET 
 
 struct Params {
   double gamma, R, Cp, prandtl;
-  double sqrt_gm1, inv_gamma;   // sqrt(gamma - 1), 1/gamma
+  double sqrt_gm1, inv_gamma, inv_gm1;   // sqrt(gamma - 1), 1/gamma, 1/(gamma - 1)
   double mu_ref, T0, Tref, omega;
   double ev_alpha, ev_beta, tvbM;
   double cfl;
@@ -45,23 +45,25 @@ struct Flx { double m, x, y, e; };
 __device__ __forceinline__ double dmin_(double a, double b) { return (b < a) ? b : a; }  // std::min
 __device__ __forceinline__ double dmax_(double a, double b) { return (a < b) ? b : a; }  // std::max
 
-// src/material.h:24-42
-__device__ __forceinline__ double logavg(double a, double b) {
-  double xi = b / a;
-  double f = (xi - 1.0) / (xi + 1.0);
+// Ismail-Roe logarithmic mean (a - b)/ln(a/b), src/material.h:24-42: returns
+// F with logmean = 0.5 (a + b) / F.  The reference forms f = (xi - 1)/(xi + 1)
+// from xi = b/a; f = (b - a)/(b + a) is the same quantity with one division
+// instead of two (and no cancellation in xi - 1), and the series divides by
+// 3, 5, 7 where multiplying by the reciprocals differs by at most an ulp.
+__device__ __forceinline__ double logavg_F(double a, double b) {
+  double f = (b - a) / (b + a);
   double u = f * f;
-  double F;
   if (u < 1.0e-2) {
-    // the reference divides by 3, 5, 7; multiplying by the rounded reciprocals
-    // differs by at most an ulp per term and saves three FP64 divisions
     double u2 = u * u;
     double u3 = u2 * u;
-    F = 1.0 + u * (1.0 / 3.0) + u2 * (1.0 / 5.0) + u3 * (1.0 / 7.0);
-  } else {
-    F = log(xi) / 2.0 / f;
+    return 1.0 + u * (1.0 / 3.0) + u2 * (1.0 / 5.0) + u3 * (1.0 / 7.0);
   }
-  return 0.5 * (a + b) / F;
+  return log(b / a) / 2.0 / f;
 }
+
+__device__ __forceinline__ double logavg(double a, double b) { return 0.5 * (a + b) / logavg_F(a, b); }
+// 1 / logavg(a, b), for the callers that only ever divide by the log mean
+__device__ __forceinline__ double inv_logavg(double a, double b) { return logavg_F(a, b) / (0.5 * (a + b)); }
 
 __device__ __forceinline__ double density(const Params& k, const Prim& q) { return q.p / (k.R * q.T); }
 __device__ __forceinline__ double sound_speed(const Params& k, const Prim& q) { return sqrt(k.gamma * k.R * q.T); }
@@ -130,6 +132,24 @@ __device__ __forceinline__ double limited_slope(double ul, double ur, double h, 
   }
 }
 
+// Jump Z_ji - Z_ij of Material::reconstruct (src/reconstruct.cc:139-188) for
+// one component, from the first-order jump d = Z_r - Z_l and the slopes.
+template <int RECON>
+__device__ __forceinline__ double reconstructed_jump(double d, double gl, double gr, double h, double M) {
+  if (RECON == RECON_FIRST) {
+    return d;
+  } else if (RECON == RECON_SECOND) {
+    return d - 0.5 * gr - 0.5 * gl;
+  } else if (RECON == RECON_SECOND_MUSCL) {
+    const double K = 1.0 / 3.0;
+    double sl = ((2.0 * gl - d) * (1.0 - K) + d * (1.0 + K)) * 0.25;
+    double sr = ((2.0 * gr - d) * (1.0 - K) + d * (1.0 + K)) * 0.25;
+    return d - sr - sl;
+  } else {
+    return d - limited_slope<RECON>(2.0 * gr - d, d, h, M) - limited_slope<RECON>(2.0 * gl - d, d, h, M);
+  }
+}
+
 // Material::reconstruct (src/reconstruct.cc:139-188) for one component.
 template <int RECON>
 __device__ __forceinline__ void reconstruct1(double l, double r, double gl, double gr, double h, double M,
@@ -190,10 +210,10 @@ __device__ __forceinline__ VRec make_vrec(const Params& k, const Prim& q) {
 }
 
 __device__ __forceinline__ Flx kepec_flux(const Params& k, const VRec& L, const VRec& R, double unx, double uny) {
-  // src/kepec.cc:10-38
+  // src/kepec.cc:10-38; 1/((gamma-1) beta_ln) is formed from 1/beta_ln directly
   double rho = logavg(L.rho, R.rho);
   double vel2 = 0.5 * ((L.u * L.u + L.v * L.v) + (R.u * R.u + R.v * R.v));
-  double beta = logavg(L.beta, R.beta);
+  double ibeta = inv_logavg(L.beta, R.beta);
   double p = 0.5 * (L.rho + R.rho) / (L.beta + R.beta);
   double vx = L.u * 0.5 + R.u * 0.5, vy = L.v * 0.5 + R.v * 0.5;
   double vn = vx * unx + vy * uny;
@@ -201,7 +221,7 @@ __device__ __forceinline__ Flx kepec_flux(const Params& k, const VRec& L, const 
   F.m = rho * vn;
   F.x = unx * p + vx * F.m;
   F.y = uny * p + vy * F.m;
-  F.e = 0.5 * (1.0 / ((k.gamma - 1.0) * beta) - vel2) * F.m + (F.x * vx + F.y * vy);
+  F.e = 0.5 * (ibeta * k.inv_gm1 - vel2) * F.m + (F.x * vx + F.y * vy);
   return F;
 }
 
@@ -270,8 +290,8 @@ __device__ __forceinline__ Flx tecno_flux(const Params& k, const VRec& L, const 
                                           double dx, double dy, const double* dEl, const double* dEr) {
   const double g = k.gamma;
   double rho = logavg(L.rho, Rp.rho);
-  double beta = logavg(L.beta, Rp.beta);
-  double a = sqrt(0.5 * g / beta);
+  double ibeta = inv_logavg(L.beta, Rp.beta);    // 1 / beta_ln
+  double a = sqrt(0.5 * g * ibeta);
   double p = 0.5 * (L.rho + Rp.rho) / (L.beta + Rp.beta);
   double vx = L.u * 0.5 + Rp.u * 0.5, vy = L.v * 0.5 + Rp.v * 0.5;
   double vn = vx * unx + vy * uny;
@@ -282,7 +302,7 @@ __device__ __forceinline__ Flx tecno_flux(const Params& k, const VRec& L, const 
     F.m = rho * vn;
     F.x = unx * p + vx * F.m;
     F.y = uny * p + vy * F.m;
-    F.e = 0.5 * (1.0 / ((g - 1.0) * beta) - vel2) * F.m + (F.x * vx + F.y * vy);
+    F.e = 0.5 * (ibeta * k.inv_gm1 - vel2) * F.m + (F.x * vx + F.y * vy);
   }
   if (!k.nd) return F;
 
@@ -309,8 +329,10 @@ __device__ __forceinline__ Flx tecno_flux(const Params& k, const VRec& L, const 
     double lr = fabs(vn) + fabs(a);
     Lam[0] = Lam[1] = Lam[2] = Lam[3] = lr;
   }
-  double Vl[4] = {L.V1, 2 * L.u * L.beta, 2 * L.v * L.beta, -2 * L.beta};
-  double Vr[4] = {Rp.V1, 2 * Rp.u * Rp.beta, 2 * Rp.v * Rp.beta, -2 * Rp.beta};
+  // Every reconstruction reads Z_l, Z_r only through Z_r - Z_l (src/reconstruct.cc:31-96),
+  // so the jump is formed as R^T (V_r - V_l) with one product instead of two.
+  double dV[4] = {Rp.V1 - L.V1, 2 * Rp.u * Rp.beta - 2 * L.u * L.beta, 2 * Rp.v * Rp.beta - 2 * L.v * L.beta,
+                  -2 * Rp.beta - -2 * L.beta};
   double h = (RECON == RECON_TVB_MINMOD) ? sqrt(dx * dx + dy * dy) : 0.0;
   double gl[4], gr[4];
 #pragma unroll
@@ -321,17 +343,14 @@ __device__ __forceinline__ Flx tecno_flux(const Params& k, const VRec& L, const 
   double dZ[4];
 #pragma unroll
   for (int i = 0; i < 4; ++i) {
-    double Zl = 0.0, Zr = 0.0, sgl = 0.0, sgr = 0.0;
+    double d = 0.0, sgl = 0.0, sgr = 0.0;
 #pragma unroll
     for (int j = 0; j < 4; ++j) {
-      Zl += R[j][i] * Vl[j];
-      Zr += R[j][i] * Vr[j];
+      d += R[j][i] * dV[j];
       sgl += R[j][i] * gl[j];
       sgr += R[j][i] * gr[j];
     }
-    double zij, zji;
-    reconstruct1<RECON>(Zl, Zr, sgl, sgr, h, k.tvbM, zij, zji);
-    dZ[i] = zji - zij;
+    dZ[i] = reconstructed_jump<RECON>(d, sgl, sgr, h, k.tvbM);
   }
   double Diff[4];
 #pragma unroll

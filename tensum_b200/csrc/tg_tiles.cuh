@@ -2,12 +2,17 @@
 //
 // A tile is a contiguous range of owned vertices (Hilbert order) plus every
 // vertex one edge away (periodic copies' neighbourhoods included).  One CTA
-// per tile stages the tile's vertex data in shared memory once, so that
+// per tile stages everything the tile needs -- the gathered vertex data, the
+// tile's edge arrays and the owned vertices' gather lists -- into shared
+// memory with asynchronous copies issued all at once (cp.async), so a CTA has
+// its whole working set in flight before it waits.  Then:
 //   * each vertex's derived quantities (density, beta, entropy variables,
 //     sound speed, logs) are evaluated once per staged copy instead of once
-//     per incident edge, and
-//   * each edge flux is computed once per tile into shared memory and summed
-//     per owned vertex in a fixed order (deterministic, no flux buffer in HBM).
+//     per incident edge,
+//   * each edge flux is computed once per tile and written over the edge's own
+//     (already consumed) geometry slots, and
+//   * every owned vertex sums its edge fluxes in a fixed order
+//     (deterministic; no flux buffer in HBM).
 //
 // k_tile_grad   compute_gradients (src/fv.cc:699-1059) for the owned vertices;
 //               at the first stage of a step it also evaluates the local time
@@ -20,6 +25,19 @@
 
 #include "tg_kernels.cuh"
 
+#ifndef TG_TILE_OWNED
+#define TG_TILE_OWNED 256      // owned vertices per tile (<= kTileThreads)
+#endif
+#ifndef TG_TILE_LCAP
+#define TG_TILE_LCAP 448       // local (owned + halo) vertices per tile
+#endif
+#ifndef TG_TILE_ECAP
+#define TG_TILE_ECAP 1152      // edges per tile
+#endif
+#ifndef TG_FLUX_MINB
+#define TG_FLUX_MINB 2         // resident flux CTAs per SM the register budget is sized for
+#endif
+
 namespace tg {
 
 struct TileView {
@@ -27,12 +45,23 @@ struct TileView {
   const unsigned int* ab;
   const double *nx, *ny, *g0x, *g0y, *g1x, *g1y;
   const double *ux, *uy, *ar;   // unit normal and |n| per tile edge
-  const int* cv_off;
+  const int* cv_off;            // per vertex (nv + 1); cv_ent has an even length
   const unsigned short* cv_ent;
-  const double *x, *y;    // vertex coordinates (device order)
+  const double *x, *y;          // vertex coordinates (device order)
 };
 
 constexpr int kTileThreads = 256;
+
+// ---- asynchronous global -> shared copies (sm_80+ cp.async)
+__device__ __forceinline__ void cp_async8(void* smem, const void* gmem) {
+  unsigned s = (unsigned)__cvta_generic_to_shared(smem);
+  asm volatile("cp.async.ca.shared.global [%0], [%1], 8;\n" ::"r"(s), "l"(gmem) : "memory");
+}
+__device__ __forceinline__ void cp_async4(void* smem, const void* gmem) {
+  unsigned s = (unsigned)__cvta_generic_to_shared(smem);
+  asm volatile("cp.async.ca.shared.global [%0], [%1], 4;\n" ::"r"(s), "l"(gmem) : "memory");
+}
+__device__ __forceinline__ void cp_async_wait_all() { asm volatile("cp.async.wait_all;\n" ::: "memory"); }
 
 __device__ __forceinline__ unsigned long long block_min_u64(unsigned long long bits) {
   bits = warp_min_u64(bits);
@@ -47,62 +76,117 @@ __device__ __forceinline__ unsigned long long block_min_u64(unsigned long long b
   return bits;
 }
 
-// Gradients of the owned vertices; FIRST also computes dt and U_old.
-template <bool FIRST>
+// Stage the owned vertices' gather lists: the entries, in whole 4-byte words
+// from the even entry at or below the tile's first one (returned as the base
+// the offsets are taken relative to), and the offsets.
+__device__ __forceinline__ int stage_lists(const TileView& t, int vb, int nown, unsigned int* sC, int* sO) {
+  const int base = t.cv_off[vb] & ~1;
+  const int nwords = (t.cv_off[vb + nown] - base + 1) >> 1;
+  const unsigned int* src = reinterpret_cast<const unsigned int*>(t.cv_ent + base);
+  for (int i = threadIdx.x; i < nwords; i += blockDim.x) cp_async4(sC + i, src + i);
+  for (int i = threadIdx.x; i <= nown; i += blockDim.x) cp_async4(sO + i, t.cv_off + vb + i);
+  return base;
+}
+
+__device__ __forceinline__ int list_entry(const unsigned int* sC, int j) {
+  return (int)((sC[j >> 1] >> ((j & 1) * 16)) & 0xffffu);
+}
+
+// ---------------------------------------------------------------- gradients
+// Shared memory: W (4 per local vertex) [+ T, u, v at FIRST];
+// per edge: gradient weights (4) [+ normal (2) at FIRST] + endpoints (4 bytes);
+// gather lists.
+__host__ __device__ constexpr int grad_vertex_doubles(bool first) { return first ? 7 : 4; }
+__host__ __device__ constexpr int grad_edge_doubles(bool first) { return first ? 6 : 4; }
+
+template <bool FIRST, bool GRAD>
 __global__ void __launch_bounds__(kTileThreads) k_tile_grad(Params k, MeshView m, TileView t, StateView s,
-                                                            Scalars* sc, const int* __restrict__ done) {
+                                                            Scalars* sc, int lmax, int emax,
+                                                            const int* __restrict__ done) {
   if (*done) return;
   extern __shared__ double sm[];
   const int tile = blockIdx.x;
   const int l0 = t.loff[tile], L = t.loff[tile + 1] - l0;
-  const int e0 = t.eoff[tile];
+  const int e0 = t.eoff[tile], NE = t.eoff[tile + 1] - e0;
+  const int vb = t.vbeg[tile], nown = t.vbeg[tile + 1] - vb;
   const int nv = m.nv;
-  double* sW = sm;              // 4 * L
-  double* sU = sm + 4 * L;      // FIRST: u, v, c (3 * L)
+  double* sW = sm;                                   // 4 * L
+  double* sU = sm + 4 * lmax;                        // FIRST: T, u, v -> c, u, v (3 * L)
+  double* sE = sm + grad_vertex_doubles(FIRST) * lmax;   // g0x g0y g1x g1y [nx ny]
+  unsigned int* sAB = reinterpret_cast<unsigned int*>(sE + grad_edge_doubles(FIRST) * emax);
+  int* sO = reinterpret_cast<int*>(sAB + emax);      // nown + 1
+  unsigned int* sC = reinterpret_cast<unsigned int*>(sO + kTileThreads + 2);
+
   for (int i = threadIdx.x; i < L; i += blockDim.x) {
     int g = t.lv[l0 + i];
+    if (GRAD)
 #pragma unroll
-    for (int c = 0; c < 4; ++c) sW[c * L + i] = s.W[c * nv + g];
+      for (int c = 0; c < 4; ++c) cp_async8(sW + c * L + i, s.W + (size_t)c * nv + g);
     if (FIRST) {
-      Prim q = load_prim(s.P, nv, g);
-      sU[i] = q.u;
-      sU[L + i] = q.v;
-      sU[2 * L + i] = sound_speed(k, q);
+      cp_async8(sU + i, s.P + g);                              // T
+      cp_async8(sU + L + i, s.P + (size_t)nv + g);             // u
+      cp_async8(sU + 2 * L + i, s.P + (size_t)2 * nv + g);     // v
     }
   }
+  for (int le = threadIdx.x; le < NE; le += blockDim.x) {
+    if (GRAD) {
+      cp_async8(sE + le, t.g0x + e0 + le);
+      cp_async8(sE + NE + le, t.g0y + e0 + le);
+      cp_async8(sE + 2 * NE + le, t.g1x + e0 + le);
+      cp_async8(sE + 3 * NE + le, t.g1y + e0 + le);
+    }
+    if (FIRST) {
+      cp_async8(sE + 4 * NE + le, t.nx + e0 + le);
+      cp_async8(sE + 5 * NE + le, t.ny + e0 + le);
+    }
+    cp_async4(sAB + le, t.ab + e0 + le);
+  }
+  const int cbase = stage_lists(t, vb, nown, sC, sO);
+  cp_async_wait_all();
   __syncthreads();
-  const int v = t.vbeg[tile] + threadIdx.x;
-  const bool own = v < t.vbeg[tile + 1];
+  if (FIRST) {
+    for (int i = threadIdx.x; i < L; i += blockDim.x) {
+      Prim q;
+      q.T = sU[i];
+      sU[i] = sound_speed(k, q);
+    }
+    __syncthreads();
+  }
+  const int tid = threadIdx.x;
+  const int v = vb + tid;
   unsigned long long bits = 0x7ff0000000000000ull;
-  if (own) {
+  if (tid < nown) {
     double acc[8];
 #pragma unroll
     for (int c = 0; c < 8; ++c) acc[c] = 0.0;
     double lam = 0.0;
-    for (int j = t.cv_off[v]; j < t.cv_off[v + 1]; ++j) {
-      int ent = t.cv_ent[j];
-      int le = e0 + (ent >> 1), side = ent & 1;
-      unsigned int ab = t.ab[le];
+    const int j0 = sO[tid] - cbase, j1 = sO[tid + 1] - cbase;
+    for (int j = j0; j < j1; ++j) {
+      int ent = list_entry(sC, j);
+      int le = ent >> 1, side = ent & 1;
+      unsigned int ab = sAB[le];
       int la = ab & 0xffff, lb = ab >> 16;
       int self = side ? lb : la, other = side ? la : lb;
-      double gx = side ? t.g1x[le] : t.g0x[le];
-      double gy = side ? t.g1y[le] : t.g0y[le];
+      if (GRAD) {
+        double gx = sE[(side ? 2 : 0) * NE + le];
+        double gy = sE[(side ? 3 : 1) * NE + le];
 #pragma unroll
-      for (int c = 0; c < 4; ++c) {
-        double dW = sW[c * L + other] - sW[c * L + self];
-        acc[2 * c] += gx * dW;
-        acc[2 * c + 1] += gy * dW;
+        for (int c = 0; c < 4; ++c) {
+          double dW = sW[c * L + other] - sW[c * L + self];
+          acc[2 * c] += gx * dW;
+          acc[2 * c + 1] += gy * dW;
+        }
       }
       if (FIRST) {
-        double nx = t.nx[le], ny = t.ny[le];
+        double nx = sE[4 * NE + le], ny = sE[5 * NE + le];
         double area = sqrt(nx * nx + ny * ny);
-        lam += (fabs(sU[self] * nx + sU[L + self] * ny) + sU[2 * L + self] * area) * 1.0;
+        lam += (fabs(sU[L + self] * nx + sU[2 * L + self] * ny) + sU[self] * area) * 1.0;
       }
     }
     for (int j = m.cb_off[v]; j < m.cb_off[v + 1]; ++j) {
       int ent = m.cb_ent[j];
       int type = ent & 3, idx = ent >> 2;
-      if (type == 1) {
+      if (GRAD && type == 1) {
         double dW[4];
         bface_grad_corr(k, m, s, idx, dW);
 #pragma unroll
@@ -119,20 +203,22 @@ __global__ void __launch_bounds__(kTileThreads) k_tile_grad(Params k, MeshView m
         lam += 0.5 * (fabs(q.u * nx + q.v * ny) + sound_speed(k, q) * area);
       }
     }
-    double f = m.inv6mc[v];
+    if (GRAD) {
+      double f = m.inv6mc[v];
 #pragma unroll
-    for (int c = 0; c < 8; ++c) s.G[c * nv + v] = acc[c] * f;
+      for (int c = 0; c < 8; ++c) s.G[(size_t)c * nv + v] = acc[c] * f;
+    }
     if (FIRST) {
       if (k.model == 1) {
-        for (int j = t.cv_off[v]; j < t.cv_off[v + 1]; ++j) {
-          int ent = t.cv_ent[j];
-          int le = e0 + (ent >> 1), side = ent & 1;
-          unsigned int ab = t.ab[le];
+        for (int j = j0; j < j1; ++j) {
+          int ent = list_entry(sC, j);
+          int le = ent >> 1, side = ent & 1;
+          unsigned int ab = sAB[le];
           int la = ab & 0xffff, lb = ab >> 16;
           int selfg = t.lv[l0 + (side ? lb : la)];
           int ga = t.lv[l0 + la], gb = t.lv[l0 + lb];
           Prim q = load_prim(s.P, nv, selfg);
-          double nx = t.nx[le], ny = t.ny[le];
+          double nx = sE[4 * NE + le], ny = sE[5 * NE + le];
           double area = sqrt(nx * nx + ny * ny);
           double dx = t.x[gb] - t.x[ga], dy = t.y[gb] - t.y[ga];
           double dl = sqrt(dx * dx + dy * dy);
@@ -153,49 +239,119 @@ __global__ void __launch_bounds__(kTileThreads) k_tile_grad(Params k, MeshView m
   }
 }
 
+// --------------------------------------------------------------------- fluxes
 enum : int { MODE_RESIDUAL = 0, MODE_UPDATE = 1 };
 
-// Shared-memory layout of one staged vertex (doubles, structure of arrays).
-constexpr int kVRecFields = 8;   // rho u v p beta V1 a b
-constexpr int kFluxSmemPerVertex = kVRecFields + 8 + 2;   // + gradient + coordinates
+// Shared-memory slots of the per-vertex record fields each flux reads
+// (-1: unused).  T and p are staged into slots Ts and ps and replaced in place.
+template <int FLUX> struct VLayout;
+template <> struct VLayout<FLUX_TECNO_ROE> { enum { rho = 0, u = 1, v = 2, p = -1, beta = 3, V1 = 4, a = 5, b = -1, n = 6, Ts = 0, ps = 3 }; };
+template <> struct VLayout<FLUX_TECNO_RUSANOV> { enum { rho = 0, u = 1, v = 2, p = -1, beta = 3, V1 = 4, a = -1, b = -1, n = 5, Ts = 0, ps = 3 }; };
+template <> struct VLayout<FLUX_KEPEC> { enum { rho = 0, u = 1, v = 2, p = -1, beta = 3, V1 = -1, a = -1, b = -1, n = 4, Ts = 0, ps = 3 }; };
+template <> struct VLayout<FLUX_KEP> { enum { rho = 0, u = 1, v = 2, p = 3, beta = -1, V1 = -1, a = 4, b = -1, n = 5, Ts = 0, ps = 3 }; };
+template <> struct VLayout<FLUX_ROE_EC> { enum { rho = -1, u = 0, v = 1, p = 2, beta = -1, V1 = -1, a = -1, b = 3, n = 4, Ts = 3, ps = 2 }; };
+template <> struct VLayout<FLUX_AVG> { enum { rho = 0, u = 1, v = 2, p = 3, beta = -1, V1 = -1, a = -1, b = -1, n = 4, Ts = 0, ps = 3 }; };
+
+template <int FLUX, int RECON>
+__host__ __device__ constexpr bool flux_needs_grad() {
+  return (FLUX == FLUX_TECNO_ROE || FLUX == FLUX_TECNO_RUSANOV) && RECON != RECON_FIRST;
+}
+// doubles per staged vertex: record fields [+ gradient (8) + coordinates (2)]
+template <int FLUX, int RECON>
+__host__ __device__ constexpr int flux_vertex_doubles() {
+  return VLayout<FLUX>::n + (flux_needs_grad<FLUX, RECON>() ? 10 : 0);
+}
+
+template <int FLUX>
+__device__ __forceinline__ void store_vrec(double* sV, int L, int i, const VRec& q) {
+  typedef VLayout<FLUX> Y;
+  if (Y::rho >= 0) sV[Y::rho * L + i] = q.rho;
+  if (Y::u >= 0) sV[Y::u * L + i] = q.u;
+  if (Y::v >= 0) sV[Y::v * L + i] = q.v;
+  if (Y::p >= 0) sV[Y::p * L + i] = q.p;
+  if (Y::beta >= 0) sV[Y::beta * L + i] = q.beta;
+  if (Y::V1 >= 0) sV[Y::V1 * L + i] = q.V1;
+  if (Y::a >= 0) sV[Y::a * L + i] = q.a;
+  if (Y::b >= 0) sV[Y::b * L + i] = q.b;
+}
+
+template <int FLUX>
+__device__ __forceinline__ VRec load_vrec(const double* sV, int L, int i) {
+  typedef VLayout<FLUX> Y;
+  VRec q;
+  q.rho = Y::rho >= 0 ? sV[(Y::rho >= 0 ? Y::rho : 0) * L + i] : 0.0;
+  q.u = Y::u >= 0 ? sV[(Y::u >= 0 ? Y::u : 0) * L + i] : 0.0;
+  q.v = Y::v >= 0 ? sV[(Y::v >= 0 ? Y::v : 0) * L + i] : 0.0;
+  q.p = Y::p >= 0 ? sV[(Y::p >= 0 ? Y::p : 0) * L + i] : 0.0;
+  q.beta = Y::beta >= 0 ? sV[(Y::beta >= 0 ? Y::beta : 0) * L + i] : 0.0;
+  q.V1 = Y::V1 >= 0 ? sV[(Y::V1 >= 0 ? Y::V1 : 0) * L + i] : 0.0;
+  q.a = Y::a >= 0 ? sV[(Y::a >= 0 ? Y::a : 0) * L + i] : 0.0;
+  q.b = Y::b >= 0 ? sV[(Y::b >= 0 ? Y::b : 0) * L + i] : 0.0;
+  return q;
+}
 
 template <int FLUX, int RECON, int MODE>
-__global__ void __launch_bounds__(kTileThreads) k_tile_flux(Params k, MeshView m, TileView t, StateView s,
-                                                            Control ctl, Scalars* sc, int r, int do_norm,
-                                                            double* __restrict__ Pout, double* __restrict__ Wout,
-                                                            const int* __restrict__ done) {
+__global__ void __launch_bounds__(kTileThreads, TG_FLUX_MINB)
+    k_tile_flux(Params k, MeshView m, TileView t, StateView s, Control ctl, Scalars* sc, int r, int do_norm,
+                double* __restrict__ Pout, double* __restrict__ Wout, int lmax, int emax,
+                const int* __restrict__ done) {
   if (*done) return;
   extern __shared__ double sm[];
+  typedef VLayout<FLUX> Y;
   const int tile = blockIdx.x;
   const int l0 = t.loff[tile], L = t.loff[tile + 1] - l0;
   const int e0 = t.eoff[tile], NE = t.eoff[tile + 1] - e0;
+  const int vb = t.vbeg[tile], nown = t.vbeg[tile + 1] - vb;
   const int nv = m.nv;
-  constexpr bool kGrad = (FLUX == FLUX_TECNO_ROE || FLUX == FLUX_TECNO_RUSANOV) && RECON != RECON_FIRST;
-  double* sV = sm;                          // kVRecFields * L
-  double* sG = sm + kVRecFields * L;        // 8 * L
-  double* sX = sG + 8 * L;                  // 2 * L
-  double* sF = sX + 2 * L;                  // 4 * NE
+  constexpr bool kGrad = flux_needs_grad<FLUX, RECON>();
+  double* sV = sm;                                          // Y::n * L
+  double* sG = sm + Y::n * lmax;                            // 8 * L (gradient fluxes only)
+  double* sX = sG + 8 * lmax;                               // 2 * L
+  double* sE = sm + flux_vertex_doubles<FLUX, RECON>() * lmax;   // 4 * NE: ux uy ar ab -> fluxes
+  int* sO = reinterpret_cast<int*>(sE + 4 * emax);
+  unsigned int* sC = reinterpret_cast<unsigned int*>(sO + kTileThreads + 2);
+
+  // ---- stage: vertex gathers, edge arrays, gather lists (all in flight at once)
   for (int i = threadIdx.x; i < L; i += blockDim.x) {
     int g = t.lv[l0 + i];
-    VRec q = make_vrec<FLUX>(k, load_prim(s.P, nv, g));
-    sV[0 * L + i] = q.rho; sV[1 * L + i] = q.u; sV[2 * L + i] = q.v; sV[3 * L + i] = q.p;
-    sV[4 * L + i] = q.beta; sV[5 * L + i] = q.V1; sV[6 * L + i] = q.a; sV[7 * L + i] = q.b;
+    cp_async8(sV + Y::Ts * L + i, s.P + g);
+    if (Y::u >= 0) cp_async8(sV + (Y::u >= 0 ? Y::u : 0) * L + i, s.P + (size_t)nv + g);
+    if (Y::v >= 0) cp_async8(sV + (Y::v >= 0 ? Y::v : 0) * L + i, s.P + (size_t)2 * nv + g);
+    cp_async8(sV + Y::ps * L + i, s.P + (size_t)3 * nv + g);
     if (kGrad) {
 #pragma unroll
-      for (int c = 0; c < 8; ++c) sG[c * L + i] = s.G[c * nv + g];
-      sX[i] = t.x[g];
-      sX[L + i] = t.y[g];
+      for (int c = 0; c < 8; ++c) cp_async8(sG + c * L + i, s.G + (size_t)c * nv + g);
+      cp_async8(sX + i, t.x + g);
+      cp_async8(sX + L + i, t.y + g);
     }
   }
-  __syncthreads();
   for (int le = threadIdx.x; le < NE; le += blockDim.x) {
-    unsigned int ab = t.ab[e0 + le];
+    cp_async8(sE + le, t.ux + e0 + le);
+    cp_async8(sE + NE + le, t.uy + e0 + le);
+    cp_async8(sE + 2 * NE + le, t.ar + e0 + le);
+    cp_async4(sE + 3 * NE + le, t.ab + e0 + le);
+  }
+  const int cbase = stage_lists(t, vb, nown, sC, sO);
+  cp_async_wait_all();
+  __syncthreads();
+
+  // ---- per-vertex records, in place
+  for (int i = threadIdx.x; i < L; i += blockDim.x) {
+    Prim q;
+    q.T = sV[Y::Ts * L + i];
+    q.u = Y::u >= 0 ? sV[(Y::u >= 0 ? Y::u : 0) * L + i] : 0.0;
+    q.v = Y::v >= 0 ? sV[(Y::v >= 0 ? Y::v : 0) * L + i] : 0.0;
+    q.p = sV[Y::ps * L + i];
+    store_vrec<FLUX>(sV, L, i, make_vrec<FLUX>(k, q));
+  }
+  __syncthreads();
+
+  // ---- edge fluxes; each result overwrites its edge's geometry slots
+  for (int le = threadIdx.x; le < NE; le += blockDim.x) {
+    double unx = sE[le], uny = sE[NE + le], area = sE[2 * NE + le];
+    unsigned int ab = *reinterpret_cast<const unsigned int*>(sE + 3 * NE + le);
     int la = ab & 0xffff, lb = ab >> 16;
-    VRec A, B;
-    A.rho = sV[la]; A.u = sV[L + la]; A.v = sV[2 * L + la]; A.p = sV[3 * L + la];
-    A.beta = sV[4 * L + la]; A.V1 = sV[5 * L + la]; A.a = sV[6 * L + la]; A.b = sV[7 * L + la];
-    B.rho = sV[lb]; B.u = sV[L + lb]; B.v = sV[2 * L + lb]; B.p = sV[3 * L + lb];
-    B.beta = sV[4 * L + lb]; B.V1 = sV[5 * L + lb]; B.a = sV[6 * L + lb]; B.b = sV[7 * L + lb];
+    VRec A = load_vrec<FLUX>(sV, L, la), B = load_vrec<FLUX>(sV, L, lb);
     double gl[8], gr[8], dx = 0.0, dy = 0.0;
     if (kGrad) {
 #pragma unroll
@@ -203,20 +359,33 @@ __global__ void __launch_bounds__(kTileThreads) k_tile_flux(Params k, MeshView m
       dx = sX[lb] - sX[la];
       dy = sX[L + lb] - sX[L + la];
     }
-    Flx F = num_flux_unit<FLUX, RECON>(k, A, B, t.ux[e0 + le], t.uy[e0 + le], t.ar[e0 + le], dx, dy, gl, gr);
-    sF[le] = F.m; sF[NE + le] = F.x; sF[2 * NE + le] = F.y; sF[3 * NE + le] = F.e;
+    Flx F = num_flux_unit<FLUX, RECON>(k, A, B, unx, uny, area, dx, dy, gl, gr);
+    sE[le] = F.m; sE[NE + le] = F.x; sE[2 * NE + le] = F.y; sE[3 * NE + le] = F.e;
   }
   __syncthreads();
-  const int v = t.vbeg[tile] + threadIdx.x;
-  const bool own = v < t.vbeg[tile + 1];
+
+  // ---- owned vertices: fixed-order sum, then residual or RK update
+  const int tid = threadIdx.x;
+  const int v = vb + tid;
   double nrm[4] = {0.0, 0.0, 0.0, 0.0};
-  if (own) {
+  if (tid < nown) {
+    Prim q0;
+    double uo[4], area = 0.0, w = 0.0, dtl = 0.0;
+    if (MODE == MODE_UPDATE) {   // issue the update's loads before the gather
+      q0 = load_prim(s.P, nv, v);
+#pragma unroll
+      for (int c = 0; c < 4; ++c) uo[c] = s.Uold[(size_t)c * nv + v];
+      area = m.dcarea[v];
+      w = m.pweight[v];
+      if (!(ctl.time_mode == 1 || ctl.time_step > 0.0)) dtl = s.dt[v];
+    }
     double r0 = 0.0, r1 = 0.0, r2 = 0.0, r3 = 0.0;
-    for (int j = t.cv_off[v]; j < t.cv_off[v + 1]; ++j) {
-      int ent = t.cv_ent[j];
+    const int j0 = sO[tid] - cbase, j1 = sO[tid + 1] - cbase;
+    for (int j = j0; j < j1; ++j) {
+      int ent = list_entry(sC, j);
       int le = ent >> 1;
       double sg = (ent & 1) ? -1.0 : 1.0;
-      r0 += sF[le] * sg; r1 += sF[NE + le] * sg; r2 += sF[2 * NE + le] * sg; r3 += sF[3 * NE + le] * sg;
+      r0 += sE[le] * sg; r1 += sE[NE + le] * sg; r2 += sE[2 * NE + le] * sg; r3 += sE[3 * NE + le] * sg;
     }
     const int n2 = 2 * m.nb, n3 = 3 * m.nvu;
     for (int j = m.cb_off[v]; j < m.cb_off[v + 1]; ++j) {
@@ -235,22 +404,19 @@ __global__ void __launch_bounds__(kTileThreads) k_tile_flux(Params k, MeshView m
     } else {
       const double a_rk[3] = {0.0, 3.0 / 4.0, 1.0 / 3.0};
       const double b_rk[3] = {1.0, 1.0 / 4.0, 2.0 / 3.0};
-      double area = m.dcarea[v];
       if (do_norm) {
-        double w = m.pweight[v];
-        double q0 = r0 / area, q1 = r1 / area, q2 = r2 / area, q3 = r3 / area;
-        nrm[0] = q0 * q0 * w; nrm[1] = q1 * q1 * w; nrm[2] = q2 * q2 * w; nrm[3] = q3 * q3 * w;
+        double a0 = r0 / area, a1 = r1 / area, a2 = r2 / area, a3 = r3 / area;
+        nrm[0] = a0 * a0 * w; nrm[1] = a1 * a1 * w; nrm[2] = a2 * a2 * w; nrm[3] = a3 * a3 * w;
       }
-      double dtv = (ctl.time_mode == 1 || ctl.time_step > 0.0) ? sc->dt_global : s.dt[v];
+      double dtv = (ctl.time_mode == 1 || ctl.time_step > 0.0) ? sc->dt_global : dtl;
       double factor = dtv / (1.0 * area);
-      Prim q0 = load_prim(s.P, nv, v);
       Cons c = prim2con(k, q0);
       double br = b_rk[r], ar = a_rk[r], c2 = -factor * br;
       c.r *= br; c.mx *= br; c.my *= br; c.E *= br;
-      c.r += s.Uold[v] * ar + r0 * c2;
-      c.mx += s.Uold[nv + v] * ar + r1 * c2;
-      c.my += s.Uold[2 * nv + v] * ar + r2 * c2;
-      c.E += s.Uold[3 * nv + v] * ar + r3 * c2;
+      c.r += uo[0] * ar + r0 * c2;
+      c.mx += uo[1] * ar + r1 * c2;
+      c.my += uo[2] * ar + r2 * c2;
+      c.E += uo[3] * ar + r3 * c2;
       Prim q = con2prim(k, c);
       Ent e = prim2ent(k, q);
       Pout[v] = q.T; Pout[nv + v] = q.u; Pout[2 * nv + v] = q.v; Pout[3 * nv + v] = q.p;
@@ -260,7 +426,7 @@ __global__ void __launch_bounds__(kTileThreads) k_tile_flux(Params k, MeshView m
     }
   }
   if (MODE == MODE_UPDATE && do_norm) {
-    // the smem tile buffers are no longer needed: reuse them for the block reduction
+    // the tile buffers are no longer needed: reuse them for the block reduction
     __syncthreads();
     double* red = sm;
 #pragma unroll
@@ -278,9 +444,20 @@ __global__ void __launch_bounds__(kTileThreads) k_tile_flux(Params k, MeshView m
   }
 }
 
-inline size_t tile_grad_smem(int lmax, bool first) { return (size_t)lmax * (first ? 7 : 4) * sizeof(double); }
-inline size_t tile_flux_smem(int lmax, int emax) {
-  size_t a = ((size_t)lmax * kFluxSmemPerVertex + 4 * (size_t)emax) * sizeof(double);
+// gather-list words (cmax entries, two per word) + offsets
+inline size_t tile_list_bytes(int cmax) {
+  return (kTileThreads + 2) * sizeof(int) + (size_t)((cmax + 2) / 2 + 1) * sizeof(unsigned int);
+}
+
+inline size_t tile_grad_smem(int lmax, int emax, int cmax, bool first) {
+  return ((size_t)lmax * grad_vertex_doubles(first) + (size_t)emax * grad_edge_doubles(first)) * sizeof(double) +
+         (size_t)emax * sizeof(unsigned int) + tile_list_bytes(cmax);
+}
+
+template <int FLUX, int RECON>
+size_t tile_flux_smem_t(int lmax, int emax, int cmax) {
+  size_t a = ((size_t)lmax * flux_vertex_doubles<FLUX, RECON>() + 4 * (size_t)emax) * sizeof(double) +
+             tile_list_bytes(cmax);
   size_t b = 4 * kTileThreads * sizeof(double);
   return a > b ? a : b;
 }
