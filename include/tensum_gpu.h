@@ -255,6 +255,37 @@ typedef enum {
 } tg_query_key;
 tg_status tg_query(tg_handle* h, int key, double* out);
 
+/* ---- allocation-free residual norm ------------------------------------ */
+
+#define TG_NOALLOC_MAX_VERTICES 268435456
+
+/* No counterpart in the reference (whose norm is a member of FiniteVolume
+ * working on its own arrays).  For callers that cannot allocate device memory
+ * while they run -- hosts that reserve all GPU memory up front, code running
+ * while another part of the program captures a CUDA graph, real-time loops --
+ * this computes the residual norms of compute_residual_norm
+ * (src/fv.cc:1801-1879) from buffers the caller already owns, with no handle
+ * and no cudaMalloc/cudaFree: its scratch is a fixed 64 KiB device array in
+ * the library, held by every GPU that loads it until exit.
+ *   res_dev     device array n_vertex x 5, the reference's Flux layout
+ *               (mass, mx, my, mz, energy); the z component is ignored
+ *   dcarea_dev  device array n_vertex, dual areas
+ *   weight_dev  device array n_vertex, 1/|P_i| for periodic vertices, else 1
+ *   total0      normaliser; <= 0 marks the first iteration (total becomes it)
+ *   out6_dev    device array of 6: mass, mx, my, energy norms, normalised
+ *               total, normaliser
+ *   stream      cudaStream_t (NULL = default stream); the call is
+ *               asynchronous on it.
+ * n_vertex must be at most TG_NOALLOC_MAX_VERTICES (TG_INVALID_ARG otherwise).
+ * The first call on each device looks up the scratch array's device address,
+ * so make it before any stream capture that should contain later calls.
+ * All calls share the scratch array: calls whose kernels overlap on the GPU
+ * (e.g. on two streams) race and may return wrong norms.
+ * On failure tg_noalloc_last_error() describes the problem. */
+tg_status tg_residual_norm_noalloc(const double* res_dev, const double* dcarea_dev, const double* weight_dev,
+                                   int n_vertex, double total0, double* out6_dev, void* stream);
+const char* tg_noalloc_last_error(void);
+
 #ifdef __cplusplus
 }
 #endif
