@@ -209,6 +209,29 @@ __device__ __forceinline__ VRec make_vrec(const Params& k, const Prim& q) {
   return r;
 }
 
+// The same record from the stored entropy variables: V5 = -2 beta gives
+// beta = -V5/2 and rho = 2 beta p = -V5 p, and V1 is the stored first entropy
+// variable, so no division or logarithm is needed per vertex.  The stored
+// variables come from prim2ent (beta = rho/(2p), src/material.h:534-546), the
+// flux recomputes them from (T, p) (beta = 0.5/(R T)); the two differ in the
+// last ulp only.
+template <int FLUX>
+__device__ __forceinline__ VRec make_vrec_w(const Params& k, double u, double v, double p, double T, double V1,
+                                            double V5) {
+  VRec r;
+  r.rho = -V5 * p;
+  r.u = u;
+  r.v = v;
+  r.p = p;
+  r.beta = -0.5 * V5;
+  r.V1 = V1;
+  r.a = 0.0;
+  r.b = 0.0;
+  if (FLUX == FLUX_TECNO_ROE || FLUX == FLUX_KEP) r.a = sqrt(k.gamma * k.R * T);
+  if (FLUX == FLUX_ROE_EC) r.b = sqrt(-V5);
+  return r;
+}
+
 __device__ __forceinline__ Flx kepec_flux(const Params& k, const VRec& L, const VRec& R, double unx, double uny) {
   // src/kepec.cc:10-38; 1/((gamma-1) beta_ln) is formed from 1/beta_ln directly
   double rho = logavg(L.rho, R.rho);

@@ -242,15 +242,23 @@ __global__ void __launch_bounds__(kTileThreads) k_tile_grad(Params k, MeshView m
 // --------------------------------------------------------------------- fluxes
 enum : int { MODE_RESIDUAL = 0, MODE_UPDATE = 1 };
 
-// Shared-memory slots of the per-vertex record fields each flux reads
-// (-1: unused).  T and p are staged into slots Ts and ps and replaced in place.
+// Shared-memory slots of the per-vertex record fields each flux reads (-1:
+// unused), and where the raw inputs are staged before the record is formed in
+// place: p, u, v from P, the entropy variables V1 (W0) and V5 = -2 beta (W3)
+// from W, and T where a sound speed is needed.
 template <int FLUX> struct VLayout;
-template <> struct VLayout<FLUX_TECNO_ROE> { enum { rho = 0, u = 1, v = 2, p = -1, beta = 3, V1 = 4, a = 5, b = -1, n = 6, Ts = 0, ps = 3 }; };
-template <> struct VLayout<FLUX_TECNO_RUSANOV> { enum { rho = 0, u = 1, v = 2, p = -1, beta = 3, V1 = 4, a = -1, b = -1, n = 5, Ts = 0, ps = 3 }; };
-template <> struct VLayout<FLUX_KEPEC> { enum { rho = 0, u = 1, v = 2, p = -1, beta = 3, V1 = -1, a = -1, b = -1, n = 4, Ts = 0, ps = 3 }; };
-template <> struct VLayout<FLUX_KEP> { enum { rho = 0, u = 1, v = 2, p = 3, beta = -1, V1 = -1, a = 4, b = -1, n = 5, Ts = 0, ps = 3 }; };
-template <> struct VLayout<FLUX_ROE_EC> { enum { rho = -1, u = 0, v = 1, p = 2, beta = -1, V1 = -1, a = -1, b = 3, n = 4, Ts = 3, ps = 2 }; };
-template <> struct VLayout<FLUX_AVG> { enum { rho = 0, u = 1, v = 2, p = 3, beta = -1, V1 = -1, a = -1, b = -1, n = 4, Ts = 0, ps = 3 }; };
+template <> struct VLayout<FLUX_TECNO_ROE> { enum { rho = 0, u = 1, v = 2, p = -1, beta = 3, V1 = 4, a = 5, b = -1, n = 6,
+                                                    Rp = 0, Ru = 1, Rv = 2, RW3 = 3, RW0 = 4, RT = 5 }; };
+template <> struct VLayout<FLUX_TECNO_RUSANOV> { enum { rho = 0, u = 1, v = 2, p = -1, beta = 3, V1 = 4, a = -1, b = -1, n = 5,
+                                                        Rp = 0, Ru = 1, Rv = 2, RW3 = 3, RW0 = 4, RT = -1 }; };
+template <> struct VLayout<FLUX_KEPEC> { enum { rho = 0, u = 1, v = 2, p = -1, beta = 3, V1 = -1, a = -1, b = -1, n = 4,
+                                                Rp = 0, Ru = 1, Rv = 2, RW3 = 3, RW0 = -1, RT = -1 }; };
+template <> struct VLayout<FLUX_KEP> { enum { rho = 0, u = 1, v = 2, p = 3, beta = -1, V1 = -1, a = 4, b = -1, n = 5,
+                                              Rp = 3, Ru = 1, Rv = 2, RW3 = 0, RW0 = -1, RT = 4 }; };
+template <> struct VLayout<FLUX_ROE_EC> { enum { rho = -1, u = 0, v = 1, p = 2, beta = -1, V1 = -1, a = -1, b = 3, n = 4,
+                                                 Rp = 2, Ru = 0, Rv = 1, RW3 = 3, RW0 = -1, RT = -1 }; };
+template <> struct VLayout<FLUX_AVG> { enum { rho = 0, u = 1, v = 2, p = 3, beta = -1, V1 = -1, a = -1, b = -1, n = 4,
+                                              Rp = 3, Ru = 1, Rv = 2, RW3 = 0, RW0 = -1, RT = -1 }; };
 
 template <int FLUX, int RECON>
 __host__ __device__ constexpr bool flux_needs_grad() {
@@ -314,10 +322,12 @@ __global__ void __launch_bounds__(kTileThreads, TG_FLUX_MINB)
   // ---- stage: vertex gathers, edge arrays, gather lists (all in flight at once)
   for (int i = threadIdx.x; i < L; i += blockDim.x) {
     int g = t.lv[l0 + i];
-    cp_async8(sV + Y::Ts * L + i, s.P + g);
-    if (Y::u >= 0) cp_async8(sV + (Y::u >= 0 ? Y::u : 0) * L + i, s.P + (size_t)nv + g);
-    if (Y::v >= 0) cp_async8(sV + (Y::v >= 0 ? Y::v : 0) * L + i, s.P + (size_t)2 * nv + g);
-    cp_async8(sV + Y::ps * L + i, s.P + (size_t)3 * nv + g);
+    cp_async8(sV + Y::Ru * L + i, s.P + (size_t)nv + g);
+    cp_async8(sV + Y::Rv * L + i, s.P + (size_t)2 * nv + g);
+    cp_async8(sV + Y::Rp * L + i, s.P + (size_t)3 * nv + g);
+    cp_async8(sV + Y::RW3 * L + i, s.W + (size_t)3 * nv + g);
+    if (Y::RW0 >= 0) cp_async8(sV + (Y::RW0 >= 0 ? Y::RW0 : 0) * L + i, s.W + g);
+    if (Y::RT >= 0) cp_async8(sV + (Y::RT >= 0 ? Y::RT : 0) * L + i, s.P + g);
     if (kGrad) {
 #pragma unroll
       for (int c = 0; c < 8; ++c) cp_async8(sG + c * L + i, s.G + (size_t)c * nv + g);
@@ -337,12 +347,10 @@ __global__ void __launch_bounds__(kTileThreads, TG_FLUX_MINB)
 
   // ---- per-vertex records, in place
   for (int i = threadIdx.x; i < L; i += blockDim.x) {
-    Prim q;
-    q.T = sV[Y::Ts * L + i];
-    q.u = Y::u >= 0 ? sV[(Y::u >= 0 ? Y::u : 0) * L + i] : 0.0;
-    q.v = Y::v >= 0 ? sV[(Y::v >= 0 ? Y::v : 0) * L + i] : 0.0;
-    q.p = sV[Y::ps * L + i];
-    store_vrec<FLUX>(sV, L, i, make_vrec<FLUX>(k, q));
+    double u = sV[Y::Ru * L + i], v = sV[Y::Rv * L + i], p = sV[Y::Rp * L + i], w3 = sV[Y::RW3 * L + i];
+    double w0 = Y::RW0 >= 0 ? sV[(Y::RW0 >= 0 ? Y::RW0 : 0) * L + i] : 0.0;
+    double T = Y::RT >= 0 ? sV[(Y::RT >= 0 ? Y::RT : 0) * L + i] : 0.0;
+    store_vrec<FLUX>(sV, L, i, make_vrec_w<FLUX>(k, u, v, p, T, w0, w3));
   }
   __syncthreads();
 
