@@ -335,11 +335,19 @@ __device__ __forceinline__ Flx tecno_flux(const Params& k, const VRec& L, const 
   double const1 = sqrt(rho * k.inv_gamma);
   double psqrt = sqrt(p);
   double S0 = sqrt(0.5) * const1, S1 = k.sqrt_gm1 * const1, S2 = psqrt;
-  // scaled eigenvector matrix; rows = (mass, mx, my, energy), cols = waves (u-a, entropy, shear, u+a)
-  double R[4][4] = {{1 * S0, 1 * S1, 0 * S2, 1 * S0},
-                    {(vx - a * unx) * S0, vx * S1, uny * S2, (vx + a * unx) * S0},
-                    {(vy - a * uny) * S0, vy * S1, -unx * S2, (vy + a * uny) * S0},
-                    {(H - a * vn) * S0, (0.5 * vsq) * S1, v1 * S2, (H + a * vn) * S0}};
+  // The scaled eigenvector matrix (src/kepes_tecno_roe.cc:61-77) has the columns
+  //   (u-a): S0 (1, vx - a nx, vy - a ny, H - a vn)   (entropy): S1 (1, vx, vy, |v|^2/2)
+  //   (shear): S2 (0, ny, -nx, v1)                    (u+a): S0 (1, vx + a nx, vy + a ny, H + a vn)
+  // and is applied through that structure below instead of being stored.
+  auto RT = [&](const double* x, double* z) {
+    double A = x[0] + vx * x[1] + vy * x[2];
+    double B = unx * x[1] + uny * x[2] + vn * x[3];
+    double C = A + H * x[3];
+    z[0] = S0 * (C - a * B);
+    z[1] = S1 * (A + (0.5 * vsq) * x[3]);
+    z[2] = S2 * (uny * x[1] - unx * x[2] + v1 * x[3]);
+    z[3] = S0 * (C + a * B);
+  };
   double Lam[4];
   if (ROE) {
     double vnl = L.u * unx + L.v * uny, vnr = Rp.u * unx + Rp.v * uny;
@@ -363,30 +371,20 @@ __device__ __forceinline__ Flx tecno_flux(const Params& k, const VRec& L, const 
     gl[i] = dEl[2 * i] * dx + dEl[2 * i + 1] * dy;
     gr[i] = dEr[2 * i] * dx + dEr[2 * i + 1] * dy;
   }
-  double dZ[4];
+  double d[4], sgl[4], sgr[4];
+  RT(dV, d);
+  RT(gl, sgl);
+  RT(gr, sgr);
+  // q = S (Lambda dZ); Diff = R Lambda dZ from the columns above
+  double q[4];
 #pragma unroll
-  for (int i = 0; i < 4; ++i) {
-    double d = 0.0, sgl = 0.0, sgr = 0.0;
-#pragma unroll
-    for (int j = 0; j < 4; ++j) {
-      d += R[j][i] * dV[j];
-      sgl += R[j][i] * gl[j];
-      sgr += R[j][i] * gr[j];
-    }
-    dZ[i] = reconstructed_jump<RECON>(d, sgl, sgr, h, k.tvbM);
-  }
-  double Diff[4];
-#pragma unroll
-  for (int i = 0; i < 4; ++i) {
-    double d = 0.0;
-#pragma unroll
-    for (int j = 0; j < 4; ++j) d += R[i][j] * Lam[j] * dZ[j];
-    Diff[i] = d;
-  }
-  F.m -= 0.5 * Diff[0];
-  F.x -= 0.5 * Diff[1];
-  F.y -= 0.5 * Diff[2];
-  F.e -= 0.5 * Diff[3];
+  for (int i = 0; i < 4; ++i) q[i] = Lam[i] * reconstructed_jump<RECON>(d[i], sgl[i], sgr[i], h, k.tvbM);
+  q[0] *= S0; q[1] *= S1; q[2] *= S2; q[3] *= S0;
+  double sum = q[0] + q[1] + q[3], dif = q[3] - q[0];
+  F.m -= 0.5 * sum;
+  F.x -= 0.5 * (vx * sum + a * unx * dif + uny * q[2]);
+  F.y -= 0.5 * (vy * sum + a * uny * dif - unx * q[2]);
+  F.e -= 0.5 * (H * (q[0] + q[3]) + a * vn * dif + (0.5 * vsq) * q[1] + v1 * q[2]);
   return F;
 }
 

@@ -34,8 +34,12 @@
 #ifndef TG_TILE_ECAP
 #define TG_TILE_ECAP 1152      // edges per tile
 #endif
+// resident flux CTAs per SM the register budget is sized for: TeCNO fluxes / central fluxes
 #ifndef TG_FLUX_MINB
-#define TG_FLUX_MINB 2         // resident flux CTAs per SM the register budget is sized for
+#define TG_FLUX_MINB 2
+#endif
+#ifndef TG_FLUX_MINB_CENTRAL
+#define TG_FLUX_MINB_CENTRAL 3
 #endif
 
 namespace tg {
@@ -299,7 +303,8 @@ __device__ __forceinline__ VRec load_vrec(const double* sV, int L, int i) {
 }
 
 template <int FLUX, int RECON, int MODE>
-__global__ void __launch_bounds__(kTileThreads, TG_FLUX_MINB)
+__global__ void __launch_bounds__(kTileThreads, (FLUX == FLUX_TECNO_ROE || FLUX == FLUX_TECNO_RUSANOV)
+                                                    ? TG_FLUX_MINB : TG_FLUX_MINB_CENTRAL)
     k_tile_flux(Params k, MeshView m, TileView t, StateView s, Control ctl, Scalars* sc, int r, int do_norm,
                 double* __restrict__ Pout, double* __restrict__ Wout, int lmax, int emax,
                 const int* __restrict__ done) {
