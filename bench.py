@@ -300,26 +300,37 @@ def run_ours(args):
                  "frac": step_bytes * args.steps / (total_ms / 1e3) / 1e9 / peak,
                  "bytes_per_step": step_bytes, "model": "408V+56E per stage (TeCNO), 224V+32E (central fluxes)"}
 
-    # end to end through the C ABI with host buffers every step (dominant flux)
+    # end to end through the C ABI with host buffers every step (dominant flux):
+    # PrimVar records in and out of pinned host memory (DMA, no staging), and
+    # the same through pageable numpy arrays (the library's staging ring)
     s_e2e = dict((f, s) for f, s, _ in solvers)[dom_flux]
-    host_out = np.empty((V, 5))
+    pin_in = torch.empty((V, 5), dtype=torch.float64, pin_memory=True).numpy()
+    pin_out = torch.empty((V, 5), dtype=torch.float64, pin_memory=True).numpy()
+    pin_in[:] = prim0
+    page_out = np.empty((V, 5))
     ne2e = max(1, min(args.e2e_steps, args.steps))
-    torch.cuda.synchronize()
-    if dist:
-        dist.barrier()
-    t0 = time.perf_counter()
-    for _ in range(ne2e):
-        s_e2e.set_state(prim0)
-        s_e2e.step(1)
-        host_out[:] = s_e2e.get_state()
-    e2e_s = time.perf_counter() - t0
-    if dist:
-        t = torch.tensor([e2e_s], device="cuda", dtype=torch.float64)
-        dist.all_reduce(t, op=dist.ReduceOp.MAX)
-        e2e_s = float(t.item())
-    e2e = {"value": V * 3 * ne2e * world / e2e_s, "unit": UNIT, "h2d_bytes_per_step": 32 * V,
-           "d2h_bytes_per_step": 32 * V, "steps": ne2e, "flux": dom_flux,
-           "path": "tg_set_state(host AoS) + tg_step(1) + tg_get_state(host AoS) per step"}
+
+    def e2e_run(src, dst):
+        torch.cuda.synchronize()
+        if dist:
+            dist.barrier()
+        t0 = time.perf_counter()
+        for _ in range(ne2e):
+            s_e2e.set_state(src)
+            s_e2e.step(1)
+            s_e2e.get_state(out=dst)
+        el = time.perf_counter() - t0
+        if dist:
+            t = torch.tensor([el], device="cuda", dtype=torch.float64)
+            dist.all_reduce(t, op=dist.ReduceOp.MAX)
+            el = float(t.item())
+        return V * 3 * ne2e * world / el
+
+    e2e_run(pin_in, pin_out)   # first touch of the staging paths
+    e2e = {"value": e2e_run(pin_in, pin_out), "unit": UNIT, "h2d_bytes_per_step": 40 * V,
+           "d2h_bytes_per_step": 40 * V, "steps": ne2e, "flux": dom_flux,
+           "path": "tg_set_state(pinned host PrimVar[V]) + tg_step(1) + tg_get_state(pinned host PrimVar[V]) per step",
+           "pageable_value": e2e_run(np.ascontiguousarray(prim0), page_out)}
 
     cpu = None
     if rank == 0 and world == 1 and not args.no_cpu_baseline:

@@ -9,8 +9,10 @@
 #include <cstdio>
 #include <cstdlib>
 #include <cstring>
+#include <algorithm>
 #include <new>
 #include <string>
+#include <thread>
 #include <vector>
 
 #include "../../include/tensum_gpu.h"
@@ -23,6 +25,20 @@ using namespace tg;
 namespace {
 
 thread_local std::string g_last_error;
+
+// Pinned staging for state transfers from and to pageable caller buffers: up to
+// kMaxLanes host threads, each with its own stream and two kSlot slots, so the
+// host memcpy into one slot overlaps the DMA of the other.  Pinned caller
+// buffers bypass it (one cudaMemcpyAsync on the handle's stream).
+struct Stager {
+  static constexpr int kMaxLanes = 8;
+  static constexpr size_t kSlot = size_t(2) << 20;
+  int lanes = 0;
+  char* slots = nullptr;   // pinned, lanes * 2 * kSlot bytes
+  cudaStream_t st[kMaxLanes] = {};
+  cudaEvent_t ev[kMaxLanes][2] = {};
+  char* slot(int lane, int k) const { return slots + (2 * (size_t)lane + k) * kSlot; }
+};
 
 }  // namespace
 
@@ -49,8 +65,12 @@ struct tg_handle {
   bool grads_needed = false;
   cudaGraph_t graph = nullptr;
   cudaGraphExec_t graph_exec = nullptr;
-  // pinned host staging for state transfers (4*nv doubles)
-  double* hP = nullptr;
+  // state transfers: PrimVar records in the caller's order on the device
+  double* raw = nullptr;              // 5 * nv doubles
+  const int* old_of_new = nullptr;    // device copy of the vertex permutation
+  int* bad = nullptr;                 // device flag of k_state_check
+  cudaEvent_t raw_ready = nullptr;
+  Stager stage;
   size_t device_bytes = 0;
   int kernels_per_step = 0;
   int kernels_per_flux = 0;
@@ -259,6 +279,102 @@ tg_status sync(tg_handle* h) {
   return TG_OK;
 }
 
+bool host_pinned(const void* p) {
+  cudaPointerAttributes a;
+  if (cudaPointerGetAttributes(&a, p) != cudaSuccess) {
+    cudaGetLastError();
+    return false;
+  }
+  return a.type == cudaMemoryTypeHost;
+}
+
+// One lane of a staged host->device copy of len bytes.
+cudaError_t lane_h2d(const tg_handle* h, int lane, char* dst, const char* src, size_t len) {
+  const Stager& S = h->stage;
+  cudaError_t e = cudaSetDevice(h->device);
+  for (size_t off = 0, k = 0; e == cudaSuccess && off < len; off += Stager::kSlot, ++k) {
+    const int s = (int)(k & 1);
+    const size_t n = std::min(Stager::kSlot, len - off);
+    if (k >= 2 && (e = cudaEventSynchronize(S.ev[lane][s])) != cudaSuccess) break;
+    std::memcpy(S.slot(lane, s), src + off, n);
+    if ((e = cudaMemcpyAsync(dst + off, S.slot(lane, s), n, cudaMemcpyHostToDevice, S.st[lane])) != cudaSuccess) break;
+    e = cudaEventRecord(S.ev[lane][s], S.st[lane]);
+  }
+  cudaError_t e2 = cudaStreamSynchronize(S.st[lane]);
+  return e != cudaSuccess ? e : e2;
+}
+
+// One lane of a staged device->host copy; the lane's stream first waits for `ready`.
+cudaError_t lane_d2h(const tg_handle* h, int lane, char* dst, const char* src, size_t len, cudaEvent_t ready) {
+  const Stager& S = h->stage;
+  cudaError_t e = cudaSetDevice(h->device);
+  if (e == cudaSuccess) e = cudaStreamWaitEvent(S.st[lane], ready, 0);
+  const size_t nk = (len + Stager::kSlot - 1) / Stager::kSlot;
+  auto issue = [&](size_t k) {
+    const int s = (int)(k & 1);
+    const size_t n = std::min(Stager::kSlot, len - k * Stager::kSlot);
+    cudaError_t ei = cudaMemcpyAsync(S.slot(lane, s), src + k * Stager::kSlot, n, cudaMemcpyDeviceToHost, S.st[lane]);
+    return ei != cudaSuccess ? ei : cudaEventRecord(S.ev[lane][s], S.st[lane]);
+  };
+  for (size_t k = 0; e == cudaSuccess && k < std::min<size_t>(2, nk); ++k) e = issue(k);
+  for (size_t k = 0; e == cudaSuccess && k < nk; ++k) {
+    const int s = (int)(k & 1);
+    if ((e = cudaEventSynchronize(S.ev[lane][s])) != cudaSuccess) break;
+    std::memcpy(dst + k * Stager::kSlot, S.slot(lane, s), std::min(Stager::kSlot, len - k * Stager::kSlot));
+    if (k + 2 < nk) e = issue(k + 2);
+  }
+  cudaError_t e2 = cudaStreamSynchronize(S.st[lane]);
+  return e != cudaSuccess ? e : e2;
+}
+
+// Splits a staged copy over the lanes (lane 0 on the calling thread).
+template <class Lane>
+cudaError_t run_lanes(const tg_handle* h, size_t bytes, Lane lane) {
+  const int n = (int)std::max<size_t>(1, std::min<size_t>(h->stage.lanes, bytes / (2 * Stager::kSlot)));
+  const size_t per = ((bytes + n - 1) / n + 255) & ~size_t(255);
+  std::vector<cudaError_t> errs(n, cudaSuccess);
+  std::vector<std::thread> th;
+  for (int t = 1; t < n; ++t) {
+    const size_t off = t * per;
+    if (off >= bytes) break;
+    th.emplace_back([&, t, off] { errs[t] = lane(t, off, std::min(per, bytes - off)); });
+  }
+  errs[0] = lane(0, 0, std::min(per, bytes));
+  for (auto& x : th) x.join();
+  for (cudaError_t e : errs)
+    if (e != cudaSuccess) return e;
+  return cudaSuccess;
+}
+
+// Caller buffer -> h->raw, ordered before the next work on h->stream.
+tg_status state_h2d(tg_handle* h, const double* prim, size_t bytes) {
+  if (host_pinned(prim)) {
+    TG_CUDA(h, cudaMemcpyAsync(h->raw, prim, bytes, cudaMemcpyHostToDevice, h->stream));
+    return TG_OK;
+  }
+  TG_CUDA(h, cudaStreamSynchronize(h->stream));   // h->raw may still be read by an earlier transfer
+  const char* src = (const char*)prim;
+  char* dst = (char*)h->raw;
+  TG_CUDA(h, run_lanes(h, bytes, [&](int t, size_t off, size_t len) { return lane_h2d(h, t, dst + off, src + off, len); }));
+  return TG_OK;
+}
+
+// h->raw -> caller buffer, after the work enqueued so far on h->stream; returns when the data is in `prim`.
+tg_status state_d2h(tg_handle* h, double* prim, size_t bytes) {
+  if (host_pinned(prim)) {
+    TG_CUDA(h, cudaMemcpyAsync(prim, h->raw, bytes, cudaMemcpyDeviceToHost, h->stream));
+    TG_CUDA(h, cudaStreamSynchronize(h->stream));
+    return TG_OK;
+  }
+  TG_CUDA(h, cudaEventRecord(h->raw_ready, h->stream));
+  const char* src = (const char*)h->raw;
+  char* dst = (char*)prim;
+  TG_CUDA(h, run_lanes(h, bytes, [&](int t, size_t off, size_t len) {
+    return lane_d2h(h, t, dst + off, src + off, len, h->raw_ready);
+  }));
+  return TG_OK;
+}
+
 tg_status read_scalars(tg_handle* h, Scalars* out) {
   TG_CUDA(h, cudaMemcpyAsync(out, h->sc, sizeof(Scalars), cudaMemcpyDeviceToHost, h->stream));
   return sync(h);
@@ -427,8 +543,19 @@ tg_status tg_create(const tg_mesh* mesh, const tg_material* mat, const tg_bc_tab
   // + norm_final + step_end
   h->kernels_per_step = 1 + (1 + (h->grads_needed ? 2 : 0)) + 3 * residual_kernels(h) + (c.time_step > 0.0 ? 1 : 0) +
                         1 + 1 + 1;
+  if ((st = dev_alloc(h, 5 * nv, &h->raw)) != TG_OK) { tg_destroy(h); return st; }
+  if ((st = dev_alloc(h, 1, &h->bad)) != TG_OK) { tg_destroy(h); return st; }
+  if ((st = dev_upload(h, L.old_of_new, &h->old_of_new)) != TG_OK) { tg_destroy(h); return st; }
   {
-    cudaError_t ep = cudaMallocHost((void**)&h->hP, 4 * nv * sizeof(double));
+    Stager& S = h->stage;
+    const size_t bytes = 5 * nv * sizeof(double);
+    S.lanes = (int)std::max<size_t>(1, std::min<size_t>(Stager::kMaxLanes, bytes / (2 * Stager::kSlot)));
+    cudaError_t ep = cudaMallocHost((void**)&S.slots, 2 * (size_t)S.lanes * Stager::kSlot);
+    for (int t = 0; t < S.lanes && ep == cudaSuccess; ++t) {
+      ep = cudaStreamCreateWithFlags(&S.st[t], cudaStreamNonBlocking);
+      for (int k = 0; k < 2 && ep == cudaSuccess; ++k) ep = cudaEventCreateWithFlags(&S.ev[t][k], cudaEventDisableTiming);
+    }
+    if (ep == cudaSuccess) ep = cudaEventCreateWithFlags(&h->raw_ready, cudaEventDisableTiming);
     if (ep != cudaSuccess) { tg_destroy(h); return fail(nullptr, TG_CUDA_ERROR, cudaGetErrorString(ep)); }
   }
   cudaError_t e = cudaStreamCreateWithFlags(&h->stream, cudaStreamNonBlocking);
@@ -445,7 +572,14 @@ tg_status tg_destroy(tg_handle* h) {
   if (h->graph) cudaGraphDestroy(h->graph);
   if (h->stream) cudaStreamSynchronize(h->stream);
   for (void* p : h->allocs) cudaFree(p);
-  if (h->hP) cudaFreeHost(h->hP);
+  for (int t = 0; t < Stager::kMaxLanes; ++t) {
+    if (h->stage.st[t]) cudaStreamSynchronize(h->stage.st[t]);
+    for (int k = 0; k < 2; ++k)
+      if (h->stage.ev[t][k]) cudaEventDestroy(h->stage.ev[t][k]);
+    if (h->stage.st[t]) cudaStreamDestroy(h->stage.st[t]);
+  }
+  if (h->stage.slots) cudaFreeHost(h->stage.slots);
+  if (h->raw_ready) cudaEventDestroy(h->raw_ready);
   if (h->stream) cudaStreamDestroy(h->stream);
   delete h;
   return TG_OK;
@@ -455,12 +589,15 @@ tg_status tg_set_state(tg_handle* h, const double* prim, int n_vertex, double t0
   if (!h || !prim) return fail(h, TG_INVALID_ARG, "NULL argument");
   if (n_vertex != h->L.nv) return fail(h, TG_INVALID_ARG, "n_vertex does not match the mesh");
   const int nv = h->L.nv;
-  for (int i = 0; i < nv; ++i) {
-    const double* q = prim + 5 * (size_t)h->L.old_of_new[i];
-    if (!(q[0] > 0.0) || !(q[4] > 0.0)) return fail(h, TG_INVALID_ARG, "state needs T > 0 and p > 0 (src/fv.cc:388-389)");
-    h->hP[i] = q[0]; h->hP[nv + i] = q[1]; h->hP[2 * (size_t)nv + i] = q[2]; h->hP[3 * (size_t)nv + i] = q[4];
-  }
-  TG_CUDA(h, cudaMemcpyAsync(h->sv.P, h->hP, 4 * (size_t)nv * sizeof(double), cudaMemcpyHostToDevice, h->stream));
+  tg_status st = state_h2d(h, prim, 5 * (size_t)nv * sizeof(double));
+  if (st != TG_OK) return st;
+  TG_CUDA(h, cudaMemsetAsync(h->bad, 0, sizeof(int), h->stream));
+  k_state_check<<<nblk(nv), kBlock, 0, h->stream>>>(nv, h->raw, h->bad);
+  k_state_in<<<nblk(nv), kBlock, 0, h->stream>>>(nv, h->raw, h->old_of_new, h->bad, h->sv.P);
+  int bad = 0;
+  TG_CUDA(h, cudaMemcpyAsync(&bad, h->bad, sizeof(int), cudaMemcpyDeviceToHost, h->stream));
+  if ((st = sync(h)) != TG_OK) return st;
+  if (bad) return fail(h, TG_INVALID_ARG, "state needs T > 0 and p > 0 (src/fv.cc:388-389)");
   k_prim2ent<<<nblk(nv), kBlock, 0, h->stream>>>(h->prm, nv, h->sv.P, h->sv.W);
   Scalars s;
   std::memset(&s, 0, sizeof(s));
@@ -481,14 +618,9 @@ tg_status tg_get_state(tg_handle* h, double* prim, int n_vertex) {
   if (!h || !prim) return fail(h, TG_INVALID_ARG, "NULL argument");
   if (n_vertex != h->L.nv) return fail(h, TG_INVALID_ARG, "n_vertex does not match the mesh");
   const int nv = h->L.nv;
-  TG_CUDA(h, cudaMemcpyAsync(h->hP, h->sv.P, 4 * (size_t)nv * sizeof(double), cudaMemcpyDeviceToHost, h->stream));
-  tg_status st = sync(h);
-  if (st != TG_OK) return st;
-  for (int i = 0; i < nv; ++i) {
-    double* q = prim + 5 * (size_t)h->L.old_of_new[i];
-    q[0] = h->hP[i]; q[1] = h->hP[nv + i]; q[2] = h->hP[2 * (size_t)nv + i]; q[3] = 0.0; q[4] = h->hP[3 * (size_t)nv + i];
-  }
-  return TG_OK;
+  k_state_out<<<nblk(nv), kBlock, 0, h->stream>>>(nv, h->sv.P, h->old_of_new, h->raw);
+  TG_CUDA(h, cudaGetLastError());
+  return state_d2h(h, prim, 5 * (size_t)nv * sizeof(double));
 }
 
 tg_status tg_store_conserved_old(tg_handle* h) {

@@ -104,6 +104,36 @@ __global__ void k_prim2ent(Params k, int nv, const double* __restrict__ P, doubl
   W[i] = e.f; W[nv + i] = e.vx; W[2 * nv + i] = e.vy; W[3 * nv + i] = e.l;
 }
 
+// A caller state arrives as PrimVar records (T, u, v, w, p) in the caller's
+// vertex order.  k_state_check flags any vertex the reference would refuse at
+// initialisation (src/fv.cc:388-389: T > 0 and p > 0, NaN refused too);
+// k_state_in then reorders into the device SoA only when nothing was flagged,
+// so a refused state leaves the previous one in place.
+__global__ void k_state_check(int nv, const double* __restrict__ raw, int* __restrict__ bad) {
+  int i = blockIdx.x * blockDim.x + threadIdx.x;
+  if (i >= nv) return;
+  const double* q = raw + 5 * (size_t)i;
+  if (!(q[0] > 0.0) || !(q[4] > 0.0)) atomicOr(bad, 1);
+}
+
+__global__ void k_state_in(int nv, const double* __restrict__ raw, const int* __restrict__ old_of_new,
+                           const int* __restrict__ bad, double* __restrict__ P) {
+  if (*bad) return;
+  int i = blockIdx.x * blockDim.x + threadIdx.x;
+  if (i >= nv) return;
+  const double* q = raw + 5 * (size_t)old_of_new[i];
+  P[i] = q[0]; P[nv + i] = q[1]; P[2 * (size_t)nv + i] = q[2]; P[3 * (size_t)nv + i] = q[4];
+}
+
+// Device SoA -> PrimVar records in the caller's order (w = 0 in 2D).
+__global__ void k_state_out(int nv, const double* __restrict__ P, const int* __restrict__ old_of_new,
+                            double* __restrict__ raw) {
+  int i = blockIdx.x * blockDim.x + threadIdx.x;
+  if (i >= nv) return;
+  double* q = raw + 5 * (size_t)old_of_new[i];
+  q[0] = P[i]; q[1] = P[nv + i]; q[2] = P[2 * (size_t)nv + i]; q[3] = 0.0; q[4] = P[3 * (size_t)nv + i];
+}
+
 // store_conserved_old (src/fv.cc:1626-1630)
 __global__ void k_store_old(Params k, MeshView m, StateView s, const int* __restrict__ done) {
   if (*done) return;

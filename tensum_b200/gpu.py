@@ -105,8 +105,14 @@ class Solver:
         prim = np.ascontiguousarray(prim, np.float64)
         self._chk(self.L.tg_set_state(self.h, _d(prim), self.nv, t0))
 
-    def get_state(self) -> np.ndarray:
-        out = np.empty((self.nv, 5))
+    def get_state(self, out: np.ndarray | None = None) -> np.ndarray:
+        """The state as (n_vertex, 5) PrimVar records; written into `out` when given
+        (C-contiguous float64, e.g. a view of pinned host memory, which is copied by DMA
+        without staging)."""
+        if out is None:
+            out = np.empty((self.nv, 5))
+        elif out.shape != (self.nv, 5) or out.dtype != np.float64 or not out.flags.c_contiguous:
+            raise ValueError("out must be a C-contiguous float64 array of shape (n_vertex, 5)")
         self._chk(self.L.tg_get_state(self.h, _d(out), self.nv))
         return out
 
