@@ -185,7 +185,7 @@ int tg_abi_version(void);
 
 /* ---- state ------------------------------------------------------------- */
 
-/* primitive[] <- prim_aos (T,u,v,w,p per vertex, PrimVar layout, src/primvar.h:17-18),
+/* primitive[] <- prim_aos (T,p,u,v,w per vertex: the PrimVar layout of src/primvar.h:17-18),
  * then entropy_var = prim2ent(primitive) (src/fv.cc:392-393).  Resets time to t0. */
 tg_status tg_set_state(tg_handle* h, const double* prim_aos, int n_vertex, double t0);
 /* prim_aos <- primitive[] (periodic copies receive their set's value). */

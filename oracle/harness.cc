@@ -16,7 +16,7 @@
 //
 // case_dir holds PARTITION/part_file_0.dat.  ic.bin (optional, "-" to use the
 // parameter file's initial condition) is n_vertex x 5 doubles in the reference
-// PrimVar order (T, u, v, w, p), indexed like the part file's active vertices.
+// PrimVar memory order (T, p, u, v, w), indexed like the part file's active vertices.
 // Full per-stage arrays are dumped for the first n_dump_steps steps; the state
 // after the last step is always dumped.  The wall time of the stepping loop is
 // written as record "wall_s" so the harness doubles as the reference CPU timer.
@@ -81,11 +81,11 @@ std::vector<double> prim_vec(const std::vector<PrimVar>& p) {
   std::vector<double> out;
   out.reserve(p.size() * 5);
   for (const auto& q : p) {
-    out.push_back(q.temperature);
+    out.push_back(q.temperature);   // PrimVar memory order (src/primvar.h:17-18)
+    out.push_back(q.pressure);
     out.push_back(q.velocity.x);
     out.push_back(q.velocity.y);
     out.push_back(q.velocity.z);
-    out.push_back(q.pressure);
   }
   return out;
 }
@@ -183,11 +183,11 @@ int main(int argc, char* argv[]) {
     ic.read(reinterpret_cast<char*>(buf.data()), (std::streamsize)(buf.size() * sizeof(double)));
     if (!ic) { std::fprintf(stderr, "short initial-condition file %s\n", argv[3]); return 2; }
     for (unsigned int i = 0; i < fv.grid.n_vertex; ++i) {
-      fv.primitive[i].temperature = buf[5 * i + 0];
-      fv.primitive[i].velocity.x = buf[5 * i + 1];
-      fv.primitive[i].velocity.y = buf[5 * i + 2];
-      fv.primitive[i].velocity.z = buf[5 * i + 3];
-      fv.primitive[i].pressure = buf[5 * i + 4];
+      fv.primitive[i].temperature = buf[5 * i + 0];   // PrimVar memory order (src/primvar.h:17-18)
+      fv.primitive[i].pressure = buf[5 * i + 1];
+      fv.primitive[i].velocity.x = buf[5 * i + 2];
+      fv.primitive[i].velocity.y = buf[5 * i + 3];
+      fv.primitive[i].velocity.z = buf[5 * i + 4];
       fv.entropy_var[i] = fv.param.material.prim2ent(fv.primitive[i]);
     }
   }

@@ -11,7 +11,7 @@
  * reference bit for bit (checked by tests/test_oracle_pinned.py against
  * fixtures produced by oracle/_ref/tensum_harness).
  *
- * Layouts match the reference: primitive (T,u,v,w,p), residual (mass,mx,my,mz,
+ * Layouts match the reference: primitive (T,p,u,v,w, the PrimVar memory order), residual (mass,mx,my,mz,
  * energy), gradient dE[v][var][xyz] with var order (V1,V2,V3,V4,V5).
  */
 #ifndef TENSUM_ORACLE_H

@@ -2,7 +2,7 @@
 
 Each case is a seeded stand-in for one of the reference's benchmark setups;
 initial conditions are returned in the reference's PrimVar order
-(T, u, v, w, p) per vertex (src/primvar.h:17-18), i.e. exactly the array a
+(T, p, u, v, w) per vertex (src/primvar.h:17-18), i.e. exactly the array a
 reference caller hands to ``tg_set_state``.
 """
 from __future__ import annotations
@@ -31,7 +31,7 @@ def vortex_ic(coords: np.ndarray, beta: float = 5.0, gamma: float = GAMMA,
     p = T ** (gamma / (gamma - 1.0))
     rho = p / (gas_const * T)
     T = p / (gas_const * rho)
-    return np.stack([T, u, v, np.zeros_like(T), p], axis=1)
+    return np.stack([T, p, u, v, np.zeros_like(T)], axis=1)
 
 
 def kh_mesh(n: int = 1025, seed: int = 0) -> _mesh.TriMesh:
@@ -57,7 +57,7 @@ def kh_ic(coords: np.ndarray, a: np.ndarray, phi: np.ndarray, gas_const: float =
     v = 0.01 * np.sum(a[None, :] * np.sin(2.0 * np.pi * k[None, :] * x[:, None] + phi[None, :]), axis=1)
     p = np.full_like(x, 2.5)
     T = p / (gas_const * rho)
-    return np.stack([T, u, v, np.zeros_like(T), p], axis=1)
+    return np.stack([T, p, u, v, np.zeros_like(T)], axis=1)
 
 
 def cylinder_mesh(n_r: int = 256, n_t: int = 512, seed: int = 0) -> _mesh.TriMesh:
@@ -78,7 +78,7 @@ def cylinder_freestream(mach: float = 0.2, angle_deg: float = 0.0, gamma: float 
 def cylinder_ic(coords: np.ndarray, mach: float = 0.2, angle_deg: float = 0.0) -> np.ndarray:
     T, u, v, p = cylinder_freestream(mach, angle_deg)
     n = coords.shape[0]
-    return np.stack([np.full(n, T), np.full(n, u), np.full(n, v), np.zeros(n), np.full(n, p)], axis=1)
+    return np.stack([np.full(n, T), np.full(n, p), np.full(n, u), np.full(n, v), np.zeros(n)], axis=1)
 
 
 def cylinder_viscosity(mach: float = 0.2, reynolds: float = 100.0, diameter: float = 1.0) -> float:

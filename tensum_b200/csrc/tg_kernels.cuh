@@ -104,7 +104,7 @@ __global__ void k_prim2ent(Params k, int nv, const double* __restrict__ P, doubl
   W[i] = e.f; W[nv + i] = e.vx; W[2 * nv + i] = e.vy; W[3 * nv + i] = e.l;
 }
 
-// A caller state arrives as PrimVar records (T, u, v, w, p) in the caller's
+// A caller state arrives as PrimVar records (T, p, u, v, w; src/primvar.h:17-18) in the caller's
 // vertex order.  k_state_check flags any vertex the reference would refuse at
 // initialisation (src/fv.cc:388-389: T > 0 and p > 0, NaN refused too);
 // k_state_in then reorders into the device SoA only when nothing was flagged,
@@ -113,7 +113,7 @@ __global__ void k_state_check(int nv, const double* __restrict__ raw, int* __res
   int i = blockIdx.x * blockDim.x + threadIdx.x;
   if (i >= nv) return;
   const double* q = raw + 5 * (size_t)i;
-  if (!(q[0] > 0.0) || !(q[4] > 0.0)) atomicOr(bad, 1);
+  if (!(q[0] > 0.0) || !(q[1] > 0.0)) atomicOr(bad, 1);
 }
 
 __global__ void k_state_in(int nv, const double* __restrict__ raw, const int* __restrict__ old_of_new,
@@ -122,16 +122,16 @@ __global__ void k_state_in(int nv, const double* __restrict__ raw, const int* __
   int i = blockIdx.x * blockDim.x + threadIdx.x;
   if (i >= nv) return;
   const double* q = raw + 5 * (size_t)old_of_new[i];
-  P[i] = q[0]; P[nv + i] = q[1]; P[2 * (size_t)nv + i] = q[2]; P[3 * (size_t)nv + i] = q[4];
+  P[i] = q[0]; P[nv + i] = q[2]; P[2 * (size_t)nv + i] = q[3]; P[3 * (size_t)nv + i] = q[1];
 }
 
-// Device SoA -> PrimVar records in the caller's order (w = 0 in 2D).
+// Device SoA (T, u, v, p) -> PrimVar records in the caller's order (w = 0 in 2D).
 __global__ void k_state_out(int nv, const double* __restrict__ P, const int* __restrict__ old_of_new,
                             double* __restrict__ raw) {
   int i = blockIdx.x * blockDim.x + threadIdx.x;
   if (i >= nv) return;
   double* q = raw + 5 * (size_t)old_of_new[i];
-  q[0] = P[i]; q[1] = P[nv + i]; q[2] = P[2 * (size_t)nv + i]; q[3] = 0.0; q[4] = P[3 * (size_t)nv + i];
+  q[0] = P[i]; q[1] = P[3 * (size_t)nv + i]; q[2] = P[nv + i]; q[3] = P[2 * (size_t)nv + i]; q[4] = 0.0;
 }
 
 // store_conserved_old (src/fv.cc:1626-1630)

@@ -59,8 +59,8 @@ def build_case(spec: dict):
         m = M.annulus(spec["nr"], spec["nt"], 0.5, 20.0, 0.3, spec["seed"])
         prim0 = cases.cylinder_ic(m.coords)
         # perturb so that gradients and viscous terms are non-trivial
-        prim0[:, 1] += 0.05 * np.sin(m.coords[:, 1])
-        prim0[:, 4] *= 1.0 + 0.01 * np.cos(m.coords[:, 0])
+        prim0[:, 2] += 0.05 * np.sin(m.coords[:, 1])   # u (PrimVar order T, p, u, v, w)
+        prim0[:, 1] *= 1.0 + 0.01 * np.cos(m.coords[:, 0])   # p
         wall = spec.get("wall", "noslip")
         if wall == "noslip":
             bnd = {1: ("noslip", WALL), 2: ("farfield", FAR)}

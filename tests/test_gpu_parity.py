@@ -99,7 +99,7 @@ def test_vortex_cfg0_mesh_1000_steps_matches_oracle():
 def test_cylinder_ns_multistep_matches_oracle(recon):
     m = M.annulus(16, 32, 0.5, 20.0, 0.05, seed=2)
     prim0 = cases.cylinder_ic(m.coords)
-    prim0[:, 2] += 0.02 * np.cos(m.coords[:, 0])
+    prim0[:, 3] += 0.02 * np.cos(m.coords[:, 0])   # v
     cfg = dict(flux="kepes_tecno_roe", reconstruct=recon, model="ns", mu_ref=0.002, tvb_M=1.0,
                boundary={1: ("noslip", {"xvelocity": 0.0, "yvelocity": 0.0, "zvelocity": 0.0}),
                          2: ("farfield", {"temperature": 1 / 1.4, "xvelocity": 0.2, "yvelocity": 0.0,

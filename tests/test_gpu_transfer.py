@@ -1,6 +1,6 @@
 """State transfers through tg_set_state / tg_get_state.
 
-The state crosses the boundary as PrimVar records (T, u, v, w, p) in the
+The state crosses the boundary as PrimVar records (T, p, u, v, w) in the
 caller's vertex order (src/fv.h PrimVar, src/fv.cc:388-389 for the check).
 The library reorders on the device and copies either by DMA straight from a
 pinned caller buffer or through its threaded pinned staging ring for a
@@ -34,7 +34,7 @@ def _pinned(shape):
 def test_round_trip_is_exact_pageable_and_pinned(n):
     s, prim0 = _solver(n)
     prim0 = prim0.copy()
-    prim0[:, 3] = 0.0
+    prim0[:, 4] = 0.0   # w
     s.set_state(prim0)
     assert np.array_equal(s.get_state(), prim0)
     out = _pinned(prim0.shape)
@@ -60,11 +60,11 @@ def test_refused_state_leaves_previous_state():
     s.step(1)
     before = s.get_state()
     bad = prim0.copy()
-    bad[123, 4] = -1.0
+    bad[123, 1] = -1.0   # p
     with pytest.raises(gpu.TensumError) as e:
         s.set_state(bad)
     assert abi.STATUS[e.value.status] == "TG_INVALID_ARG"
-    bad[123, 4] = prim0[123, 4]
+    bad[123, 1] = prim0[123, 1]
     bad[7, 0] = np.nan
     with pytest.raises(gpu.TensumError):
         s.set_state(bad)
