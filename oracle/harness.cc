@@ -13,6 +13,12 @@
 //
 // Usage:
 //   tensum_harness <param.in> <case_dir> <ic.bin|-> <n_steps> <n_dump_steps> <out.bin>
+//   tensum_harness <param.in> <case_dir> mc 0 0 <out.bin>
+//
+// The "mc" form runs the reference's own Monte Carlo driver FiniteVolume::run
+// (src/fv.cc:2401-2492: per-sample extract_rnd_nos + initial condition with
+// pert(), solve with increment_moments at every output time, reduce_moments)
+// and dumps the reduced moments of every output time instance.
 //
 // case_dir holds PARTITION/part_file_0.dat.  ic.bin (optional, "-" to use the
 // parameter file's initial condition) is n_vertex x 5 doubles in the reference
@@ -151,6 +157,45 @@ void dump_geometry(Dump& d, const Grid& g) {
   d.rec("periodic", periodic);
 }
 
+// One moment array of instance t as n_vertex x (5 + extras): PrimVar memory
+// order, then density, mach, entropy, vorticity when present.
+std::vector<double> moment_vec(FiniteVolume& fv, unsigned t, int which) {
+  const std::vector<PrimVar>& P = which == 0 ? fv.primitive_fm[t] : which == 1 ? fv.primitive_sm[t] : fv.primitive_variance[t];
+  std::vector<double> out;
+  for (unsigned i = 0; i < fv.grid.n_vertex; ++i) {
+    const PrimVar& q = P[i];
+    out.push_back(q.temperature); out.push_back(q.pressure);
+    out.push_back(q.velocity.x); out.push_back(q.velocity.y); out.push_back(q.velocity.z);
+    if (fv.has_density) out.push_back(which == 0 ? fv.density_fm[t][i] : which == 1 ? fv.density_sm[t][i] : fv.density_variance[t][i]);
+    if (fv.has_mach) out.push_back(which == 0 ? fv.mach_fm[t][i] : which == 1 ? fv.mach_sm[t][i] : fv.mach_variance[t][i]);
+    if (fv.has_entropy) out.push_back(which == 0 ? fv.entropy_fm[t][i] : which == 1 ? fv.entropy_sm[t][i] : fv.entropy_variance[t][i]);
+    if (fv.has_vorticity) out.push_back(which == 0 ? fv.vorticity_fm[t][i] : which == 1 ? fv.vorticity_sm[t][i] : fv.vorticity_variance[t][i]);
+  }
+  return out;
+}
+
+int run_mc(char* param, char* case_dir, const char* out) {
+  Dump dump(out);
+  FiniteVolume fv(param, case_dir);
+  // found_stop_file is never initialised in the reference (src/fv.h:171) yet
+  // gates reduce_moments (src/fv.cc:2462); its stop-file check is commented
+  // out, so the intended value is false.
+  fv.found_stop_file = false;
+  fv.run();
+  dump.rec("time_instance", fv.time_instance);
+  dump.rec("n_samples", std::vector<double>(1, (double)fv.param.n_samples));
+  for (unsigned t = 0; t < fv.time_instance.size(); ++t) {
+    std::ostringstream tg;
+    tg << "m" << t << "_";
+    dump.rec(tg.str() + "fm", moment_vec(fv, t, 0));
+    dump.rec(tg.str() + "sm", moment_vec(fv, t, 1));
+    dump.rec(tg.str() + "var", moment_vec(fv, t, 2));
+  }
+  dump.rec("prim_final", prim_vec(fv.primitive));
+  mpi_finalize();
+  return 0;
+}
+
 }  // namespace
 
 int main(int argc, char* argv[]) {
@@ -164,6 +209,7 @@ int main(int argc, char* argv[]) {
   PERIODIC = false;
   dim = two;
   debug = restart = preprocess = bounds = verbose = false;
+  if (std::strcmp(argv[3], "mc") == 0) return run_mc(argv[1], argv[2], argv[6]);
 
   const long n_steps = std::atol(argv[4]);
   const long n_dump = std::atol(argv[5]);

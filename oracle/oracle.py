@@ -50,6 +50,12 @@ def lib():
         L.tor_num_flux.argtypes = [vp] + [dp] * 8
         L.tor_logavg.argtypes = [C.c_double, C.c_double]
         L.tor_logavg.restype = C.c_double
+        L.tor_counter.argtypes = [vp]
+        L.tor_moment_nvars.argtypes = [C.c_int]
+        L.tor_moments_increment.argtypes = [vp, C.c_long, C.c_int, dp, dp, dp]
+        L.tor_moments_merge.argtypes = [C.c_int, C.c_int, C.c_long, dp, dp, dp, C.c_long, dp, dp, dp]
+        L.tor_moments_merge.restype = C.c_long
+        L.tor_moments_finalize.argtypes = [C.c_int, C.c_int, C.c_long, dp, dp]
         _lib = L
     return _lib
 
@@ -125,3 +131,43 @@ class Oracle:
         b = C.c_double()
         self.L.tor_global(self.h, C.byref(a), C.byref(b))
         return a.value, b.value
+
+
+def moment_nvars(extras: int) -> int:
+    return lib().tor_moment_nvars(extras)
+
+
+def moments_merge(n_old, fm, sm, m2, n_other, fm_o, sm_o, m2_o):
+    """reduce_moments' merge of one received group into (fm, sm, m2), in place; returns the new count."""
+    nv, nvar = fm.shape
+    return lib().tor_moments_merge(nv, nvar, n_old, _d(fm), _d(sm), _d(m2), n_other,
+                                   _d(np.ascontiguousarray(fm_o)), _d(np.ascontiguousarray(sm_o)),
+                                   _d(np.ascontiguousarray(m2_o)))
+
+
+def moments_finalize(n, sm, m2):
+    nv, nvar = sm.shape
+    lib().tor_moments_finalize(nv, nvar, n, _d(sm), _d(m2))
+
+
+def run_mc(problem, ics, n_instances: int, extras: int):
+    """The reference's per-group Monte Carlo loop (src/fv.cc:2401-2466 with
+    solve's increment_moments calls, src/fv.cc:2230-2380) over the given
+    initial states, unsteady mode.  Returns the raw (unscaled) group moments
+    fm, sm, m2 of shape (n_instances, n_vertex, nvars)."""
+    o = Oracle(problem)
+    L = o.L
+    nvar = L.tor_moment_nvars(extras)
+    shape = (n_instances, o.nv, nvar)
+    fm, sm, m2 = np.zeros(shape), np.zeros(shape), np.zeros(shape)
+    for k, ic in enumerate(ics, 1):
+        o.set_prim(ic)
+        L.tor_compute_gradients(o.h, None)       # solve() starts with compute_gradients
+        L.tor_moments_increment(o.h, k, extras, _d(fm[0]), _d(sm[0]), _d(m2[0]))
+        for t in range(1, n_instances):
+            while L.tor_counter(o.h) <= t:
+                done, _ = o.step(1)
+                if done == 0:
+                    raise RuntimeError("oracle run ended before output instance %d" % t)
+            L.tor_moments_increment(o.h, k, extras, _d(fm[t]), _d(sm[t]), _d(m2[t]))
+    return fm, sm, m2

@@ -34,6 +34,9 @@ def param_text(cfg: dict) -> str:
     Keys: flux, reconstruct, tvb_M, model ('euler'|'ns'), mu_ref, prandtl,
     gamma, gas_const, cfl, time_mode, time_step, final_time, max_iter,
     time_stamps, ev_alpha, ev_beta, boundary: {tag: (type, {var: expr})}.
+    Monte Carlo keys: samples (list of sample ids), rnd_per_sample,
+    ic ({variable: fparser expression}), constants ({name: value}),
+    online_stat (bool), variables (extra moment variables, e.g. ["density"]).
     """
     flux = cfg.get("flux", "kepes_tecno_roe")
     recon = cfg.get("reconstruct", "minmod")
@@ -47,6 +50,15 @@ def param_text(cfg: dict) -> str:
         body = "\n".join(f"      {k}   {v}" for k, v in vals.items())
         bnd.append(f"   {tag}\n   {{\n      type   {btype}\n{body}\n   }}")
     bnd_text = "\n".join(bnd)
+    samples = "\n".join(f"         {int(s)}" for s in cfg.get("samples", []))
+    ic = cfg.get("ic", {})
+    ic_text = "\n".join(f"   {v}  {ic.get(v, d)}" for v, d in (("temperature", "1.0"), ("xvelocity", "0.0"),
+                                                                ("yvelocity", "0.0"), ("zvelocity", "0.0"),
+                                                                ("pressure", "1.0")))
+    consts = cfg.get("constants", {"dummy": 0.0})
+    const_text = "\n".join(f"   {k} {v:.17g}" for k, v in consts.items())
+    var_text = "\n".join(f"      {v}" for v in cfg.get("variables", []))
+    online = "yes" if cfg.get("online_stat", False) else "no"
     return f"""grid
 {{
    cell      median
@@ -73,10 +85,11 @@ numeric
       }}
       free_list
       {{
+{samples}
       }}
    }}
    rnd_file_loc    rnd_nos.dat
-   rnd_per_sample  0
+   rnd_per_sample  {int(cfg.get('rnd_per_sample', 0))}
 }}
 
 material
@@ -107,16 +120,12 @@ material
 
 constants
 {{
-   dummy 0.0
+{const_text}
 }}
 
 initial_condition
 {{
-   temperature  1.0
-   xvelocity    0.0
-   yvelocity    0.0
-   zvelocity    0.0
-   pressure     1.0
+{ic_text}
 }}
 
 boundary
@@ -138,9 +147,10 @@ output
    format                vtk
    frequency             100000000
    time_stamps           {cfg.get('time_stamps', 1)}
-   use_online_stat_tool  no
+   use_online_stat_tool  {online}
    variables
    {{
+{var_text}
    }}
    surfaces
    {{
@@ -171,8 +181,12 @@ def read_dump(path: str) -> dict:
 
 
 def run_case(mesh, cfg: dict, prim0: np.ndarray | None, n_steps: int, n_dump: int,
-             workdir: str | None = None, timeout: float = 3600.0) -> dict:
-    """Write the case, run the harness, return the parsed dump."""
+             workdir: str | None = None, timeout: float = 3600.0, rnd_rows: dict | None = None) -> dict:
+    """Write the case, run the harness, return the parsed dump.
+
+    With prim0 None the reference evaluates the parameter file's initial
+    condition itself (fparser, with pert() reading rnd_rows for the first
+    sample of cfg["samples"])."""
     from tensum_b200.mesh import write_part_file  # local import: tests put repo on sys.path
 
     if not harness_available():
@@ -184,6 +198,9 @@ def run_case(mesh, cfg: dict, prim0: np.ndarray | None, n_steps: int, n_dump: in
             write_part_file(mesh, wd)
         with open(os.path.join(wd, "param.in"), "w") as fh:
             fh.write(param_text(cfg))
+        if rnd_rows is not None:
+            with open(os.path.join(wd, "rnd_nos.dat"), "w") as fh:
+                fh.write(rnd_file_text(rnd_rows))
         ic = "-"
         if prim0 is not None:
             ic = os.path.join(wd, "ic.bin")
@@ -201,3 +218,45 @@ def run_case(mesh, cfg: dict, prim0: np.ndarray | None, n_steps: int, n_dump: in
         if own:
             import shutil
             shutil.rmtree(wd, ignore_errors=True)
+
+
+def rnd_file_text(rows: dict) -> str:
+    """The reference's random-number file (src/fv.cc:502-551): the number of rows,
+    then one row per sample: sample id followed by its random numbers."""
+    lines = [str(len(rows))]
+    for sid in sorted(rows):
+        lines.append(" ".join([str(int(sid))] + [repr(float(x)) for x in rows[sid]]))
+    return "\n".join(lines) + "\n"
+
+
+def run_mc(mesh, cfg: dict, rnd_rows: dict, timeout: float = 3600.0) -> dict:
+    """Run the reference's own Monte Carlo driver (FiniteVolume::run) on a case.
+
+    cfg carries the MC keys of param_text (samples, rnd_per_sample, ic,
+    online_stat=True, ...); rnd_rows maps sample id -> random numbers.  Returns
+    the dump: time_instance, n_samples, m{t}_fm / m{t}_sm / m{t}_var per output
+    instance (n_vertex x (5 + extras), PrimVar memory order then the extra
+    variables) and prim_final (the last sample's final state).
+    """
+    from tensum_b200.mesh import write_part_file
+
+    if not harness_available():
+        raise RuntimeError("oracle/_ref/tensum_harness is not built (make -C oracle ref)")
+    wd = tempfile.mkdtemp(prefix="tensum_mc_")
+    try:
+        write_part_file(mesh, wd)
+        with open(os.path.join(wd, "param.in"), "w") as fh:
+            fh.write(param_text(dict(cfg, online_stat=True)))
+        with open(os.path.join(wd, "rnd_nos.dat"), "w") as fh:
+            fh.write(rnd_file_text(rnd_rows))
+        out = os.path.join(wd, "dump.bin")
+        r = subprocess.run([HARNESS, "param.in", ".", "mc", "0", "0", out],
+                           cwd=wd, capture_output=True, text=True, timeout=timeout)
+        if r.returncode != 0 or not os.path.exists(out):
+            raise RuntimeError(f"reference MC run failed ({r.returncode}):\n{r.stdout[-2000:]}\n{r.stderr[-2000:]}")
+        if "ERROR" in r.stdout:
+            raise RuntimeError("reference MC run reported an error:\n" + r.stdout[-2000:])
+        return read_dump(out)
+    finally:
+        import shutil
+        shutil.rmtree(wd, ignore_errors=True)

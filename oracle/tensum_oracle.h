@@ -51,7 +51,18 @@ void tor_num_flux(const tor_state* s, const double* cl, const double* cr, const 
                   double* flux5);
 double tor_logavg(double a, double b);
 
+/* Monte Carlo moments (increment_moments src/fv.cc:595-694, reduce_moments
+ * src/reduce_moments.cc:14-221).  Records per vertex: PrimVar (T,p,u,v,w),
+ * then density, mach, entropy, vorticity as selected by the bits of extras. */
+int tor_counter(const tor_state* s);   /* next output-time index (FiniteVolume::counter) */
+int tor_moment_nvars(int extras);
+void tor_moments_increment(const tor_state* s, long k, int extras, double* fm, double* sm, double* m2);
+long tor_moments_merge(int nv, int nvar, long n_old, double* fm, double* sm, double* m2, long n_other,
+                       const double* fm_o, const double* sm_o, const double* m2_o);
+void tor_moments_finalize(int nv, int nvar, long n, double* sm, double* m2);
+
 #ifdef __cplusplus
 }
+
 #endif
 #endif

@@ -47,6 +47,37 @@ def kh_coefficients(seed: int, n_modes: int = 10):
     return a, phi
 
 
+KH_RND_PER_SAMPLE = 20
+
+
+def kh_rnd_row(seed: int, n_modes: int = 10) -> np.ndarray:
+    """One sample's random numbers in the layout of the reference's rnd file
+    (src/fv.cc:502-551): r_1..r_M are the amplitudes a_k ~ U[0,1] and
+    r_{M+1}..r_{2M} the phases as fractions of a turn, phi_k = 2 pi r_{M+k}."""
+    rng = np.random.default_rng(seed)
+    return rng.uniform(0.0, 1.0, 2 * n_modes)
+
+
+def kh_ic_rnd(coords: np.ndarray, row: np.ndarray, gas_const: float = 1.0) -> np.ndarray:
+    """The Kelvin-Helmholtz initial state of one Monte Carlo sample from its
+    random-number row.  It is the value of the parameter-file initial condition
+
+        yvelocity  0.01*(pert(4,x,y,1)*sin(2*pi*1*x+2*pi*pert(4,x,y,M+1)) + ...
+                         + pert(4,x,y,M)*sin(2*pi*M*x+2*pi*pert(4,x,y,2M)))
+
+    (pert type 4 returns r_id, src/perturb.cc:196-208) with the shear layer of
+    kh_ic, summed over the modes in order."""
+    m = row.size // 2
+    x, y = coords[:, 0], coords[:, 1]
+    s = np.zeros_like(x)
+    for k in range(1, m + 1):
+        s = s + row[k - 1] * np.sin(2.0 * np.pi * k * x + 2.0 * np.pi * row[m + k - 1])
+    inside = np.abs(y - 0.5) < 0.25
+    rho = np.where(inside, 2.0, 1.0)
+    p = np.full_like(x, 2.5)
+    return np.stack([p / (gas_const * rho), p, np.where(inside, 0.5, -0.5), 0.01 * s, np.zeros_like(x)], axis=1)
+
+
 def kh_ic(coords: np.ndarray, a: np.ndarray, phi: np.ndarray, gas_const: float = 1.0) -> np.ndarray:
     """Kelvin-Helmholtz shear layer with a multimodal vertical-velocity perturbation."""
     x, y = coords[:, 0], coords[:, 1]

@@ -75,3 +75,31 @@ def build_case(spec: dict):
                tvb_M=spec.get("tvb_M", 1.0), ev_alpha=spec.get("ev_alpha", 0.0), ev_beta=spec.get("ev_beta", 0.0),
                time_stamps=1, cfl=0.8)
     return m, cfg, prim0
+
+
+# Monte Carlo case: Kelvin-Helmholtz samples whose perturbation comes from the
+# rnd file through pert(4, ...) in the parameter file, run by the reference's
+# own MC driver with online statistics.
+MC_CASE = dict(n=17, seed=2, samples=[0, 1, 2, 3, 4], rnd_seed_base=100, flux="kepes_tecno_rusanov",
+               reconstruct="minmod", final_time=0.06, time_stamps=3,
+               variables=["density", "mach", "entropy", "vorticity"])
+MC_EXTRAS = 1 | 2 | 4 | 8   # density, mach, entropy, vorticity
+
+
+def kh_expressions(n_modes: int = 10) -> dict:
+    """fparser initial condition equal to tensum_b200.cases.kh_ic_rnd."""
+    terms = " + ".join(f"pert(4,x,y,{k})*sin(2*pi*{k}*x+2*pi*pert(4,x,y,{n_modes + k}))"
+                       for k in range(1, n_modes + 1))
+    return {"temperature": "2.5/(1+(abs(y-0.5)<0.25))", "xvelocity": "(abs(y-0.5)<0.25)-0.5",
+            "yvelocity": f"0.01*({terms})", "zvelocity": "0.0", "pressure": "2.5"}
+
+
+def build_mc_case(spec: dict = MC_CASE):
+    """Mesh, reference configuration and per-sample random rows of the MC case."""
+    m = M.periodic_square(spec["n"], 0.0, 1.0, 0.0, 1.0, spec["seed"])
+    rows = {s: cases.kh_rnd_row(spec["rnd_seed_base"] + s) for s in spec["samples"]}
+    cfg = dict(flux=spec["flux"], reconstruct=spec["reconstruct"], boundary=dict(PERIODIC4),
+               final_time=spec["final_time"], time_stamps=spec["time_stamps"], cfl=0.8,
+               samples=list(spec["samples"]), rnd_per_sample=cases.KH_RND_PER_SAMPLE, ic=kh_expressions(),
+               variables=list(spec["variables"]))
+    return m, cfg, rows

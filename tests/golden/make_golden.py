@@ -23,7 +23,7 @@ ROOT = os.path.dirname(os.path.dirname(os.path.dirname(os.path.abspath(__file__)
 sys.path.insert(0, ROOT)
 sys.path.insert(0, os.path.join(ROOT, "oracle"))
 
-from tests.golden.cases_spec import CASES, build_case  # noqa: E402
+from tests.golden.cases_spec import build_mc_case, MC_CASE, CASES, build_case  # noqa: E402
 import ref_runner  # noqa: E402
 
 OUT = os.path.dirname(os.path.abspath(__file__))
@@ -39,6 +39,23 @@ def main():
         keep["prim_in"] = prim0.ravel()
         np.savez_compressed(os.path.join(OUT, f"{name}.npz"), spec=np.array(json.dumps(spec)), **keep)
         print(name, "vertices", mesh.n_vertex, "records", len(keep))
+    make_mc()
+
+
+def make_mc():
+    """mc_kh.npz: the reference MC driver's reduced moments and each sample's
+    initial state as the reference evaluates it (fparser + pert from the rnd file)."""
+    mesh, cfg, rows = build_mc_case()
+    d = ref_runner.run_mc(mesh, cfg, rows)
+    ics = []
+    for s in cfg["samples"]:
+        one = ref_runner.run_case(mesh, dict(cfg, samples=[s]), None, 0, 0, rnd_rows=rows)
+        ics.append(one["prim0"].reshape(-1, 5))
+    keep = {k: v for k, v in d.items() if k.startswith("m") or k in ("time_instance", "n_samples")}
+    keep["ics"] = np.stack(ics)
+    keep["rows"] = np.stack([rows[s] for s in cfg["samples"]])
+    np.savez_compressed(os.path.join(OUT, "mc_kh.npz"), spec=np.array(json.dumps(MC_CASE)), **keep)
+    print("mc_kh vertices", mesh.n_vertex, "instances", len(d["time_instance"]), "samples", int(d["n_samples"][0]))
 
 
 if __name__ == "__main__":

@@ -12,7 +12,9 @@ GOLDEN = os.path.join(ROOT, "tests", "golden")
 
 
 def golden_names():
-    return sorted(os.path.basename(p)[:-4] for p in glob.glob(os.path.join(GOLDEN, "*.npz")))
+    """Single-solve fixtures (the Monte Carlo fixtures mc_*.npz have their own tests)."""
+    return sorted(os.path.basename(p)[:-4] for p in glob.glob(os.path.join(GOLDEN, "*.npz"))
+                  if not os.path.basename(p).startswith("mc_"))
 
 
 def load_golden(name):
