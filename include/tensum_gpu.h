@@ -226,6 +226,39 @@ tg_status tg_step(tg_handle* h, int n_steps, double* info4);
 /* Global kinetic energy and entropy integrals, compute_global (src/fv.cc:2175-2225). */
 tg_status tg_global(tg_handle* h, double* ke_out, double* entropy_out);
 
+/* Steps, as tg_step, until output time `instance` has been reached (the
+ * unsteady counter of src/fv.cc:2317-2336 exceeds it), the run is over, or
+ * max_steps steps have been issued (a step past the stop is a no-op).
+ * info5 (may be NULL): tg_step's four values, then the output-time counter. */
+tg_status tg_advance(tg_handle* h, int instance, long max_steps, double* info5);
+
+/* ---- Monte Carlo moments ---------------------------------------------- */
+/* The per-group online statistics of increment_moments (src/fv.cc:595-694) and
+ * their reduction over groups, reduce_moments (src/reduce_moments.cc:14-221).
+ * Per output instance the handle keeps fm (running mean), sm (sum of squares)
+ * and m2 (sum of squared deviations), each n_vertex records of nvar doubles:
+ * PrimVar (T, p, u, v, w), then density, mach, entropy and vorticity for the
+ * bits 1, 2, 4, 8 of `extras` (the output section's write_variables), in the
+ * order reduce_moments packs them.  Host arrays are in the caller's vertex
+ * order; device group blocks (tg_moments_export) are three [nvar][n_vertex]
+ * arrays fm, sm, m2 in the handle's internal vertex order. */
+tg_status tg_moments_init(tg_handle* h, int n_instances, int extras);
+/* increment_moments at output `instance` for the k-th sample of the group
+ * (k = 1 starts the group).  Vorticity uses the gradients of the state's
+ * last residual evaluation, or of the state itself before its first step. */
+tg_status tg_moments_increment(tg_handle* h, int instance, long k);
+/* Raw group moments of one instance to host arrays (any may be NULL). */
+tg_status tg_moments_get(tg_handle* h, int instance, double* fm, double* sm, double* m2);
+/* The group block of one instance into caller device memory (3*nvar*n_vertex doubles). */
+tg_status tg_moments_export(tg_handle* h, int instance, void* dev_dst);
+/* Merge another group (n_other samples) into this one (n_self samples), the
+ * per-group update of reduce_moments; from host arrays or a device block. */
+tg_status tg_moments_merge(tg_handle* h, int instance, long n_self, long n_other, const double* fm_other,
+                           const double* sm_other, const double* m2_other);
+tg_status tg_moments_merge_device(tg_handle* h, int instance, long n_self, long n_other, const void* dev_group);
+/* reduce_moments' final scaling for n samples in all: m2 /= (n-1), sm /= n. */
+tg_status tg_moments_finalize(tg_handle* h, int instance, long n);
+
 /* ---- measurement (no counterpart in the reference, whose Timer class,
  *      src/timer.h:8-72, wraps MPI_Wtime around each phase) -------------- */
 

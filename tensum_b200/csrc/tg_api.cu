@@ -10,6 +10,7 @@
 #include <cstdlib>
 #include <cstring>
 #include <algorithm>
+#include <climits>
 #include <new>
 #include <string>
 #include <thread>
@@ -71,6 +72,10 @@ struct tg_handle {
   int* bad = nullptr;                 // device flag of k_state_check
   cudaEvent_t raw_ready = nullptr;
   Stager stage;
+  // Monte Carlo moments: per output instance three [nvar][nv] arrays (fm, sm, m2)
+  int mom_ninst = 0, mom_extras = 0, mom_nvar = 0;
+  double* mom = nullptr;
+  double* mom_in = nullptr;   // upload area for a host-side group in tg_moments_merge
   size_t device_bytes = 0;
   int kernels_per_step = 0;
   int kernels_per_flux = 0;
@@ -572,6 +577,8 @@ tg_status tg_destroy(tg_handle* h) {
   if (h->graph) cudaGraphDestroy(h->graph);
   if (h->stream) cudaStreamSynchronize(h->stream);
   for (void* p : h->allocs) cudaFree(p);
+  if (h->mom) cudaFree(h->mom);
+  if (h->mom_in) cudaFree(h->mom_in);
   for (int t = 0; t < Stager::kMaxLanes; ++t) {
     if (h->stage.st[t]) cudaStreamSynchronize(h->stage.st[t]);
     for (int k = 0; k < 2; ++k)
@@ -610,6 +617,7 @@ tg_status tg_set_state(tg_handle* h, const double* prim, int n_vertex, double t0
     while (s.counter < h->ctl.ntinst - 1 && s.counter * dti <= t0) s.counter++;
   }
   s.dtmin_bits = 0x7ff0000000000000ull;
+  s.stop_counter = INT_MAX;
   TG_CUDA(h, cudaMemcpyAsync(h->sc, &s, sizeof(s), cudaMemcpyHostToDevice, h->stream));
   return sync(h);
 }
@@ -735,6 +743,169 @@ tg_status tg_step(tg_handle* h, int n_steps, double* info4) {
   if (info4) { info4[0] = s.elapsed; info4[1] = s.dt_global; info4[2] = s.rtotal; info4[3] = (double)s.iter; }
   if (s.bad) return fail(h, TG_BAD_STATE, "non-finite or non-positive state produced by an update");
   return TG_OK;
+}
+
+}  // extern "C"
+
+// ---- output-time stepping and Monte Carlo moments
+
+namespace {
+
+// The solve loop's continuation test (src/fv.cc:2273-2275) on the host copy of the scalars.
+bool run_over(const tg_handle* h, const Scalars& s) {
+  const bool go = s.rtotal > h->ctl.min_residue && (h->ctl.time_mode == 1 || s.iter < h->ctl.max_iter) &&
+                  s.elapsed < h->ctl.final_time;
+  return !go;
+}
+
+double* mom_array(tg_handle* h, int instance, int which) {
+  return h->mom + ((size_t)instance * 3 + which) * (size_t)h->mom_nvar * h->L.nv;
+}
+
+tg_status mom_check(tg_handle* h, int instance) {
+  if (!h) return fail(h, TG_INVALID_ARG, "NULL handle");
+  if (!h->mom) return fail(h, TG_INVALID_ARG, "tg_moments_init has not been called");
+  if (instance < 0 || instance >= h->mom_ninst) return fail(h, TG_INVALID_ARG, "output instance out of range");
+  return TG_OK;
+}
+
+}  // namespace
+
+extern "C" {
+
+tg_status tg_advance(tg_handle* h, int instance, long max_steps, double* info5) {
+  if (!h) return fail(h, TG_INVALID_ARG, "NULL handle");
+  if (max_steps < 0) return fail(h, TG_INVALID_ARG, "max_steps < 0");
+  tg_status st = capture_step_graph(h);
+  if (st != TG_OK) return st;
+  int stop = instance;
+  TG_CUDA(h, cudaMemcpyAsync(&h->sc->stop_counter, &stop, sizeof(int), cudaMemcpyHostToDevice, h->stream));
+  Scalars s;
+  if ((st = read_scalars(h, &s)) != TG_OK) return st;
+  long launched = 0;
+  while (launched < max_steps && !s.bad && s.counter <= instance && !run_over(h, s)) {
+    const long chunk = std::min<long>(16, max_steps - launched);
+    for (long i = 0; i < chunk; ++i) TG_CUDA(h, cudaGraphLaunch(h->graph_exec, h->stream));
+    launched += chunk;
+    if ((st = read_scalars(h, &s)) != TG_OK) return st;
+  }
+  stop = INT_MAX;
+  TG_CUDA(h, cudaMemcpyAsync(&h->sc->stop_counter, &stop, sizeof(int), cudaMemcpyHostToDevice, h->stream));
+  if ((st = sync(h)) != TG_OK) return st;
+  if (info5) {
+    info5[0] = s.elapsed; info5[1] = s.dt_global; info5[2] = s.rtotal; info5[3] = (double)s.iter;
+    info5[4] = (double)s.counter;
+  }
+  if (s.bad) return fail(h, TG_BAD_STATE, "non-finite or non-positive state produced by an update");
+  return TG_OK;
+}
+
+tg_status tg_moments_init(tg_handle* h, int n_instances, int extras) {
+  if (!h) return fail(h, TG_INVALID_ARG, "NULL handle");
+  if (n_instances < 1 || extras < 0 || extras > 15) return fail(h, TG_INVALID_ARG, "bad moment layout");
+  if (h->mom) { cudaFree(h->mom); h->mom = nullptr; }
+  if (h->mom_in) { cudaFree(h->mom_in); h->mom_in = nullptr; }
+  h->mom_ninst = n_instances;
+  h->mom_extras = extras;
+  h->mom_nvar = 5 + ((extras & 1) + ((extras >> 1) & 1) + ((extras >> 2) & 1) + ((extras >> 3) & 1));
+  const size_t bytes = (size_t)n_instances * 3 * h->mom_nvar * h->L.nv * sizeof(double);
+  TG_CUDA(h, cudaMalloc((void**)&h->mom, bytes));
+  TG_CUDA(h, cudaMemsetAsync(h->mom, 0, bytes, h->stream));
+  return sync(h);
+}
+
+tg_status tg_moments_increment(tg_handle* h, int instance, long k) {
+  tg_status st = mom_check(h, instance);
+  if (st != TG_OK) return st;
+  if (k < 1) return fail(h, TG_INVALID_ARG, "sample index k starts at 1");
+  if (h->mom_extras & 8) {
+    // vorticity reads dE: the gradients of the initial state before the first
+    // step (solve starts with compute_gradients, src/fv.cc:2237), else those of
+    // the last stage's input (buffer 2), which the step left in G when its
+    // fluxes needed gradients
+    Scalars s;
+    if ((st = read_scalars(h, &s)) != TG_OK) return st;
+    if (s.iter == 0) enqueue_gradient(h, 0, false, true, h->never);
+    else if (!h->grads_needed) enqueue_gradient(h, 2, false, true, h->never);
+  }
+  k_moments_increment<<<nblk(h->L.nv), kBlock, 0, h->stream>>>(h->prm, h->L.nv, h->sv.P, h->sv.G, h->mom_extras,
+                                                                 h->mom_nvar, (long long)k, mom_array(h, instance, 0),
+                                                                 mom_array(h, instance, 1), mom_array(h, instance, 2));
+  return sync(h);
+}
+
+tg_status tg_moments_get(tg_handle* h, int instance, double* fm, double* sm, double* m2) {
+  tg_status st = mom_check(h, instance);
+  if (st != TG_OK) return st;
+  const size_t nv = h->L.nv, nvar = h->mom_nvar;
+  std::vector<double> buf(3 * nvar * nv);
+  TG_CUDA(h, cudaMemcpyAsync(buf.data(), mom_array(h, instance, 0), buf.size() * sizeof(double),
+                             cudaMemcpyDeviceToHost, h->stream));
+  if ((st = sync(h)) != TG_OK) return st;
+  double* out[3] = {fm, sm, m2};
+  for (int w = 0; w < 3; ++w) {
+    if (!out[w]) continue;
+    const double* src = buf.data() + (size_t)w * nvar * nv;
+    for (size_t i = 0; i < nv; ++i) {
+      double* d = out[w] + nvar * (size_t)h->L.old_of_new[i];
+      for (size_t c = 0; c < nvar; ++c) d[c] = src[c * nv + i];
+    }
+  }
+  return TG_OK;
+}
+
+tg_status tg_moments_export(tg_handle* h, int instance, void* dev_dst) {
+  tg_status st = mom_check(h, instance);
+  if (st != TG_OK) return st;
+  if (!dev_dst) return fail(h, TG_INVALID_ARG, "NULL destination");
+  TG_CUDA(h, cudaMemcpyAsync(dev_dst, mom_array(h, instance, 0), 3 * (size_t)h->mom_nvar * h->L.nv * sizeof(double),
+                             cudaMemcpyDeviceToDevice, h->stream));
+  return sync(h);
+}
+
+tg_status tg_moments_merge_device(tg_handle* h, int instance, long n_self, long n_other, const void* dev_group) {
+  tg_status st = mom_check(h, instance);
+  if (st != TG_OK) return st;
+  if (!dev_group || n_self < 0 || n_other < 0 || n_self + n_other < 1) return fail(h, TG_INVALID_ARG, "bad group");
+  const size_t n = (size_t)h->mom_nvar * h->L.nv;
+  const long n_new = n_self + n_other;
+  const double fact1 = (double)n_other / (double)n_new;
+  const double fact2 = fact1 * (double)n_self;
+  const double* g = (const double*)dev_group;
+  k_moments_merge<<<(unsigned)((n + kBlock - 1) / kBlock), kBlock, 0, h->stream>>>(
+      n, fact1, fact2, mom_array(h, instance, 0), mom_array(h, instance, 1), mom_array(h, instance, 2), g, g + n,
+      g + 2 * n);
+  return sync(h);
+}
+
+tg_status tg_moments_merge(tg_handle* h, int instance, long n_self, long n_other, const double* fm_o,
+                           const double* sm_o, const double* m2_o) {
+  tg_status st = mom_check(h, instance);
+  if (st != TG_OK) return st;
+  if (!fm_o || !sm_o || !m2_o) return fail(h, TG_INVALID_ARG, "NULL group array");
+  const size_t nv = h->L.nv, nvar = h->mom_nvar;
+  std::vector<double> buf(3 * nvar * nv);
+  const double* in[3] = {fm_o, sm_o, m2_o};
+  for (int w = 0; w < 3; ++w) {
+    double* dst = buf.data() + (size_t)w * nvar * nv;
+    for (size_t i = 0; i < nv; ++i) {
+      const double* s = in[w] + nvar * (size_t)h->L.old_of_new[i];
+      for (size_t c = 0; c < nvar; ++c) dst[c * nv + i] = s[c];
+    }
+  }
+  if (!h->mom_in) TG_CUDA(h, cudaMalloc((void**)&h->mom_in, buf.size() * sizeof(double)));
+  TG_CUDA(h, cudaMemcpyAsync(h->mom_in, buf.data(), buf.size() * sizeof(double), cudaMemcpyHostToDevice, h->stream));
+  return tg_moments_merge_device(h, instance, n_self, n_other, h->mom_in);
+}
+
+tg_status tg_moments_finalize(tg_handle* h, int instance, long n) {
+  tg_status st = mom_check(h, instance);
+  if (st != TG_OK) return st;
+  if (n < 2) return fail(h, TG_INVALID_ARG, "moments need at least two samples (src/parameter.cc:804-805)");
+  const size_t m = (size_t)h->mom_nvar * h->L.nv;
+  k_moments_scale<<<(unsigned)((m + kBlock - 1) / kBlock), kBlock, 0, h->stream>>>(
+      m, 1.0 / ((double)n - 1.0), 1.0 / (double)n, mom_array(h, instance, 1), mom_array(h, instance, 2));
+  return sync(h);
 }
 
 tg_status tg_global(tg_handle* h, double* ke, double* ent) {

@@ -58,6 +58,7 @@ struct Scalars {
   int done;
   int bad;
   unsigned long long dtmin_bits;
+  int stop_counter;    // steps stop once counter exceeds it (output-time stepping)
 };
 
 struct Control {
@@ -307,7 +308,7 @@ __global__ void k_dt(Params k, MeshView m, StateView s, Scalars* sc, const int* 
 __global__ void k_step_begin(Control ctl, Scalars* sc, int* done) {
   // unsteady runs never advance the iteration bound (term_iter stays 0, src/fv.cc:2266-2268)
   bool go = sc->rtotal > ctl.min_residue && (ctl.time_mode == 1 || sc->iter < ctl.max_iter) &&
-            sc->elapsed < ctl.final_time;
+            sc->elapsed < ctl.final_time && sc->counter <= sc->stop_counter;
   *done = go ? 0 : 1;
   sc->dtmin_bits = 0x7ff0000000000000ull;
 }
@@ -480,6 +481,65 @@ __global__ void k_global(Params k, MeshView m, StateView s) {
     __syncthreads();
   }
   if (threadIdx.x == 0) { s.part[(size_t)blockIdx.x * 4] = red[0][0]; s.part[(size_t)blockIdx.x * 4 + 1] = red[1][0]; }
+}
+
+// ------------------------------------------------------------ MC moments
+// increment_moments (src/fv.cc:595-694) for the k-th sample of a group, one
+// thread per vertex.  Moment arrays are [var][vertex] with the per-vertex
+// record of the reference's reduce_moments packing: PrimVar (T, p, u, v, w)
+// then density, mach, entropy, vorticity as selected by `extras` (bits 0-3).
+// Vorticity (src/material.h:623-627) reads the entropy-variable gradients G of
+// the last gradient pass: V2 = 2 beta u, V3 = 2 beta v, V5 = -2 beta.
+__global__ void k_moments_increment(Params k, int nv, const double* __restrict__ P, const double* __restrict__ G,
+                                    int extras, int nvar, long long kk, double* __restrict__ fm,
+                                    double* __restrict__ sm, double* __restrict__ m2) {
+  int i = blockIdx.x * blockDim.x + threadIdx.x;
+  if (i >= nv) return;
+  Prim q = load_prim(P, nv, i);
+  double x[9];
+  x[0] = q.T; x[1] = q.p; x[2] = q.u; x[3] = q.v; x[4] = 0.0;
+  int j = 5;
+  if (extras & 1) x[j++] = density(k, q);
+  if (extras & 2) x[j++] = sqrt(q.u * q.u + q.v * q.v) / sound_speed(k, q);
+  if (extras & 4) x[j++] = entropy_fn(k, q);
+  if (extras & 8)
+    x[j++] = k.R * q.T * (G[4 * (size_t)nv + i] + q.v * G[6 * (size_t)nv + i] - G[3 * (size_t)nv + i] -
+                          q.u * G[7 * (size_t)nv + i]);
+  const double K = (double)kk, c1 = 1.0 / K, c2 = (K - 1.0) / K;
+  for (int c = 0; c < nvar; ++c) {
+    const size_t o = (size_t)c * nv + i;
+    const double xc = x[c];
+    if (kk == 1) {
+      fm[o] = xc; sm[o] = xc * xc; m2[o] = 0.0;
+    } else {
+      const double mkm1 = fm[o];
+      const double mk = c < 5 ? xc * c1 + mkm1 * c2 : mkm1 + (xc - mkm1) / K;   // PrimVar::equ / scalar form
+      fm[o] = mk;
+      sm[o] += xc * xc;
+      m2[o] += (xc - mkm1) * (xc - mk);
+    }
+  }
+}
+
+// One received group of reduce_moments (src/reduce_moments.cc:36-113).
+__global__ void k_moments_merge(size_t n, double fact1, double fact2, double* __restrict__ fm,
+                                double* __restrict__ sm, double* __restrict__ m2, const double* __restrict__ fo,
+                                const double* __restrict__ so, const double* __restrict__ mo) {
+  size_t j = blockIdx.x * (size_t)blockDim.x + threadIdx.x;
+  if (j >= n) return;
+  const double diff = fo[j] - fm[j];
+  fm[j] += diff * fact1;
+  m2[j] += mo[j] + (diff * diff) * fact2;
+  sm[j] += so[j];
+}
+
+// Final scaling of reduce_moments (src/reduce_moments.cc:115-141).
+__global__ void k_moments_scale(size_t n, double fact3, double fact4, double* __restrict__ sm,
+                                double* __restrict__ m2) {
+  size_t j = blockIdx.x * (size_t)blockDim.x + threadIdx.x;
+  if (j >= n) return;
+  m2[j] *= fact3;
+  sm[j] *= fact4;
 }
 
 }  // namespace tg

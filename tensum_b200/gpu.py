@@ -18,7 +18,9 @@ LIB_PATH = os.path.join(HERE, "libtensum_b200.so")
 
 EXPORTS = ["tg_create", "tg_destroy", "tg_last_error", "tg_abi_version", "tg_set_state", "tg_get_state",
            "tg_store_conserved_old", "tg_compute_dt", "tg_gradients", "tg_residual", "tg_update",
-           "tg_residual_norm", "tg_end_step", "tg_step", "tg_global", "tg_stream", "tg_time_phase", "tg_query"]
+           "tg_residual_norm", "tg_end_step", "tg_step", "tg_global", "tg_stream", "tg_time_phase", "tg_query",
+           "tg_advance", "tg_moments_init", "tg_moments_increment", "tg_moments_get", "tg_moments_export",
+           "tg_moments_merge", "tg_moments_merge_device", "tg_moments_finalize"]
 
 PHASE = {"gradient": 0, "flux": 1, "update": 2, "dt": 3, "step": 4}
 QUERY = {"n_vertex": 0, "n_edge": 1, "n_bface": 2, "kernels_per_step": 3, "device_bytes": 4, "kernels_per_flux": 5}
@@ -60,6 +62,14 @@ def load():
     L.tg_stream.argtypes = [vp, C.POINTER(vp)]
     L.tg_time_phase.argtypes = [vp, i, i, dp]
     L.tg_query.argtypes = [vp, i, dp]
+    L.tg_advance.argtypes = [vp, i, C.c_long, dp]
+    L.tg_moments_init.argtypes = [vp, i, i]
+    L.tg_moments_increment.argtypes = [vp, i, C.c_long]
+    L.tg_moments_get.argtypes = [vp, i, dp, dp, dp]
+    L.tg_moments_export.argtypes = [vp, i, vp]
+    L.tg_moments_merge.argtypes = [vp, i, C.c_long, C.c_long, dp, dp, dp]
+    L.tg_moments_merge_device.argtypes = [vp, i, C.c_long, C.c_long, vp]
+    L.tg_moments_finalize.argtypes = [vp, i, C.c_long]
     for name in EXPORTS:
         f = getattr(L, name)
         if name not in ("tg_last_error", "tg_abi_version"):
@@ -157,6 +167,40 @@ class Solver:
         a, b = C.c_double(), C.c_double()
         self._chk(self.L.tg_global(self.h, C.byref(a), C.byref(b)))
         return a.value, b.value
+
+    # ---- output-time stepping and Monte Carlo moments
+    def advance(self, instance: int, max_steps: int = 1 << 40) -> np.ndarray:
+        """Step until output time `instance` is reached; returns elapsed, dt,
+        residual, iterations and the output-time counter."""
+        info = np.empty(5)
+        self._chk(self.L.tg_advance(self.h, instance, max_steps, _d(info)))
+        return info
+
+    def moments_init(self, n_instances: int, extras: int = 0):
+        self._chk(self.L.tg_moments_init(self.h, n_instances, extras))
+        self.mom_nvar = 5 + bin(extras).count("1")
+
+    def moments_increment(self, instance: int, k: int):
+        self._chk(self.L.tg_moments_increment(self.h, instance, k))
+
+    def moments_get(self, instance: int):
+        """Raw group moments (fm, sm, m2) of one instance, each (n_vertex, nvar)."""
+        out = [np.empty((self.nv, self.mom_nvar)) for _ in range(3)]
+        self._chk(self.L.tg_moments_get(self.h, instance, *[_d(a) for a in out]))
+        return out
+
+    def moments_export(self, instance: int, dev_ptr: int):
+        self._chk(self.L.tg_moments_export(self.h, instance, C.c_void_p(dev_ptr)))
+
+    def moments_merge(self, instance: int, n_self: int, n_other: int, fm, sm, m2):
+        arrs = [np.ascontiguousarray(a, np.float64) for a in (fm, sm, m2)]
+        self._chk(self.L.tg_moments_merge(self.h, instance, n_self, n_other, *[_d(a) for a in arrs]))
+
+    def moments_merge_device(self, instance: int, n_self: int, n_other: int, dev_ptr: int):
+        self._chk(self.L.tg_moments_merge_device(self.h, instance, n_self, n_other, C.c_void_p(dev_ptr)))
+
+    def moments_finalize(self, instance: int, n: int):
+        self._chk(self.L.tg_moments_finalize(self.h, instance, n))
 
     def stream_ptr(self) -> int:
         """cudaStream_t of this handle (for torch.cuda.ExternalStream / CUDA events)."""
