@@ -288,6 +288,65 @@ typedef enum {
 } tg_query_key;
 tg_status tg_query(tg_handle* h, int key, double* out);
 
+/* ---- batched FP32 ensembles (no counterpart in the reference, which runs
+ *      one sample after another per MC group, src/fv.cc:2440-2456) ------- */
+/* A batch advances every sample of one or more levels (a fully periodic mesh
+ * and its samples; up to 4 levels, e.g. a multilevel hierarchy) together, one
+ * CUDA graph per time step.  Members are FP32 ([component][vertex][sample]
+ * with samples innermost); geometry is formed in FP64, the near-equal branch
+ * of the log mean runs in FP64, each sample keeps its own FP64 clock and dt
+ * (the per-sample time step of src/fv.cc:1499-1618), and ensemble moments
+ * are accumulated in FP64.  Euler, kepes_tecno_roe / kepes_tecno_rusanov /
+ * kepec, first-order or minmod reconstruction, unsteady SSP-RK3. */
+typedef struct tg_batch tg_batch;
+typedef struct tg_batch_level {
+  const tg_mesh* mesh;
+  const tg_bc_table* bc;       /* every boundary tag periodic */
+  int n_samples;               /* a positive multiple of 32 */
+} tg_batch_level;
+tg_status tg_batch_create(const tg_batch_level* levels, int n_levels, const tg_material* mat, const tg_options* opt,
+                          tg_batch** out);
+tg_status tg_batch_destroy(tg_batch* b);
+const char* tg_batch_last_error(const tg_batch* b);
+/* One sample's state from PrimVar records (caller vertex order); its clock restarts at t = 0. */
+tg_status tg_batch_set_state(tg_batch* b, int level, int sample, const double* prim_aos, int n_vertex);
+tg_status tg_batch_get_state(tg_batch* b, int level, int sample, double* prim_aos, int n_vertex);
+/* Every sample of a level from its random-number row (n_samples x n_rnd, the
+ * rnd-file layout of src/fv.cc:502-551), generated on the device: the
+ * Kelvin-Helmholtz layer with v' = 0.01 sum_k r_k sin(2 pi k x + 2 pi r_{M+k}),
+ * M = n_rnd / 2 (pert type 4, src/perturb.cc:196-208). */
+tg_status tg_batch_set_kh(tg_batch* b, int level, const double* rows, int n_rnd);
+/* Steps until every sample has reached output time `instance` (samples that
+ * arrive first hold), the run is over, or max_steps steps were issued.
+ * info4 (may be NULL): steps issued, min and max elapsed time, samples flagged bad. */
+tg_status tg_batch_advance(tg_batch* b, int instance, long max_steps, double* info4);
+/* Per-sample elapsed time, output counter and bad flag (any may be NULL). */
+tg_status tg_batch_clock(tg_batch* b, int level, double* elapsed, int* counter, int* bad);
+/* FP64 ensemble moments of a level's current states, the per-group recurrence of
+ * increment_moments applied in sample order (mean by Welford, m2 the sum of
+ * squared deviations, sm a Kahan-compensated sum of squares).  Records as for
+ * tg_moments_get, extras bits 1 density, 2 mach, 4 entropy. */
+tg_status tg_batch_moments(tg_batch* b, int level, int extras, double* fm, double* sm, double* m2);
+/* Launch shape of the flux and gradient kernels (sample tile x block size,
+ * enumerated by TG_BQ_N_SHAPES), and the autotuner that times every shape for
+ * `steps` steps from the current state (restored afterwards) and keeps the
+ * fastest; ms_out (may be NULL) gets one time per shape. */
+tg_status tg_batch_set_shape(tg_batch* b, int shape);
+tg_status tg_batch_tune(tg_batch* b, int steps, int* shape_out, double* ms_out);
+/* Device time per step over `steps` steps (the batch advances). */
+tg_status tg_batch_time_steps(tg_batch* b, int steps, double* ms_per_step);
+tg_status tg_batch_stream(tg_batch* b, void** stream_out);
+typedef enum {
+  TG_BQ_N_LEVELS = 0,
+  TG_BQ_KERNELS_PER_STEP = 1,
+  TG_BQ_DEVICE_BYTES = 2,
+  TG_BQ_SHAPE = 3,
+  TG_BQ_SAMPLE_TILE = 4,
+  TG_BQ_BLOCK = 5,
+  TG_BQ_N_SHAPES = 6
+} tg_batch_query_key;
+tg_status tg_batch_query(tg_batch* b, int key, double* out);
+
 /* ---- allocation-free residual norm ------------------------------------ */
 
 #define TG_NOALLOC_MAX_VERTICES 268435456

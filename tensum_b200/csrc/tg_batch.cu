@@ -1,0 +1,601 @@
+// tg_batch.cu -- C ABI of the batched FP32 Monte Carlo ensembles (tensum_gpu.h,
+// "batched ensembles").
+//
+// A batch holds one or more levels (a periodic mesh and its samples); every
+// level advances in the same launches.  One time step of the whole batch is
+// captured once into a CUDA graph and replayed; the launch shape (sample tile
+// and block size of the flux and gradient kernels) is chosen by tg_batch_tune.
+#include <cuda_runtime.h>
+
+#include <algorithm>
+#include <climits>
+#include <cmath>
+#include <cstring>
+#include <new>
+#include <string>
+#include <vector>
+
+#include "../../include/tensum_gpu.h"
+#include "tg_batch.cuh"
+#include "tg_mesh.h"
+
+using namespace tg;
+using namespace tg::batch;
+
+namespace {
+
+thread_local std::string g_batch_error;
+
+struct LevelHost {
+  HostLayout L;
+  int S = 0;
+  std::vector<void*> allocs;
+};
+
+struct Shape {
+  int st, bs;
+};
+const Shape kShapes[] = {{32, 256}, {32, 128}, {16, 256}, {16, 128}};
+
+}  // namespace
+
+struct tg_batch {
+  int device = 0;
+  cudaStream_t stream = nullptr;
+  int nlev = 0;
+  LevelHost lh[kMaxLevels];
+  Batch B{};
+  BParams prm{};
+  int* stop = nullptr;           // device stop counter (read by kb_step_begin)
+  double* tinst = nullptr;
+  int shape = 0;                 // index into kShapes
+  int dt_chunks = 1;
+  cudaGraphExec_t graph_exec = nullptr;
+  cudaGraph_t graph = nullptr;
+  std::vector<void*> allocs;
+  std::string err;
+  size_t device_bytes = 0;
+};
+
+namespace {
+
+tg_status bfail(tg_batch* b, tg_status st, const std::string& msg) {
+  if (b) b->err = msg;
+  g_batch_error = msg;
+  return st;
+}
+
+#define TB_CUDA(b, call)                                                                          \
+  do {                                                                                            \
+    cudaError_t e_ = (call);                                                                      \
+    if (e_ != cudaSuccess)                                                                        \
+      return bfail((b), TG_CUDA_ERROR, std::string(#call " failed: ") + cudaGetErrorString(e_)); \
+  } while (0)
+
+template <class T>
+tg_status balloc(tg_batch* b, size_t n, T** out) {
+  void* p = nullptr;
+  const size_t bytes = std::max<size_t>(1, n) * sizeof(T);
+  cudaError_t e = cudaMalloc(&p, bytes);
+  if (e != cudaSuccess) return bfail(b, TG_CUDA_ERROR, std::string("cudaMalloc: ") + cudaGetErrorString(e));
+  b->allocs.push_back(p);
+  b->device_bytes += bytes;
+  e = cudaMemset(p, 0, bytes);
+  if (e != cudaSuccess) return bfail(b, TG_CUDA_ERROR, std::string("cudaMemset: ") + cudaGetErrorString(e));
+  *out = (T*)p;
+  return TG_OK;
+}
+
+template <class T, class U>
+tg_status bupload(tg_batch* b, const std::vector<U>& v, const T** out) {
+  T* p = nullptr;
+  tg_status st = balloc(b, v.size(), &p);
+  if (st != TG_OK) return st;
+  std::vector<T> tmp(v.begin(), v.end());
+  if (!tmp.empty()) TB_CUDA(b, cudaMemcpy(p, tmp.data(), tmp.size() * sizeof(T), cudaMemcpyHostToDevice));
+  *out = p;
+  return TG_OK;
+}
+
+tg_status bsync(tg_batch* b) {
+  TB_CUDA(b, cudaGetLastError());
+  TB_CUDA(b, cudaStreamSynchronize(b->stream));
+  return TG_OK;
+}
+
+// Sets the warp offsets of every level for sample tile st; returns the total.
+template <int ST>
+long long layout_warps(Batch& B) {
+  long long w = 0;
+  for (int l = 0; l < B.nlev; ++l) {
+    B.lev[l].w_begin = w;
+    w += level_warps<ST>(B.lev[l].m.nv, B.lev[l].S);
+  }
+  B.work = w;
+  return w;
+}
+
+typedef void (*FluxK)(Batch, BParams, int);
+
+template <int F, int R>
+FluxK flux_kernel_fr(int shape) {
+  switch (shape) {
+    case 0: return kb_flux_update<F, R, 32, 256>;
+    case 1: return kb_flux_update<F, R, 32, 128>;
+    case 2: return kb_flux_update<F, R, 16, 256>;
+    default: return kb_flux_update<F, R, 16, 128>;
+  }
+}
+
+template <int F>
+FluxK flux_kernel_f(int recon, int shape) {
+  return recon == RECON_FIRST ? flux_kernel_fr<F, RECON_FIRST>(shape) : flux_kernel_fr<F, RECON_TVD_MINMOD>(shape);
+}
+
+FluxK flux_kernel(int flux, int recon, int shape) {
+  switch (flux) {
+    case FLUX_TECNO_ROE: return flux_kernel_f<FLUX_TECNO_ROE>(recon, shape);
+    case FLUX_TECNO_RUSANOV: return flux_kernel_f<FLUX_TECNO_RUSANOV>(recon, shape);
+    default: return flux_kernel_fr<FLUX_KEPEC, RECON_FIRST>(shape);
+  }
+}
+
+bool needs_grad(const tg_batch* b) {
+  return b->prm.recon != RECON_FIRST && (b->prm.flux == FLUX_TECNO_ROE || b->prm.flux == FLUX_TECNO_RUSANOV);
+}
+
+int max_samples(const tg_batch* b) {
+  int m = 0;
+  for (int l = 0; l < b->nlev; ++l) m = std::max(m, b->B.lev[l].S);
+  return m;
+}
+
+// One full step of every level on b->stream.
+void enqueue_step(tg_batch* b) {
+  const Shape sh = kShapes[b->shape];
+  Batch B = b->B;
+  if (sh.st == 32) layout_warps<32>(B); else layout_warps<16>(B);
+  const dim3 gs((max_samples(b) + 255) / 256, b->nlev);
+  kb_step_begin<<<gs, 256, 0, b->stream>>>(B, b->prm);
+  long long dt_blocks = 0;
+  for (int l = 0; l < b->nlev; ++l) dt_blocks += (long long)(B.lev[l].S >> 5) * b->dt_chunks;
+  kb_dt<8><<<(unsigned)dt_blocks, 256, 0, b->stream>>>(B, b->prm, b->dt_chunks);
+  kb_dt_final<<<gs, 256, 0, b->stream>>>(B, b->prm);
+  const unsigned blocks = (unsigned)((B.work * 32 + sh.bs - 1) / sh.bs);
+  FluxK fk = flux_kernel(b->prm.flux, b->prm.recon, b->shape);
+  for (int r = 0; r < 3; ++r) {
+    if (needs_grad(b)) {
+      if (sh.st == 32) kb_grad<32><<<blocks, sh.bs, 0, b->stream>>>(B, b->prm, r);
+      else kb_grad<16><<<blocks, sh.bs, 0, b->stream>>>(B, b->prm, r);
+    }
+    fk<<<blocks, sh.bs, 0, b->stream>>>(B, b->prm, r);
+  }
+  kb_step_end<<<gs, 256, 0, b->stream>>>(B, b->prm);
+}
+
+int kernels_per_step(const tg_batch* b) { return 4 + 3 * (needs_grad(b) ? 2 : 1); }
+
+void drop_graph(tg_batch* b) {
+  if (b->graph_exec) cudaGraphExecDestroy(b->graph_exec);
+  if (b->graph) cudaGraphDestroy(b->graph);
+  b->graph_exec = nullptr;
+  b->graph = nullptr;
+}
+
+tg_status capture(tg_batch* b) {
+  if (b->graph_exec) return TG_OK;
+  TB_CUDA(b, cudaStreamBeginCapture(b->stream, cudaStreamCaptureModeThreadLocal));
+  enqueue_step(b);
+  cudaError_t e = cudaStreamEndCapture(b->stream, &b->graph);
+  if (e != cudaSuccess) return bfail(b, TG_CUDA_ERROR, std::string("graph capture: ") + cudaGetErrorString(e));
+  TB_CUDA(b, cudaGraphInstantiate(&b->graph_exec, b->graph, 0));
+  return TG_OK;
+}
+
+struct ClockHost {
+  std::vector<double> elapsed;
+  std::vector<int> counter, bad;
+};
+
+tg_status read_clock(tg_batch* b, int l, ClockHost& c) {
+  const int S = b->B.lev[l].S;
+  c.elapsed.resize(S); c.counter.resize(S); c.bad.resize(S);
+  TB_CUDA(b, cudaMemcpyAsync(c.elapsed.data(), b->B.lev[l].c.elapsed, S * sizeof(double), cudaMemcpyDeviceToHost, b->stream));
+  TB_CUDA(b, cudaMemcpyAsync(c.counter.data(), b->B.lev[l].c.counter, S * sizeof(int), cudaMemcpyDeviceToHost, b->stream));
+  TB_CUDA(b, cudaMemcpyAsync(c.bad.data(), b->B.lev[l].c.bad, S * sizeof(int), cudaMemcpyDeviceToHost, b->stream));
+  return bsync(b);
+}
+
+// Every sample of every level is past output `instance`, finished, or bad.
+tg_status all_reached(tg_batch* b, int instance, bool* yes, int* nbad) {
+  *yes = true;
+  *nbad = 0;
+  for (int l = 0; l < b->nlev; ++l) {
+    ClockHost c;
+    tg_status st = read_clock(b, l, c);
+    if (st != TG_OK) return st;
+    for (int s = 0; s < b->B.lev[l].S; ++s) {
+      if (c.bad[s]) { ++*nbad; continue; }
+      if (c.counter[s] <= instance && c.elapsed[s] < b->prm.final_time) *yes = false;
+    }
+  }
+  return TG_OK;
+}
+
+tg_status reset_clock(tg_batch* b, int l, int s0, int n) {
+  const LevelClock& c = b->B.lev[l].c;
+  std::vector<double> z(n, 0.0);
+  std::vector<int> one(n, 1), zero(n, 0);
+  TB_CUDA(b, cudaMemcpyAsync(c.elapsed + s0, z.data(), n * sizeof(double), cudaMemcpyHostToDevice, b->stream));
+  TB_CUDA(b, cudaMemcpyAsync(c.counter + s0, one.data(), n * sizeof(int), cudaMemcpyHostToDevice, b->stream));
+  TB_CUDA(b, cudaMemcpyAsync(c.reached + s0, zero.data(), n * sizeof(int), cudaMemcpyHostToDevice, b->stream));
+  TB_CUDA(b, cudaMemcpyAsync(c.bad + s0, zero.data(), n * sizeof(int), cudaMemcpyHostToDevice, b->stream));
+  return bsync(b);
+}
+
+}  // namespace
+
+extern "C" {
+
+tg_status tg_batch_create(const tg_batch_level* levels, int n_levels, const tg_material* mat, const tg_options* opt,
+                          tg_batch** out) {
+  if (!out) return bfail(nullptr, TG_INVALID_ARG, "out is NULL");
+  *out = nullptr;
+  if (!levels || !mat || !opt || n_levels < 1 || n_levels > kMaxLevels)
+    return bfail(nullptr, TG_INVALID_ARG, "need 1 to 4 levels, a material and options");
+  int ndev = 0;
+  if (cudaGetDeviceCount(&ndev) != cudaSuccess || ndev == 0)
+    return bfail(nullptr, TG_NO_DEVICE, "no CUDA device visible; the GPU path has no CPU fallback");
+  if (mat->model != 0) return bfail(nullptr, TG_NOT_SUPPORTED, "batched ensembles are Euler only");
+  if (!(mat->flux_scheme == FLUX_TECNO_ROE || mat->flux_scheme == FLUX_TECNO_RUSANOV || mat->flux_scheme == FLUX_KEPEC))
+    return bfail(nullptr, TG_NOT_SUPPORTED, "batched ensembles run kepes_tecno_roe, kepes_tecno_rusanov or kepec");
+  if (!(mat->reconstruct_scheme == RECON_FIRST || mat->reconstruct_scheme == RECON_TVD_MINMOD))
+    return bfail(nullptr, TG_NOT_SUPPORTED, "batched ensembles reconstruct first order or with minmod");
+  if (opt->time_scheme != TG_TIME_SSPRK3 || opt->time_mode != TG_UNSTEADY || !(opt->cfl > 0.0) || opt->time_step > 0.0 ||
+      opt->n_time_stamps <= 0)
+    return bfail(nullptr, TG_NOT_SUPPORTED, "batched ensembles run unsteady SSP-RK3 with a CFL time step");
+  tg_batch* b = new (std::nothrow) tg_batch();
+  if (!b) return bfail(nullptr, TG_INVALID_ARG, "out of host memory");
+  cudaGetDevice(&b->device);
+  b->nlev = n_levels;
+  b->B.nlev = n_levels;
+  tg_status st;
+  for (int l = 0; l < n_levels; ++l) {
+    if (!levels[l].mesh || levels[l].n_samples < 32 || levels[l].n_samples % 32 != 0) {
+      tg_batch_destroy(b);
+      return bfail(nullptr, TG_INVALID_ARG, "every level needs a mesh and a positive multiple of 32 samples");
+    }
+    LevelHost& H = b->lh[l];
+    std::string msg = build_layout(*levels[l].mesh, levels[l].bc, false, H.L);
+    if (!msg.empty()) { tg_batch_destroy(b); return bfail(nullptr, TG_INVALID_ARG, msg); }
+    if (H.L.nb != 0) {
+      tg_batch_destroy(b);
+      return bfail(nullptr, TG_NOT_SUPPORTED, "batched ensembles need fully periodic meshes");
+    }
+    H.S = levels[l].n_samples;
+    const HostLayout& L = H.L;
+    Level& V = b->B.lev[l];
+    V.S = H.S;
+    LevelMesh& m = V.m;
+    m.nv = L.nv; m.ne = L.ne;
+    // geometry formed in FP64, stored in FP32
+    std::vector<double> ux(L.ne), uy(L.ne), ar(L.ne);
+    for (int e = 0; e < L.ne; ++e) {
+      const double a = std::sqrt(L.e_nx[e] * L.e_nx[e] + L.e_ny[e] * L.e_ny[e]);
+      const double ia = 1.0 / a;
+      ux[e] = L.e_nx[e] * ia; uy[e] = L.e_ny[e] * ia; ar[e] = a;
+    }
+#define BU(vec, field) \
+    if ((st = bupload(b, vec, &m.field)) != TG_OK) { tg_batch_destroy(b); return st; }
+    BU(L.e_a, e_a) BU(L.e_b, e_b) BU(ux, ux) BU(uy, uy) BU(ar, ar) BU(L.e_nx, nx) BU(L.e_ny, ny)
+    BU(L.e_dx, dx) BU(L.e_dy, dy) BU(L.e_g0x, g0x) BU(L.e_g0y, g0y) BU(L.e_g1x, g1x) BU(L.e_g1y, g1y)
+    BU(L.ce_off, ce_off) BU(L.ce_ent, ce_ent) BU(L.dcarea, area) BU(L.inv6mc, inv6mc) BU(L.x, x) BU(L.y, y)
+#undef BU
+    const size_t vs = (size_t)L.nv * H.S;
+    for (int r = 0; r < 3; ++r)
+      if ((st = balloc(b, kQ * vs, &V.Q[r])) != TG_OK) { tg_batch_destroy(b); return st; }
+    if ((st = balloc(b, 4 * vs, &V.Uold)) != TG_OK) { tg_batch_destroy(b); return st; }
+    if (mat->reconstruct_scheme != RECON_FIRST && mat->flux_scheme != FLUX_KEPEC) {
+      if ((st = balloc(b, kG * vs, &V.G)) != TG_OK) { tg_batch_destroy(b); return st; }
+    }
+    LevelClock& c = V.c;
+    if ((st = balloc(b, H.S, &c.elapsed)) != TG_OK || (st = balloc(b, H.S, &c.dt)) != TG_OK ||
+        (st = balloc(b, H.S, &c.dtmin_bits)) != TG_OK || (st = balloc(b, H.S, &c.counter)) != TG_OK ||
+        (st = balloc(b, H.S, &c.reached)) != TG_OK || (st = balloc(b, H.S, &c.active)) != TG_OK ||
+        (st = balloc(b, H.S, &c.bad)) != TG_OK) {
+      tg_batch_destroy(b);
+      return st;
+    }
+  }
+  BParams& k = b->prm;
+  k.gamma = (float)mat->gamma; k.R = (float)mat->gas_const;
+  k.inv_gm1 = (float)(1.0 / (mat->gamma - 1.0)); k.inv_gamma = (float)(1.0 / mat->gamma);
+  k.sqrt_gm1 = (float)std::sqrt(mat->gamma - 1.0); k.cfl = (float)opt->cfl;
+  k.ev_alpha = (float)mat->ev_mod_alpha; k.ev_beta = (float)mat->ev_mod_beta;
+  k.final_time = opt->final_time;
+  k.flux = mat->flux_scheme; k.recon = mat->reconstruct_scheme;
+  // output time instances (src/fv.cc:52-62)
+  std::vector<double> ti;
+  const double dti = opt->final_time / opt->n_time_stamps;
+  for (int i = 0; i <= opt->n_time_stamps; ++i) ti.push_back(i * dti);
+  const double* tip = nullptr;
+  if ((st = bupload(b, ti, &tip)) != TG_OK) { tg_batch_destroy(b); return st; }
+  k.tinst = tip;
+  k.ntinst = (int)ti.size();
+  if ((st = balloc(b, 1, &b->stop)) != TG_OK) { tg_batch_destroy(b); return st; }
+  k.stop_counter = INT_MAX;
+  k.stop = b->stop;
+  int inf = INT_MAX;
+  cudaMemcpy(b->stop, &inf, sizeof(int), cudaMemcpyHostToDevice);
+  // dt kernel: about four blocks per SM over all sample groups
+  long long groups = 0;
+  for (int l = 0; l < n_levels; ++l) groups += b->B.lev[l].S >> 5;
+  int sms = 148;
+  cudaDeviceGetAttribute(&sms, cudaDevAttrMultiProcessorCount, b->device);
+  b->dt_chunks = (int)std::max<long long>(1, (4LL * sms + groups - 1) / groups);
+  cudaError_t e = cudaStreamCreateWithFlags(&b->stream, cudaStreamNonBlocking);
+  if (e != cudaSuccess) { tg_batch_destroy(b); return bfail(nullptr, TG_CUDA_ERROR, cudaGetErrorString(e)); }
+  for (int l = 0; l < n_levels; ++l)
+    if ((st = reset_clock(b, l, 0, b->B.lev[l].S)) != TG_OK) { tg_batch_destroy(b); return st; }
+  *out = b;
+  return TG_OK;
+}
+
+tg_status tg_batch_destroy(tg_batch* b) {
+  if (!b) return TG_OK;
+  drop_graph(b);
+  if (b->stream) cudaStreamSynchronize(b->stream);
+  for (void* p : b->allocs) cudaFree(p);
+  if (b->stream) cudaStreamDestroy(b->stream);
+  delete b;
+  return TG_OK;
+}
+
+const char* tg_batch_last_error(const tg_batch* b) { return b ? b->err.c_str() : g_batch_error.c_str(); }
+
+tg_status tg_batch_set_state(tg_batch* b, int level, int sample, const double* prim_aos, int n_vertex) {
+  if (!b || !prim_aos || level < 0 || level >= b->nlev) return bfail(b, TG_INVALID_ARG, "bad level or NULL state");
+  const Level& V = b->B.lev[level];
+  const HostLayout& L = b->lh[level].L;
+  if (sample < 0 || sample >= V.S || n_vertex != L.nv) return bfail(b, TG_INVALID_ARG, "bad sample or vertex count");
+  std::vector<float> q((size_t)kQ * L.nv);
+  const double g = b->prm.gamma;
+  for (int i = 0; i < L.nv; ++i) {
+    const double* p = prim_aos + 5 * (size_t)L.old_of_new[i];   // PrimVar T, p, u, v, w
+    const double T = p[0], pr = p[1], u = p[2], v = p[3];
+    if (!(T > 0.0) || !(pr > 0.0)) return bfail(b, TG_INVALID_ARG, "state needs T > 0 and p > 0 (src/fv.cc:388-389)");
+    const double rho = pr / (b->prm.R * T);
+    const double beta = rho / (2.0 * pr);
+    const double s = std::log(pr) - g * std::log(rho);
+    q[0 * (size_t)L.nv + i] = (float)u;
+    q[1 * (size_t)L.nv + i] = (float)v;
+    q[2 * (size_t)L.nv + i] = (float)pr;
+    q[3 * (size_t)L.nv + i] = (float)((g - s) / (g - 1.0) - (u * u + v * v) * beta);
+    q[4 * (size_t)L.nv + i] = (float)(-2.0 * beta);
+  }
+  for (int c = 0; c < kQ; ++c)
+    TB_CUDA(b, cudaMemcpy2DAsync(V.Q[0] + (size_t)c * L.nv * V.S + sample, V.S * sizeof(float),
+                                 q.data() + (size_t)c * L.nv, sizeof(float), sizeof(float), L.nv,
+                                 cudaMemcpyHostToDevice, b->stream));
+  return reset_clock(b, level, sample, 1);
+}
+
+tg_status tg_batch_get_state(tg_batch* b, int level, int sample, double* prim_aos, int n_vertex) {
+  if (!b || !prim_aos || level < 0 || level >= b->nlev) return bfail(b, TG_INVALID_ARG, "bad level or NULL state");
+  const Level& V = b->B.lev[level];
+  const HostLayout& L = b->lh[level].L;
+  if (sample < 0 || sample >= V.S || n_vertex != L.nv) return bfail(b, TG_INVALID_ARG, "bad sample or vertex count");
+  std::vector<float> q((size_t)kQ * L.nv);
+  for (int c = 0; c < kQ; ++c)
+    TB_CUDA(b, cudaMemcpy2DAsync(q.data() + (size_t)c * L.nv, sizeof(float), V.Q[0] + (size_t)c * L.nv * V.S + sample,
+                                 V.S * sizeof(float), sizeof(float), L.nv, cudaMemcpyDeviceToHost, b->stream));
+  tg_status st = bsync(b);
+  if (st != TG_OK) return st;
+  for (int i = 0; i < L.nv; ++i) {
+    double* p = prim_aos + 5 * (size_t)L.old_of_new[i];
+    const double u = q[i], v = q[(size_t)L.nv + i], pr = q[2 * (size_t)L.nv + i], V5 = q[4 * (size_t)L.nv + i];
+    const double rho = -V5 * pr;
+    p[0] = pr / (b->prm.R * rho); p[1] = pr; p[2] = u; p[3] = v; p[4] = 0.0;
+  }
+  return TG_OK;
+}
+
+tg_status tg_batch_set_kh(tg_batch* b, int level, const double* rows, int n_rnd) {
+  if (!b || !rows || level < 0 || level >= b->nlev || n_rnd < 2 || n_rnd % 2)
+    return bfail(b, TG_INVALID_ARG, "bad level, NULL rows or odd row length");
+  const Level& V = b->B.lev[level];
+  double* d = nullptr;
+  const size_t n = (size_t)V.S * n_rnd;
+  TB_CUDA(b, cudaMalloc((void**)&d, n * sizeof(double)));
+  cudaError_t e = cudaMemcpyAsync(d, rows, n * sizeof(double), cudaMemcpyHostToDevice, b->stream);
+  if (e == cudaSuccess) {
+    const long long t = (long long)V.m.nv * V.S;
+    kb_ic_kh<<<(unsigned)((t + 255) / 256), 256, 0, b->stream>>>(V, b->prm, d, n_rnd);
+    e = cudaStreamSynchronize(b->stream);
+  }
+  cudaFree(d);
+  if (e != cudaSuccess) return bfail(b, TG_CUDA_ERROR, cudaGetErrorString(e));
+  return reset_clock(b, level, 0, V.S);
+}
+
+tg_status tg_batch_advance(tg_batch* b, int instance, long max_steps, double* info4) {
+  if (!b) return bfail(b, TG_INVALID_ARG, "NULL batch");
+  if (max_steps < 0) return bfail(b, TG_INVALID_ARG, "max_steps < 0");
+  tg_status st = capture(b);
+  if (st != TG_OK) return st;
+  TB_CUDA(b, cudaMemcpyAsync(b->stop, &instance, sizeof(int), cudaMemcpyHostToDevice, b->stream));
+  bool done = false;
+  int nbad = 0;
+  long launched = 0;
+  if ((st = all_reached(b, instance, &done, &nbad)) != TG_OK) return st;
+  while (!done && launched < max_steps) {
+    const long chunk = std::min<long>(8, max_steps - launched);
+    for (long i = 0; i < chunk; ++i) TB_CUDA(b, cudaGraphLaunch(b->graph_exec, b->stream));
+    launched += chunk;
+    if ((st = all_reached(b, instance, &done, &nbad)) != TG_OK) return st;
+  }
+  int inf = INT_MAX;
+  TB_CUDA(b, cudaMemcpyAsync(b->stop, &inf, sizeof(int), cudaMemcpyHostToDevice, b->stream));
+  if ((st = bsync(b)) != TG_OK) return st;
+  if (info4) {
+    double lo = 1e300, hi = -1e300;
+    for (int l = 0; l < b->nlev; ++l) {
+      ClockHost c;
+      if ((st = read_clock(b, l, c)) != TG_OK) return st;
+      for (double x : c.elapsed) { lo = std::min(lo, x); hi = std::max(hi, x); }
+    }
+    info4[0] = (double)launched; info4[1] = lo; info4[2] = hi; info4[3] = (double)nbad;
+  }
+  if (nbad) return bfail(b, TG_BAD_STATE, std::to_string(nbad) + " sample(s) produced a non-finite or non-positive state");
+  return TG_OK;
+}
+
+tg_status tg_batch_clock(tg_batch* b, int level, double* elapsed, int* counter, int* bad) {
+  if (!b || level < 0 || level >= b->nlev) return bfail(b, TG_INVALID_ARG, "bad level");
+  ClockHost c;
+  tg_status st = read_clock(b, level, c);
+  if (st != TG_OK) return st;
+  const int S = b->B.lev[level].S;
+  if (elapsed) std::memcpy(elapsed, c.elapsed.data(), S * sizeof(double));
+  if (counter) std::memcpy(counter, c.counter.data(), S * sizeof(int));
+  if (bad) std::memcpy(bad, c.bad.data(), S * sizeof(int));
+  return TG_OK;
+}
+
+tg_status tg_batch_moments(tg_batch* b, int level, int extras, double* fm, double* sm, double* m2) {
+  if (!b || level < 0 || level >= b->nlev || extras < 0 || extras > 7)
+    return bfail(b, TG_INVALID_ARG, "bad level or extras (density, mach, entropy: bits 1, 2, 4)");
+  const Level& V = b->B.lev[level];
+  const HostLayout& L = b->lh[level].L;
+  const int nvar = 5 + (extras & 1) + ((extras >> 1) & 1) + ((extras >> 2) & 1);
+  const size_t n = (size_t)nvar * L.nv;
+  double* d = nullptr;
+  TB_CUDA(b, cudaMalloc((void**)&d, 3 * n * sizeof(double)));
+  kb_moments<<<(unsigned)((n + 127) / 128), 128, 0, b->stream>>>(V, b->prm, extras, nvar, d, d + n, d + 2 * n);
+  std::vector<double> h(3 * n);
+  cudaError_t e = cudaMemcpyAsync(h.data(), d, 3 * n * sizeof(double), cudaMemcpyDeviceToHost, b->stream);
+  if (e == cudaSuccess) e = cudaStreamSynchronize(b->stream);
+  cudaFree(d);
+  if (e != cudaSuccess) return bfail(b, TG_CUDA_ERROR, cudaGetErrorString(e));
+  double* out[3] = {fm, sm, m2};
+  for (int w = 0; w < 3; ++w) {
+    if (!out[w]) continue;
+    for (int i = 0; i < L.nv; ++i) {
+      double* dst = out[w] + (size_t)nvar * L.old_of_new[i];
+      for (int c = 0; c < nvar; ++c) dst[c] = h[(size_t)w * n + (size_t)c * L.nv + i];
+    }
+  }
+  return TG_OK;
+}
+
+tg_status tg_batch_set_shape(tg_batch* b, int shape) {
+  if (!b || shape < 0 || shape >= (int)(sizeof(kShapes) / sizeof(kShapes[0])))
+    return bfail(b, TG_INVALID_ARG, "unknown launch shape");
+  if (shape != b->shape) {
+    drop_graph(b);
+    b->shape = shape;
+  }
+  return TG_OK;
+}
+
+tg_status tg_batch_time_steps(tg_batch* b, int steps, double* ms) {
+  if (!b || !ms || steps < 1) return bfail(b, TG_INVALID_ARG, "bad argument");
+  tg_status st = capture(b);
+  if (st != TG_OK) return st;
+  cudaEvent_t e0, e1;
+  TB_CUDA(b, cudaEventCreate(&e0));
+  TB_CUDA(b, cudaEventCreate(&e1));
+  TB_CUDA(b, cudaEventRecord(e0, b->stream));
+  for (int i = 0; i < steps; ++i) TB_CUDA(b, cudaGraphLaunch(b->graph_exec, b->stream));
+  TB_CUDA(b, cudaEventRecord(e1, b->stream));
+  if ((st = bsync(b)) != TG_OK) return st;
+  float t = 0.0f;
+  cudaEventElapsedTime(&t, e0, e1);
+  cudaEventDestroy(e0);
+  cudaEventDestroy(e1);
+  *ms = t / steps;
+  return TG_OK;
+}
+
+// Autotuner: times `steps` steps of every launch shape from the current state
+// (restored after each trial) and keeps the fastest.  ms_out (may be NULL)
+// receives the per-shape times in shape order.
+tg_status tg_batch_tune(tg_batch* b, int steps, int* shape_out, double* ms_out) {
+  if (!b || steps < 1) return bfail(b, TG_INVALID_ARG, "bad argument");
+  const int nshape = (int)(sizeof(kShapes) / sizeof(kShapes[0]));
+  // save Q[0] and the clocks of every level
+  std::vector<void*> saved;
+  auto save = [&](const void* src, size_t bytes) -> void* {
+    void* p = nullptr;
+    if (cudaMalloc(&p, bytes) != cudaSuccess) return nullptr;
+    cudaMemcpyAsync(p, src, bytes, cudaMemcpyDeviceToDevice, b->stream);
+    saved.push_back(p);
+    return p;
+  };
+  struct Save { void *q, *el, *cnt, *rch, *bad; };
+  std::vector<Save> sv(b->nlev);
+  for (int l = 0; l < b->nlev; ++l) {
+    const Level& V = b->B.lev[l];
+    sv[l].q = save(V.Q[0], (size_t)kQ * V.m.nv * V.S * sizeof(float));
+    sv[l].el = save(V.c.elapsed, V.S * sizeof(double));
+    sv[l].cnt = save(V.c.counter, V.S * sizeof(int));
+    sv[l].rch = save(V.c.reached, V.S * sizeof(int));
+    sv[l].bad = save(V.c.bad, V.S * sizeof(int));
+    if (!sv[l].q || !sv[l].el || !sv[l].cnt || !sv[l].rch || !sv[l].bad) {
+      for (void* p : saved) cudaFree(p);
+      return bfail(b, TG_CUDA_ERROR, "no device memory for the tuning snapshot");
+    }
+  }
+  auto restore = [&]() {
+    for (int l = 0; l < b->nlev; ++l) {
+      const Level& V = b->B.lev[l];
+      cudaMemcpyAsync(V.Q[0], sv[l].q, (size_t)kQ * V.m.nv * V.S * sizeof(float), cudaMemcpyDeviceToDevice, b->stream);
+      cudaMemcpyAsync(V.c.elapsed, sv[l].el, V.S * sizeof(double), cudaMemcpyDeviceToDevice, b->stream);
+      cudaMemcpyAsync(V.c.counter, sv[l].cnt, V.S * sizeof(int), cudaMemcpyDeviceToDevice, b->stream);
+      cudaMemcpyAsync(V.c.reached, sv[l].rch, V.S * sizeof(int), cudaMemcpyDeviceToDevice, b->stream);
+      cudaMemcpyAsync(V.c.bad, sv[l].bad, V.S * sizeof(int), cudaMemcpyDeviceToDevice, b->stream);
+    }
+  };
+  int best = b->shape;
+  double best_ms = 1e300;
+  tg_status st = TG_OK;
+  for (int i = 0; i < nshape && st == TG_OK; ++i) {
+    if ((st = tg_batch_set_shape(b, i)) != TG_OK) break;
+    double warm, ms;
+    if ((st = tg_batch_time_steps(b, 1, &warm)) != TG_OK) break;
+    restore();
+    if ((st = tg_batch_time_steps(b, steps, &ms)) != TG_OK) break;
+    restore();
+    if (ms_out) ms_out[i] = ms;
+    if (ms < best_ms) { best_ms = ms; best = i; }
+  }
+  cudaStreamSynchronize(b->stream);
+  for (void* p : saved) cudaFree(p);
+  if (st != TG_OK) return st;
+  if ((st = tg_batch_set_shape(b, best)) != TG_OK) return st;
+  if (shape_out) *shape_out = best;
+  return bsync(b);
+}
+
+tg_status tg_batch_query(tg_batch* b, int key, double* out) {
+  if (!b || !out) return bfail(b, TG_INVALID_ARG, "NULL argument");
+  switch (key) {
+    case TG_BQ_N_LEVELS: *out = b->nlev; break;
+    case TG_BQ_KERNELS_PER_STEP: *out = kernels_per_step(b); break;
+    case TG_BQ_DEVICE_BYTES: *out = (double)b->device_bytes; break;
+    case TG_BQ_SHAPE: *out = b->shape; break;
+    case TG_BQ_SAMPLE_TILE: *out = kShapes[b->shape].st; break;
+    case TG_BQ_BLOCK: *out = kShapes[b->shape].bs; break;
+    case TG_BQ_N_SHAPES: *out = (double)(sizeof(kShapes) / sizeof(kShapes[0])); break;
+    default: return bfail(b, TG_INVALID_ARG, "unknown query key");
+  }
+  return TG_OK;
+}
+
+tg_status tg_batch_stream(tg_batch* b, void** out) {
+  if (!b || !out) return bfail(b, TG_INVALID_ARG, "NULL argument");
+  *out = (void*)b->stream;
+  return TG_OK;
+}
+
+}  // extern "C"
