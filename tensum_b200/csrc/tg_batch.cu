@@ -103,27 +103,30 @@ tg_status bsync(tg_batch* b) {
   return TG_OK;
 }
 
-// Sets the warp offsets of every level for sample tile st; returns the total.
+// Sets the warp offsets of every level for sample tile ST over its vertices
+// (or edges); returns the total.
 template <int ST>
-long long layout_warps(Batch& B) {
+long long layout_warps(Batch& B, bool edges) {
   long long w = 0;
   for (int l = 0; l < B.nlev; ++l) {
     B.lev[l].w_begin = w;
-    w += level_warps<ST>(B.lev[l].m.nv, B.lev[l].S);
+    w += level_warps<ST>(edges ? B.lev[l].m.ne : B.lev[l].m.nv, B.lev[l].S);
   }
   B.work = w;
   return w;
 }
+
+long long layout(Batch& B, int st, bool edges) { return st == 32 ? layout_warps<32>(B, edges) : layout_warps<16>(B, edges); }
 
 typedef void (*FluxK)(Batch, BParams, int);
 
 template <int F, int R>
 FluxK flux_kernel_fr(int shape) {
   switch (shape) {
-    case 0: return kb_flux_update<F, R, 32, 256>;
-    case 1: return kb_flux_update<F, R, 32, 128>;
-    case 2: return kb_flux_update<F, R, 16, 256>;
-    default: return kb_flux_update<F, R, 16, 128>;
+    case 0: return kb_edge_flux<F, R, 32, 256>;
+    case 1: return kb_edge_flux<F, R, 32, 128>;
+    case 2: return kb_edge_flux<F, R, 16, 256>;
+    default: return kb_edge_flux<F, R, 16, 128>;
   }
 }
 
@@ -140,6 +143,15 @@ FluxK flux_kernel(int flux, int recon, int shape) {
   }
 }
 
+FluxK gather_kernel(int shape) {
+  switch (shape) {
+    case 0: return kb_gather_update<32, 256>;
+    case 1: return kb_gather_update<32, 128>;
+    case 2: return kb_gather_update<16, 256>;
+    default: return kb_gather_update<16, 128>;
+  }
+}
+
 bool needs_grad(const tg_batch* b) {
   return b->prm.recon != RECON_FIRST && (b->prm.flux == FLUX_TECNO_ROE || b->prm.flux == FLUX_TECNO_RUSANOV);
 }
@@ -153,8 +165,9 @@ int max_samples(const tg_batch* b) {
 // One full step of every level on b->stream.
 void enqueue_step(tg_batch* b) {
   const Shape sh = kShapes[b->shape];
-  Batch B = b->B;
-  if (sh.st == 32) layout_warps<32>(B); else layout_warps<16>(B);
+  Batch B = b->B, BE = b->B;
+  layout(B, sh.st, false);
+  layout(BE, sh.st, true);
   const dim3 gs((max_samples(b) + 255) / 256, b->nlev);
   kb_step_begin<<<gs, 256, 0, b->stream>>>(B, b->prm);
   long long dt_blocks = 0;
@@ -162,18 +175,21 @@ void enqueue_step(tg_batch* b) {
   kb_dt<8><<<(unsigned)dt_blocks, 256, 0, b->stream>>>(B, b->prm, b->dt_chunks);
   kb_dt_final<<<gs, 256, 0, b->stream>>>(B, b->prm);
   const unsigned blocks = (unsigned)((B.work * 32 + sh.bs - 1) / sh.bs);
+  const unsigned eblocks = (unsigned)((BE.work * 32 + sh.bs - 1) / sh.bs);
   FluxK fk = flux_kernel(b->prm.flux, b->prm.recon, b->shape);
+  FluxK gk = gather_kernel(b->shape);
   for (int r = 0; r < 3; ++r) {
     if (needs_grad(b)) {
       if (sh.st == 32) kb_grad<32><<<blocks, sh.bs, 0, b->stream>>>(B, b->prm, r);
       else kb_grad<16><<<blocks, sh.bs, 0, b->stream>>>(B, b->prm, r);
     }
-    fk<<<blocks, sh.bs, 0, b->stream>>>(B, b->prm, r);
+    fk<<<eblocks, sh.bs, 0, b->stream>>>(BE, b->prm, r);
+    gk<<<blocks, sh.bs, 0, b->stream>>>(B, b->prm, r);
   }
   kb_step_end<<<gs, 256, 0, b->stream>>>(B, b->prm);
 }
 
-int kernels_per_step(const tg_batch* b) { return 4 + 3 * (needs_grad(b) ? 2 : 1); }
+int kernels_per_step(const tg_batch* b) { return 4 + 3 * (needs_grad(b) ? 3 : 2); }
 
 void drop_graph(tg_batch* b) {
   if (b->graph_exec) cudaGraphExecDestroy(b->graph_exec);
@@ -276,6 +292,7 @@ tg_status tg_batch_create(const tg_batch_level* levels, int n_levels, const tg_m
     const HostLayout& L = H.L;
     Level& V = b->B.lev[l];
     V.S = H.S;
+    V.P = H.S + 32;
     LevelMesh& m = V.m;
     m.nv = L.nv; m.ne = L.ne;
     // geometry formed in FP64, stored in FP32
@@ -291,10 +308,11 @@ tg_status tg_batch_create(const tg_batch_level* levels, int n_levels, const tg_m
     BU(L.e_dx, dx) BU(L.e_dy, dy) BU(L.e_g0x, g0x) BU(L.e_g0y, g0y) BU(L.e_g1x, g1x) BU(L.e_g1y, g1y)
     BU(L.ce_off, ce_off) BU(L.ce_ent, ce_ent) BU(L.dcarea, area) BU(L.inv6mc, inv6mc) BU(L.x, x) BU(L.y, y)
 #undef BU
-    const size_t vs = (size_t)L.nv * H.S;
+    const size_t vs = (size_t)L.nv * V.P;
     for (int r = 0; r < 3; ++r)
       if ((st = balloc(b, kQ * vs, &V.Q[r])) != TG_OK) { tg_batch_destroy(b); return st; }
     if ((st = balloc(b, 4 * vs, &V.Uold)) != TG_OK) { tg_batch_destroy(b); return st; }
+    if ((st = balloc(b, 4 * (size_t)L.ne * V.P, &V.F)) != TG_OK) { tg_batch_destroy(b); return st; }
     if (mat->reconstruct_scheme != RECON_FIRST && mat->flux_scheme != FLUX_KEPEC) {
       if ((st = balloc(b, kG * vs, &V.G)) != TG_OK) { tg_batch_destroy(b); return st; }
     }
@@ -367,16 +385,15 @@ tg_status tg_batch_set_state(tg_batch* b, int level, int sample, const double* p
     const double rho = pr / (b->prm.R * T);
     const double beta = rho / (2.0 * pr);
     const double s = std::log(pr) - g * std::log(rho);
-    q[0 * (size_t)L.nv + i] = (float)u;
-    q[1 * (size_t)L.nv + i] = (float)v;
-    q[2 * (size_t)L.nv + i] = (float)pr;
-    q[3 * (size_t)L.nv + i] = (float)((g - s) / (g - 1.0) - (u * u + v * v) * beta);
-    q[4 * (size_t)L.nv + i] = (float)(-2.0 * beta);
+    float* r = q.data() + (size_t)kQ * i;     // device rows [vertex][component]
+    r[0] = (float)u;
+    r[1] = (float)v;
+    r[2] = (float)pr;
+    r[3] = (float)((g - s) / (g - 1.0) - (u * u + v * v) * beta);
+    r[4] = (float)(-2.0 * beta);
   }
-  for (int c = 0; c < kQ; ++c)
-    TB_CUDA(b, cudaMemcpy2DAsync(V.Q[0] + (size_t)c * L.nv * V.S + sample, V.S * sizeof(float),
-                                 q.data() + (size_t)c * L.nv, sizeof(float), sizeof(float), L.nv,
-                                 cudaMemcpyHostToDevice, b->stream));
+  TB_CUDA(b, cudaMemcpy2DAsync(V.Q[0] + sample, V.P * sizeof(float), q.data(), sizeof(float), sizeof(float),
+                               (size_t)kQ * L.nv, cudaMemcpyHostToDevice, b->stream));
   return reset_clock(b, level, sample, 1);
 }
 
@@ -386,14 +403,14 @@ tg_status tg_batch_get_state(tg_batch* b, int level, int sample, double* prim_ao
   const HostLayout& L = b->lh[level].L;
   if (sample < 0 || sample >= V.S || n_vertex != L.nv) return bfail(b, TG_INVALID_ARG, "bad sample or vertex count");
   std::vector<float> q((size_t)kQ * L.nv);
-  for (int c = 0; c < kQ; ++c)
-    TB_CUDA(b, cudaMemcpy2DAsync(q.data() + (size_t)c * L.nv, sizeof(float), V.Q[0] + (size_t)c * L.nv * V.S + sample,
-                                 V.S * sizeof(float), sizeof(float), L.nv, cudaMemcpyDeviceToHost, b->stream));
+  TB_CUDA(b, cudaMemcpy2DAsync(q.data(), sizeof(float), V.Q[0] + sample, V.P * sizeof(float), sizeof(float),
+                               (size_t)kQ * L.nv, cudaMemcpyDeviceToHost, b->stream));
   tg_status st = bsync(b);
   if (st != TG_OK) return st;
   for (int i = 0; i < L.nv; ++i) {
     double* p = prim_aos + 5 * (size_t)L.old_of_new[i];
-    const double u = q[i], v = q[(size_t)L.nv + i], pr = q[2 * (size_t)L.nv + i], V5 = q[4 * (size_t)L.nv + i];
+    const float* r = q.data() + (size_t)kQ * i;
+    const double u = r[0], v = r[1], pr = r[2], V5 = r[4];
     const double rho = -V5 * pr;
     p[0] = pr / (b->prm.R * rho); p[1] = pr; p[2] = u; p[3] = v; p[4] = 0.0;
   }
@@ -536,7 +553,7 @@ tg_status tg_batch_tune(tg_batch* b, int steps, int* shape_out, double* ms_out) 
   std::vector<Save> sv(b->nlev);
   for (int l = 0; l < b->nlev; ++l) {
     const Level& V = b->B.lev[l];
-    sv[l].q = save(V.Q[0], (size_t)kQ * V.m.nv * V.S * sizeof(float));
+    sv[l].q = save(V.Q[0], (size_t)kQ * V.m.nv * V.P * sizeof(float));
     sv[l].el = save(V.c.elapsed, V.S * sizeof(double));
     sv[l].cnt = save(V.c.counter, V.S * sizeof(int));
     sv[l].rch = save(V.c.reached, V.S * sizeof(int));
@@ -549,7 +566,7 @@ tg_status tg_batch_tune(tg_batch* b, int steps, int* shape_out, double* ms_out) 
   auto restore = [&]() {
     for (int l = 0; l < b->nlev; ++l) {
       const Level& V = b->B.lev[l];
-      cudaMemcpyAsync(V.Q[0], sv[l].q, (size_t)kQ * V.m.nv * V.S * sizeof(float), cudaMemcpyDeviceToDevice, b->stream);
+      cudaMemcpyAsync(V.Q[0], sv[l].q, (size_t)kQ * V.m.nv * V.P * sizeof(float), cudaMemcpyDeviceToDevice, b->stream);
       cudaMemcpyAsync(V.c.elapsed, sv[l].el, V.S * sizeof(double), cudaMemcpyDeviceToDevice, b->stream);
       cudaMemcpyAsync(V.c.counter, sv[l].cnt, V.S * sizeof(int), cudaMemcpyDeviceToDevice, b->stream);
       cudaMemcpyAsync(V.c.reached, sv[l].rch, V.S * sizeof(int), cudaMemcpyDeviceToDevice, b->stream);

@@ -1,21 +1,20 @@
 // tg_batch.cuh -- batched FP32 Monte Carlo ensembles: physics and kernels.
 //
 // An ensemble level is S samples of one periodic mesh, advanced together.
-// Every per-sample array is [component][vertex][sample] with the sample index
-// innermost, so the 32 lanes of a warp hold 32 samples of one vertex: state
-// loads are 128-byte coalesced and the mesh data of the vertex and of its
-// edges is read once per warp (a broadcast).  Members are FP32; geometry is
+// Every per-sample array is [vertex or edge][component][sample] with the
+// sample index innermost, so the 32 lanes of a warp hold 32 samples of one
+// vertex: state loads are 128-byte coalesced, all components of a vertex are
+// reached from one base address by immediate offsets, and the mesh data of the
+// vertex and of its edges is read once per warp (a broadcast).  Members are FP32; geometry is
 // formed in FP64 on the host and stored in FP32, the near-equal branch of the
 // logarithmic mean is evaluated in FP64, and the per-sample clock (elapsed
 // time, dt) is FP64 so output times are met exactly.
 //
-// Residual assembly is a per-vertex gather: the thread of (vertex, sample)
-// evaluates the flux of each incident edge in the edge's own orientation and
-// adds it with the side's sign, then applies the SSP-RK3 stage update in the
-// same pass.  Both endpoints of an edge evaluate the identical expression, so
-// what one gains the other loses bit for bit (exact conservation) and no
-// residual array is written.  The flux work is twice that of an edge loop;
-// in exchange there is no scatter, no atomics and no stored flux.
+// Each stage is an edge pass (one flux per edge and sample, stored
+// [component][edge][sample]) and a vertex pass that gathers the fluxes of the
+// vertex's edges in a fixed order and applies the SSP-RK3 stage update: every
+// flux is computed once, an edge's flux enters both endpoints bit for bit
+// (exact conservation), and there are no atomics.
 #pragma once
 
 #include <cstdint>
@@ -57,9 +56,11 @@ struct Level {
   LevelMesh m;
   LevelClock c;
   int S;                           // samples (a multiple of 32)
-  float* Q[3];                     // rotating states, kQ x nv x S
-  float* Uold;                     // 4 x nv x S
-  float* G;                        // kG x nv x S
+  int P;                           // row pitch in floats: S plus a pad that breaks power-of-two strides
+  float* Q[3];                     // rotating states, nv x kQ x S
+  float* Uold;                     // nv x 4 x S
+  float* G;                        // nv x kG x S
+  float* F;                        // ne x 4 x S: area-weighted edge fluxes of the current stage
   long long w_begin;               // first warp of this level in a fused launch (set per launch shape)
 };
 
@@ -85,9 +86,17 @@ struct FFlx { float m, x, y, e; };
 
 // Ismail-Roe logarithmic mean F (logmean = (a+b)/2 / F) with the near-equal
 // series branch in FP64 (src/material.h:24-42).
+// 1 / d from the FP32 reciprocal refined by one Newton-Raphson step,
+// y1 = y0 (2 - d y0): relative error 2^-24 -> about 2^-46, ample for FP32
+// inputs, in three FP64 operations instead of a full FP64 division.
+__device__ __forceinline__ double recip_nr(double d) {
+  const double y = (double)__frcp_rn((float)d);
+  return y * (2.0 - d * y);
+}
+
 __device__ __forceinline__ float logavg_F_mixed(float a, float b) {
   const double da = a, db = b;
-  const double f = (db - da) / (db + da);
+  const double f = (db - da) * recip_nr(db + da);   // b - a and b + a are exact in FP64
   const double u = f * f;
   if (u < 1.0e-2) {
     const double u2 = u * u;
@@ -122,9 +131,10 @@ __device__ __forceinline__ float fjump(float d, float gl, float gr) {
 // KEPEC central flux (src/kepec.cc:10-38) on a unit normal.
 __device__ __forceinline__ FFlx fkepec(const BParams& k, const FRec& L, const FRec& R, float unx, float uny,
                                        float& rho_ln, float& ibeta) {
-  rho_ln = 0.5f * (L.rho + R.rho) / logavg_F_mixed(L.rho, R.rho);
-  ibeta = logavg_F_mixed(L.beta, R.beta) / (0.5f * (L.beta + R.beta));
-  const float p = 0.5f * (L.rho + R.rho) / (L.beta + R.beta);
+  // __fdividef: at most 2 ulp for the magnitudes of densities and beta
+  rho_ln = __fdividef(0.5f * (L.rho + R.rho), logavg_F_mixed(L.rho, R.rho));
+  ibeta = __fdividef(logavg_F_mixed(L.beta, R.beta), 0.5f * (L.beta + R.beta));
+  const float p = __fdividef(0.5f * (L.rho + R.rho), L.beta + R.beta);
   const float vx = 0.5f * (L.u + R.u), vy = 0.5f * (L.v + R.v);
   const float vn = vx * unx + vy * uny;
   const float vel2 = 0.5f * ((L.u * L.u + L.v * L.v) + (R.u * R.u + R.v * R.v));
@@ -144,11 +154,11 @@ __device__ __forceinline__ FFlx ftecno(const BParams& k, const FRec& L, const FR
   float rho, ibeta;
   FFlx F = fkepec(k, L, R, unx, uny, rho, ibeta);
   const float a = sqrtf(0.5f * k.gamma * ibeta);
-  const float p = 0.5f * (L.rho + R.rho) / (L.beta + R.beta);
+  const float p = __fdividef(0.5f * (L.rho + R.rho), L.beta + R.beta);
   const float vx = 0.5f * (L.u + R.u), vy = 0.5f * (L.v + R.v);
   const float vn = vx * unx + vy * uny;
   const float vsq = vx * vx + vy * vy;
-  const float H = a * a / (k.gamma - 1.0f) + 0.5f * vsq;
+  const float H = a * a * k.inv_gm1 + 0.5f * vsq;
   const float v1 = vx * uny - vy * unx;
   const float c1 = sqrtf(rho * k.inv_gamma);
   const float S0 = 0.70710678118654752f * c1, S1 = k.sqrt_gm1 * c1, S2 = sqrtf(p);
@@ -220,7 +230,8 @@ __host__ __device__ __forceinline__ long long level_warps(int nv, int S) {
   return (long long)((nv + VPW - 1) / VPW) * (S / ST);
 }
 
-template <int ST>
+// EDGE: items are (edge, sample) instead of (vertex, sample).
+template <int ST, bool EDGE = false>
 __device__ __forceinline__ Item item_of(const Batch& B, long long w, int lane) {
   constexpr int VPW = 32 / ST;
   Item it{0, 0, 0, false};
@@ -230,17 +241,17 @@ __device__ __forceinline__ Item item_of(const Batch& B, long long w, int lane) {
   for (int i = 1; i < kMaxLevels; ++i)
     if (i < B.nlev && w >= B.lev[i].w_begin) l = i;
   const long long r = w - B.lev[l].w_begin;
-  const int nvw = (B.lev[l].m.nv + VPW - 1) / VPW;
+  const int n = EDGE ? B.lev[l].m.ne : B.lev[l].m.nv;
+  const int nvw = (n + VPW - 1) / VPW;
   it.l = l;
   it.s = (int)(r / nvw) * ST + (lane % ST);
   it.v = (int)(r % nvw) * VPW + lane / ST;
-  it.ok = it.v < B.lev[l].m.nv;
+  it.ok = it.v < n;
   return it;
 }
 
-__device__ __forceinline__ size_t at(const Level& L, int c, int v, int s) {
-  return ((size_t)c * L.m.nv + v) * (size_t)L.S + s;
-}
+// Row block of item i in a [item][C][sample] array (add the sample, then c * S).
+__device__ __forceinline__ size_t rows(int i, int C, int S) { return (size_t)i * C * S; }
 
 // -------------------------------------------------------------------- kernels
 // Per-sample step start: which samples advance, reset of the running dt min.
@@ -281,8 +292,8 @@ __global__ void __launch_bounds__(32 * VT) kb_dt(Batch B, BParams k, int chunks)
     const int per = (L.m.nv + chunks - 1) / chunks;
     const int v0 = ch * per, v1 = min(L.m.nv, v0 + per);
     for (int v = v0 + vg; v < v1; v += VT) {
-      const float u = L.Q[0][at(L, 0, v, s)], w = L.Q[0][at(L, 1, v, s)], p = L.Q[0][at(L, 2, v, s)];
-      const float V5 = L.Q[0][at(L, 4, v, s)];
+      const float* q = L.Q[0] + rows(v, kQ, L.P) + s;
+      const float u = q[0], w = q[L.P], p = q[2 * L.P], V5 = q[4 * L.P];
       const float rho = -V5 * p;
       const float c = sqrtf(k.gamma * p / rho);
       float lam = 0.0f;
@@ -294,10 +305,11 @@ __global__ void __launch_bounds__(32 * VT) kb_dt(Batch B, BParams k, int chunks)
       const float dtv = k.cfl * L.m.area[v] / lam;
       m = fminf(m, dtv > 0.0f ? dtv : __int_as_float(0x7f800000));
       // U_old
-      L.Uold[at(L, 0, v, s)] = rho;
-      L.Uold[at(L, 1, v, s)] = rho * u;
-      L.Uold[at(L, 2, v, s)] = rho * w;
-      L.Uold[at(L, 3, v, s)] = p * k.inv_gm1 + 0.5f * (u * u + w * w) * rho;
+      float* uo = L.Uold + rows(v, 4, L.P) + s;
+      uo[0] = rho;
+      uo[L.P] = rho * u;
+      uo[2 * L.P] = rho * w;
+      uo[3 * L.P] = p * k.inv_gm1 + 0.5f * (u * u + w * w) * rho;
     }
   }
   __shared__ float red[VT][32];
@@ -334,11 +346,13 @@ __global__ void kb_grad(Batch B, BParams k, int r) {
   if (!it.ok) return;
   const Level& L = B.lev[it.l];
   if (!L.c.active[it.s]) return;
-  const float* Q = L.Q[r];
   const int v = it.v, s = it.s;
+  const int S = L.P;   // row pitch
+  const float* Q = L.Q[r] + s;
   auto W = [&](int x, float* o) {
-    const float u = Q[at(L, 0, x, s)], vv = Q[at(L, 1, x, s)], V5 = Q[at(L, 4, x, s)];
-    o[0] = Q[at(L, 3, x, s)]; o[1] = -V5 * u; o[2] = -V5 * vv; o[3] = V5;   // V2 = 2 beta u = -V5 u
+    const float* q = Q + rows(x, kQ, S);
+    const float u = q[0], vv = q[S], V5 = q[4 * S];
+    o[0] = q[3 * S]; o[1] = -V5 * u; o[2] = -V5 * vv; o[3] = V5;   // V2 = 2 beta u = -V5 u
   };
   float ws[4];
   W(v, ws);
@@ -359,82 +373,94 @@ __global__ void kb_grad(Batch B, BParams k, int r) {
     }
   }
   const float f = L.m.inv6mc[v];
+  float* G = L.G + rows(v, kG, S) + s;
 #pragma unroll
-  for (int c = 0; c < kG; ++c) L.G[at(L, c, v, s)] = acc[c] * f;
+  for (int c = 0; c < kG; ++c) G[c * S] = acc[c] * f;
 }
 
-// Residual of every incident edge and the SSP-RK3 stage update (src/fv.cc:
-// 1066-1192, 1635-1658), state r -> state (r+1) % 3.  Held or finished samples
-// copy their state through.
+// Edge fluxes of one stage (src/fv.cc:1066-1192, src/material.cc:27-74): one
+// (edge, sample) per thread, the flux of the edge's own orientation (a left,
+// b right) times |n|, stored for the gather.  Held samples skip.
 template <int FLUX, int RECON, int ST, int BS>
-__global__ void __launch_bounds__(BS) kb_flux_update(Batch B, BParams k, int r) {
+__global__ void __launch_bounds__(BS) kb_edge_flux(Batch B, BParams k, int r) {
+  const long long w = (blockIdx.x * (long long)blockDim.x + threadIdx.x) >> 5;
+  const Item it = item_of<ST, true>(B, w, threadIdx.x & 31);
+  if (!it.ok) return;
+  const Level& L = B.lev[it.l];
+  const int e = it.v, s = it.s;
+  if (!L.c.active[s]) return;
+  constexpr bool kA = (FLUX == FLUX_TECNO_ROE);
+  constexpr bool kGr = (RECON != RECON_FIRST) && (FLUX == FLUX_TECNO_ROE || FLUX == FLUX_TECNO_RUSANOV);
+  const int S = L.P;   // row pitch
+  const int ia = L.m.e_a[e], ib = L.m.e_b[e];
+  const float* qa = L.Q[r] + rows(ia, kQ, S) + s;
+  const float* qb = L.Q[r] + rows(ib, kQ, S) + s;
+  const FRec A = frec(k, qa[0], qa[S], qa[2 * S], qa[3 * S], qa[4 * S], kA);
+  const FRec Bv = frec(k, qb[0], qb[S], qb[2 * S], qb[3 * S], qb[4 * S], kA);
+  float ga[kG], gb[kG];
+  if (kGr) {
+    const float* Ga = L.G + rows(ia, kG, S) + s;
+    const float* Gb = L.G + rows(ib, kG, S) + s;
+#pragma unroll
+    for (int c = 0; c < kG; ++c) { ga[c] = Ga[c * S]; gb[c] = Gb[c * S]; }
+  }
+  const FFlx F = fflux<FLUX, RECON>(k, A, Bv, L.m.ux[e], L.m.uy[e], L.m.dx[e], L.m.dy[e], ga, gb);
+  const float ar = L.m.ar[e];
+  float* Fo = L.F + rows(e, 4, S) + s;
+  Fo[0] = F.m * ar; Fo[S] = F.x * ar; Fo[2 * S] = F.y * ar; Fo[3 * S] = F.e * ar;
+}
+
+// Residual gather in the fixed per-vertex edge order and the SSP-RK3 stage
+// update (src/fv.cc:1635-1658), state r -> state (r+1) % 3.  Held or finished
+// samples copy their state through.
+template <int ST, int BS>
+__global__ void __launch_bounds__(BS) kb_gather_update(Batch B, BParams k, int r) {
   const long long w = (blockIdx.x * (long long)blockDim.x + threadIdx.x) >> 5;
   const Item it = item_of<ST>(B, w, threadIdx.x & 31);
   if (!it.ok) return;
   const Level& L = B.lev[it.l];
-  const float* Q = L.Q[r];
-  float* Qn = L.Q[(r + 1) % 3];
   const int v = it.v, s = it.s;
+  const int S = L.P;   // row pitch
+  const size_t ov = rows(v, kQ, S) + s;
+  const float* Q = L.Q[r] + ov;
+  float* Qn = L.Q[(r + 1) % 3] + ov;
   if (!L.c.active[s]) {
 #pragma unroll
-    for (int c = 0; c < kQ; ++c) Qn[at(L, c, v, s)] = Q[at(L, c, v, s)];
+    for (int c = 0; c < kQ; ++c) Qn[c * S] = Q[c * S];
     return;
   }
-  constexpr bool kA = (FLUX == FLUX_TECNO_ROE);
-  constexpr bool kGr = (RECON != RECON_FIRST) && (FLUX == FLUX_TECNO_ROE || FLUX == FLUX_TECNO_RUSANOV);
-  auto rec = [&](int x) {
-    return frec(k, Q[at(L, 0, x, s)], Q[at(L, 1, x, s)], Q[at(L, 2, x, s)], Q[at(L, 3, x, s)], Q[at(L, 4, x, s)], kA);
-  };
-  const FRec me = rec(v);
-  float gme[kG];
-  if (kGr) {
-#pragma unroll
-    for (int c = 0; c < kG; ++c) gme[c] = L.G[at(L, c, v, s)];
-  }
   float r0 = 0.0f, r1 = 0.0f, r2 = 0.0f, r3 = 0.0f;
-  for (int j = L.m.ce_off[v]; j < L.m.ce_off[v + 1]; ++j) {
-    const int ent = L.m.ce_ent[j], e = ent >> 1, side = ent & 1;
-    const int ea = L.m.e_a[e], eb = L.m.e_b[e];
-    const int o = side ? ea : eb;
-    const FRec ot = rec(o);
-    float go[kG];
-    if (kGr) {
-#pragma unroll
-      for (int c = 0; c < kG; ++c) go[c] = L.G[at(L, c, o, s)];
-    }
-    // the edge's own orientation: a = left, b = right
-    const bool mine_a = (side == 0);
-    const FRec& A = mine_a ? me : ot;
-    const FRec& Bv = mine_a ? ot : me;
-    const float* gA = mine_a ? gme : go;
-    const float* gB = mine_a ? go : gme;
-    FFlx F = fflux<FLUX, RECON>(k, A, Bv, L.m.ux[e], L.m.uy[e], L.m.dx[e], L.m.dy[e], gA, gB);
-    const float ar = L.m.ar[e];
-    const float sg = side ? -ar : ar;
-    r0 += F.m * sg; r1 += F.x * sg; r2 += F.y * sg; r3 += F.e * sg;
+  const int j0 = L.m.ce_off[v], j1 = L.m.ce_off[v + 1];
+#pragma unroll 4
+  for (int j = j0; j < j1; ++j) {
+    const int ent = L.m.ce_ent[j];
+    const float* Fe = L.F + rows(ent >> 1, 4, S) + s;
+    const float sg = (ent & 1) ? -1.0f : 1.0f;
+    r0 += Fe[0] * sg; r1 += Fe[S] * sg; r2 += Fe[2 * S] * sg; r3 += Fe[3 * S] * sg;
   }
+  const float u0 = Q[0], v0 = Q[S], p0 = Q[2 * S], V50 = Q[4 * S];
+  const float rho0 = -V50 * p0;
   // Shu-Osher SSP-RK3 stage (src/constants.h:4-6)
   const float a_rk = r == 0 ? 0.0f : (r == 1 ? 0.75f : 1.0f / 3.0f);
   const float b_rk = r == 0 ? 1.0f : (r == 1 ? 0.25f : 2.0f / 3.0f);
   const float factor = (float)L.c.dt[s] / L.m.area[v];
   const float c2 = -factor * b_rk;
-  float cr = me.rho, cx = me.rho * me.u, cy = me.rho * me.v;
-  float cE = me.p * k.inv_gm1 + 0.5f * (me.u * me.u + me.v * me.v) * me.rho;
-  cr = cr * b_rk + L.Uold[at(L, 0, v, s)] * a_rk + r0 * c2;
-  cx = cx * b_rk + L.Uold[at(L, 1, v, s)] * a_rk + r1 * c2;
-  cy = cy * b_rk + L.Uold[at(L, 2, v, s)] * a_rk + r2 * c2;
-  cE = cE * b_rk + L.Uold[at(L, 3, v, s)] * a_rk + r3 * c2;
+  const float* Uo = L.Uold + rows(v, 4, S) + s;
+  const float cr = rho0 * b_rk + Uo[0] * a_rk + r0 * c2;
+  const float cx = rho0 * u0 * b_rk + Uo[S] * a_rk + r1 * c2;
+  const float cy = rho0 * v0 * b_rk + Uo[2 * S] * a_rk + r2 * c2;
+  const float cE = (p0 * k.inv_gm1 + 0.5f * (u0 * u0 + v0 * v0) * rho0) * b_rk + Uo[3 * S] * a_rk + r3 * c2;
   const float ir = 1.0f / cr;
   const float u = cx * ir, vv = cy * ir;
   const float p = (k.gamma - 1.0f) * (cE - 0.5f * (cx * u + cy * vv));
-  const float beta = cr / (2.0f * p);
+  const float beta = 0.5f * cr / p;
   const float sent = logf(p) - k.gamma * logf(cr);
   const float V1 = (k.gamma - sent) * k.inv_gm1 - (u * u + vv * vv) * beta;
-  Qn[at(L, 0, v, s)] = u;
-  Qn[at(L, 1, v, s)] = vv;
-  Qn[at(L, 2, v, s)] = p;
-  Qn[at(L, 3, v, s)] = V1;
-  Qn[at(L, 4, v, s)] = -2.0f * beta;
+  Qn[0] = u;
+  Qn[S] = vv;
+  Qn[2 * S] = p;
+  Qn[3 * S] = V1;
+  Qn[4 * S] = -2.0f * beta;
   if (!(p > 0.0f) || !(cr > 0.0f) || !isfinite(u) || !isfinite(vv) || !isfinite(p)) L.c.bad[s] = 1;
 }
 
@@ -455,12 +481,12 @@ __global__ void kb_step_end(Batch B, BParams k) {
 // Initial states of Kelvin-Helmholtz samples from their random-number rows
 // (the parameter-file condition with pert(4, ...), src/perturb.cc:196-208):
 // v' = 0.01 sum_k r_k sin(2 pi k x + 2 pi r_{M+k}), evaluated in FP64.
-__global__ void kb_ic_kh(Level L, BParams k, const double* __restrict__ rows, int nrnd) {
+__global__ void kb_ic_kh(Level L, BParams k, const double* __restrict__ rnd, int nrnd) {
   const long long t = blockIdx.x * (long long)blockDim.x + threadIdx.x;
   if (t >= (long long)L.m.nv * L.S) return;
   const int v = (int)(t / L.S), s = (int)(t % L.S);
   const double x = L.m.x[v], y = L.m.y[v];
-  const double* row = rows + (size_t)s * nrnd;
+  const double* row = rnd + (size_t)s * nrnd;
   const int M = nrnd / 2;
   const double two_pi = 6.283185307179586;
   double acc = 0.0;
@@ -470,11 +496,12 @@ __global__ void kb_ic_kh(Level L, BParams k, const double* __restrict__ rows, in
   const double beta = rho / (2.0 * p);
   const double sent = log(p) - (double)k.gamma * log(rho);
   const double V1 = ((double)k.gamma - sent) / ((double)k.gamma - 1.0) - (u * u + vv * vv) * beta;
-  L.Q[0][at(L, 0, v, s)] = (float)u;
-  L.Q[0][at(L, 1, v, s)] = (float)vv;
-  L.Q[0][at(L, 2, v, s)] = (float)p;
-  L.Q[0][at(L, 3, v, s)] = (float)V1;
-  L.Q[0][at(L, 4, v, s)] = (float)(-2.0 * beta);
+  float* q = L.Q[0] + rows(v, kQ, L.P) + s;
+  q[0] = (float)u;
+  q[L.P] = (float)vv;
+  q[2 * L.P] = (float)p;
+  q[3 * L.P] = (float)V1;
+  q[4 * L.P] = (float)(-2.0 * beta);
 }
 
 // Ensemble moments of one level at its current state, FP64: Welford mean and
@@ -497,8 +524,9 @@ __global__ void kb_moments(Level L, BParams k, int extras, int nvar, double* __r
   }
   double mean = 0.0, ssd = 0.0, sq = 0.0, comp = 0.0;
   for (int s = 0; s < L.S; ++s) {
-    const double u = L.Q[0][at(L, 0, v, s)], w = L.Q[0][at(L, 1, v, s)], p = L.Q[0][at(L, 2, v, s)];
-    const double V5 = L.Q[0][at(L, 4, v, s)];
+    const float* q = L.Q[0] + rows(v, kQ, L.P) + s;
+    const double u = q[0], w = q[L.P], p = q[2 * L.P];
+    const double V5 = q[4 * L.P];
     const double rho = -V5 * p;
     double x;
     switch (kind) {
