@@ -226,6 +226,14 @@ tg_status tg_step(tg_handle* h, int n_steps, double* info4);
 /* Global kinetic energy and entropy integrals, compute_global (src/fv.cc:2175-2225). */
 tg_status tg_global(tg_handle* h, double* ke_out, double* entropy_out);
 
+/* compute_forces (src/force.cc:116-219) on the current state: for each force
+ * f (its face tags are tags[sum n_tags[<f] .. +n_tags[f]), the integrals over
+ * its boundary faces of the pressure force and, for Navier-Stokes, the viscous
+ * stress.  out[4f..4f+3] = inviscid x, y, viscous x, y.  Like the reference
+ * it applies the boundary condition of bface[f] (f the force index) on every
+ * face of force f. */
+tg_status tg_forces(tg_handle* h, int n_forces, const int* n_tags, const int* tags, double* out4);
+
 /* Steps, as tg_step, until output time `instance` has been reached (the
  * unsteady counter of src/fv.cc:2317-2336 exceeds it), the run is over, or
  * max_steps steps have been issued (a step past the stop is a no-op).
@@ -327,6 +335,11 @@ tg_status tg_batch_clock(tg_batch* b, int level, double* elapsed, int* counter, 
  * squared deviations, sm a Kahan-compensated sum of squares).  Records as for
  * tg_moments_get, extras bits 1 density, 2 mach, 4 entropy. */
 tg_status tg_batch_moments(tg_batch* b, int level, int extras, double* fm, double* sm, double* m2);
+/* Per-sample FP64 integrals of a level's current states, out[3 s + q]:
+ * q0 = sum 0.5 rho v^2 A, q1 = sum 0.5 rho u^2 A, q2 = sum -rho s/(gamma-1) A
+ * (the compute_global quantities, src/fv.cc:2186-2203, with the vertical
+ * kinetic energy first), periodic copies weighted as there. */
+tg_status tg_batch_integrals(tg_batch* b, int level, double* out);
 /* Launch shape of the flux and gradient kernels (sample tile x block size,
  * enumerated by TG_BQ_N_SHAPES), and the autotuner that times every shape for
  * `steps` steps from the current state (restored afterwards) and keeps the
@@ -346,6 +359,28 @@ typedef enum {
   TG_BQ_N_SHAPES = 6
 } tg_batch_query_key;
 tg_status tg_batch_query(tg_batch* b, int key, double* out);
+
+/* ---- surrogate network (no counterpart in the reference) ---------------- */
+/* The multilayer perceptron din -> 64 -> 64 -> 64 -> dout (GELU) used as the
+ * control variate of the multi-fidelity Monte Carlo estimator: FP32 training
+ * by hand-written forward / backward passes (mean squared error, Adam, batch
+ * reductions in fixed order) and BF16 tensor-core evaluation.  Parameters are
+ * one FP32 vector W1[64][din] b1 W2[64][64] b2 W3[64][64] b3 W4[dout][64] b4.
+ * din <= 32, dout <= 8. */
+typedef struct tg_mlp tg_mlp;
+tg_status tg_mlp_create(int din, int dout, unsigned long long seed, tg_mlp** out);
+tg_status tg_mlp_destroy(tg_mlp* m);
+const char* tg_mlp_last_error(const tg_mlp* m);
+int tg_mlp_n_params(const tg_mlp* m);
+tg_status tg_mlp_get_params(tg_mlp* m, float* theta);
+tg_status tg_mlp_set_params(tg_mlp* m, const float* theta);    /* also resets the optimiser */
+/* Mean squared error of one batch and its gradient with respect to theta. */
+tg_status tg_mlp_loss_grad(tg_mlp* m, const float* X, const float* T, int n, float* loss, float* grad);
+/* Adam over `epochs` passes of in-order mini-batches; losses[epoch] = last batch loss. */
+tg_status tg_mlp_train(tg_mlp* m, const float* X, const float* T, int n, int epochs, int batch, float lr,
+                       float* losses);
+/* precision 0: FP32, 1: BF16 tensor cores; on_device: X and Y are device pointers. */
+tg_status tg_mlp_predict(tg_mlp* m, const float* X, int n, float* Y, int precision, int on_device);
 
 /* ---- allocation-free residual norm ------------------------------------ */
 

@@ -284,6 +284,18 @@ int main(int argc, char* argv[]) {
     }
     ++iter;
     step_s.push_back(std::chrono::duration<double>(std::chrono::steady_clock::now() - ts).count());
+    if (full && !fv.param.force_data.empty()) {
+      // compute_forces follows every step in FiniteVolume::solve (src/fv.cc:2313)
+      fv.compute_forces(iter);
+      std::vector<double> fr;
+      for (unsigned f = 0; f < fv.param.force_data.size(); ++f) {
+        fr.push_back(fv.inv_force[f].value.x); fr.push_back(fv.inv_force[f].value.y);
+        fr.push_back(fv.visc_force[f].value.x); fr.push_back(fv.visc_force[f].value.y);
+      }
+      std::ostringstream tg;
+      tg << "s" << step << "_force";
+      dump.rec(tg.str(), fr);
+    }
     fv.elapsed_time += fv.dt_global;
     if (fv.time_instance_reached && fv.param.time_mode == "unsteady") {
       fv.counter++;

@@ -51,6 +51,7 @@ def lib():
         L.tor_logavg.argtypes = [C.c_double, C.c_double]
         L.tor_logavg.restype = C.c_double
         L.tor_counter.argtypes = [vp]
+        L.tor_forces.argtypes = [vp, C.c_int, C.POINTER(C.c_int), C.POINTER(C.c_int), dp]
         L.tor_moment_nvars.argtypes = [C.c_int]
         L.tor_moments_increment.argtypes = [vp, C.c_long, C.c_int, dp, dp, dp]
         L.tor_moments_merge.argtypes = [C.c_int, C.c_int, C.c_long, dp, dp, dp, C.c_long, dp, dp, dp]
@@ -125,6 +126,15 @@ class Oracle:
         info = np.empty(4)
         done = self.L.tor_step(self.h, n, _d(info))
         return done, info
+
+    def forces(self, forces: dict) -> np.ndarray:
+        """compute_forces for {name: [tags]} (insertion order): rows inviscid x, y, viscous x, y."""
+        n = np.array([len(t) for t in forces.values()], np.int32)
+        tags = np.array([x for t in forces.values() for x in t], np.int32)
+        out = np.empty((len(n), 4))
+        ip = C.POINTER(C.c_int)
+        self.L.tor_forces(self.h, len(n), n.ctypes.data_as(ip), tags.ctypes.data_as(ip), _d(out))
+        return out
 
     def global_integrals(self):
         a = C.c_double()

@@ -37,6 +37,7 @@ def param_text(cfg: dict) -> str:
     Monte Carlo keys: samples (list of sample ids), rnd_per_sample,
     ic ({variable: fparser expression}), constants ({name: value}),
     online_stat (bool), variables (extra moment variables, e.g. ["density"]).
+    forces: {name: [face tags]} (integrals section, compute_forces).
     """
     flux = cfg.get("flux", "kepes_tecno_roe")
     recon = cfg.get("reconstruct", "minmod")
@@ -58,6 +59,8 @@ def param_text(cfg: dict) -> str:
     consts = cfg.get("constants", {"dummy": 0.0})
     const_text = "\n".join(f"   {k} {v:.17g}" for k, v in consts.items())
     var_text = "\n".join(f"      {v}" for v in cfg.get("variables", []))
+    force_text = "\n".join("   force\n   {\n      " + name + "   " + "   ".join(str(t) for t in tags) + "\n   }"
+                           for name, tags in cfg.get("forces", {}).items())
     online = "yes" if cfg.get("online_stat", False) else "no"
     return f"""grid
 {{
@@ -140,6 +143,7 @@ exact_soln
 
 integrals
 {{
+{force_text}
 }}
 
 output

@@ -44,10 +44,11 @@ def _lib():
         L.tg_batch_time_steps.argtypes = [vp, i, dp]
         L.tg_batch_stream.argtypes = [vp, C.POINTER(vp)]
         L.tg_batch_query.argtypes = [vp, i, dp]
+        L.tg_batch_integrals.argtypes = [vp, i, dp]
         for n in ("tg_batch_create", "tg_batch_destroy", "tg_batch_set_state", "tg_batch_get_state",
                   "tg_batch_set_kh", "tg_batch_advance", "tg_batch_clock", "tg_batch_moments",
                   "tg_batch_set_shape", "tg_batch_tune", "tg_batch_time_steps", "tg_batch_stream",
-                  "tg_batch_query"):
+                  "tg_batch_query", "tg_batch_integrals"):
             getattr(L, n).restype = i
         _bound = True
     return L
@@ -123,6 +124,12 @@ class Batch:
         nvar = 5 + bin(extras).count("1")
         out = [np.empty((self.nv[level], nvar)) for _ in range(3)]
         self._chk(self.L.tg_batch_moments(self.h, level, extras, *[_d(a) for a in out]))
+        return out
+
+    def integrals(self, level: int) -> np.ndarray:
+        """(n_samples, 3): 0.5 rho v^2, 0.5 rho u^2 and -rho s/(gamma-1) integrated over the mesh."""
+        out = np.empty((self.S[level], 3))
+        self._chk(self.L.tg_batch_integrals(self.h, level, _d(out)))
         return out
 
     def set_shape(self, shape: int):

@@ -800,6 +800,60 @@ tg_status tg_advance(tg_handle* h, int instance, long max_steps, double* info5) 
   return TG_OK;
 }
 
+tg_status tg_forces(tg_handle* h, int n_forces, const int* n_tags, const int* tags, double* out) {
+  if (!h || n_forces < 1 || !n_tags || !tags || !out) return fail(h, TG_INVALID_ARG, "bad force specification");
+  const HostLayout& L = h->L;
+  const int nbf = (int)L.rb_type.size();
+  std::vector<int4> rec;
+  std::vector<int> off(1, 0);
+  const int* t = tags;
+  for (int f = 0; f < n_forces; ++f) {
+    if (n_tags[f] < 1) return fail(h, TG_INVALID_ARG, "a force needs at least one face tag (src/parameter.cc:652)");
+    // the condition the reference applies on every face of force f is that of bface[f] (src/force.cc:144-150)
+    int dq = -1, k0 = 0, k1 = 0;
+    for (int b = 0; b < nbf; ++b) {
+      bool mine = false;
+      for (int q = 0; q < n_tags[f]; ++q) mine = mine || L.rb_type[b] == t[q];
+      if (!mine) continue;
+      if (L.rb_dev[b] < 0) return fail(h, TG_INVALID_ARG, "force faces must not be periodic");
+      if (f < nbf) {
+        dq = L.rb_dev[f];
+        const int dv0 = L.b_v0[L.rb_dev[b]], dv1 = L.b_v1[L.rb_dev[b]];
+        const int q0 = L.new_of_old[L.rb_v0[f]];
+        k0 = (q0 == dv0) ? 0 : 1;   // value slot: vertex 0 of bface[f] or not (src/bc.h:568-654 via the table)
+        k1 = (q0 == dv1) ? 0 : 1;
+      }
+      rec.push_back(make_int4(L.rb_dev[b], dq, k0, k1));
+    }
+    if ((int)rec.size() == off.back()) return fail(h, TG_INVALID_ARG, "a force tag matches no boundary face");
+    off.push_back((int)rec.size());
+    t += n_tags[f];
+  }
+  tg_status st;
+  const int4* drec = nullptr;
+  const int* doff = nullptr;
+  double* dout = nullptr;
+  int4* r = nullptr;
+  int* o = nullptr;
+  TG_CUDA(h, cudaMalloc((void**)&r, rec.size() * sizeof(int4)));
+  TG_CUDA(h, cudaMalloc((void**)&o, off.size() * sizeof(int)));
+  TG_CUDA(h, cudaMalloc((void**)&dout, 4 * (size_t)n_forces * sizeof(double)));
+  drec = r; doff = o;
+  TG_CUDA(h, cudaMemcpyAsync(r, rec.data(), rec.size() * sizeof(int4), cudaMemcpyHostToDevice, h->stream));
+  TG_CUDA(h, cudaMemcpyAsync(o, off.data(), off.size() * sizeof(int), cudaMemcpyHostToDevice, h->stream));
+  // Navier-Stokes forces recompute the gradients of the current state (src/force.cc:123)
+  if (h->prm.model == 1) enqueue_gradient(h, 0, false, true, h->never);
+  k_forces<<<n_forces, kBlock, 0, h->stream>>>(h->prm, h->mv, view(h, 0), drec, doff, dout);
+  std::vector<double> hout(4 * (size_t)n_forces);
+  cudaError_t e = cudaMemcpyAsync(hout.data(), dout, hout.size() * sizeof(double), cudaMemcpyDeviceToHost, h->stream);
+  st = sync(h);
+  cudaFree(r); cudaFree(o); cudaFree(dout);
+  if (e != cudaSuccess) return fail(h, TG_CUDA_ERROR, cudaGetErrorString(e));
+  if (st != TG_OK) return st;
+  std::memcpy(out, hout.data(), hout.size() * sizeof(double));
+  return TG_OK;
+}
+
 tg_status tg_moments_init(tg_handle* h, int n_instances, int extras) {
   if (!h) return fail(h, TG_INVALID_ARG, "NULL handle");
   if (n_instances < 1 || extras < 0 || extras > 15) return fail(h, TG_INVALID_ARG, "bad moment layout");

@@ -296,7 +296,8 @@ tg_status tg_batch_create(const tg_batch_level* levels, int n_levels, const tg_m
     LevelMesh& m = V.m;
     m.nv = L.nv; m.ne = L.ne;
     // geometry formed in FP64, stored in FP32
-    std::vector<double> ux(L.ne), uy(L.ne), ar(L.ne);
+    std::vector<double> ux(L.ne), uy(L.ne), ar(L.ne), aw(L.nv);
+    for (int v = 0; v < L.nv; ++v) aw[v] = L.dcarea[v] * L.pweight[v];
     for (int e = 0; e < L.ne; ++e) {
       const double a = std::sqrt(L.e_nx[e] * L.e_nx[e] + L.e_ny[e] * L.e_ny[e]);
       const double ia = 1.0 / a;
@@ -306,7 +307,7 @@ tg_status tg_batch_create(const tg_batch_level* levels, int n_levels, const tg_m
     if ((st = bupload(b, vec, &m.field)) != TG_OK) { tg_batch_destroy(b); return st; }
     BU(L.e_a, e_a) BU(L.e_b, e_b) BU(ux, ux) BU(uy, uy) BU(ar, ar) BU(L.e_nx, nx) BU(L.e_ny, ny)
     BU(L.e_dx, dx) BU(L.e_dy, dy) BU(L.e_g0x, g0x) BU(L.e_g0y, g0y) BU(L.e_g1x, g1x) BU(L.e_g1y, g1y)
-    BU(L.ce_off, ce_off) BU(L.ce_ent, ce_ent) BU(L.dcarea, area) BU(L.inv6mc, inv6mc) BU(L.x, x) BU(L.y, y)
+    BU(L.ce_off, ce_off) BU(L.ce_ent, ce_ent) BU(L.dcarea, area) BU(L.inv6mc, inv6mc) BU(L.x, x) BU(L.y, y) BU(aw, aw)
 #undef BU
     const size_t vs = (size_t)L.nv * V.P;
     for (int r = 0; r < 3; ++r)
@@ -502,6 +503,28 @@ tg_status tg_batch_moments(tg_batch* b, int level, int extras, double* fm, doubl
       for (int c = 0; c < nvar; ++c) dst[c] = h[(size_t)w * n + (size_t)c * L.nv + i];
     }
   }
+  return TG_OK;
+}
+
+tg_status tg_batch_integrals(tg_batch* b, int level, double* out) {
+  if (!b || !out || level < 0 || level >= b->nlev) return bfail(b, TG_INVALID_ARG, "bad level or NULL output");
+  const Level& V = b->B.lev[level];
+  const int chunks = 16;
+  double* d = nullptr;
+  const size_t n = (size_t)chunks * V.S * 3;
+  TB_CUDA(b, cudaMalloc((void**)&d, n * sizeof(double)));
+  kb_integrals<8><<<(V.S >> 5) * chunks, 256, 0, b->stream>>>(V, b->prm, chunks, d);
+  std::vector<double> h(n);
+  cudaError_t e = cudaMemcpyAsync(h.data(), d, n * sizeof(double), cudaMemcpyDeviceToHost, b->stream);
+  if (e == cudaSuccess) e = cudaStreamSynchronize(b->stream);
+  cudaFree(d);
+  if (e != cudaSuccess) return bfail(b, TG_CUDA_ERROR, cudaGetErrorString(e));
+  for (int s = 0; s < V.S; ++s)
+    for (int c = 0; c < 3; ++c) {
+      double acc = 0.0;
+      for (int ch = 0; ch < chunks; ++ch) acc += h[((size_t)ch * V.S + s) * 3 + c];
+      out[(size_t)s * 3 + c] = acc;
+    }
   return TG_OK;
 }
 

@@ -38,6 +38,7 @@ struct LevelMesh {
   const float *g0x, *g0y, *g1x, *g1y;   // P1 gradient weights of the a / b side
   const int *ce_off, *ce_ent;      // per-vertex gather: (edge << 1) | side
   const float *area, *inv6mc;      // dual area, 1 / (6 median area)
+  const double* aw;                // dual area x periodic-copy weight (integrals)
   const double *x, *y;             // coordinates (initial conditions)
 };
 
@@ -552,6 +553,41 @@ __global__ void kb_moments(Level L, BParams k, int extras, int nvar, double* __r
   fm[o] = mean;
   sm[o] = sq;
   m2[o] = ssd;
+}
+
+// Per-sample integrals (FP64) of one level's current states, the
+// compute_global quantities (src/fv.cc:2186-2203) plus the vertical kinetic
+// energy: q0 = sum 0.5 rho v^2 A w, q1 = sum 0.5 rho u^2 A w,
+// q2 = sum -rho s / (gamma - 1) A w.  Block (sample group, vertex chunk);
+// partial[chunk][sample][3], summed over chunks in order by the host.
+template <int VT>
+__global__ void __launch_bounds__(32 * VT) kb_integrals(Level L, BParams k, int chunks, double* __restrict__ partial) {
+  const int lane = threadIdx.x & 31, vg = threadIdx.x >> 5;
+  const int sg = blockIdx.x / chunks, ch = blockIdx.x % chunks;
+  const int s = sg * 32 + lane;
+  const int per = (L.m.nv + chunks - 1) / chunks;
+  const int v0 = ch * per, v1 = min(L.m.nv, v0 + per);
+  double q[3] = {0.0, 0.0, 0.0};
+  for (int v = v0 + vg; v < v1; v += VT) {
+    const float* r = L.Q[0] + rows(v, kQ, L.P) + s;
+    const double u = r[0], w = r[L.P], p = r[2 * L.P], V5 = r[4 * L.P];
+    const double rho = -V5 * p;
+    const double aw = L.m.aw[v];
+    q[0] += 0.5 * rho * w * w * aw;
+    q[1] += 0.5 * rho * u * u * aw;
+    q[2] += -rho * (log(p) - (double)k.gamma * log(rho)) / ((double)k.gamma - 1.0) * aw;
+  }
+  __shared__ double red[3][VT][32];
+#pragma unroll
+  for (int c = 0; c < 3; ++c) red[c][vg][lane] = q[c];
+  __syncthreads();
+  if (vg == 0) {
+    for (int i = 1; i < VT; ++i)
+#pragma unroll
+      for (int c = 0; c < 3; ++c) q[c] += red[c][i][lane];
+#pragma unroll
+    for (int c = 0; c < 3; ++c) partial[((size_t)ch * L.S + s) * 3 + c] = q[c];
+  }
 }
 
 }  // namespace batch

@@ -483,6 +483,69 @@ __global__ void k_global(Params k, MeshView m, StateView s) {
   if (threadIdx.x == 0) { s.part[(size_t)blockIdx.x * 4] = red[0][0]; s.part[(size_t)blockIdx.x * 4 + 1] = red[1][0]; }
 }
 
+// ------------------------------------------------------------ forces
+// compute_forces (src/force.cc:116-219) for the force of block f: pressure
+// force sum over faces of 0.5 (p0 + p1) n and, for Navier-Stokes, the viscous
+// stress from the vertex gradients of u and v recovered from those of the
+// entropy variables.  Face record (d, dq, k0, k1): the face's device index, and
+// -- as the reference applies the condition of bface[f] with f the force
+// index -- the device index of bface[f] (-1: no condition) with the value
+// slots its evaluation uses.  Fixed-order block reduction.
+__global__ void k_forces(Params k, MeshView m, StateView s, const int4* __restrict__ faces,
+                         const int* __restrict__ off, double* __restrict__ out) {
+  const int f = blockIdx.x;
+  double acc[4] = {0.0, 0.0, 0.0, 0.0};
+  const int nv = m.nv;
+  for (int j = off[f] + threadIdx.x; j < off[f + 1]; j += blockDim.x) {
+    const int4 r = faces[j];
+    const int d = r.x, dq = r.y;
+    const int v0 = m.b_v0[d], v1 = m.b_v1[d];
+    const double nx = m.b_nx[d], ny = m.b_ny[d];
+    Prim s0 = load_prim(s.P, nv, v0), s1 = load_prim(s.P, nv, v1);
+    if (dq >= 0) {
+      bc_apply1(m.b_kind[dq], m.b_adiab[dq], m.b_val + (size_t)dq * 10 + 5 * r.z, m.b_nx[dq], m.b_ny[dq], s0);
+      bc_apply1(m.b_kind[dq], m.b_adiab[dq], m.b_val + (size_t)dq * 10 + 5 * r.w, m.b_nx[dq], m.b_ny[dq], s1);
+    }
+    const double pr = 0.5 * (s0.p + s1.p);
+    acc[0] += nx * pr;
+    acc[1] += ny * pr;
+    if (k.model == 1) {
+      const Ent e0 = prim2ent(k, s0), e1 = prim2ent(k, s1);
+      const double T = (s0.T + s1.T) / 2.0;
+      const double mu = viscosity(k, T);
+      const double f0 = 1.0 / e0.l, f1 = 1.0 / e1.l;
+      const double* G = s.G;
+      auto g = [&](int c, int v) { return G[(size_t)c * nv + v]; };
+      // u = -V2 / V5: grad u = -grad V2 / V5 + V2 grad V5 / V5^2 (src/force.cc:169-179)
+      const double ux0 = g(2, v0) * -f0 + g(6, v0) * (f0 * e0.vx / e0.l), uy0 = g(3, v0) * -f0 + g(7, v0) * (f0 * e0.vx / e0.l);
+      const double ux1 = g(2, v1) * -f1 + g(6, v1) * (f1 * e1.vx / e1.l), uy1 = g(3, v1) * -f1 + g(7, v1) * (f1 * e1.vx / e1.l);
+      const double vx0 = g(4, v0) * -f0 + g(6, v0) * (f0 * e0.vy / e0.l), vy0 = g(5, v0) * -f0 + g(7, v0) * (f0 * e0.vy / e0.l);
+      const double vx1 = g(4, v1) * -f1 + g(6, v1) * (f1 * e1.vy / e1.l), vy1 = g(5, v1) * -f1 + g(7, v1) * (f1 * e1.vy / e1.l);
+      const double gux = ux0 * 0.5 + ux1 * 0.5, guy = uy0 * 0.5 + uy1 * 0.5;
+      const double gvx = vx0 * 0.5 + vx1 * 0.5, gvy = vy0 * 0.5 + vy1 * 0.5;
+      const double div = gux + gvy;
+      const double sxx = 2.0 * mu * (gux - (1.0 / 3.0) * div);
+      const double syy = 2.0 * mu * (gvy - (1.0 / 3.0) * div);
+      const double sxy = mu * (guy + gvx);
+      acc[2] += -(sxx * nx + sxy * ny);
+      acc[3] += -(sxy * nx + syy * ny);
+    }
+  }
+  __shared__ double red[4][kBlock];
+#pragma unroll
+  for (int c = 0; c < 4; ++c) red[c][threadIdx.x] = acc[c];
+  __syncthreads();
+  for (int o = kBlock / 2; o > 0; o >>= 1) {
+    if ((int)threadIdx.x < o)
+#pragma unroll
+      for (int c = 0; c < 4; ++c) red[c][threadIdx.x] += red[c][threadIdx.x + o];
+    __syncthreads();
+  }
+  if (threadIdx.x == 0)
+#pragma unroll
+    for (int c = 0; c < 4; ++c) out[4 * f + c] = red[c][0];
+}
+
 // ------------------------------------------------------------ MC moments
 // increment_moments (src/fv.cc:595-694) for the k-th sample of a group, one
 // thread per vertex.  Moment arrays are [var][vertex] with the per-vertex

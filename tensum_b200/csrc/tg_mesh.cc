@@ -227,6 +227,10 @@ std::string build_layout(const tg_mesh& m, const tg_bc_table* bc, bool need_visc
   L.b_nx.resize(nb); L.b_ny.resize(nb); L.b_val.assign((size_t)nb * 10, 0.0);
   L.bf_face_nx.resize(nb); L.bf_face_ny.resize(nb); L.bf_face_v0.resize(nb); L.bf_face_v1.resize(nb);
   std::vector<int> ref_bface_of_dev(nb);
+  L.rb_type.assign(m.bface_type, m.bface_type + nbf);
+  L.rb_v0.resize(nbf);
+  L.rb_dev.resize(nbf);
+  for (int b = 0; b < nbf; ++b) { L.rb_v0[b] = m.bface_vertex[2 * b]; L.rb_dev[b] = dev_bface[b]; }
   for (int b = 0; b < nbf; ++b) {
     int d = dev_bface[b];
     if (d < 0) continue;

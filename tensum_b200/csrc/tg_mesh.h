@@ -38,6 +38,9 @@ struct HostLayout {
   // non-periodic boundary faces
   std::vector<int> b_v0, b_v1, b_kind, b_adiab, b_cell;
   std::vector<double> b_nx, b_ny, b_val;  // b_val: nb*2*5 (T,u,v,w,p) at vertex 0 / 1
+  // every reference boundary face: its tag, vertex 0 (reference numbering) and
+  // its device index (-1 for periodic faces), for the force integrals
+  std::vector<int> rb_type, rb_v0, rb_dev;
   // per-vertex boundary / viscous gather: entry = (index << 2) | type
   //   type 0: inviscid boundary flux (2*b + k)     type 1: gradient boundary correction (b)
   //   type 2: viscous unit contribution (3*u + k)  type 3: viscous boundary flux (b)

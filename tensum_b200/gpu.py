@@ -20,7 +20,7 @@ EXPORTS = ["tg_create", "tg_destroy", "tg_last_error", "tg_abi_version", "tg_set
            "tg_store_conserved_old", "tg_compute_dt", "tg_gradients", "tg_residual", "tg_update",
            "tg_residual_norm", "tg_end_step", "tg_step", "tg_global", "tg_stream", "tg_time_phase", "tg_query",
            "tg_advance", "tg_moments_init", "tg_moments_increment", "tg_moments_get", "tg_moments_export",
-           "tg_moments_merge", "tg_moments_merge_device", "tg_moments_finalize"]
+           "tg_moments_merge", "tg_moments_merge_device", "tg_moments_finalize", "tg_forces"]
 
 PHASE = {"gradient": 0, "flux": 1, "update": 2, "dt": 3, "step": 4}
 QUERY = {"n_vertex": 0, "n_edge": 1, "n_bface": 2, "kernels_per_step": 3, "device_bytes": 4, "kernels_per_flux": 5}
@@ -63,6 +63,7 @@ def load():
     L.tg_time_phase.argtypes = [vp, i, i, dp]
     L.tg_query.argtypes = [vp, i, dp]
     L.tg_advance.argtypes = [vp, i, C.c_long, dp]
+    L.tg_forces.argtypes = [vp, i, C.POINTER(i), C.POINTER(i), dp]
     L.tg_moments_init.argtypes = [vp, i, i]
     L.tg_moments_increment.argtypes = [vp, i, C.c_long]
     L.tg_moments_get.argtypes = [vp, i, dp, dp, dp]
@@ -167,6 +168,17 @@ class Solver:
         a, b = C.c_double(), C.c_double()
         self._chk(self.L.tg_global(self.h, C.byref(a), C.byref(b)))
         return a.value, b.value
+
+    def forces(self, forces: dict) -> np.ndarray:
+        """compute_forces on the current state for {name: [face tags]} (in insertion
+        order, like the reference's integrals section): one row per force with the
+        inviscid x, y and viscous x, y components."""
+        n = np.array([len(t) for t in forces.values()], np.int32)
+        tags = np.array([x for t in forces.values() for x in t], np.int32)
+        out = np.empty((len(n), 4))
+        ip = C.POINTER(C.c_int)
+        self._chk(self.L.tg_forces(self.h, len(n), n.ctypes.data_as(ip), tags.ctypes.data_as(ip), _d(out)))
+        return out
 
     # ---- output-time stepping and Monte Carlo moments
     def advance(self, instance: int, max_steps: int = 1 << 40) -> np.ndarray:

@@ -41,6 +41,8 @@ CASES = {
     "cyl_ns_isothermal": _cyl("kepes_tecno_roe", "minmod", "ns", bc="isothermal"),
     "cyl_slip": _cyl("kepes_tecno_roe", "minmod", "euler", bc="slip"),
     "cyl_inlet_outlet": _cyl("kepes_tecno_roe", "minmod", "euler", bc="inlet_outlet"),
+    "cyl_ns_forces": _cyl("kepes_tecno_roe", "minmod", "ns", forces={"cyl": [1], "outer": [2]}),
+    "cyl_slip_forces": _cyl("kepes_tecno_rusanov", "minmod", "euler", bc="slip", forces={"cyl": [1]}),
 }
 
 
@@ -74,6 +76,8 @@ def build_case(spec: dict):
                model=spec.get("model", "euler"), mu_ref=0.002 if spec.get("model") == "ns" else 0.0,
                tvb_M=spec.get("tvb_M", 1.0), ev_alpha=spec.get("ev_alpha", 0.0), ev_beta=spec.get("ev_beta", 0.0),
                time_stamps=1, cfl=0.8)
+    if "forces" in spec:
+        cfg["forces"] = dict(spec["forces"])
     return m, cfg, prim0
 
 

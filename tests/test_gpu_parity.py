@@ -29,7 +29,7 @@ def make_solver(mesh, cfg):
 @pytest.mark.parametrize("name", golden_names())
 def test_stage_parity_with_reference(name):
     spec, mesh, cfg, prim0, d = load_golden(name)
-    s, _ = make_solver(mesh, cfg)
+    s, P = make_solver(mesh, cfg)
     s.set_state(prim0)
     if spec["dump_steps"] == 0:
         info = s.step(spec["steps"])
@@ -52,6 +52,16 @@ def test_stage_parity_with_reference(name):
             s.update(r)
             assert rel_l2(s.get_state(), d[f"s{st}r{r}_prim"]) <= TOL_STATE_STAGE, f"state step {st} stage {r}"
         s.end_step()
+        if "forces" in cfg:
+            got, ref = s.forces(cfg["forces"]), d[f"s{st}_force"].reshape(-1, 4)
+            # a force is a sum over a closed boundary that cancels to far below its
+            # terms: the tolerance scales with the summed term magnitude max|p| sum|n|
+            g = P.geom
+            nrm = np.hypot(g.bface_normal[:, 0], g.bface_normal[:, 1])
+            pmax = np.abs(s.get_state()[:, 1]).max()
+            for f, tags in enumerate(cfg["forces"].values()):
+                scale = pmax * nrm[np.isin(g.bface_type, tags)].sum()
+                assert np.all(np.abs(got[f] - ref[f]) <= 1e-12 * scale), (st, f, got[f], ref[f])
 
 
 def _run_pair(mesh, cfg, prim0, steps):

@@ -37,6 +37,8 @@ def test_oracle_matches_reference_exactly(name):
             o.update(r)
             assert np.array_equal(o.get_prim().ravel(), d[f"s{s}r{r}_prim"]), f"state step {s} stage {r}"
         o.end_step()
+        if "forces" in cfg:
+            assert np.array_equal(o.forces(cfg["forces"]).ravel(), d[f"s{s}_force"]), f"forces step {s}"
 
 
 @pytest.mark.parametrize("name", ["sq_roe_minmod", "cyl_ns"])
