@@ -22,6 +22,16 @@ Keys beyond the base contract:
   cpu_baseline  the reference's own CPU code on this host (rank 0, N = 1)
   e2e           same metric through the C ABI with host buffers every step
   clocks        SM clock and throttle reasons sampled during the timed region
+
+    python bench.py --workload mc [--samples S] [--n 257] [--steps K]
+
+measures the Monte Carlo configuration instead: S Kelvin-Helmholtz samples
+(rnd rows, device-generated initial states) on an n x n mesh advanced together
+by the batched FP32 engine (KEPES-TeCNO-Rusanov, minmod), against the FP64
+per-sample path on the same GPU, with the QoI error of the FP32 members
+against FP64 runs and the time to a 1 % relative standard error of the mean
+QoI for plain FP64 MC, batched FP32 MC and batched FP32 with the surrogate
+control variate.
 """
 from __future__ import annotations
 
@@ -58,6 +68,9 @@ def parse():
     ap.add_argument("--seed", type=int, default=0)
     ap.add_argument("--e2e-steps", type=int, default=10)
     ap.add_argument("--no-cpu-baseline", action="store_true")
+    ap.add_argument("--workload", default="single", choices=["single", "mc"])
+    ap.add_argument("--samples", type=int, default=4096, help="ensemble size of --workload mc")
+    ap.add_argument("--no-mc", action="store_true", help="skip the Monte Carlo object of the default line")
     a = ap.parse_args()
     a.flux_list = [(f, r) for f, r in FLUXES if f in a.fluxes.split(",")]
     return a
@@ -338,6 +351,15 @@ def run_ours(args):
         if r is not None:
             cpu = {k: r[k] for k in ("value", "unit", "cores", "kind", "sample", "per_flux")}
 
+    mc = None
+    if rank == 0 and world == 1 and not args.no_mc:
+        solvers.clear()          # release the single-solve handles before the ensemble
+        s_e2e = None
+        mc = mc_line(257, 4096, 20, 3, args.seed)
+        mc = {k: mc[k] for k in ("metric", "value", "unit", "ms_per_step", "config", "autotune", "fp64_per_sample",
+                                 "roofline", "qoi", "time_to_rse", "cv", "clocks")}
+        mc["command"] = "python bench.py --workload mc --steps 20 --warmup 3"
+
     if dist:
         dist.barrier()
         dist.destroy_process_group()
@@ -347,13 +369,150 @@ def run_ours(args):
             "warmup": max(3, args.warmup), "ms_per_step": total_ms / args.steps, "higher_is_better": True,
             "scaling": "weak", "vs_baseline": None, "dtype": "f64", "data": "synthetic (seeded mesh and field)",
             "config": config_dict(args, m, E), "per_flux": per, "roofline": roof, "step_roofline": step_roof,
-            "cpu_baseline": cpu, "e2e": e2e, "gpu_launches": launches, "clocks": clk.summary(), "impl": "ours"}
+            "cpu_baseline": cpu, "e2e": e2e, "gpu_launches": launches, "clocks": clk.summary(), "impl": "ours",
+            "mc": mc}
     print(json.dumps(line))
+    return 0
+
+
+# ----------------------------------------------------------------------------- Monte Carlo workload
+MC_BYTES_PER_VSS = 187.0   # FP32 batched compulsory bytes per vertex-sample-stage (state, U_old, gradients)
+
+
+def mc_line(n, S, K, W, seed):
+    """Batched FP32 ensemble throughput and time to QoI error (one GPU): the JSON object."""
+    import torch
+    from tensum_b200 import abi, batch, cases, cv, gpu, mlp, preproc
+    torch.cuda.set_device(0)
+    m = cases.kh_mesh(n, seed)
+    V = m.n_vertex
+    g = preproc.preprocess(m)
+    base = dict(flux="kepes_tecno_rusanov", reconstruct="minmod", boundary={t: ("periodic", {}) for t in (1, 2, 3, 4)},
+                cfl=0.8, time_stamps=1)
+    t_q = 0.05                                     # QoI time for the accuracy and time-to-error parts
+    rows = np.stack([cases.kh_rnd_row(seed * 1000003 + s) for s in range(S)])
+
+    # throughput: K graph-replayed steps of every sample (final time far away)
+    P_long = abi.Problem(g, dict(base, final_time=1.0e9))
+    b = batch.Batch([(P_long, S)])
+    b.set_kh(0, rows)
+    shape, tune_ms = b.tune(3)
+    b.time_steps(W)
+    with ClockSampler(0) as clk:
+        ms = b.time_steps(K) * K           # CUDA events on the batch's stream around K graph replays
+    value = V * S * 3 * K / (ms / 1e3)
+    launches = int(b.query("kernels_per_step")) * K
+    del b
+    peak, peak_kind = measured_peaks()
+
+    # FP64 per-sample path on the same mesh
+    s64 = gpu.Solver(P_long)
+    s64.set_state(cases.kh_ic_rnd(m.coords, rows[0]))
+    s64.step(W)
+    ms64 = s64.time_phase("step", max(20, K))
+    del s64
+
+    # QoIs at t_q: every sample batched, a subset in FP64
+    P_q = abi.Problem(g, dict(base, final_time=t_q))
+    bq = batch.Batch([(P_q, S)])
+    bq.set_kh(0, rows)
+    torch.cuda.synchronize()
+    t0 = time.perf_counter()
+    info = bq.advance(1)
+    torch.cuda.synchronize()
+    t_batch = time.perf_counter() - t0
+    y = bq.integrals(0)
+    n_sub = 32
+    s64 = gpu.Solver(P_q)
+    y64, steps64 = [], []
+    w = np.ones(V)
+    for st in m.periodic_sets:
+        w[st] = 1.0 / len(st)
+    aw = g.dcarea * w
+    t0 = time.perf_counter()
+    for s in range(n_sub):
+        s64.set_state(cases.kh_ic_rnd(m.coords, rows[s]))
+        inf = s64.advance(1)
+        steps64.append(inf[3])
+        q = s64.get_state()
+        rho = q[:, 1] / q[:, 0]
+        ent = np.log(q[:, 1]) - 1.4 * np.log(rho)
+        y64.append([np.sum(0.5 * rho * q[:, 3] ** 2 * aw), np.sum(0.5 * rho * q[:, 2] ** 2 * aw),
+                    np.sum(-rho * ent / 0.4 * aw)])
+    t_fp64_sample = (time.perf_counter() - t0) / n_sub
+    y64 = np.array(y64)
+    qerr = np.abs(y[:n_sub] - y64) / np.abs(y64)
+    fm32, _, m232 = bq.moments(0)
+    del bq
+
+    # time to a 1 % relative standard error of the mean of q0 (vertical kinetic energy)
+    n_train = min(1024, S // 4)
+    net = mlp.MLP(rows.shape[1], 3, seed=1)
+    torch.cuda.synchronize()
+    t0 = time.perf_counter()
+    net.fit(rows[:n_train], y[:n_train], epochs=300, batch=128, lr=2e-3)
+    t_train = time.perf_counter() - t0
+    x_extra = np.random.default_rng(10 ** 7 + seed).uniform(0.0, 1.0, size=(1 << 20, rows.shape[1]))
+    t0 = time.perf_counter()
+    g_extra = net.predict(x_extra, precision=1)
+    t_surr = time.perf_counter() - t0
+    g_ev = net.predict(rows[n_train:], precision=1)
+    r = cv.estimate(y[n_train:], g_ev, g_extra)
+    t_batch_sample = t_batch / S
+    ttr = {}
+    for rse in (0.01, 0.001):
+        n_plain = float(cv.samples_for_rse(y[n_train:, 0], None, rse)[0])
+        n_cv = float(cv.samples_for_rse(y[n_train:, 0], g_ev[:, 0], rse)[0])
+        t = {"plain_fp64_mc_s": n_plain * t_fp64_sample, "batched_fp32_mc_s": n_plain * t_batch_sample,
+             "batched_fp32_cv_s": (n_train + n_cv) * t_batch_sample + t_train + t_surr}
+        ttr[f"rse_{rse:g}"] = dict(t, samples_plain=n_plain, samples_cv=n_cv,
+                                   speedup_batched_vs_plain_fp64=t["plain_fp64_mc_s"] / t["batched_fp32_mc_s"],
+                                   speedup_cv_vs_plain_fp64=t["plain_fp64_mc_s"] / t["batched_fp32_cv_s"])
+    line = {"metric": "vertex-sample-stage updates/s (FP32 ensemble); time to 1% RSE of the mean QoI vs plain FP64 MC",
+            "value": value, "unit": "vertex-sample-stage updates/s", "n_gpus": 1, "steps": K, "warmup": W,
+            "ms_per_step": ms / K, "higher_is_better": True, "scaling": "weak", "vs_baseline": None,
+            "dtype": "f32 members, f64 geometry / log-mean series / moments", "data": "synthetic (seeded rnd rows)",
+            "config": {"workload": f"kelvin-helmholtz {n}x{n} periodic ensemble of {S} samples, kepes_tecno_rusanov(minmod), "
+                                   "ssprk3 cfl 0.8", "mesh_vertices": V, "samples": S,
+                       "l2": "working set > L2 (no flush needed)"},
+            "autotune": {"shape": shape, "ms_per_step_by_shape": [float(x) for x in tune_ms]},
+            "fp64_per_sample": {"ms_per_step": ms64, "value": V * 3 / (ms64 / 1e3),
+                                "batched_speedup_per_sample_stage": value / (V * 3 / (ms64 / 1e3))},
+            "roofline": {"bound": "hbm", "kernel": "whole batched step", "bytes_per_vertex_sample_stage": MC_BYTES_PER_VSS,
+                         "achieved": MC_BYTES_PER_VSS * value / 1e9, "peak": peak, "unit": "GB/s",
+                         "frac": MC_BYTES_PER_VSS * value / 1e9 / peak, "traffic": None, "peak_source": peak_kind},
+            "qoi": {"time": t_q, "names": ["0.5 rho v^2", "0.5 rho u^2", "-rho s/(gamma-1)"],
+                    "fp32_vs_fp64_rel_err_max": [float(x) for x in qerr.max(0)], "fp64_subset": n_sub,
+                    "batched_steps_issued": float(info[0]), "fp64_steps_mean": float(np.mean(steps64))},
+            "time_to_rse": dict(ttr, qoi="0.5 rho v^2 (mean)", n_train=n_train, train_s=t_train,
+                                surrogate_evals=1 << 20, surrogate_eval_s=t_surr,
+                                fp64_sample_s=t_fp64_sample, batched_sample_s=t_batch_sample,
+                                note="sample counts from the ensemble's variance and control-variate residual "
+                                     "variance; FP64 per-sample time measured on a 32-sample subset"),
+            "cv": {"gain": [float(x) for x in r["gain"]], "used": [bool(x) for x in r["used"]],
+                   "mean": [float(x) for x in r["mean"]], "plain_mean": [float(x) for x in r["plain_mean"]],
+                   "se_mean": [float(x) for x in r["se_mean"]]},
+            "gpu_launches": launches, "clocks": clk.summary(), "impl": "ours",
+            "e2e": {"value": V * S * 3 * float(info[0]) / t_batch, "unit": "vertex-sample-stage updates/s",
+                    "h2d_bytes_per_step": 0, "d2h_bytes_per_step": 0,
+                    "path": "tg_batch_advance to the QoI time, wall clock, inputs generated on the device from rnd rows"}}
+    return line
+
+
+def run_mc(args):
+    n = args.n if args.n != 1025 else 257
+    print(json.dumps(mc_line(n, args.samples, args.steps, max(3, args.warmup), args.seed)))
     return 0
 
 
 def main():
     args = parse()
+    if args.workload == "mc":
+        if args.impl == "reference":
+            print(json.dumps({"impl": "reference", "unavailable": "the reference has no batched ensemble path; its MC "
+                              "groups run one sample after another (see the single-solve reference arm)"}))
+            return 0
+        return run_mc(args)
     if args.impl == "reference":
         return run_reference(args)
     return run_ours(args)
