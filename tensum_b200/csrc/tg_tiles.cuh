@@ -41,6 +41,9 @@
 #ifndef TG_FLUX_MINB_CENTRAL
 #define TG_FLUX_MINB_CENTRAL 3
 #endif
+#ifndef TG_GRAD_MINB
+#define TG_GRAD_MINB 3         // resident gradient / dt CTAs per SM the register budget is sized for
+#endif
 
 namespace tg {
 
@@ -104,7 +107,7 @@ __host__ __device__ constexpr int grad_vertex_doubles(bool first) { return first
 __host__ __device__ constexpr int grad_edge_doubles(bool first) { return first ? 6 : 4; }
 
 template <bool FIRST, bool GRAD>
-__global__ void __launch_bounds__(kTileThreads) k_tile_grad(Params k, MeshView m, TileView t, StateView s,
+__global__ void __launch_bounds__(kTileThreads, TG_GRAD_MINB) k_tile_grad(Params k, MeshView m, TileView t, StateView s,
                                                             Scalars* sc, int lmax, int emax,
                                                             const int* __restrict__ done) {
   if (*done) return;
