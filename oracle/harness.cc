@@ -259,6 +259,8 @@ int main(int argc, char* argv[]) {
       dump.rec(tg.str() + "g", std::vector<double>(1, fv.dt_global));
     }
     if (fv.param.liou_fix) fv.compute_ssw();
+    if (fv.param.time_scheme == "rk4")   // src/fv.cc:2287-2293
+      for (unsigned int i = 0; i < fv.grid.n_vertex; ++i) fv.residual2[i].zero();
     for (unsigned int r = 0; r < fv.param.n_rks; ++r) {
       fv.compute_residual();
       if (r == fv.param.n_rks - 1) fv.compute_residual_norm(iter);

@@ -262,17 +262,21 @@ void enqueue_norm_final(tg_handle* h, int nblocks, bool use_sc_iter, long long i
 // stage r reads buffer r and writes buffer (r+1)%3, so the step ends in buffer 0.
 void enqueue_step(tg_handle* h) {
   k_step_begin<<<1, 1, 0, h->stream>>>(h->ctl, h->sc, h->done);
-  for (int r = 0; r < 3; ++r) {
-    const bool first = (r == 0), last = (r == 2);
+  // stage r reads buffer bin and writes bout: ssprk3 0->1->2->0, rk4 0->1->2->1->0,
+  // so a step always ends in buffer 0 and no stage writes the buffer it reads
+  const int rk4_in[4] = {0, 1, 2, 1}, rk4_out[4] = {1, 2, 1, 0};
+  for (int r = 0; r < h->ctl.n_rks; ++r) {
+    const bool first = (r == 0), last = (r == h->ctl.n_rks - 1);
+    const int bin = h->ctl.scheme == 1 ? rk4_in[r] : r, bout = h->ctl.scheme == 1 ? rk4_out[r] : (r + 1) % 3;
     if (first && h->ctl.time_step > 0.0) {
       k_store_old<<<nblk(h->mv.nv), kBlock, 0, h->stream>>>(h->prm, h->mv, view(h, 0), h->done);
-      enqueue_gradient(h, r, false, h->grads_needed, h->done);
+      enqueue_gradient(h, bin, false, h->grads_needed, h->done);
     } else {
-      enqueue_gradient(h, r, first, h->grads_needed, h->done);   // first stage: + dt, U_old
+      enqueue_gradient(h, bin, first, h->grads_needed, h->done);   // first stage: + dt, U_old
     }
     if (first) k_dt_final<<<1, 1, 0, h->stream>>>(h->ctl, h->sc, h->done);
-    enqueue_boundary(h, r, h->done);
-    enqueue_tile_flux(h, r, MODE_UPDATE, r, last, (r + 1) % 3, h->done);
+    enqueue_boundary(h, bin, h->done);
+    enqueue_tile_flux(h, bin, MODE_UPDATE, r, last, bout, h->done);
     if (last) enqueue_norm_final(h, h->L.ntiles, true, 0, h->done);
   }
   k_step_end<<<1, 1, 0, h->stream>>>(h->ctl, h->sc, h->done);
@@ -435,8 +439,11 @@ tg_status tg_create(const tg_mesh* mesh, const tg_material* mat, const tg_bc_tab
   int ndev = 0;
   if (cudaGetDeviceCount(&ndev) != cudaSuccess || ndev == 0)
     return fail(nullptr, TG_NO_DEVICE, "no CUDA device visible; the GPU path has no CPU fallback");
-  if (opt->time_scheme != TG_TIME_SSPRK3)
-    return fail(nullptr, TG_NOT_SUPPORTED, "only the ssprk3 time scheme is implemented on the device");
+  // Heun is not offered: the reference's update (src/fv.cc:1681-1690) assigns
+  // U = (r/2) U_old - (1 - r/2) dt R after scaling U, which drops U at r = 0,
+  // so there is no working reference behaviour to reproduce.
+  if (opt->time_scheme != TG_TIME_SSPRK3 && opt->time_scheme != TG_TIME_RK4)
+    return fail(nullptr, TG_NOT_SUPPORTED, "the device path runs ssprk3 and rk4 (heuns: see tg_create)");
   if (mat->flux_scheme < 0 || mat->flux_scheme > 5 || mat->reconstruct_scheme < 0 || mat->reconstruct_scheme > 6)
     return fail(nullptr, TG_INVALID_ARG, "unknown flux or reconstruction scheme");
   if (!(mat->gamma > 1.0) || !(mat->gas_const > 0.0)) return fail(nullptr, TG_INVALID_ARG, "gamma must be > 1, gas_const > 0");
@@ -498,7 +505,7 @@ tg_status tg_create(const tg_mesh* mesh, const tg_material* mat, const tg_bc_tab
   if ((st = dev_alloc(h, (n), &h->sv.field)) != TG_OK) { tg_destroy(h); return st; }
   AL(P, 4 * nv) AL(W, 4 * nv) AL(G, 8 * nv) AL(R, 4 * nv) AL(Uold, 4 * nv) AL(dt, nv)
   AL(Fb, 8 * (size_t)L.nb) AL(Fv, 9 * (size_t)L.nvu) AL(Fvb, 3 * (size_t)L.nb)
-  AL(part, 4 * (size_t)std::max(h->nblocks_v, L.ntiles))
+  AL(part, 4 * (size_t)std::max(h->nblocks_v, L.ntiles)) AL(R2, 4 * nv)
 #undef AL
   h->Pb[0] = h->sv.P;
   h->Wb[0] = h->sv.W;
@@ -540,13 +547,15 @@ tg_status tg_create(const tg_mesh* mesh, const tg_material* mat, const tg_bc_tab
   const double* tip = nullptr;
   if ((st = dev_upload(h, ti, &tip)) != TG_OK) { tg_destroy(h); return st; }
   Control& c = h->ctl;
-  c.time_mode = opt->time_mode; c.n_rks = 3; c.ntinst = (int)ti.size(); c.time_step = opt->time_step;
+  c.time_mode = opt->time_mode; c.n_rks = opt->time_scheme == TG_TIME_RK4 ? 4 : 3;
+  c.scheme = opt->time_scheme == TG_TIME_RK4 ? 1 : 0;
+  c.ntinst = (int)ti.size(); c.time_step = opt->time_step;
   c.min_residue = opt->min_residue; c.max_iter = opt->max_iter; c.final_time = opt->final_time; c.tinst = tip;
 
   h->kernels_per_flux = residual_kernels(h);
   // step_begin + gradient/dt passes + per stage (boundary, viscous, tiled flux) + [store_old] + dt_final
   // + norm_final + step_end
-  h->kernels_per_step = 1 + (1 + (h->grads_needed ? 2 : 0)) + 3 * residual_kernels(h) + (c.time_step > 0.0 ? 1 : 0) +
+  h->kernels_per_step = 1 + (1 + (h->grads_needed ? c.n_rks - 1 : 0)) + c.n_rks * residual_kernels(h) + (c.time_step > 0.0 ? 1 : 0) +
                         1 + 1 + 1;
   if ((st = dev_alloc(h, 5 * nv, &h->raw)) != TG_OK) { tg_destroy(h); return st; }
   if ((st = dev_alloc(h, 1, &h->bad)) != TG_OK) { tg_destroy(h); return st; }
@@ -700,7 +709,7 @@ tg_status tg_residual(tg_handle* h, double* res_out) {
 
 tg_status tg_update(tg_handle* h, int r) {
   if (!h) return fail(h, TG_INVALID_ARG, "NULL handle");
-  if (r < 0 || r > 2) return fail(h, TG_INVALID_ARG, "stage index must be 0..2 for ssprk3");
+  if (r < 0 || r >= h->ctl.n_rks) return fail(h, TG_INVALID_ARG, "stage index out of range for the time scheme");
   enqueue_update(h, r, false, h->never);
   tg_status st = sync(h);
   if (st != TG_OK) return st;

@@ -43,6 +43,7 @@ struct StateView {
   double* Fv;     // 3*3*nvu  (x-mom, y-mom, energy)
   double* Fvb;    // 3*nb
   double* part;   // block partial sums
+  double* R2;     // 4*nv  RK4 residual accumulator (residual2 of src/fv.h)
 };
 
 // Step bookkeeping kept on the device so that whole steps replay from a CUDA graph.
@@ -63,7 +64,8 @@ struct Scalars {
 
 struct Control {
   int time_mode;       // 0 steady, 1 unsteady
-  int n_rks;
+  int n_rks;           // stages per step: 3 (ssprk3) or 4 (rk4)
+  int scheme;          // 0 ssprk3, 1 rk4
   int ntinst;
   double time_step;
   double min_residue;
@@ -336,6 +338,42 @@ __global__ void k_dt_final(Control ctl, Scalars* sc, const int* __restrict__ don
 
 // update_solution for SSP-RK3 (src/fv.cc:1641-1652), fused with the residual-norm
 // partial sums of compute_residual_norm (src/fv.cc:1822-1841) at the last stage.
+// New conserved state of vertex v at stage r from its residual: the Shu-Osher
+// SSP-RK3 stage (src/fv.cc:1635-1658, src/constants.h:4-6) or the classical RK4
+// stage (src/fv.cc:1667-1679, src/constants.h:9), which accumulates
+// sum_r R_r / rks_r in R2 (zero before the first stage, src/fv.cc:2287-2293).
+// q0 is the stage's input state, uo U_old, factor = dt / area.
+__device__ __forceinline__ Cons rk_stage(const Params& k, const Control& ctl, const StateView& s, int nv, int v, int r,
+                                         const Prim& q0, const double* uo, double factor, double r0, double r1,
+                                         double r2, double r3) {
+  Cons c;
+  if (ctl.scheme == 1) {
+    const double rks[4] = {1.0, 1.0 / 2.0, 1.0 / 2.0, 1.0};
+    const double inv = 1.0 / rks[r];
+    double a0 = 0.0, a1 = 0.0, a2 = 0.0, a3 = 0.0;
+    if (r > 0) { a0 = s.R2[v]; a1 = s.R2[nv + v]; a2 = s.R2[2 * nv + v]; a3 = s.R2[3 * nv + v]; }
+    a0 += r0 * inv; a1 += r1 * inv; a2 += r2 * inv; a3 += r3 * inv;
+    if (r < 3) { s.R2[v] = a0; s.R2[nv + v] = a1; s.R2[2 * nv + v] = a2; s.R2[3 * nv + v] = a3; }
+    const bool fin = (r == 3);
+    const double c2 = fin ? -factor / 6.0 : -factor * rks[r < 3 ? r + 1 : 3];
+    c.r = uo[0] * 1.0 + (fin ? a0 : r0) * c2;
+    c.mx = uo[1] * 1.0 + (fin ? a1 : r1) * c2;
+    c.my = uo[2] * 1.0 + (fin ? a2 : r2) * c2;
+    c.E = uo[3] * 1.0 + (fin ? a3 : r3) * c2;
+    return c;
+  }
+  const double a_rk[3] = {0.0, 3.0 / 4.0, 1.0 / 3.0};
+  const double b_rk[3] = {1.0, 1.0 / 4.0, 2.0 / 3.0};
+  c = prim2con(k, q0);
+  const double br = b_rk[r], ar = a_rk[r], c2 = -factor * br;
+  c.r *= br; c.mx *= br; c.my *= br; c.E *= br;
+  c.r += uo[0] * ar + r0 * c2;
+  c.mx += uo[1] * ar + r1 * c2;
+  c.my += uo[2] * ar + r2 * c2;
+  c.E += uo[3] * ar + r3 * c2;
+  return c;
+}
+
 __global__ void k_update(Params k, MeshView m, StateView s, Control ctl, Scalars* sc, int r, int do_norm,
                          const int* __restrict__ done) {
   if (*done) return;
@@ -343,8 +381,6 @@ __global__ void k_update(Params k, MeshView m, StateView s, Control ctl, Scalars
   const int nv = m.nv;
   double nrm[4] = {0.0, 0.0, 0.0, 0.0};
   if (i < nv) {
-    const double a_rk[3] = {0.0, 3.0 / 4.0, 1.0 / 3.0};
-    const double b_rk[3] = {1.0, 1.0 / 4.0, 2.0 / 3.0};
     double R0 = s.R[i], R1 = s.R[nv + i], R2 = s.R[2 * nv + i], R3 = s.R[3 * nv + i];
     double area = m.dcarea[i];
     if (do_norm) {
@@ -354,13 +390,8 @@ __global__ void k_update(Params k, MeshView m, StateView s, Control ctl, Scalars
     }
     double dtv = (ctl.time_mode == 1 || ctl.time_step > 0.0) ? sc->dt_global : s.dt[i];
     double factor = dtv / (1.0 * area);
-    Cons c = prim2con(k, load_prim(s.P, nv, i));
-    double br = b_rk[r], ar = a_rk[r], c2 = -factor * br;
-    c.r *= br; c.mx *= br; c.my *= br; c.E *= br;
-    c.r += s.Uold[i] * ar + R0 * c2;
-    c.mx += s.Uold[nv + i] * ar + R1 * c2;
-    c.my += s.Uold[2 * nv + i] * ar + R2 * c2;
-    c.E += s.Uold[3 * nv + i] * ar + R3 * c2;
+    const double uo[4] = {s.Uold[i], s.Uold[nv + i], s.Uold[2 * nv + i], s.Uold[3 * nv + i]};
+    Cons c = rk_stage(k, ctl, s, nv, i, r, load_prim(s.P, nv, i), uo, factor, R0, R1, R2, R3);
     Prim q = con2prim(k, c);
     Ent e = prim2ent(k, q);
     s.P[i] = q.T; s.P[nv + i] = q.u; s.P[2 * nv + i] = q.v; s.P[3 * nv + i] = q.p;

@@ -418,21 +418,13 @@ __global__ void __launch_bounds__(kTileThreads, (FLUX == FLUX_TECNO_ROE || FLUX 
     if (MODE == MODE_RESIDUAL) {
       s.R[v] = r0; s.R[nv + v] = r1; s.R[2 * nv + v] = r2; s.R[3 * nv + v] = r3;
     } else {
-      const double a_rk[3] = {0.0, 3.0 / 4.0, 1.0 / 3.0};
-      const double b_rk[3] = {1.0, 1.0 / 4.0, 2.0 / 3.0};
       if (do_norm) {
         double a0 = r0 / area, a1 = r1 / area, a2 = r2 / area, a3 = r3 / area;
         nrm[0] = a0 * a0 * w; nrm[1] = a1 * a1 * w; nrm[2] = a2 * a2 * w; nrm[3] = a3 * a3 * w;
       }
       double dtv = (ctl.time_mode == 1 || ctl.time_step > 0.0) ? sc->dt_global : dtl;
       double factor = dtv / (1.0 * area);
-      Cons c = prim2con(k, q0);
-      double br = b_rk[r], ar = a_rk[r], c2 = -factor * br;
-      c.r *= br; c.mx *= br; c.my *= br; c.E *= br;
-      c.r += uo[0] * ar + r0 * c2;
-      c.mx += uo[1] * ar + r1 * c2;
-      c.my += uo[2] * ar + r2 * c2;
-      c.E += uo[3] * ar + r3 * c2;
+      Cons c = rk_stage(k, ctl, s, nv, v, r, q0, uo, factor, r0, r1, r2, r3);
       Prim q = con2prim(k, c);
       Ent e = prim2ent(k, q);
       Pout[v] = q.T; Pout[nv + v] = q.u; Pout[2 * nv + v] = q.v; Pout[3 * nv + v] = q.p;

@@ -43,6 +43,9 @@ CASES = {
     "cyl_inlet_outlet": _cyl("kepes_tecno_roe", "minmod", "euler", bc="inlet_outlet"),
     "cyl_ns_forces": _cyl("kepes_tecno_roe", "minmod", "ns", forces={"cyl": [1], "outer": [2]}),
     "cyl_slip_forces": _cyl("kepes_tecno_rusanov", "minmod", "euler", bc="slip", forces={"cyl": [1]}),
+    "sq_roe_minmod_rk4": _sq("kepes_tecno_roe", "minmod", time_scheme="rk4"),
+    "sq_kepec_rk4_long": _sq("kepec", "first", n=17, seed=11, steps=40, dump=0, time_scheme="rk4"),
+    "cyl_ns_rk4": _cyl("kepes_tecno_roe", "minmod", "ns", time_scheme="rk4"),
 }
 
 
@@ -78,6 +81,8 @@ def build_case(spec: dict):
                time_stamps=1, cfl=0.8)
     if "forces" in spec:
         cfg["forces"] = dict(spec["forces"])
+    if "time_scheme" in spec:
+        cfg["time_scheme"] = spec["time_scheme"]
     return m, cfg, prim0
 
 
