@@ -28,7 +28,7 @@
 extern "C" {
 #endif
 
-#define TG_ABI_VERSION 1
+#define TG_ABI_VERSION 2
 
 typedef enum {
   TG_OK = 0,
@@ -169,6 +169,8 @@ typedef struct {
   long max_iter;
   double min_residue;
   int bad_state_check;  /* nonzero: flag non-finite / p<=0 / rho<=0 in updates  */
+  int liou_fix;         /* numeric liou_fix: Liou's carbuncle switch for kepes_tecno_roe */
+  int bc_strong;        /* numeric bc_scheme strong (1) or weak (0)                */
 } tg_options;
 
 typedef struct tg_handle tg_handle;

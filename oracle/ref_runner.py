@@ -38,6 +38,7 @@ def param_text(cfg: dict) -> str:
     ic ({variable: fparser expression}), constants ({name: value}),
     online_stat (bool), variables (extra moment variables, e.g. ["density"]).
     forces: {name: [face tags]} (integrals section, compute_forces).
+    liou_fix (bool), bc_scheme ('weak' | 'strong').
     """
     flux = cfg.get("flux", "kepes_tecno_roe")
     recon = cfg.get("reconstruct", "minmod")
@@ -79,8 +80,8 @@ numeric
    reconstruct
    {{
 {rec}   }}
-   bc_scheme    weak
-   liou_fix     no
+   bc_scheme    {cfg.get('bc_scheme', 'weak')}
+   liou_fix     {'yes' if cfg.get('liou_fix', False) else 'no'}
    sample_list
    {{
       groups

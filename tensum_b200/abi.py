@@ -50,7 +50,8 @@ class TgBcTable(C.Structure):
 class TgOptions(C.Structure):
     _fields_ = [("time_scheme", C.c_int), ("time_mode", C.c_int), ("time_step", C.c_double),
                 ("cfl", C.c_double), ("final_time", C.c_double), ("n_time_stamps", C.c_int),
-                ("max_iter", C.c_long), ("min_residue", C.c_double), ("bad_state_check", C.c_int)]
+                ("max_iter", C.c_long), ("min_residue", C.c_double), ("bad_state_check", C.c_int),
+                ("liou_fix", C.c_int), ("bc_strong", C.c_int)]
 
 
 def _p(a: np.ndarray, t):
@@ -153,4 +154,6 @@ class Problem:
         o.max_iter = cfg.get("max_iter", 1000000000)
         o.min_residue = 0.0
         o.bad_state_check = 1
+        o.liou_fix = 1 if cfg.get("liou_fix", False) else 0
+        o.bc_strong = 1 if cfg.get("bc_scheme", "weak") == "strong" else 0
         self.options = o

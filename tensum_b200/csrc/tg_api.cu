@@ -244,10 +244,18 @@ void enqueue_residual(tg_handle* h, const int* done) {
   enqueue_tile_flux(h, 0, MODE_RESIDUAL, 0, false, 0, done);
 }
 
+// compute_ssw follows compute_dt in FiniteVolume::solve (src/fv.cc:2282-2285)
+void enqueue_ssw(tg_handle* h, const int* done) {
+  if (!h->prm.liou) return;
+  cudaMemsetAsync(h->sv.ssw, 0, h->mv.nv * sizeof(int), h->stream);
+  k_ssw<<<(h->mv.ne + kBlock - 1) / kBlock, kBlock, 0, h->stream>>>(h->prm, h->mv, view(h, 0), done);
+}
+
 void enqueue_dt(tg_handle* h, const int* done) {
   if (h->ctl.time_step <= 0.0)
     k_dt<<<nblk(h->mv.nv), kBlock, 0, h->stream>>>(h->prm, h->mv, view(h, 0), h->sc, done);
   k_dt_final<<<1, 1, 0, h->stream>>>(h->ctl, h->sc, done);
+  enqueue_ssw(h, done);
 }
 
 void enqueue_update(tg_handle* h, int r, bool norm, const int* done) {
@@ -275,6 +283,7 @@ void enqueue_step(tg_handle* h) {
       enqueue_gradient(h, bin, first, h->grads_needed, h->done);   // first stage: + dt, U_old
     }
     if (first) k_dt_final<<<1, 1, 0, h->stream>>>(h->ctl, h->sc, h->done);
+    if (first) enqueue_ssw(h, h->done);
     enqueue_boundary(h, bin, h->done);
     enqueue_tile_flux(h, bin, MODE_UPDATE, r, last, bout, h->done);
     if (last) enqueue_norm_final(h, h->L.ntiles, true, 0, h->done);
@@ -478,6 +487,7 @@ tg_status tg_create(const tg_mesh* mesh, const tg_material* mat, const tg_bc_tab
   k.ev_alpha = mat->ev_mod_alpha; k.ev_beta = mat->ev_mod_beta; k.tvbM = mat->tvb_minmod_coef; k.cfl = opt->cfl;
   k.model = mat->model; k.flux = mat->flux_scheme; k.mu_model = mat->mu_model; k.recon = mat->reconstruct_scheme;
   k.nd = mat->nd_active; k.visc = mat->visc_active; k.heat = mat->heat_active;
+  k.liou = (opt->liou_fix && mat->flux_scheme == FLUX_TECNO_ROE) ? 1 : 0;
 
   tg_status st;
 #define UP(vec, field) \
@@ -505,7 +515,7 @@ tg_status tg_create(const tg_mesh* mesh, const tg_material* mat, const tg_bc_tab
   if ((st = dev_alloc(h, (n), &h->sv.field)) != TG_OK) { tg_destroy(h); return st; }
   AL(P, 4 * nv) AL(W, 4 * nv) AL(G, 8 * nv) AL(R, 4 * nv) AL(Uold, 4 * nv) AL(dt, nv)
   AL(Fb, 8 * (size_t)L.nb) AL(Fv, 9 * (size_t)L.nvu) AL(Fvb, 3 * (size_t)L.nb)
-  AL(part, 4 * (size_t)std::max(h->nblocks_v, L.ntiles)) AL(R2, 4 * nv)
+  AL(part, 4 * (size_t)std::max(h->nblocks_v, L.ntiles)) AL(R2, 4 * nv) AL(ssw, nv)
 #undef AL
   h->Pb[0] = h->sv.P;
   h->Wb[0] = h->sv.W;
@@ -555,7 +565,7 @@ tg_status tg_create(const tg_mesh* mesh, const tg_material* mat, const tg_bc_tab
   h->kernels_per_flux = residual_kernels(h);
   // step_begin + gradient/dt passes + per stage (boundary, viscous, tiled flux) + [store_old] + dt_final
   // + norm_final + step_end
-  h->kernels_per_step = 1 + (1 + (h->grads_needed ? c.n_rks - 1 : 0)) + c.n_rks * residual_kernels(h) + (c.time_step > 0.0 ? 1 : 0) +
+  h->kernels_per_step = 1 + (1 + (h->grads_needed ? c.n_rks - 1 : 0)) + (k.liou ? 1 : 0) + c.n_rks * residual_kernels(h) + (c.time_step > 0.0 ? 1 : 0) +
                         1 + 1 + 1;
   if ((st = dev_alloc(h, 5 * nv, &h->raw)) != TG_OK) { tg_destroy(h); return st; }
   if ((st = dev_alloc(h, 1, &h->bad)) != TG_OK) { tg_destroy(h); return st; }

@@ -44,6 +44,7 @@ struct StateView {
   double* Fvb;    // 3*nb
   double* part;   // block partial sums
   double* R2;     // 4*nv  RK4 residual accumulator (residual2 of src/fv.h)
+  int* ssw;       // nv    Liou shock switch (src/fv.h:160)
 };
 
 // Step bookkeeping kept on the device so that whole steps replay from a CUDA graph.
@@ -307,6 +308,27 @@ __global__ void k_dt(Params k, MeshView m, StateView s, Scalars* sc, const int* 
 }
 
 // Start of a solve-loop iteration (src/fv.cc:2273-2276): loop condition and dt reset.
+// compute_ssw (src/compute_ssw.cc:7-38): flags both endpoints of every edge
+// (all faces, boundary ones included) across which u.n - a|n| or u.n + a|n|
+// changes sign from positive to negative.  Writers only ever store 1.
+__global__ void k_ssw(Params k, MeshView m, StateView s, const int* __restrict__ done) {
+  if (*done) return;
+  const int e = blockIdx.x * blockDim.x + threadIdx.x;
+  if (e >= m.ne) return;
+  const int a = m.e_a[e], b = m.e_b[e];
+  const Prim qa = load_prim(s.P, m.nv, a), qb = load_prim(s.P, m.nv, b);
+  const double nx = m.e_nx[e], ny = m.e_ny[e];
+  const double ui = qa.u * nx + qa.v * ny, uj = qb.u * nx + qb.v * ny;
+  const double ai = sound_speed(k, qa), aj = sound_speed(k, qb);
+  const double area = sqrt(nx * nx + ny * ny);
+  const double l1i = ui - ai * area, l1j = uj - aj * area;
+  const double l5i = ui + ai * area, l5j = uj + aj * area;
+  if ((l1i > 0 && l1j < 0) || (l5i > 0 && l5j < 0)) {
+    s.ssw[a] = 1;
+    s.ssw[b] = 1;
+  }
+}
+
 __global__ void k_step_begin(Control ctl, Scalars* sc, int* done) {
   // unsteady runs never advance the iteration bound (term_iter stays 0, src/fv.cc:2266-2268)
   bool go = sc->rtotal > ctl.min_residue && (ctl.time_mode == 1 || sc->iter < ctl.max_iter) &&

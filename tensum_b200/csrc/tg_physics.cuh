@@ -35,6 +35,7 @@ struct Params {
   int model;      // 0 euler, 1 ns
   int flux, mu_model, recon;
   int nd, visc, heat;
+  int liou;       // Liou's carbuncle switch active (liou_fix with kepes_tecno_roe)
 };
 
 struct Prim { double T, u, v, p; };
@@ -310,7 +311,7 @@ __device__ __forceinline__ Flx avg_flux(const Params& k, const VRec& L, const VR
 // edge vector x_r - x_l.
 template <int ROE, int RECON>
 __device__ __forceinline__ Flx tecno_flux(const Params& k, const VRec& L, const VRec& Rp, double unx, double uny,
-                                          double dx, double dy, const double* dEl, const double* dEr) {
+                                          double dx, double dy, const double* dEl, const double* dEr, int ssw = 0) {
   const double g = k.gamma;
   double rho = logavg(L.rho, Rp.rho);
   double ibeta = inv_logavg(L.beta, Rp.beta);    // 1 / beta_ln
@@ -354,7 +355,7 @@ __device__ __forceinline__ Flx tecno_flux(const Params& k, const VRec& L, const 
     double l2 = fabs(vn);
     Lam[0] = (1 + k.ev_beta) * fabs(vn - a) + k.ev_alpha * fabs((vnl - L.a) - (vnr - Rp.a));
     Lam[1] = l2;
-    Lam[2] = l2;
+    Lam[2] = ssw > 0 ? dmax_(l2, a) : l2;   // Liou's modification (src/kepes_tecno_roe.cc:85-87)
     Lam[3] = (1 + k.ev_beta) * fabs(vn + a) + k.ev_alpha * fabs((vnl + L.a) - (vnr + Rp.a));
   } else {
     double lr = fabs(vn) + fabs(a);
@@ -392,9 +393,10 @@ __device__ __forceinline__ Flx tecno_flux(const Params& k, const VRec& L, const 
 // (area = |n|, unit normal = n * (1/area), as the fluxes compute them).
 template <int FLUX, int RECON>
 __device__ __forceinline__ Flx num_flux_unit(const Params& k, const VRec& L, const VRec& R, double unx, double uny,
-                                             double area, double dx, double dy, const double* dEl, const double* dEr) {
+                                             double area, double dx, double dy, const double* dEl, const double* dEr,
+                                             int ssw = 0) {
   Flx F;
-  if (FLUX == FLUX_TECNO_ROE) F = tecno_flux<1, RECON>(k, L, R, unx, uny, dx, dy, dEl, dEr);
+  if (FLUX == FLUX_TECNO_ROE) F = tecno_flux<1, RECON>(k, L, R, unx, uny, dx, dy, dEl, dEr, ssw);
   else if (FLUX == FLUX_TECNO_RUSANOV) F = tecno_flux<0, RECON>(k, L, R, unx, uny, dx, dy, dEl, dEr);
   else if (FLUX == FLUX_KEPEC) F = kepec_flux(k, L, R, unx, uny);
   else if (FLUX == FLUX_KEP) F = kep_flux(k, L, R, unx, uny);

@@ -324,7 +324,9 @@ __global__ void __launch_bounds__(kTileThreads, (FLUX == FLUX_TECNO_ROE || FLUX 
   double* sG = sm + Y::n * lmax;                            // 8 * L (gradient fluxes only)
   double* sX = sG + 8 * lmax;                               // 2 * L
   double* sE = sm + flux_vertex_doubles<FLUX, RECON>() * lmax;   // 4 * NE: ux uy ar ab -> fluxes
-  int* sO = reinterpret_cast<int*>(sE + 4 * emax);
+  constexpr bool kRoe = (FLUX == FLUX_TECNO_ROE);
+  int* sS = reinterpret_cast<int*>(sE + 4 * emax);                 // Liou switch of the local vertices (Roe)
+  int* sO = sS + (kRoe ? lmax : 0);
   unsigned int* sC = reinterpret_cast<unsigned int*>(sO + kTileThreads + 2);
 
   // ---- stage: vertex gathers, edge arrays, gather lists (all in flight at once)
@@ -341,6 +343,10 @@ __global__ void __launch_bounds__(kTileThreads, (FLUX == FLUX_TECNO_ROE || FLUX 
       for (int c = 0; c < 8; ++c) cp_async8(sG + c * L + i, s.G + (size_t)c * nv + g);
       cp_async8(sX + i, t.x + g);
       cp_async8(sX + L + i, t.y + g);
+    }
+    if (kRoe) {
+      if (k.liou) cp_async4(sS + i, s.ssw + g);
+      else sS[i] = 0;
     }
   }
   for (int le = threadIdx.x; le < NE; le += blockDim.x) {
@@ -375,7 +381,7 @@ __global__ void __launch_bounds__(kTileThreads, (FLUX == FLUX_TECNO_ROE || FLUX 
       dx = sX[lb] - sX[la];
       dy = sX[L + lb] - sX[L + la];
     }
-    Flx F = num_flux_unit<FLUX, RECON>(k, A, B, unx, uny, area, dx, dy, gl, gr);
+    Flx F = num_flux_unit<FLUX, RECON>(k, A, B, unx, uny, area, dx, dy, gl, gr, kRoe ? sS[la] + sS[lb] : 0);
     sE[le] = F.m; sE[NE + le] = F.x; sE[2 * NE + le] = F.y; sE[3 * NE + le] = F.e;
   }
   __syncthreads();
@@ -465,7 +471,7 @@ inline size_t tile_grad_smem(int lmax, int emax, int cmax, bool first) {
 template <int FLUX, int RECON>
 size_t tile_flux_smem_t(int lmax, int emax, int cmax) {
   size_t a = ((size_t)lmax * flux_vertex_doubles<FLUX, RECON>() + 4 * (size_t)emax) * sizeof(double) +
-             tile_list_bytes(cmax);
+             (FLUX == FLUX_TECNO_ROE ? (size_t)lmax * sizeof(int) : 0) + tile_list_bytes(cmax);
   size_t b = 4 * kTileThreads * sizeof(double);
   return a > b ? a : b;
 }

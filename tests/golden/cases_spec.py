@@ -46,6 +46,8 @@ CASES = {
     "sq_roe_minmod_rk4": _sq("kepes_tecno_roe", "minmod", time_scheme="rk4"),
     "sq_kepec_rk4_long": _sq("kepec", "first", n=17, seed=11, steps=40, dump=0, time_scheme="rk4"),
     "cyl_ns_rk4": _cyl("kepes_tecno_roe", "minmod", "ns", time_scheme="rk4"),
+    "sq_roe_liou": _sq("kepes_tecno_roe", "minmod", ic="collide", liou_fix=True, cfl=0.3),
+    "sq_roe_first_liou": _sq("kepes_tecno_roe", "first", n=11, ic="collide", liou_fix=True, steps=3, dump=3, cfl=0.3),
 }
 
 
@@ -56,6 +58,12 @@ def build_case(spec: dict):
             m = M.periodic_square(spec["n"], 0.0, 1.0, 0.0, 1.0, spec["seed"])
             a, phi = cases.kh_coefficients(spec["seed"])
             prim0 = cases.kh_ic(m.coords, a, phi)
+        elif spec["ic"] == "collide":
+            # two streams colliding at x = 0 faster than sound: sonic points for the Liou switch
+            m = cases.vortex_mesh(spec["n"], spec["seed"])
+            prim0 = cases.vortex_ic(m.coords)
+            prim0[:, 2] = np.where(m.coords[:, 0] < 0.0, 1.25, -1.25)
+            prim0[:, 3] = 0.1 * np.sin(m.coords[:, 1])
         else:
             m = cases.vortex_mesh(spec["n"], spec["seed"])
             prim0 = cases.vortex_ic(m.coords)
@@ -78,11 +86,13 @@ def build_case(spec: dict):
     cfg = dict(flux=spec["flux"], reconstruct=spec["reconstruct"], boundary=bnd, final_time=100.0,
                model=spec.get("model", "euler"), mu_ref=0.002 if spec.get("model") == "ns" else 0.0,
                tvb_M=spec.get("tvb_M", 1.0), ev_alpha=spec.get("ev_alpha", 0.0), ev_beta=spec.get("ev_beta", 0.0),
-               time_stamps=1, cfl=0.8)
+               time_stamps=1, cfl=spec.get("cfl", 0.8))
     if "forces" in spec:
         cfg["forces"] = dict(spec["forces"])
     if "time_scheme" in spec:
         cfg["time_scheme"] = spec["time_scheme"]
+    if spec.get("liou_fix"):
+        cfg["liou_fix"] = True
     return m, cfg, prim0
 
 
