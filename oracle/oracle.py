@@ -51,6 +51,7 @@ def lib():
         L.tor_logavg.argtypes = [C.c_double, C.c_double]
         L.tor_logavg.restype = C.c_double
         L.tor_counter.argtypes = [vp]
+        L.tor_get_residual.argtypes = [vp, dp]
         L.tor_forces.argtypes = [vp, C.c_int, C.POINTER(C.c_int), C.POINTER(C.c_int), dp]
         L.tor_moment_nvars.argtypes = [C.c_int]
         L.tor_moments_increment.argtypes = [vp, C.c_long, C.c_int, dp, dp, dp]
@@ -110,6 +111,11 @@ class Oracle:
         dE = np.empty((self.nv, 5, 3))
         self.L.tor_compute_residual(self.h, _d(res), _d(dE))
         return res, dE
+
+    def current_residual(self):
+        out = np.empty((self.nv, 5))
+        self.L.tor_get_residual(self.h, _d(out))
+        return out
 
     def update(self, r):
         self.L.tor_update(self.h, r)

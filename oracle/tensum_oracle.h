@@ -55,6 +55,7 @@ double tor_logavg(double a, double b);
  * src/reduce_moments.cc:14-221).  Records per vertex: PrimVar (T,p,u,v,w),
  * then density, mach, entropy, vorticity as selected by the bits of extras. */
 void tor_forces(tor_state* s, int n_forces, const int* n_tags, const int* tags, double* out4);
+void tor_get_residual(const tor_state* s, double* out5);
 int tor_counter(const tor_state* s);   /* next output-time index (FiniteVolume::counter) */
 int tor_moment_nvars(int extras);
 void tor_moments_increment(const tor_state* s, long k, int extras, double* fm, double* sm, double* m2);

@@ -46,6 +46,10 @@ CASES = {
     "sq_roe_minmod_rk4": _sq("kepes_tecno_roe", "minmod", time_scheme="rk4"),
     "sq_kepec_rk4_long": _sq("kepec", "first", n=17, seed=11, steps=40, dump=0, time_scheme="rk4"),
     "cyl_ns_rk4": _cyl("kepes_tecno_roe", "minmod", "ns", time_scheme="rk4"),
+    "cyl_ns_strong": _cyl("kepes_tecno_roe", "minmod", "ns", bc_scheme="strong"),
+    "cyl_ns_isothermal_strong": _cyl("kepes_tecno_rusanov", "minmod", "ns", bc="isothermal", bc_scheme="strong"),
+    "cyl_slip_strong": _cyl("kepes_tecno_roe", "minmod", "euler", bc="slip", bc_scheme="strong"),
+    "cyl_inlet_outlet_strong": _cyl("kepec", "first", "euler", bc="inlet_outlet", bc_scheme="strong"),
     "sq_roe_liou": _sq("kepes_tecno_roe", "minmod", ic="collide", liou_fix=True, cfl=0.3),
     "sq_roe_first_liou": _sq("kepes_tecno_roe", "first", n=11, ic="collide", liou_fix=True, steps=3, dump=3, cfl=0.3),
 }
@@ -93,6 +97,8 @@ def build_case(spec: dict):
         cfg["time_scheme"] = spec["time_scheme"]
     if spec.get("liou_fix"):
         cfg["liou_fix"] = True
+    if "bc_scheme" in spec:
+        cfg["bc_scheme"] = spec["bc_scheme"]
     return m, cfg, prim0
 
 

@@ -32,9 +32,12 @@ def test_oracle_matches_reference_exactly(name):
         for r in range(n_rks):
             res, dE = o.residual()
             assert np.array_equal(dE.ravel(), d[f"s{s}r{r}_grad"]), f"gradient step {s} stage {r}"
-            assert np.array_equal(res.ravel(), d[f"s{s}r{r}_res"]), f"residual step {s} stage {r}"
             if r == n_rks - 1:
+                # the harness dumps the last stage's residual after compute_residual_norm,
+                # which zeroes the no-slip momentum residual under strong conditions
                 assert np.array_equal(o.residual_norm(s), d[f"s{s}_norm"])
+                res = o.current_residual()
+            assert np.array_equal(res.ravel(), d[f"s{s}r{r}_res"]), f"residual step {s} stage {r}"
             o.update(r)
             assert np.array_equal(o.get_prim().ravel(), d[f"s{s}r{r}_prim"]), f"state step {s} stage {r}"
         o.end_step()
