@@ -286,6 +286,8 @@ void enqueue_step(tg_handle* h) {
     if (first) enqueue_ssw(h, h->done);
     enqueue_boundary(h, bin, h->done);
     enqueue_tile_flux(h, bin, MODE_UPDATE, r, last, bout, h->done);
+    if (h->prm.strong && h->mv.nsb > 0)
+      k_strong_bc<<<nblk(h->mv.nsb), kBlock, 0, h->stream>>>(h->mv, h->Pb[bout], h->done);
     if (last) enqueue_norm_final(h, h->L.ntiles, true, 0, h->done);
   }
   k_step_end<<<1, 1, 0, h->stream>>>(h->ctl, h->sc, h->done);
@@ -488,6 +490,7 @@ tg_status tg_create(const tg_mesh* mesh, const tg_material* mat, const tg_bc_tab
   k.model = mat->model; k.flux = mat->flux_scheme; k.mu_model = mat->mu_model; k.recon = mat->reconstruct_scheme;
   k.nd = mat->nd_active; k.visc = mat->visc_active; k.heat = mat->heat_active;
   k.liou = (opt->liou_fix && mat->flux_scheme == FLUX_TECNO_ROE) ? 1 : 0;
+  k.strong = opt->bc_strong ? 1 : 0;
 
   tg_status st;
 #define UP(vec, field) \
@@ -502,6 +505,32 @@ tg_status tg_create(const tg_mesh* mesh, const tg_material* mat, const tg_bc_tab
   UP(bf_face_nx, bf_face_nx) UP(bf_face_ny, bf_face_ny) UP(bf_face_v0, bf_face_v0) UP(bf_face_v1, bf_face_v1)
   UP(u_cell, u_cell) UP(c_v, c_v) UP(c_n, c_n) UP(c_inv2a, c_inv2a)
   UP(c_bf_off, c_bf_off) UP(c_bf, c_bf) UP(c_nbr_off, c_nbr_off) UP(c_nbr, c_nbr)
+  {
+    // bc_scheme strong: which vertices a condition resets (slip, no-slip, pressure,
+    // inlet) and in which face order, and which lie on no-slip faces
+    std::vector<int> sflag(L.nv, 0), sb_v, sb_off(1, 0), sb_ent;
+    std::vector<std::vector<int>> per(L.nv);
+    for (int d = 0; d < L.nb; ++d) {
+      const int kind = L.b_kind[d];
+      const bool resets = kind == BC_SLIP || kind == BC_NOSLIP || kind == BC_PRESSURE || kind == BC_INLET;
+      for (int slot = 0; slot < 2; ++slot) {
+        const int v = slot ? L.b_v1[d] : L.b_v0[d];
+        if (resets) { per[v].push_back((d << 1) | slot); sflag[v] |= 1; }
+        if (kind == BC_NOSLIP) sflag[v] |= 2;
+      }
+    }
+    for (int v = 0; v < L.nv; ++v) {
+      if (per[v].empty()) continue;
+      sb_v.push_back(v);
+      sb_ent.insert(sb_ent.end(), per[v].begin(), per[v].end());
+      sb_off.push_back((int)sb_ent.size());
+    }
+    h->mv.nsb = opt->bc_strong ? (int)sb_v.size() : 0;
+    if ((st = dev_upload(h, sflag, &h->mv.sflag)) != TG_OK) { tg_destroy(h); return st; }
+    if ((st = dev_upload(h, sb_v, &h->mv.sb_v)) != TG_OK) { tg_destroy(h); return st; }
+    if ((st = dev_upload(h, sb_off, &h->mv.sb_off)) != TG_OK) { tg_destroy(h); return st; }
+    if ((st = dev_upload(h, sb_ent, &h->mv.sb_ent)) != TG_OK) { tg_destroy(h); return st; }
+  }
 #undef UP
 #define UPT(vec, field) \
   if ((st = dev_upload(h, L.vec, &h->tv.field)) != TG_OK) { tg_destroy(h); return st; }
@@ -565,7 +594,7 @@ tg_status tg_create(const tg_mesh* mesh, const tg_material* mat, const tg_bc_tab
   h->kernels_per_flux = residual_kernels(h);
   // step_begin + gradient/dt passes + per stage (boundary, viscous, tiled flux) + [store_old] + dt_final
   // + norm_final + step_end
-  h->kernels_per_step = 1 + (1 + (h->grads_needed ? c.n_rks - 1 : 0)) + (k.liou ? 1 : 0) + c.n_rks * residual_kernels(h) + (c.time_step > 0.0 ? 1 : 0) +
+  h->kernels_per_step = 1 + (1 + (h->grads_needed ? c.n_rks - 1 : 0)) + (k.liou ? 1 : 0) + (k.strong && h->mv.nsb > 0 ? c.n_rks : 0) + c.n_rks * residual_kernels(h) + (c.time_step > 0.0 ? 1 : 0) +
                         1 + 1 + 1;
   if ((st = dev_alloc(h, 5 * nv, &h->raw)) != TG_OK) { tg_destroy(h); return st; }
   if ((st = dev_alloc(h, 1, &h->bad)) != TG_OK) { tg_destroy(h); return st; }
@@ -721,6 +750,8 @@ tg_status tg_update(tg_handle* h, int r) {
   if (!h) return fail(h, TG_INVALID_ARG, "NULL handle");
   if (r < 0 || r >= h->ctl.n_rks) return fail(h, TG_INVALID_ARG, "stage index out of range for the time scheme");
   enqueue_update(h, r, false, h->never);
+  if (h->prm.strong && h->mv.nsb > 0)
+    k_strong_bc<<<nblk(h->mv.nsb), kBlock, 0, h->stream>>>(h->mv, h->sv.P, h->never);
   tg_status st = sync(h);
   if (st != TG_OK) return st;
   return check_bad(h);
@@ -728,6 +759,7 @@ tg_status tg_update(tg_handle* h, int r) {
 
 tg_status tg_residual_norm(tg_handle* h, long iter, double* out6) {
   if (!h) return fail(h, TG_INVALID_ARG, "NULL handle");
+  if (h->prm.strong) k_strong_zero_res<<<h->nblocks_v, kBlock, 0, h->stream>>>(h->mv, h->sv);
   k_norm_part<<<h->nblocks_v, kBlock, 0, h->stream>>>(h->mv, h->sv, h->never);
   enqueue_norm_final(h, h->nblocks_v, false, iter, h->never);
   Scalars s;

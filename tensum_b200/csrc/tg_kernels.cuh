@@ -28,6 +28,12 @@ struct MeshView {
   const int* c_v;
   const double *c_n, *c_inv2a;
   const int *c_bf_off, *c_bf, *c_nbr_off, *c_nbr;
+  // bc_scheme strong: per vertex bit 0 = a boundary condition resets its state,
+  // bit 1 = on a no-slip face; the reset list (vertex, then (face << 1 | slot)
+  // entries in reference face order)
+  const int* sflag;
+  int nsb;
+  const int *sb_v, *sb_off, *sb_ent;
 };
 
 // Device state, structure-of-arrays with component stride nv (or ne, nb ...).
@@ -327,6 +333,32 @@ __global__ void k_ssw(Params k, MeshView m, StateView s, const int* __restrict__
     s.ssw[a] = 1;
     s.ssw[b] = 1;
   }
+}
+
+// bc_scheme strong, after each stage update (src/fv.cc:1694-1704): every
+// boundary face's condition applied to its vertices' primitive state in face
+// order; the entropy variables keep their values (the reference does not
+// recompute them), so gradients see the pre-condition state.
+__global__ void k_strong_bc(MeshView m, double* __restrict__ P, const int* __restrict__ done) {
+  if (*done) return;
+  const int j = blockIdx.x * blockDim.x + threadIdx.x;
+  if (j >= m.nsb) return;
+  const int v = m.sb_v[j], nv = m.nv;
+  Prim q = load_prim(P, nv, v);
+  for (int e = m.sb_off[j]; e < m.sb_off[j + 1]; ++e) {
+    const int d = m.sb_ent[e] >> 1, slot = m.sb_ent[e] & 1;
+    bc_apply1(m.b_kind[d], m.b_adiab[d], m.b_val + (size_t)d * 10 + 5 * slot, m.b_nx[d], m.b_ny[d], q);
+  }
+  P[v] = q.T; P[nv + v] = q.u; P[2 * (size_t)nv + v] = q.v; P[3 * (size_t)nv + v] = q.p;
+}
+
+// bc_scheme strong, in compute_residual_norm (src/fv.cc:1805-1819): the momentum
+// residual of no-slip vertices is zeroed (the update then uses it).
+__global__ void k_strong_zero_res(MeshView m, StateView s) {
+  const int v = blockIdx.x * blockDim.x + threadIdx.x;
+  if (v >= m.nv || !(m.sflag[v] & 2)) return;
+  s.R[m.nv + v] = 0.0;
+  s.R[2 * (size_t)m.nv + v] = 0.0;
 }
 
 __global__ void k_step_begin(Control ctl, Scalars* sc, int* done) {

@@ -36,6 +36,7 @@ struct Params {
   int flux, mu_model, recon;
   int nd, visc, heat;
   int liou;       // Liou's carbuncle switch active (liou_fix with kepes_tecno_roe)
+  int strong;     // bc_scheme strong
 };
 
 struct Prim { double T, u, v, p; };

@@ -364,7 +364,16 @@ __global__ void __launch_bounds__(kTileThreads, (FLUX == FLUX_TECNO_ROE || FLUX 
     double u = sV[Y::Ru * L + i], v = sV[Y::Rv * L + i], p = sV[Y::Rp * L + i], w3 = sV[Y::RW3 * L + i];
     double w0 = Y::RW0 >= 0 ? sV[(Y::RW0 >= 0 ? Y::RW0 : 0) * L + i] : 0.0;
     double T = Y::RT >= 0 ? sV[(Y::RT >= 0 ? Y::RT : 0) * L + i] : 0.0;
-    store_vrec<FLUX>(sV, L, i, make_vrec_w<FLUX>(k, u, v, p, T, w0, w3));
+    const int g = k.strong ? t.lv[l0 + i] : 0;
+    if (k.strong && (m.sflag[g] & 1)) {
+      // a strong condition reset this vertex's primitive state but not its entropy
+      // variables: the flux reads the primitive state, as the reference does
+      Prim q;
+      q.T = Y::RT >= 0 ? T : s.P[g]; q.u = u; q.v = v; q.p = p;
+      store_vrec<FLUX>(sV, L, i, make_vrec<FLUX>(k, q));
+    } else {
+      store_vrec<FLUX>(sV, L, i, make_vrec_w<FLUX>(k, u, v, p, T, w0, w3));
+    }
   }
   __syncthreads();
 
@@ -421,6 +430,9 @@ __global__ void __launch_bounds__(kTileThreads, (FLUX == FLUX_TECNO_ROE || FLUX 
         r1 += s.Fvb[idx] * 0.5; r2 += s.Fvb[m.nb + idx] * 0.5; r3 += s.Fvb[2 * m.nb + idx] * 0.5;
       }
     }
+    // strong conditions: compute_residual_norm zeroes the no-slip momentum residual
+    // before the last stage's update (src/fv.cc:1805-1819)
+    if (MODE == MODE_UPDATE && do_norm && k.strong && (m.sflag[v] & 2)) { r1 = 0.0; r2 = 0.0; }
     if (MODE == MODE_RESIDUAL) {
       s.R[v] = r0; s.R[nv + v] = r1; s.R[2 * nv + v] = r2; s.R[3 * nv + v] = r3;
     } else {
