@@ -228,6 +228,13 @@ tg_status tg_step(tg_handle* h, int n_steps, double* info4);
 /* Global kinetic energy and entropy integrals, compute_global (src/fv.cc:2175-2225). */
 tg_status tg_global(tg_handle* h, double* ke_out, double* entropy_out);
 
+/* New material constants and boundary values for the same mesh, e.g. per Monte
+ * Carlo sample whose inflow or viscosity is uncertain (the reference re-reads
+ * them per sample through its expressions).  The model, flux, reconstruction,
+ * viscosity law and the tag -> boundary-kind mapping stay those of tg_create;
+ * bc may be NULL (values kept).  The state is untouched. */
+tg_status tg_update_parameters(tg_handle* h, const tg_material* mat, const tg_bc_table* bc);
+
 /* compute_forces (src/force.cc:116-219) on the current state: for each force
  * f (its face tags are tags[sum n_tags[<f] .. +n_tags[f]), the integrals over
  * its boundary faces of the pressure force and, for Navier-Stokes, the viscous

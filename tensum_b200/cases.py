@@ -112,6 +112,19 @@ def cylinder_ic(coords: np.ndarray, mach: float = 0.2, angle_deg: float = 0.0) -
     return np.stack([np.full(n, T), np.full(n, p), np.full(n, u), np.full(n, v), np.zeros(n)], axis=1)
 
 
+def cylinder_config(mach: float, reynolds: float, angle_deg: float, final_time: float, time_stamps: int,
+                    flux: str = "kepes_tecno_roe", recon: str = "minmod", cfl: float = 0.8) -> dict:
+    """Navier-Stokes flow past the cylinder: adiabatic no-slip wall (tag 1),
+    characteristic far field at the free stream (tag 2), Pr 0.72, and the force
+    on the wall as the integrals section would define it."""
+    T, u, v, p = cylinder_freestream(mach, angle_deg)
+    far = {"temperature": T, "xvelocity": u, "yvelocity": v, "zvelocity": 0.0, "pressure": p}
+    wall = {"xvelocity": 0.0, "yvelocity": 0.0, "zvelocity": 0.0}
+    return dict(flux=flux, reconstruct=recon, model="ns", mu_ref=cylinder_viscosity(mach, reynolds), prandtl=0.72,
+                boundary={1: ("noslip", wall), 2: ("farfield", far)}, final_time=final_time,
+                time_stamps=time_stamps, cfl=cfl, forces={"cylinder": [1]})
+
+
 def cylinder_viscosity(mach: float = 0.2, reynolds: float = 100.0, diameter: float = 1.0) -> float:
     """Constant viscosity giving Re = rho U D / mu with rho = 1."""
     return mach * diameter / reynolds

@@ -851,6 +851,39 @@ tg_status tg_advance(tg_handle* h, int instance, long max_steps, double* info5) 
   return TG_OK;
 }
 
+tg_status tg_update_parameters(tg_handle* h, const tg_material* mat, const tg_bc_table* bc) {
+  if (!h || !mat) return fail(h, TG_INVALID_ARG, "NULL handle or material");
+  Params& k = h->prm;
+  if (mat->model != k.model || mat->flux_scheme != k.flux || mat->reconstruct_scheme != k.recon ||
+      mat->mu_model != k.mu_model)
+    return fail(h, TG_NOT_SUPPORTED, "model, flux, reconstruction and viscosity law are fixed at tg_create");
+  if (!(mat->gamma > 1.0) || !(mat->gas_const > 0.0)) return fail(h, TG_INVALID_ARG, "gamma must be > 1, gas_const > 0");
+  k.gamma = mat->gamma; k.R = mat->gas_const; k.Cp = mat->gamma * mat->gas_const / (mat->gamma - 1.0);
+  k.sqrt_gm1 = std::sqrt(mat->gamma - 1.0);
+  k.inv_gamma = 1.0 / mat->gamma;
+  k.inv_gm1 = 1.0 / (mat->gamma - 1.0);
+  k.prandtl = mat->prandtl; k.mu_ref = mat->mu_ref; k.T0 = mat->T_0; k.Tref = mat->T_ref; k.omega = mat->omega;
+  k.ev_alpha = mat->ev_mod_alpha; k.ev_beta = mat->ev_mod_beta; k.tvbM = mat->tvb_minmod_coef;
+  k.nd = mat->nd_active; k.visc = mat->visc_active; k.heat = mat->heat_active;
+  if (bc && bc->bface_values) {
+    HostLayout& L = h->L;
+    for (size_t b = 0; b < L.rb_dev.size(); ++b) {
+      const int d = L.rb_dev[b];
+      if (d < 0) continue;
+      for (int q = 0; q < 10; ++q) L.b_val[(size_t)d * 10 + q] = bc->bface_values[b * 10 + q];
+    }
+    if (!L.b_val.empty())
+      TG_CUDA(h, cudaMemcpyAsync(const_cast<double*>(h->mv.b_val), L.b_val.data(), L.b_val.size() * sizeof(double),
+                                 cudaMemcpyHostToDevice, h->stream));
+  }
+  // the captured step holds the parameters by value
+  if (h->graph_exec) cudaGraphExecDestroy(h->graph_exec);
+  if (h->graph) cudaGraphDestroy(h->graph);
+  h->graph_exec = nullptr;
+  h->graph = nullptr;
+  return sync(h);
+}
+
 tg_status tg_forces(tg_handle* h, int n_forces, const int* n_tags, const int* tags, double* out) {
   if (!h || n_forces < 1 || !n_tags || !tags || !out) return fail(h, TG_INVALID_ARG, "bad force specification");
   const HostLayout& L = h->L;

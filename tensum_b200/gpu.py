@@ -20,7 +20,7 @@ EXPORTS = ["tg_create", "tg_destroy", "tg_last_error", "tg_abi_version", "tg_set
            "tg_store_conserved_old", "tg_compute_dt", "tg_gradients", "tg_residual", "tg_update",
            "tg_residual_norm", "tg_end_step", "tg_step", "tg_global", "tg_stream", "tg_time_phase", "tg_query",
            "tg_advance", "tg_moments_init", "tg_moments_increment", "tg_moments_get", "tg_moments_export",
-           "tg_moments_merge", "tg_moments_merge_device", "tg_moments_finalize", "tg_forces"]
+           "tg_moments_merge", "tg_moments_merge_device", "tg_moments_finalize", "tg_forces", "tg_update_parameters"]
 
 PHASE = {"gradient": 0, "flux": 1, "update": 2, "dt": 3, "step": 4}
 QUERY = {"n_vertex": 0, "n_edge": 1, "n_bface": 2, "kernels_per_step": 3, "device_bytes": 4, "kernels_per_flux": 5}
@@ -64,6 +64,7 @@ def load():
     L.tg_query.argtypes = [vp, i, dp]
     L.tg_advance.argtypes = [vp, i, C.c_long, dp]
     L.tg_forces.argtypes = [vp, i, C.POINTER(i), C.POINTER(i), dp]
+    L.tg_update_parameters.argtypes = [vp, vp, vp]
     L.tg_moments_init.argtypes = [vp, i, i]
     L.tg_moments_increment.argtypes = [vp, i, C.c_long]
     L.tg_moments_get.argtypes = [vp, i, dp, dp, dp]
@@ -168,6 +169,11 @@ class Solver:
         a, b = C.c_double(), C.c_double()
         self._chk(self.L.tg_global(self.h, C.byref(a), C.byref(b)))
         return a.value, b.value
+
+    def update_parameters(self, problem):
+        """Material constants and boundary values of `problem` (same mesh and schemes)."""
+        self._keep = problem          # the ctypes structs point into its arrays
+        self._chk(self.L.tg_update_parameters(self.h, C.byref(problem.material), C.byref(problem.bc)))
 
     def forces(self, forces: dict) -> np.ndarray:
         """compute_forces on the current state for {name: [face tags]} (in insertion
