@@ -307,18 +307,21 @@ tg_status tg_query(tg_handle* h, int key, double* out);
 
 /* ---- batched FP32 ensembles (no counterpart in the reference, which runs
  *      one sample after another per MC group, src/fv.cc:2440-2456) ------- */
-/* A batch advances every sample of one or more levels (a fully periodic mesh
- * and its samples; up to 4 levels, e.g. a multilevel hierarchy) together, one
- * CUDA graph per time step.  Members are FP32 ([component][vertex][sample]
- * with samples innermost); geometry is formed in FP64, the near-equal branch
- * of the log mean runs in FP64, each sample keeps its own FP64 clock and dt
- * (the per-sample time step of src/fv.cc:1499-1618), and ensemble moments
- * are accumulated in FP64.  Euler, kepes_tecno_roe / kepes_tecno_rusanov /
- * kepec, first-order or minmod reconstruction, unsteady SSP-RK3. */
+/* A batch advances every sample of one or more levels (a mesh and its
+ * samples; up to 4 levels, e.g. a multilevel hierarchy) together, one CUDA
+ * graph per time step.  Members are FP32 ([component][vertex][sample] with
+ * samples innermost); geometry is formed in FP64, the near-equal branch of the
+ * log mean runs in FP64, each sample keeps its own FP64 clock and dt (the
+ * per-sample time step of src/fv.cc:1499-1618), and ensemble moments are
+ * accumulated in FP64.  Euler or Navier-Stokes (constant viscosity law),
+ * kepes_tecno_roe / kepes_tecno_rusanov / kepec, first-order or minmod
+ * reconstruction, unsteady SSP-RK3, periodic faces and the weak boundary
+ * conditions (no strong conditions, no Liou switch).  Boundary values and the
+ * viscosity are per sample (tg_batch_set_parameters). */
 typedef struct tg_batch tg_batch;
 typedef struct tg_batch_level {
   const tg_mesh* mesh;
-  const tg_bc_table* bc;       /* every boundary tag periodic */
+  const tg_bc_table* bc;       /* boundary kinds; its values start every sample */
   int n_samples;               /* a positive multiple of 32 */
 } tg_batch_level;
 tg_status tg_batch_create(const tg_batch_level* levels, int n_levels, const tg_material* mat, const tg_options* opt,
@@ -333,6 +336,19 @@ tg_status tg_batch_get_state(tg_batch* b, int level, int sample, double* prim_ao
  * Kelvin-Helmholtz layer with v' = 0.01 sum_k r_k sin(2 pi k x + 2 pi r_{M+k}),
  * M = n_rnd / 2 (pert type 4, src/perturb.cc:196-208). */
 tg_status tg_batch_set_kh(tg_batch* b, int level, const double* rows, int n_rnd);
+/* Per-sample uncertain parameters of a level with boundary faces or viscosity
+ * (either pointer may be NULL: kept): mu_ref[s] the constant viscosity of
+ * sample s, bface_values[(s * n_bface + f) * 10 + q] the tg_bc_table values of
+ * reference boundary face f for sample s (e.g. the free stream of a far
+ * field).  Kinds stay those of tg_batch_create.  States and clocks are untouched. */
+tg_status tg_batch_set_parameters(tg_batch* b, int level, const double* mu_ref, const double* bface_values);
+/* Every sample of a level at a uniform state, prim[5 s ..] the PrimVar record
+ * (T, p, u, v, w) of sample s (e.g. its free stream); clocks restart at t = 0. */
+tg_status tg_batch_set_uniform(tg_batch* b, int level, const double* prim);
+/* compute_forces (src/force.cc:116-219) of every sample of a level at its
+ * current state, force definitions as for tg_forces:
+ * out[(s * n_forces + f) * 4 ..] = inviscid x, y, viscous x, y. */
+tg_status tg_batch_forces(tg_batch* b, int level, int n_forces, const int* n_tags, const int* tags, double* out);
 /* Steps until every sample has reached output time `instance` (samples that
  * arrive first hold), the run is over, or max_steps steps were issued.
  * info4 (may be NULL): steps issued, min and max elapsed time, samples flagged bad. */

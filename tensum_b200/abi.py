@@ -58,6 +58,19 @@ def _p(a: np.ndarray, t):
     return a.ctypes.data_as(t)
 
 
+def bface_values(g: Geometry, boundary: dict) -> np.ndarray:
+    """(n_bface, 2, 5) values of tg_bc_table.bface_values: T, u, v, w, p at both
+    vertices of every reference boundary face, from constant boundary specs
+    {tag: (kind, {"temperature": ..., "xvelocity": ..., ...})}."""
+    vals = np.zeros((g.n_bface, 2, 5))
+    for tag, (_, spec) in sorted(boundary.items()):
+        sel = g.bface_type == int(tag)
+        for j, name in enumerate(("temperature", "xvelocity", "yvelocity", "zvelocity", "pressure")):
+            if name in spec:
+                vals[sel, :, j] = float(spec[name])
+    return vals
+
+
 @dataclasses.dataclass
 class Problem:
     """Everything tg_create needs, as numpy arrays plus the ctypes structs over them."""
@@ -127,15 +140,11 @@ class Problem:
 
         # boundary table: per tag kind / adiabatic, values per bface vertex
         tags, kinds, adiab = [], [], []
-        vals = np.zeros((g.n_bface, 2, 5))
         for tag, (btype, spec) in sorted(cfg["boundary"].items()):
             tags.append(int(tag))
             kinds.append(BC[btype])
             adiab.append(1 if btype in ("slip",) or (btype == "noslip" and "temperature" not in spec) else 0)
-            sel = g.bface_type == int(tag)
-            for j, name in enumerate(("temperature", "xvelocity", "yvelocity", "zvelocity", "pressure")):
-                if name in spec:
-                    vals[sel, :, j] = float(spec[name])
+        vals = bface_values(g, cfg["boundary"])
         bc = TgBcTable()
         bc.n_types = len(tags)
         bc.type_tag = _p(arr(np.array(tags), np.int32), ip)

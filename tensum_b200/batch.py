@@ -45,10 +45,14 @@ def _lib():
         L.tg_batch_stream.argtypes = [vp, C.POINTER(vp)]
         L.tg_batch_query.argtypes = [vp, i, dp]
         L.tg_batch_integrals.argtypes = [vp, i, dp]
+        L.tg_batch_set_parameters.argtypes = [vp, i, dp, dp]
+        L.tg_batch_set_uniform.argtypes = [vp, i, dp]
+        L.tg_batch_forces.argtypes = [vp, i, i, ip, ip, dp]
         for n in ("tg_batch_create", "tg_batch_destroy", "tg_batch_set_state", "tg_batch_get_state",
                   "tg_batch_set_kh", "tg_batch_advance", "tg_batch_clock", "tg_batch_moments",
                   "tg_batch_set_shape", "tg_batch_tune", "tg_batch_time_steps", "tg_batch_stream",
-                  "tg_batch_query", "tg_batch_integrals"):
+                  "tg_batch_query", "tg_batch_integrals", "tg_batch_set_parameters", "tg_batch_set_uniform",
+                  "tg_batch_forces"):
             getattr(L, n).restype = i
         _bound = True
     return L
@@ -107,6 +111,33 @@ class Batch:
         rows = np.ascontiguousarray(rows, np.float64)
         assert rows.shape[0] == self.S[level]
         self._chk(self.L.tg_batch_set_kh(self.h, level, _d(rows), rows.shape[1]))
+
+    def set_parameters(self, level: int, mu_ref=None, bface_values=None):
+        """Per-sample viscosity (S,) and boundary values (S, n_bface, 2, 5) of a level
+        with boundary faces or viscosity; None keeps the current ones."""
+        S = self.S[level]
+        mu = None if mu_ref is None else np.ascontiguousarray(mu_ref, np.float64).reshape(S)
+        bv = None
+        if bface_values is not None:
+            bv = np.ascontiguousarray(bface_values, np.float64)
+            assert bv.shape[0] == S and bv.size == S * self.problems[level].geom.n_bface * 10
+        self._chk(self.L.tg_batch_set_parameters(self.h, level, None if mu is None else _d(mu),
+                                                 None if bv is None else _d(bv)))
+
+    def set_uniform(self, level: int, prim: np.ndarray):
+        """Every sample at its own uniform PrimVar record prim[s] = (T, p, u, v, w)."""
+        prim = np.ascontiguousarray(prim, np.float64)
+        assert prim.shape == (self.S[level], 5)
+        self._chk(self.L.tg_batch_set_uniform(self.h, level, _d(prim)))
+
+    def forces(self, level: int, forces: dict) -> np.ndarray:
+        """(S, n_forces, 4): compute_forces of every sample for {name: [face tags]}."""
+        n = np.array([len(t) for t in forces.values()], np.int32)
+        tags = np.array([x for t in forces.values() for x in t], np.int32)
+        out = np.empty((self.S[level], len(n), 4))
+        ip = C.POINTER(C.c_int)
+        self._chk(self.L.tg_batch_forces(self.h, level, len(n), n.ctypes.data_as(ip), tags.ctypes.data_as(ip), _d(out)))
+        return out
 
     def advance(self, instance: int, max_steps: int = 1 << 40) -> np.ndarray:
         info = np.empty(4)

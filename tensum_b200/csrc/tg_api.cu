@@ -886,33 +886,11 @@ tg_status tg_update_parameters(tg_handle* h, const tg_material* mat, const tg_bc
 
 tg_status tg_forces(tg_handle* h, int n_forces, const int* n_tags, const int* tags, double* out) {
   if (!h || n_forces < 1 || !n_tags || !tags || !out) return fail(h, TG_INVALID_ARG, "bad force specification");
-  const HostLayout& L = h->L;
-  const int nbf = (int)L.rb_type.size();
-  std::vector<int4> rec;
-  std::vector<int> off(1, 0);
-  const int* t = tags;
-  for (int f = 0; f < n_forces; ++f) {
-    if (n_tags[f] < 1) return fail(h, TG_INVALID_ARG, "a force needs at least one face tag (src/parameter.cc:652)");
-    // the condition the reference applies on every face of force f is that of bface[f] (src/force.cc:144-150)
-    int dq = -1, k0 = 0, k1 = 0;
-    for (int b = 0; b < nbf; ++b) {
-      bool mine = false;
-      for (int q = 0; q < n_tags[f]; ++q) mine = mine || L.rb_type[b] == t[q];
-      if (!mine) continue;
-      if (L.rb_dev[b] < 0) return fail(h, TG_INVALID_ARG, "force faces must not be periodic");
-      if (f < nbf) {
-        dq = L.rb_dev[f];
-        const int dv0 = L.b_v0[L.rb_dev[b]], dv1 = L.b_v1[L.rb_dev[b]];
-        const int q0 = L.new_of_old[L.rb_v0[f]];
-        k0 = (q0 == dv0) ? 0 : 1;   // value slot: vertex 0 of bface[f] or not (src/bc.h:568-654 via the table)
-        k1 = (q0 == dv1) ? 0 : 1;
-      }
-      rec.push_back(make_int4(L.rb_dev[b], dq, k0, k1));
-    }
-    if ((int)rec.size() == off.back()) return fail(h, TG_INVALID_ARG, "a force tag matches no boundary face");
-    off.push_back((int)rec.size());
-    t += n_tags[f];
-  }
+  std::vector<int> rec4, off;
+  const std::string msg = force_faces(h->L, n_forces, n_tags, tags, rec4, off);
+  if (!msg.empty()) return fail(h, TG_INVALID_ARG, msg);
+  std::vector<int4> rec(rec4.size() / 4);
+  for (size_t i = 0; i < rec.size(); ++i) rec[i] = make_int4(rec4[4 * i], rec4[4 * i + 1], rec4[4 * i + 2], rec4[4 * i + 3]);
   tg_status st;
   const int4* drec = nullptr;
   const int* doff = nullptr;

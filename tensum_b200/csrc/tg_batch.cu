@@ -1,8 +1,8 @@
 // tg_batch.cu -- C ABI of the batched FP32 Monte Carlo ensembles (tensum_gpu.h,
 // "batched ensembles").
 //
-// A batch holds one or more levels (a periodic mesh and its samples); every
-// level advances in the same launches.  One time step of the whole batch is
+// A batch holds one or more levels (a mesh and its samples); every level
+// advances in the same launches.  One time step of the whole batch is
 // captured once into a CUDA graph and replayed; the launch shape (sample tile
 // and block size of the flux and gradient kernels) is chosen by tg_batch_tune.
 #include <cuda_runtime.h>
@@ -49,6 +49,7 @@ struct tg_batch {
   int* stop = nullptr;           // device stop counter (read by kb_step_begin)
   double* tinst = nullptr;
   int shape = 0;                 // index into kShapes
+  bool bnd = false;              // walls / far field or Navier-Stokes: the boundary and viscous passes run
   int dt_chunks = 1;
   cudaGraphExec_t graph_exec = nullptr;
   cudaGraph_t graph = nullptr;
@@ -103,20 +104,20 @@ tg_status bsync(tg_batch* b) {
   return TG_OK;
 }
 
-// Sets the warp offsets of every level for sample tile ST over its vertices
-// (or edges); returns the total.
+// Sets the warp offsets of every level for sample tile ST over its items of
+// the given kind (IT_VERTEX ...); returns the total.
 template <int ST>
-long long layout_warps(Batch& B, bool edges) {
+long long layout_warps(Batch& B, int kind) {
   long long w = 0;
   for (int l = 0; l < B.nlev; ++l) {
     B.lev[l].w_begin = w;
-    w += level_warps<ST>(edges ? B.lev[l].m.ne : B.lev[l].m.nv, B.lev[l].S);
+    w += level_warps<ST>(item_count(B.lev[l].m, kind), B.lev[l].S);
   }
   B.work = w;
   return w;
 }
 
-long long layout(Batch& B, int st, bool edges) { return st == 32 ? layout_warps<32>(B, edges) : layout_warps<16>(B, edges); }
+long long layout(Batch& B, int st, int kind) { return st == 32 ? layout_warps<32>(B, kind) : layout_warps<16>(B, kind); }
 
 typedef void (*FluxK)(Batch, BParams, int);
 
@@ -143,13 +144,50 @@ FluxK flux_kernel(int flux, int recon, int shape) {
   }
 }
 
-FluxK gather_kernel(int shape) {
+template <bool BND>
+FluxK gather_kernel_b(int shape) {
   switch (shape) {
-    case 0: return kb_gather_update<32, 256>;
-    case 1: return kb_gather_update<32, 128>;
-    case 2: return kb_gather_update<16, 256>;
-    default: return kb_gather_update<16, 128>;
+    case 0: return kb_gather_update<32, 256, BND>;
+    case 1: return kb_gather_update<32, 128, BND>;
+    case 2: return kb_gather_update<16, 256, BND>;
+    default: return kb_gather_update<16, 128, BND>;
   }
+}
+
+FluxK gather_kernel(int shape, bool bnd) { return bnd ? gather_kernel_b<true>(shape) : gather_kernel_b<false>(shape); }
+
+template <int F>
+FluxK bflux_kernel_f(int shape) {
+  switch (shape) {
+    case 0: return kb_bflux<F, 32, 256>;
+    case 1: return kb_bflux<F, 32, 128>;
+    case 2: return kb_bflux<F, 16, 256>;
+    default: return kb_bflux<F, 16, 128>;
+  }
+}
+
+FluxK bflux_kernel(int flux, int shape) {
+  switch (flux) {
+    case FLUX_TECNO_ROE: return bflux_kernel_f<FLUX_TECNO_ROE>(shape);
+    case FLUX_TECNO_RUSANOV: return bflux_kernel_f<FLUX_TECNO_RUSANOV>(shape);
+    default: return bflux_kernel_f<FLUX_KEPEC>(shape);
+  }
+}
+
+FluxK viscous_kernel(int shape) {
+  switch (shape) {
+    case 0: return kb_viscous<32, 256>;
+    case 1: return kb_viscous<32, 128>;
+    case 2: return kb_viscous<16, 256>;
+    default: return kb_viscous<16, 128>;
+  }
+}
+
+typedef void (*GradK)(Batch, BParams, int, int);
+
+GradK grad_kernel(int st, bool bnd) {
+  if (st == 32) return bnd ? kb_grad<32, true> : kb_grad<32, false>;
+  return bnd ? kb_grad<16, true> : kb_grad<16, false>;
 }
 
 bool needs_grad(const tg_batch* b) {
@@ -162,34 +200,46 @@ int max_samples(const tg_batch* b) {
   return m;
 }
 
+unsigned blocks_of(const Batch& B, int bs) { return (unsigned)((B.work * 32 + bs - 1) / bs); }
+
 // One full step of every level on b->stream.
 void enqueue_step(tg_batch* b) {
   const Shape sh = kShapes[b->shape];
-  Batch B = b->B, BE = b->B;
-  layout(B, sh.st, false);
-  layout(BE, sh.st, true);
+  Batch B = b->B, BE = b->B, BB = b->B, BU = b->B;
+  layout(B, sh.st, IT_VERTEX);
+  layout(BE, sh.st, IT_EDGE);
+  layout(BB, sh.st, IT_BSLOT);
+  layout(BU, sh.st, IT_UNIT);
   const dim3 gs((max_samples(b) + 255) / 256, b->nlev);
   kb_step_begin<<<gs, 256, 0, b->stream>>>(B, b->prm);
   long long dt_blocks = 0;
   for (int l = 0; l < b->nlev; ++l) dt_blocks += (long long)(B.lev[l].S >> 5) * b->dt_chunks;
-  kb_dt<8><<<(unsigned)dt_blocks, 256, 0, b->stream>>>(B, b->prm, b->dt_chunks);
+  if (b->bnd) kb_dt<8, true><<<(unsigned)dt_blocks, 256, 0, b->stream>>>(B, b->prm, b->dt_chunks);
+  else kb_dt<8, false><<<(unsigned)dt_blocks, 256, 0, b->stream>>>(B, b->prm, b->dt_chunks);
   kb_dt_final<<<gs, 256, 0, b->stream>>>(B, b->prm);
-  const unsigned blocks = (unsigned)((B.work * 32 + sh.bs - 1) / sh.bs);
-  const unsigned eblocks = (unsigned)((BE.work * 32 + sh.bs - 1) / sh.bs);
   FluxK fk = flux_kernel(b->prm.flux, b->prm.recon, b->shape);
-  FluxK gk = gather_kernel(b->shape);
+  FluxK gk = gather_kernel(b->shape, b->bnd);
+  GradK rk = grad_kernel(sh.st, b->bnd);
   for (int r = 0; r < 3; ++r) {
-    if (needs_grad(b)) {
-      if (sh.st == 32) kb_grad<32><<<blocks, sh.bs, 0, b->stream>>>(B, b->prm, r);
-      else kb_grad<16><<<blocks, sh.bs, 0, b->stream>>>(B, b->prm, r);
-    }
-    fk<<<eblocks, sh.bs, 0, b->stream>>>(BE, b->prm, r);
-    gk<<<blocks, sh.bs, 0, b->stream>>>(B, b->prm, r);
+    if (needs_grad(b)) rk<<<blocks_of(B, sh.bs), sh.bs, 0, b->stream>>>(B, b->prm, r, 0);
+    if (b->bnd && BB.work > 0) bflux_kernel(b->prm.flux, b->shape)<<<blocks_of(BB, sh.bs), sh.bs, 0, b->stream>>>(BB, b->prm, r);
+    if (b->prm.model == 1) viscous_kernel(b->shape)<<<blocks_of(BU, sh.bs), sh.bs, 0, b->stream>>>(BU, b->prm, r);
+    fk<<<blocks_of(BE, sh.bs), sh.bs, 0, b->stream>>>(BE, b->prm, r);
+    gk<<<blocks_of(B, sh.bs), sh.bs, 0, b->stream>>>(B, b->prm, r);
   }
   kb_step_end<<<gs, 256, 0, b->stream>>>(B, b->prm);
 }
 
-int kernels_per_step(const tg_batch* b) { return 4 + 3 * (needs_grad(b) ? 3 : 2); }
+bool has_bfaces(const tg_batch* b) {
+  for (int l = 0; l < b->nlev; ++l)
+    if (b->B.lev[l].m.nb > 0) return true;
+  return false;
+}
+
+int kernels_per_step(const tg_batch* b) {
+  const int per_stage = 2 + (needs_grad(b) ? 1 : 0) + (b->bnd && has_bfaces(b) ? 1 : 0) + (b->prm.model == 1 ? 1 : 0);
+  return 4 + 3 * per_stage;
+}
 
 void drop_graph(tg_batch* b) {
   if (b->graph_exec) cudaGraphExecDestroy(b->graph_exec);
@@ -262,7 +312,10 @@ tg_status tg_batch_create(const tg_batch_level* levels, int n_levels, const tg_m
   int ndev = 0;
   if (cudaGetDeviceCount(&ndev) != cudaSuccess || ndev == 0)
     return bfail(nullptr, TG_NO_DEVICE, "no CUDA device visible; the GPU path has no CPU fallback");
-  if (mat->model != 0) return bfail(nullptr, TG_NOT_SUPPORTED, "batched ensembles are Euler only");
+  if (mat->model != 0 && mat->mu_model != 0)
+    return bfail(nullptr, TG_NOT_SUPPORTED, "batched Navier-Stokes ensembles use the constant viscosity law");
+  if (opt->bc_strong || opt->liou_fix)
+    return bfail(nullptr, TG_NOT_SUPPORTED, "batched ensembles run weak boundary conditions without the Liou switch");
   if (!(mat->flux_scheme == FLUX_TECNO_ROE || mat->flux_scheme == FLUX_TECNO_RUSANOV || mat->flux_scheme == FLUX_KEPEC))
     return bfail(nullptr, TG_NOT_SUPPORTED, "batched ensembles run kepes_tecno_roe, kepes_tecno_rusanov or kepec");
   if (!(mat->reconstruct_scheme == RECON_FIRST || mat->reconstruct_scheme == RECON_TVD_MINMOD))
@@ -282,12 +335,9 @@ tg_status tg_batch_create(const tg_batch_level* levels, int n_levels, const tg_m
       return bfail(nullptr, TG_INVALID_ARG, "every level needs a mesh and a positive multiple of 32 samples");
     }
     LevelHost& H = b->lh[l];
-    std::string msg = build_layout(*levels[l].mesh, levels[l].bc, false, H.L);
+    std::string msg = build_layout(*levels[l].mesh, levels[l].bc, mat->model == 1, H.L);
     if (!msg.empty()) { tg_batch_destroy(b); return bfail(nullptr, TG_INVALID_ARG, msg); }
-    if (H.L.nb != 0) {
-      tg_batch_destroy(b);
-      return bfail(nullptr, TG_NOT_SUPPORTED, "batched ensembles need fully periodic meshes");
-    }
+    if (H.L.nb != 0 || mat->model == 1) b->bnd = true;
     H.S = levels[l].n_samples;
     const HostLayout& L = H.L;
     Level& V = b->B.lev[l];
@@ -308,14 +358,31 @@ tg_status tg_batch_create(const tg_batch_level* levels, int n_levels, const tg_m
     BU(L.e_a, e_a) BU(L.e_b, e_b) BU(ux, ux) BU(uy, uy) BU(ar, ar) BU(L.e_nx, nx) BU(L.e_ny, ny)
     BU(L.e_dx, dx) BU(L.e_dy, dy) BU(L.e_g0x, g0x) BU(L.e_g0y, g0y) BU(L.e_g1x, g1x) BU(L.e_g1y, g1y)
     BU(L.ce_off, ce_off) BU(L.ce_ent, ce_ent) BU(L.dcarea, area) BU(L.inv6mc, inv6mc) BU(L.x, x) BU(L.y, y) BU(aw, aw)
+    m.nb = L.nb; m.nvu = L.nvu; m.nic = L.n_int_cells;
+    BU(L.b_v0, b_v0) BU(L.b_v1, b_v1) BU(L.b_kind, b_kind) BU(L.b_adiab, b_adiab) BU(L.b_nx, b_nx) BU(L.b_ny, b_ny)
+    BU(L.cb_off, cb_off) BU(L.cb_ent, cb_ent)
+    BU(L.u_cell, u_cell) BU(L.c_v, c_v) BU(L.c_n, c_n) BU(L.c_inv2a, c_inv2a) BU(L.c_bf_off, c_bf_off) BU(L.c_bf, c_bf)
+    BU(L.c_nbr_off, c_nbr_off) BU(L.c_nbr, c_nbr) BU(L.bf_face_nx, bf_nx) BU(L.bf_face_ny, bf_ny)
+    BU(L.bf_face_v0, bf_v0) BU(L.bf_face_v1, bf_v1)
 #undef BU
     const size_t vs = (size_t)L.nv * V.P;
     for (int r = 0; r < 3; ++r)
       if ((st = balloc(b, kQ * vs, &V.Q[r])) != TG_OK) { tg_batch_destroy(b); return st; }
     if ((st = balloc(b, 4 * vs, &V.Uold)) != TG_OK) { tg_batch_destroy(b); return st; }
     if ((st = balloc(b, 4 * (size_t)L.ne * V.P, &V.F)) != TG_OK) { tg_batch_destroy(b); return st; }
-    if (mat->reconstruct_scheme != RECON_FIRST && mat->flux_scheme != FLUX_KEPEC) {
+    if ((mat->reconstruct_scheme != RECON_FIRST && mat->flux_scheme != FLUX_KEPEC) || L.nb > 0 || mat->model == 1) {
       if ((st = balloc(b, kG * vs, &V.G)) != TG_OK) { tg_batch_destroy(b); return st; }
+    }
+    if (L.nb > 0 || mat->model == 1) {
+      // per-sample boundary values and viscosity, initialised from the level's table and the material
+      if ((st = balloc(b, 10 * (size_t)std::max(L.nb, 1) * V.P, &V.bval)) != TG_OK ||
+          (st = balloc(b, (size_t)V.P, &V.mu)) != TG_OK ||
+          (st = balloc(b, 8 * (size_t)std::max(L.nb, 1) * V.P, &V.Fb)) != TG_OK ||
+          (st = balloc(b, 3 * (size_t)std::max(L.nb, 1) * V.P, &V.Fvb)) != TG_OK ||
+          (st = balloc(b, 9 * (size_t)std::max(L.nvu, 1) * V.P, &V.Fv)) != TG_OK) {
+        tg_batch_destroy(b);
+        return st;
+      }
     }
     LevelClock& c = V.c;
     if ((st = balloc(b, H.S, &c.elapsed)) != TG_OK || (st = balloc(b, H.S, &c.dt)) != TG_OK ||
@@ -333,6 +400,9 @@ tg_status tg_batch_create(const tg_batch_level* levels, int n_levels, const tg_m
   k.ev_alpha = (float)mat->ev_mod_alpha; k.ev_beta = (float)mat->ev_mod_beta;
   k.final_time = opt->final_time;
   k.flux = mat->flux_scheme; k.recon = mat->reconstruct_scheme;
+  k.model = mat->model;
+  k.cp_over_pr = (float)(mat->gamma * mat->gas_const / (mat->gamma - 1.0) / mat->prandtl);
+  k.visc = mat->visc_active; k.heat = mat->heat_active;
   // output time instances (src/fv.cc:52-62)
   std::vector<double> ti;
   const double dti = opt->final_time / opt->n_time_stamps;
@@ -356,6 +426,19 @@ tg_status tg_batch_create(const tg_batch_level* levels, int n_levels, const tg_m
   if (e != cudaSuccess) { tg_batch_destroy(b); return bfail(nullptr, TG_CUDA_ERROR, cudaGetErrorString(e)); }
   for (int l = 0; l < n_levels; ++l)
     if ((st = reset_clock(b, l, 0, b->B.lev[l].S)) != TG_OK) { tg_batch_destroy(b); return st; }
+  for (int l = 0; l < n_levels; ++l) {
+    if (!b->B.lev[l].mu) continue;
+    const int S = b->B.lev[l].S;
+    const size_t nbf = b->lh[l].L.rb_type.size();
+    std::vector<double> mu(S, mat->mu_ref), bv;
+    const double* bvp = nullptr;
+    if (levels[l].bc && levels[l].bc->bface_values && nbf) {
+      bv.resize((size_t)S * nbf * 10);
+      for (int s = 0; s < S; ++s) std::memcpy(bv.data() + (size_t)s * nbf * 10, levels[l].bc->bface_values, nbf * 10 * sizeof(double));
+      bvp = bv.data();
+    }
+    if ((st = tg_batch_set_parameters(b, l, mu.data(), bvp)) != TG_OK) { tg_batch_destroy(b); return st; }
+  }
   *out = b;
   return TG_OK;
 }
@@ -415,6 +498,104 @@ tg_status tg_batch_get_state(tg_batch* b, int level, int sample, double* prim_ao
     const double rho = -V5 * pr;
     p[0] = pr / (b->prm.R * rho); p[1] = pr; p[2] = u; p[3] = v; p[4] = 0.0;
   }
+  return TG_OK;
+}
+
+tg_status tg_batch_set_parameters(tg_batch* b, int level, const double* mu_ref, const double* bface_values) {
+  if (!b || level < 0 || level >= b->nlev) return bfail(b, TG_INVALID_ARG, "bad level");
+  const Level& V = b->B.lev[level];
+  const HostLayout& L = b->lh[level].L;
+  if (!V.mu) return bfail(b, TG_NOT_SUPPORTED, "a periodic Euler level has no per-sample parameters");
+  const int S = V.S;
+  if (mu_ref) {
+    std::vector<float> mu(V.P, 0.0f);
+    for (int s = 0; s < S; ++s) {
+      if (!(mu_ref[s] >= 0.0)) return bfail(b, TG_INVALID_ARG, "viscosity must be >= 0");
+      mu[s] = (float)mu_ref[s];
+    }
+    TB_CUDA(b, cudaMemcpyAsync(V.mu, mu.data(), V.P * sizeof(float), cudaMemcpyHostToDevice, b->stream));
+  }
+  if (bface_values && L.nb > 0) {
+    // reference boundary-face order (10 values per face) -> [device face][value][sample]
+    const size_t nbf = L.rb_type.size();
+    std::vector<float> h((size_t)L.nb * 10 * V.P, 0.0f);
+    for (size_t f = 0; f < nbf; ++f) {
+      const int d = L.rb_dev[f];
+      if (d < 0) continue;
+      for (int q = 0; q < 10; ++q) {
+        float* row = h.data() + ((size_t)d * 10 + q) * V.P;
+        for (int s = 0; s < S; ++s) row[s] = (float)bface_values[((size_t)s * nbf + f) * 10 + q];
+      }
+    }
+    TB_CUDA(b, cudaMemcpyAsync(V.bval, h.data(), h.size() * sizeof(float), cudaMemcpyHostToDevice, b->stream));
+  }
+  return bsync(b);
+}
+
+tg_status tg_batch_set_uniform(tg_batch* b, int level, const double* prim) {
+  if (!b || !prim || level < 0 || level >= b->nlev) return bfail(b, TG_INVALID_ARG, "bad level or NULL state");
+  const Level& V = b->B.lev[level];
+  const int S = V.S;
+  const double g = b->prm.gamma;
+  std::vector<float> rec((size_t)kQ * S);
+  for (int s = 0; s < S; ++s) {
+    const double* p = prim + 5 * (size_t)s;   // PrimVar T, p, u, v, w
+    const double T = p[0], pr = p[1], u = p[2], v = p[3];
+    if (!(T > 0.0) || !(pr > 0.0)) return bfail(b, TG_INVALID_ARG, "state needs T > 0 and p > 0 (src/fv.cc:388-389)");
+    const double rho = pr / (b->prm.R * T);
+    const double beta = rho / (2.0 * pr);
+    const double ent = std::log(pr) - g * std::log(rho);
+    rec[0 * (size_t)S + s] = (float)u;
+    rec[1 * (size_t)S + s] = (float)v;
+    rec[2 * (size_t)S + s] = (float)pr;
+    rec[3 * (size_t)S + s] = (float)((g - ent) / (g - 1.0) - (u * u + v * v) * beta);
+    rec[4 * (size_t)S + s] = (float)(-2.0 * beta);
+  }
+  float* d = nullptr;
+  TB_CUDA(b, cudaMalloc((void**)&d, rec.size() * sizeof(float)));
+  cudaError_t e = cudaMemcpyAsync(d, rec.data(), rec.size() * sizeof(float), cudaMemcpyHostToDevice, b->stream);
+  if (e == cudaSuccess) {
+    const long long t = (long long)V.m.nv * S;
+    kb_ic_uniform<<<(unsigned)((t + 255) / 256), 256, 0, b->stream>>>(V, d);
+    e = cudaStreamSynchronize(b->stream);
+  }
+  cudaFree(d);
+  if (e != cudaSuccess) return bfail(b, TG_CUDA_ERROR, cudaGetErrorString(e));
+  return reset_clock(b, level, 0, S);
+}
+
+tg_status tg_batch_forces(tg_batch* b, int level, int n_forces, const int* n_tags, const int* tags, double* out) {
+  if (!b || level < 0 || level >= b->nlev || n_forces < 1 || !n_tags || !tags || !out)
+    return bfail(b, TG_INVALID_ARG, "bad level or force specification");
+  const Level& V = b->B.lev[level];
+  if (!V.mu) return bfail(b, TG_NOT_SUPPORTED, "a periodic Euler level has no boundary faces");
+  std::vector<int> rec4, off;
+  const std::string msg = force_faces(b->lh[level].L, n_forces, n_tags, tags, rec4, off);
+  if (!msg.empty()) return bfail(b, TG_INVALID_ARG, msg);
+  // the viscous force reads the vertex gradients of the current state (src/force.cc:123)
+  const Shape sh = kShapes[0];
+  Batch B = b->B;
+  layout(B, sh.st, IT_VERTEX);
+  if (b->prm.model == 1) grad_kernel(sh.st, true)<<<blocks_of(B, sh.bs), sh.bs, 0, b->stream>>>(B, b->prm, 0, 1);
+  int* drec = nullptr;
+  int* doff = nullptr;
+  double* dout = nullptr;
+  const size_t nout = (size_t)V.S * n_forces * 4;
+  TB_CUDA(b, cudaMalloc((void**)&drec, rec4.size() * sizeof(int)));
+  cudaError_t e = cudaMalloc((void**)&doff, off.size() * sizeof(int));
+  if (e == cudaSuccess) e = cudaMalloc((void**)&dout, nout * sizeof(double));
+  if (e == cudaSuccess) e = cudaMemcpyAsync(drec, rec4.data(), rec4.size() * sizeof(int), cudaMemcpyHostToDevice, b->stream);
+  if (e == cudaSuccess) e = cudaMemcpyAsync(doff, off.data(), off.size() * sizeof(int), cudaMemcpyHostToDevice, b->stream);
+  if (e == cudaSuccess) {
+    kb_forces<8><<<(unsigned)(n_forces * (V.S >> 5)), 256, 0, b->stream>>>(V, b->prm, (const int4*)drec, doff, n_forces, dout);
+    e = cudaMemcpyAsync(out, dout, nout * sizeof(double), cudaMemcpyDeviceToHost, b->stream);
+  }
+  if (e == cudaSuccess) e = cudaStreamSynchronize(b->stream);
+  if (e == cudaSuccess) e = cudaGetLastError();
+  cudaFree(drec);
+  cudaFree(doff);
+  cudaFree(dout);
+  if (e != cudaSuccess) return bfail(b, TG_CUDA_ERROR, cudaGetErrorString(e));
   return TG_OK;
 }
 

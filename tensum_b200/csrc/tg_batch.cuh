@@ -1,6 +1,6 @@
 // tg_batch.cuh -- batched FP32 Monte Carlo ensembles: physics and kernels.
 //
-// An ensemble level is S samples of one periodic mesh, advanced together.
+// An ensemble level is S samples of one mesh, advanced together.
 // Every per-sample array is [vertex or edge][component][sample] with the
 // sample index innermost, so the 32 lanes of a warp hold 32 samples of one
 // vertex: state loads are 128-byte coalesced, all components of a vertex are
@@ -15,6 +15,12 @@
 // vertex's edges in a fixed order and applies the SSP-RK3 stage update: every
 // flux is computed once, an edge's flux enters both endpoints bit for bit
 // (exact conservation), and there are no atomics.
+//
+// Meshes with walls or far field, and Navier-Stokes, add per stage a boundary
+// pass (one flux per boundary-face vertex and sample) and a viscous pass (one
+// set of viscous fluxes per cell or boundary face and sample), both stored and
+// gathered by the vertex pass in the order of the per-vertex boundary list.
+// Boundary values and the viscosity are per sample (uncertain inflow, Re).
 #pragma once
 
 #include <cstdint>
@@ -40,6 +46,19 @@ struct LevelMesh {
   const float *area, *inv6mc;      // dual area, 1 / (6 median area)
   const double* aw;                // dual area x periodic-copy weight (integrals)
   const double *x, *y;             // coordinates (initial conditions)
+  // non-periodic boundary faces and the per-vertex boundary / viscous gather
+  // (entry (index << 2) | type, types as in tg_mesh.h)
+  int nb, nvu, nic;                // boundary faces, viscous units, interior-cell units
+  const int *b_v0, *b_v1, *b_kind, *b_adiab;
+  const float *b_nx, *b_ny;
+  const int *cb_off, *cb_ent;
+  // viscous units: interior cells, then one boundary cell per boundary face
+  const int *u_cell, *c_v;         // cell of a unit; 3 vertices per cell
+  const float *c_n, *c_inv2a;      // 6 P1 normals per cell; 1 / (2 cell area)
+  const int *c_bf_off, *c_bf;      // boundary faces with the cell on their left (gradient corrections)
+  const int *c_nbr_off, *c_nbr;    // the cell's boundary faces in cell.face slot order
+  const float *bf_nx, *bf_ny;      // face-list normal of a boundary face
+  const int *bf_v0, *bf_v1;        // face-list vertex order of a boundary face
 };
 
 // Per-sample clock of one level.
@@ -62,6 +81,12 @@ struct Level {
   float* Uold;                     // nv x 4 x S
   float* G;                        // nv x kG x S
   float* F;                        // ne x 4 x S: area-weighted edge fluxes of the current stage
+  // boundaries / Navier-Stokes (null on periodic Euler levels)
+  float* bval;                     // nb x 10 x S: boundary values (T,u,v,w,p at face vertex 0, then 1)
+  float* mu;                       // S: viscosity per sample (constant viscosity law)
+  float* Fb;                       // 2 nb x 4 x S: boundary fluxes per face vertex
+  float* Fv;                       // nvu x 9 x S: viscous fluxes (x, y, energy) toward the cell's 3 vertices
+  float* Fvb;                      // nb x 3 x S: viscous boundary fluxes
   long long w_begin;               // first warp of this level in a fused launch (set per launch shape)
 };
 
@@ -73,6 +98,8 @@ struct Batch {
 
 struct BParams {
   float gamma, R, inv_gm1, inv_gamma, sqrt_gm1, cfl, ev_alpha, ev_beta;
+  float cp_over_pr;                // Cp / Pr (heat conductivity = mu Cp / Pr)
+  int model, visc, heat;           // 0 Euler, 1 Navier-Stokes; viscous / heat terms active
   double final_time;
   const double* tinst;
   int ntinst;
@@ -218,6 +245,164 @@ __device__ __forceinline__ FFlx fflux(const BParams& k, const FRec& L, const FRe
   return fkepec(k, L, R, unx, uny, r, b);
 }
 
+// ------------------------------------------------- FP32 boundaries, viscous
+struct FPrim { float T, u, v, p; };
+struct FEnt { float f, vx, vy, l; };
+
+// Primitive state of a stored record q (u, v, p, V1, V5 at stride P).
+__device__ __forceinline__ FPrim fprim(const BParams& k, const float* q, int P) {
+  FPrim s;
+  s.u = q[0]; s.v = q[P]; s.p = q[2 * P];
+  s.T = s.p / (k.R * (-q[4 * P] * s.p));
+  return s;
+}
+
+__device__ __forceinline__ FEnt fprim2ent(const BParams& k, const FPrim& q) {   // src/material.h:534-546
+  const float rho = q.p / (k.R * q.T);
+  const float beta = rho / (2.0f * q.p);
+  const float s = logf(q.p) - k.gamma * logf(rho);
+  FEnt e;
+  e.f = (k.gamma - s) * k.inv_gm1 - (q.u * q.u + q.v * q.v) * beta;
+  e.vx = q.u * (2.0f * beta);
+  e.vy = q.v * (2.0f * beta);
+  e.l = -2.0f * beta;
+  return e;
+}
+
+// BoundaryCondition::apply, single-state form (src/bc.h:615-654); val holds
+// T, u, v, w, p of one face vertex at stride P.
+__device__ __forceinline__ void fbc_apply1(int kind, int adiabatic, const float* val, int P, float nx, float ny,
+                                           FPrim& s) {
+  switch (kind) {
+    case BC_SLIP: {
+      const float im = 1.0f / sqrtf(nx * nx + ny * ny);
+      const float ux = nx * im, uy = ny * im;
+      const float fact = s.u * ux + s.v * uy;
+      s.u += ux * -fact;
+      s.v += uy * -fact;
+      break;
+    }
+    case BC_NOSLIP:
+      s.u = val[P]; s.v = val[2 * P];
+      if (!adiabatic) s.T = val[0];
+      break;
+    case BC_PRESSURE: s.p = val[4 * P]; break;
+    case BC_INLET: s.T = val[0]; s.u = val[P]; s.v = val[2 * P]; s.p = val[4 * P]; break;
+    default: break;
+  }
+}
+
+// Two-state form (src/bc.h:568-610): s0 the state the flux sees inside, s1 the boundary state.
+__device__ __forceinline__ void fbc_apply2(int kind, int adiabatic, const float* val, int P, float nx, float ny,
+                                           FPrim& s0, FPrim& s1) {
+  switch (kind) {
+    case BC_SLIP: {
+      const float im = 1.0f / sqrtf(nx * nx + ny * ny);
+      const float ux = nx * im, uy = ny * im;
+      const float fact = s0.u * ux + s0.v * uy;
+      s0.u += ux * -fact;
+      s0.v += uy * -fact;
+      s1 = s0;
+      break;
+    }
+    case BC_NOSLIP:
+      s0.u = val[P]; s0.v = val[2 * P];
+      s1.u = s0.u; s1.v = s0.v;
+      s1.p = s0.p;
+      if (adiabatic) s1.T = s0.T;
+      else { s0.T = val[0]; s1.T = val[0]; }
+      break;
+    case BC_PRESSURE: s1.p = val[4 * P]; break;
+    case BC_INLET:
+      s0.T = val[0]; s0.u = val[P]; s0.v = val[2 * P]; s0.p = val[4 * P];
+      s1 = s0;
+      break;
+    case BC_OUTLET: s1 = s0; break;
+    case BC_FARFIELD: s1.T = val[0]; s1.u = val[P]; s1.v = val[2 * P]; s1.p = val[4 * P]; break;
+    default: break;
+  }
+}
+
+// Entropy variables of the single-state condition applied to stored record q.
+// Where the condition keeps T and p (slip, adiabatic no-slip) beta and the
+// entropy are unchanged and V1 moves by beta (|u|^2 - |u'|^2) exactly; where
+// it changes nothing the stored variables are returned; otherwise they are
+// formed anew.
+__device__ __forceinline__ FEnt fbc_ent(const BParams& k, int kind, int adiabatic, const float* val, int P, float nx,
+                                        float ny, const float* q) {
+  FPrim s = fprim(k, q, P);
+  const float u0 = s.u, v0 = s.v;
+  const float V1 = q[3 * P], V5 = q[4 * P];
+  const bool keeps_Tp = kind == BC_SLIP || (kind == BC_NOSLIP && adiabatic);
+  const bool changes = keeps_Tp || kind == BC_NOSLIP || kind == BC_PRESSURE || kind == BC_INLET;
+  if (!changes) return FEnt{V1, -V5 * u0, -V5 * v0, V5};
+  fbc_apply1(kind, adiabatic, val, P, nx, ny, s);
+  if (!keeps_Tp) return fprim2ent(k, s);
+  const float beta = -0.5f * V5;
+  return FEnt{V1 + beta * ((u0 * u0 + v0 * v0) - (s.u * s.u + s.v * s.v)), -V5 * s.u, -V5 * s.v, V5};
+}
+
+// Flux record of a boundary state (entropy formed from T and p).
+__device__ __forceinline__ FRec frec_prim(const BParams& k, const FPrim& s, bool need_a) {
+  const float rho = s.p / (k.R * s.T);
+  const float beta = rho / (2.0f * s.p);
+  const float ent = logf(s.p) - k.gamma * logf(rho);
+  const float V1 = (k.gamma - ent) * k.inv_gm1 - (s.u * s.u + s.v * s.v) * beta;
+  return frec(k, s.u, s.v, s.p, V1, -2.0f * beta, need_a);
+}
+
+// Material::inviscid_bflux (src/material.cc:110-127), normal of length |n|.
+__device__ __forceinline__ FFlx finviscid_bflux(const BParams& k, const FPrim& q, const FPrim& qb, float nx, float ny) {
+  const float vnb = qb.u * nx + qb.v * ny;
+  const float vn = q.u * nx + q.v * ny;
+  const float rho = q.p / (k.R * q.T);
+  FFlx F;
+  F.m = rho * vnb;
+  F.x = nx * qb.p + q.u * F.m;
+  F.y = ny * qb.p + q.v * F.m;
+  F.e = (0.5f * rho * (q.u * q.u + q.v * q.v) + k.gamma * q.p * k.inv_gm1) * vnb + (qb.p - q.p) * vn;
+  return F;
+}
+
+// Viscous matrices K dV (src/material.cc:158-230) at the entropy state st for
+// the cell gradient dE (V1, V2, V3, V5) x (x, y), constant viscosity mu.
+struct FViscK { float a1, a2, a4, b1, b2, b4, e4, c2; };
+
+__device__ __forceinline__ FViscK fviscous_K(const BParams& k, float mu_s, const FEnt& st, const float* dE) {
+  float mu = mu_s;
+  float kk = mu * k.cp_over_pr;
+  if (!k.visc) mu = 0.0f;
+  if (!k.heat) kk = 0.0f;
+  const float e4 = 1.0f / st.l;
+  const float e1 = st.vx * e4, e2 = st.vy * e4;
+  const float c1 = 4.0f * mu / 3.0f, c2 = kk / k.R, c3 = 2.0f * mu / 3.0f;
+  const float d1x = dE[2], d1y = dE[3], d2x = dE[4], d2y = dE[5], d4x = dE[6], d4y = dE[7];
+  const float K11_1 = c1 * (-d1x + e1 * d4x);
+  const float K11_2 = mu * (-d2x + e2 * d4x);
+  const float K11_4 = c1 * e1 * d1x + mu * (e2 * d2x) + (-c1 * e1 * e1 - mu * (e2 * e2) + c2 * e4) * d4x;
+  const float K12_1 = c3 * (d2y - e2 * d4y);
+  const float K12_2 = mu * (-d1y + e1 * d4y);
+  const float K12_4 = mu * e2 * d1y - c3 * e1 * d2y - (mu - c3) * e1 * e2 * d4y;
+  const float K21_1 = mu * (-d2x + e2 * d4x);
+  const float K21_2 = c3 * (d1x - e1 * d4x);
+  const float K21_4 = -c3 * e2 * d1x + mu * e1 * d2x - (mu - c3) * e1 * e2 * d4x;
+  const float K22_1 = mu * (-d1y + e1 * d4y);
+  const float K22_2 = c1 * (-d2y + e2 * d4y);
+  const float K22_4 = mu * (e1 * d1y) + c1 * e2 * d2y + (-mu * (e1 * e1) - c1 * e2 * e2 + c2 * e4) * d4y;
+  FViscK r;
+  r.a1 = K11_1 + K12_1; r.a2 = K11_2 + K12_2; r.a4 = K11_4 + K12_4;
+  r.b1 = K21_1 + K22_1; r.b2 = K21_2 + K22_2; r.b4 = K21_4 + K22_4;
+  r.e4 = e4;
+  r.c2 = c2;
+  return r;
+}
+
+__device__ __forceinline__ void fviscous_apply(const FViscK& K, float nx, float ny, float& fx, float& fy, float& fe) {
+  fx = -(K.a1 * nx + K.b1 * ny) * K.e4;
+  fy = -(K.a2 * nx + K.b2 * ny) * K.e4;
+  fe = -(K.a4 * nx + K.b4 * ny) * K.e4;
+}
+
 // ------------------------------------------------------------------ indexing
 // A warp covers 32/ST vertices x ST samples (the sample tile ST is 32 or 16);
 // warps are ordered sample-group-major, so consecutive warps walk neighbouring
@@ -231,8 +416,14 @@ __host__ __device__ __forceinline__ long long level_warps(int nv, int S) {
   return (long long)((nv + VPW - 1) / VPW) * (S / ST);
 }
 
-// EDGE: items are (edge, sample) instead of (vertex, sample).
-template <int ST, bool EDGE = false>
+// What a launch's items are: (vertex | edge | boundary-face vertex | viscous unit, sample).
+enum : int { IT_VERTEX = 0, IT_EDGE = 1, IT_BSLOT = 2, IT_UNIT = 3 };
+
+__host__ __device__ __forceinline__ int item_count(const LevelMesh& m, int kind) {
+  return kind == IT_VERTEX ? m.nv : kind == IT_EDGE ? m.ne : kind == IT_BSLOT ? 2 * m.nb : m.nvu;
+}
+
+template <int ST, int KIND = IT_VERTEX>
 __device__ __forceinline__ Item item_of(const Batch& B, long long w, int lane) {
   constexpr int VPW = 32 / ST;
   Item it{0, 0, 0, false};
@@ -242,7 +433,7 @@ __device__ __forceinline__ Item item_of(const Batch& B, long long w, int lane) {
   for (int i = 1; i < kMaxLevels; ++i)
     if (i < B.nlev && w >= B.lev[i].w_begin) l = i;
   const long long r = w - B.lev[l].w_begin;
-  const int n = EDGE ? B.lev[l].m.ne : B.lev[l].m.nv;
+  const int n = item_count(B.lev[l].m, KIND);
   const int nvw = (n + VPW - 1) / VPW;
   it.l = l;
   it.s = (int)(r / nvw) * ST + (lane % ST);
@@ -267,11 +458,12 @@ __global__ void kb_step_begin(Batch B, BParams k) {
   L.c.dtmin_bits[s] = 0x7f800000u;
 }
 
-// Local time step (src/fv.cc:1499-1580, inviscid) of every vertex and the
-// running per-sample minimum; U_old (src/fv.cc:1626-1630).  Each thread keeps
-// one sample and walks a strided set of vertices, so one atomic per block and
-// sample remains.
-template <int VT>
+// Local time step (src/fv.cc:1499-1580) of every vertex and the running
+// per-sample minimum; U_old (src/fv.cc:1626-1630).  Each thread keeps one
+// sample and walks a strided set of vertices, so one atomic per block and
+// sample remains.  BND adds the boundary-face terms and, for Navier-Stokes,
+// the viscous ones, in the reference's order.
+template <int VT, bool BND>
 __global__ void __launch_bounds__(32 * VT) kb_dt(Batch B, BParams k, int chunks) {
   const int lane = threadIdx.x & 31, vg = threadIdx.x >> 5;
   // blockIdx.x: (level, sample group, chunk)
@@ -302,6 +494,23 @@ __global__ void __launch_bounds__(32 * VT) kb_dt(Batch B, BParams k, int chunks)
         const int e = L.m.ce_ent[j] >> 1;
         const float nx = L.m.nx[e], ny = L.m.ny[e];
         lam += fabsf(u * nx + w * ny) + c * L.m.ar[e];
+      }
+      if (BND) {
+        for (int j = L.m.cb_off[v]; j < L.m.cb_off[v + 1]; ++j) {
+          const int ent = L.m.cb_ent[j];
+          if ((ent & 3) != 0) continue;
+          const int d = ent >> 3;           // entry (2 d + vertex slot) << 2
+          const float nx = L.m.b_nx[d], ny = L.m.b_ny[d];
+          lam += 0.5f * (fabsf(u * nx + w * ny) + c * sqrtf(nx * nx + ny * ny));
+        }
+        if (k.model == 1) {
+          const float mu = L.mu[s];
+          for (int j = L.m.ce_off[v]; j < L.m.ce_off[v + 1]; ++j) {
+            const int e = L.m.ce_ent[j] >> 1;
+            const float dx = L.m.dx[e], dy = L.m.dy[e];
+            lam += mu * L.m.ar[e] / sqrtf(dx * dx + dy * dy) / rho;
+          }
+        }
       }
       const float dtv = k.cfl * L.m.area[v] / lam;
       m = fminf(m, dtv > 0.0f ? dtv : __int_as_float(0x7f800000));
@@ -339,14 +548,16 @@ __global__ void kb_dt_final(Batch B, BParams k) {
 }
 
 // Gradients of the entropy variables (src/fv.cc:699-1059 in the edge form
-// grad_v = sum_e g_{v,e} (W_o - W_v) / (6 mcarea)), one (vertex, sample) per thread.
-template <int ST>
-__global__ void kb_grad(Batch B, BParams k, int r) {
+// grad_v = sum_e g_{v,e} (W_o - W_v) / (6 mcarea)), one (vertex, sample) per
+// thread.  BND adds the boundary-face corrections n_b (W_b0 + W_b1 - W_0 - W_1) / 2
+// (src/fv.cc:926-966).  every != 0: all samples, held ones included (forces).
+template <int ST, bool BND>
+__global__ void kb_grad(Batch B, BParams k, int r, int every) {
   const long long w = (blockIdx.x * (long long)blockDim.x + threadIdx.x) >> 5;
   const Item it = item_of<ST>(B, w, threadIdx.x & 31);
   if (!it.ok) return;
   const Level& L = B.lev[it.l];
-  if (!L.c.active[it.s]) return;
+  if (!every && !L.c.active[it.s]) return;
   const int v = it.v, s = it.s;
   const int S = L.P;   // row pitch
   const float* Q = L.Q[r] + s;
@@ -373,6 +584,30 @@ __global__ void kb_grad(Batch B, BParams k, int r) {
       acc[2 * c + 1] += gy * d;
     }
   }
+  if (BND) {
+    for (int j = L.m.cb_off[v]; j < L.m.cb_off[v + 1]; ++j) {
+      const int ent = L.m.cb_ent[j];
+      if ((ent & 3) != 1) continue;
+      const int d = ent >> 2;
+      const int kind = L.m.b_kind[d], ad = L.m.b_adiab[d];
+      const float nx = L.m.b_nx[d], ny = L.m.b_ny[d];
+      const float* val = L.bval + rows(d, 10, S) + s;
+      const float* q0 = Q + rows(L.m.b_v0[d], kQ, S);
+      const float* q1 = Q + rows(L.m.b_v1[d], kQ, S);
+      const FEnt e0 = fbc_ent(k, kind, ad, val, S, nx, ny, q0);
+      const FEnt e1 = fbc_ent(k, kind, ad, val + 5 * S, S, nx, ny, q1);
+      float w0[4], w1[4];
+      W(L.m.b_v0[d], w0);
+      W(L.m.b_v1[d], w1);
+      const float dW[4] = {(e0.f + e1.f - w0[0] - w1[0]) * 0.5f, (e0.vx + e1.vx - w0[1] - w1[1]) * 0.5f,
+                           (e0.vy + e1.vy - w0[2] - w1[2]) * 0.5f, (e0.l + e1.l - w0[3] - w1[3]) * 0.5f};
+#pragma unroll
+      for (int c = 0; c < 4; ++c) {
+        acc[2 * c] += nx * dW[c];
+        acc[2 * c + 1] += ny * dW[c];
+      }
+    }
+  }
   const float f = L.m.inv6mc[v];
   float* G = L.G + rows(v, kG, S) + s;
 #pragma unroll
@@ -385,7 +620,7 @@ __global__ void kb_grad(Batch B, BParams k, int r) {
 template <int FLUX, int RECON, int ST, int BS>
 __global__ void __launch_bounds__(BS) kb_edge_flux(Batch B, BParams k, int r) {
   const long long w = (blockIdx.x * (long long)blockDim.x + threadIdx.x) >> 5;
-  const Item it = item_of<ST, true>(B, w, threadIdx.x & 31);
+  const Item it = item_of<ST, IT_EDGE>(B, w, threadIdx.x & 31);
   if (!it.ok) return;
   const Level& L = B.lev[it.l];
   const int e = it.v, s = it.s;
@@ -411,10 +646,141 @@ __global__ void __launch_bounds__(BS) kb_edge_flux(Batch B, BParams k, int r) {
   Fo[0] = F.m * ar; Fo[S] = F.x * ar; Fo[2 * S] = F.y * ar; Fo[3 * S] = F.e * ar;
 }
 
+// Boundary-face fluxes (src/fv.cc:1100-1188): one (face vertex, sample) per
+// thread.  Far field: the interior flux against the boundary state, first
+// order (the reference passes zero gradients); otherwise inviscid_bflux.
+template <int FLUX, int ST, int BS>
+__global__ void __launch_bounds__(BS) kb_bflux(Batch B, BParams k, int r) {
+  const long long w = (blockIdx.x * (long long)blockDim.x + threadIdx.x) >> 5;
+  const Item it = item_of<ST, IT_BSLOT>(B, w, threadIdx.x & 31);
+  if (!it.ok) return;
+  const Level& L = B.lev[it.l];
+  const int t = it.v, s = it.s;
+  if (!L.c.active[s]) return;
+  constexpr bool kA = (FLUX == FLUX_TECNO_ROE);
+  const int S = L.P;   // row pitch
+  const int d = t >> 1, q = t & 1;
+  const int c = q ? L.m.b_v1[d] : L.m.b_v0[d];
+  const float* Q = L.Q[r] + rows(c, kQ, S) + s;
+  FPrim s0 = fprim(k, Q, S), s1 = s0;
+  const float nx = L.m.b_nx[d], ny = L.m.b_ny[d];
+  const int kind = L.m.b_kind[d];
+  fbc_apply2(kind, L.m.b_adiab[d], L.bval + rows(d, 10, S) + 5 * q * S + s, S, nx, ny, s0, s1);
+  FFlx F;
+  if (kind == BC_FARFIELD) {
+    // the far-field condition leaves the interior state as stored
+    const float ar = sqrtf(nx * nx + ny * ny), ia = 1.0f / ar;
+    const FRec A = frec(k, Q[0], Q[S], Q[2 * S], Q[3 * S], Q[4 * S], kA);
+    const FRec G = frec_prim(k, s1, kA);
+    float z[kG];
+#pragma unroll
+    for (int i = 0; i < kG; ++i) z[i] = 0.0f;
+    F = fflux<FLUX, RECON_FIRST>(k, A, G, nx * ia, ny * ia, 0.0f, 0.0f, z, z);
+    F.m *= ar; F.x *= ar; F.y *= ar; F.e *= ar;
+  } else {
+    F = finviscid_bflux(k, s0, s1, nx, ny);
+  }
+  float* Fo = L.Fb + rows(t, 4, S) + s;
+  Fo[0] = F.m; Fo[S] = F.x; Fo[2 * S] = F.y; Fo[3 * S] = F.e;
+}
+
+// Viscous units (src/fv.cc:1197-1320): per cell, the P1 gradient of the
+// entropy variables with boundary corrections in face order, the mean entropy
+// state (interior cells: the three vertices; boundary cells: the boundary
+// states of the cell's boundary-face vertices), and the viscous flux through
+// each vertex's P1 normal; a boundary unit adds the face's viscous flux with
+// the adiabatic heat-flux correction.  One (unit, sample) per thread.
+template <int ST, int BS>
+__global__ void __launch_bounds__(BS) kb_viscous(Batch B, BParams k, int r) {
+  const long long w = (blockIdx.x * (long long)blockDim.x + threadIdx.x) >> 5;
+  const Item it = item_of<ST, IT_UNIT>(B, w, threadIdx.x & 31);
+  if (!it.ok) return;
+  const Level& L = B.lev[it.l];
+  const int u = it.v, s = it.s;
+  if (!L.c.active[s]) return;
+  const int S = L.P;   // row pitch
+  const float* Q = L.Q[r] + s;
+  const int c = L.m.u_cell[u];
+  const int cv[3] = {L.m.c_v[3 * c], L.m.c_v[3 * c + 1], L.m.c_v[3 * c + 2]};
+  const float* n = L.m.c_n + 6 * (size_t)c;
+  float wv[3][4];
+#pragma unroll
+  for (int i = 0; i < 3; ++i) {
+    const float* q = Q + rows(cv[i], kQ, S);
+    const float V5 = q[4 * S];
+    wv[i][0] = q[3 * S]; wv[i][1] = -V5 * q[0]; wv[i][2] = -V5 * q[S]; wv[i][3] = V5;
+  }
+  float dE[kG];
+#pragma unroll
+  for (int i = 0; i < 4; ++i) {
+    dE[2 * i] = n[0] * wv[0][i] + n[2] * wv[1][i] + n[4] * wv[2][i];
+    dE[2 * i + 1] = n[1] * wv[0][i] + n[3] * wv[1][i] + n[5] * wv[2][i];
+  }
+  for (int j = L.m.c_bf_off[c]; j < L.m.c_bf_off[c + 1]; ++j) {
+    const int d = L.m.c_bf[j];
+    const int kind = L.m.b_kind[d], ad = L.m.b_adiab[d];
+    const float nx = L.m.b_nx[d], ny = L.m.b_ny[d];
+    const float* val = L.bval + rows(d, 10, S) + s;
+    const float* q0 = Q + rows(L.m.b_v0[d], kQ, S);
+    const float* q1 = Q + rows(L.m.b_v1[d], kQ, S);
+    const FEnt e0 = fbc_ent(k, kind, ad, val, S, nx, ny, q0);
+    const FEnt e1 = fbc_ent(k, kind, ad, val + 5 * S, S, nx, ny, q1);
+    const float dW[4] = {(e0.f + e1.f - q0[3 * S] - q1[3 * S]) * 0.5f,
+                         (e0.vx + e1.vx - (-q0[4 * S] * q0[0]) - (-q1[4 * S] * q1[0])) * 0.5f,
+                         (e0.vy + e1.vy - (-q0[4 * S] * q0[S]) - (-q1[4 * S] * q1[S])) * 0.5f,
+                         (e0.l + e1.l - q0[4 * S] - q1[4 * S]) * 0.5f};
+#pragma unroll
+    for (int i = 0; i < 4; ++i) {
+      dE[2 * i] += nx * dW[i];
+      dE[2 * i + 1] += ny * dW[i];
+    }
+  }
+  const float f = L.m.c_inv2a[c];
+#pragma unroll
+  for (int i = 0; i < kG; ++i) dE[i] *= f;
+  FEnt avg;
+  if (u < L.m.nic) {
+    const float t3 = 1.0f / 3.0f;
+    avg.f = wv[0][0] * t3 + wv[1][0] * t3 + wv[2][0] * t3;
+    avg.vx = wv[0][1] * t3 + wv[1][1] * t3 + wv[2][1] * t3;
+    avg.vy = wv[0][2] * t3 + wv[1][2] * t3 + wv[2][2] * t3;
+    avg.l = wv[0][3] * t3 + wv[1][3] * t3 + wv[2][3] * t3;
+  } else {
+    avg.f = avg.vx = avg.vy = avg.l = 0.0f;
+    const int cnt = L.m.c_nbr_off[c + 1] - L.m.c_nbr_off[c];
+    for (int j = L.m.c_nbr_off[c]; j < L.m.c_nbr_off[c + 1]; ++j) {
+      const int d = L.m.c_nbr[j];
+#pragma unroll
+      for (int q = 0; q < 2; ++q) {
+        const int vb = q ? L.m.bf_v1[d] : L.m.bf_v0[d];
+        const float* val = L.bval + rows(d, 10, S) + (vb == L.m.b_v0[d] ? 0 : 5) * S + s;
+        const FEnt e = fbc_ent(k, L.m.b_kind[d], L.m.b_adiab[d], val, S, L.m.bf_nx[d], L.m.bf_ny[d],
+                               Q + rows(vb, kQ, S));
+        avg.f += e.f; avg.vx += e.vx; avg.vy += e.vy; avg.l += e.l;
+      }
+    }
+    const float sc = 0.5f / (float)cnt;
+    avg.f *= sc; avg.vx *= sc; avg.vy *= sc; avg.l *= sc;
+  }
+  const FViscK K = fviscous_K(k, L.mu[s], avg, dE);
+  float* Fo = L.Fv + rows(u, 9, S) + s;
+#pragma unroll
+  for (int q = 0; q < 3; ++q) fviscous_apply(K, n[2 * q], n[2 * q + 1], Fo[(3 * q) * S], Fo[(3 * q + 1) * S], Fo[(3 * q + 2) * S]);
+  if (u >= L.m.nic) {
+    const int d = u - L.m.nic;
+    const float nbx = L.m.b_nx[d], nby = L.m.b_ny[d];
+    const float cor = L.m.b_adiab[d] ? -(K.c2 * K.e4 * K.e4 * (dE[6] * nbx + dE[7] * nby)) : 0.0f;
+    float fx, fy, fe;
+    fviscous_apply(K, nbx, nby, fx, fy, fe);
+    float* Fb = L.Fvb + rows(d, 3, S) + s;
+    Fb[0] = fx; Fb[S] = fy; Fb[2 * S] = fe - cor;
+  }
+}
+
 // Residual gather in the fixed per-vertex edge order and the SSP-RK3 stage
 // update (src/fv.cc:1635-1658), state r -> state (r+1) % 3.  Held or finished
 // samples copy their state through.
-template <int ST, int BS>
+template <int ST, int BS, bool BND>
 __global__ void __launch_bounds__(BS) kb_gather_update(Batch B, BParams k, int r) {
   const long long w = (blockIdx.x * (long long)blockDim.x + threadIdx.x) >> 5;
   const Item it = item_of<ST>(B, w, threadIdx.x & 31);
@@ -438,6 +804,22 @@ __global__ void __launch_bounds__(BS) kb_gather_update(Batch B, BParams k, int r
     const float* Fe = L.F + rows(ent >> 1, 4, S) + s;
     const float sg = (ent & 1) ? -1.0f : 1.0f;
     r0 += Fe[0] * sg; r1 += Fe[S] * sg; r2 += Fe[2 * S] * sg; r3 += Fe[3 * S] * sg;
+  }
+  if (BND) {   // boundary and viscous contributions in list order (src/fv.cc:1100-1188, 1197-1320)
+    for (int j = L.m.cb_off[v]; j < L.m.cb_off[v + 1]; ++j) {
+      const int ent = L.m.cb_ent[j];
+      const int type = ent & 3, idx = ent >> 2;
+      if (type == 0) {
+        const float* Fe = L.Fb + rows(idx, 4, S) + s;
+        r0 += Fe[0] * 0.5f; r1 += Fe[S] * 0.5f; r2 += Fe[2 * S] * 0.5f; r3 += Fe[3 * S] * 0.5f;
+      } else if (type == 2 && k.model == 1) {
+        const float* Fe = L.Fv + rows(idx, 3, S) + s;
+        r1 += Fe[0] * -0.5f; r2 += Fe[S] * -0.5f; r3 += Fe[2 * S] * -0.5f;
+      } else if (type == 3 && k.model == 1) {
+        const float* Fe = L.Fvb + rows(idx, 3, S) + s;
+        r1 += Fe[0] * 0.5f; r2 += Fe[S] * 0.5f; r3 += Fe[2 * S] * 0.5f;
+      }
+    }
   }
   const float u0 = Q[0], v0 = Q[S], p0 = Q[2 * S], V50 = Q[4 * S];
   const float rho0 = -V50 * p0;
@@ -503,6 +885,87 @@ __global__ void kb_ic_kh(Level L, BParams k, const double* __restrict__ rnd, int
   q[2 * L.P] = (float)p;
   q[3 * L.P] = (float)V1;
   q[4 * L.P] = (float)(-2.0 * beta);
+}
+
+// A uniform initial state per sample: rec[c * S + s] holds u, v, p, V1, V5 of sample s.
+__global__ void kb_ic_uniform(Level L, const float* __restrict__ rec) {
+  const long long t = blockIdx.x * (long long)blockDim.x + threadIdx.x;
+  if (t >= (long long)L.m.nv * L.S) return;
+  const int v = (int)(t / L.S), s = (int)(t % L.S);
+  float* q = L.Q[0] + rows(v, kQ, L.P) + s;
+#pragma unroll
+  for (int c = 0; c < kQ; ++c) q[c * L.P] = rec[c * L.S + s];
+}
+
+// compute_forces (src/force.cc:116-219) of every sample of a level at its
+// current state: pressure and (Navier-Stokes) viscous force on the faces of
+// each force definition.  Face records (d, dq, k0, k1) as the single-solve
+// tg_forces builds them (the condition of bface[f] applied, f the force
+// index).  Block (force, group of 32 samples), one sample per lane, warps
+// striding the faces; FP64 sums in a fixed order; out[(s nf + f) 4 + c].
+// Needs the vertex gradients G of the current state.
+template <int VT>
+__global__ void __launch_bounds__(32 * VT) kb_forces(Level L, BParams k, const int4* __restrict__ faces,
+                                                     const int* __restrict__ off, int nf, double* __restrict__ out) {
+  const int lane = threadIdx.x & 31, vg = threadIdx.x >> 5;
+  const int f = blockIdx.x % nf, s = (blockIdx.x / nf) * 32 + lane;
+  const int S = L.P;   // row pitch
+  const float* Q = L.Q[0] + s;
+  double acc[4] = {0.0, 0.0, 0.0, 0.0};
+  for (int j = off[f] + vg; j < off[f + 1]; j += VT) {
+    const int4 rr = faces[j];
+    const int d = rr.x, dq = rr.y;
+    const int v0 = L.m.b_v0[d], v1 = L.m.b_v1[d];
+    const float nx = L.m.b_nx[d], ny = L.m.b_ny[d];
+    const float* q0 = Q + rows(v0, kQ, S);
+    const float* q1 = Q + rows(v1, kQ, S);
+    FPrim s0 = fprim(k, q0, S), s1 = fprim(k, q1, S);
+    FEnt e0{q0[3 * S], -q0[4 * S] * q0[0], -q0[4 * S] * q0[S], q0[4 * S]};
+    FEnt e1{q1[3 * S], -q1[4 * S] * q1[0], -q1[4 * S] * q1[S], q1[4 * S]};
+    if (dq >= 0) {
+      const int kind = L.m.b_kind[dq], ad = L.m.b_adiab[dq];
+      const float qx = L.m.b_nx[dq], qy = L.m.b_ny[dq];
+      const float* val0 = L.bval + rows(dq, 10, S) + 5 * rr.z * S + s;
+      const float* val1 = L.bval + rows(dq, 10, S) + 5 * rr.w * S + s;
+      fbc_apply1(kind, ad, val0, S, qx, qy, s0);
+      fbc_apply1(kind, ad, val1, S, qx, qy, s1);
+      e0 = fbc_ent(k, kind, ad, val0, S, qx, qy, q0);
+      e1 = fbc_ent(k, kind, ad, val1, S, qx, qy, q1);
+    }
+    const double pr = 0.5 * ((double)s0.p + (double)s1.p);
+    acc[0] += nx * pr;
+    acc[1] += ny * pr;
+    if (k.model == 1) {
+      const float mu = L.mu[s];
+      const float f0 = 1.0f / e0.l, f1 = 1.0f / e1.l;
+      const float* G0 = L.G + rows(v0, kG, S) + s;
+      const float* G1 = L.G + rows(v1, kG, S) + s;
+      // u = -V2 / V5: grad u = -grad V2 / V5 + V2 grad V5 / V5^2 (src/force.cc:169-179)
+      const float ux0 = G0[2 * S] * -f0 + G0[6 * S] * (f0 * e0.vx * f0), uy0 = G0[3 * S] * -f0 + G0[7 * S] * (f0 * e0.vx * f0);
+      const float ux1 = G1[2 * S] * -f1 + G1[6 * S] * (f1 * e1.vx * f1), uy1 = G1[3 * S] * -f1 + G1[7 * S] * (f1 * e1.vx * f1);
+      const float vx0 = G0[4 * S] * -f0 + G0[6 * S] * (f0 * e0.vy * f0), vy0 = G0[5 * S] * -f0 + G0[7 * S] * (f0 * e0.vy * f0);
+      const float vx1 = G1[4 * S] * -f1 + G1[6 * S] * (f1 * e1.vy * f1), vy1 = G1[5 * S] * -f1 + G1[7 * S] * (f1 * e1.vy * f1);
+      const float gux = ux0 * 0.5f + ux1 * 0.5f, guy = uy0 * 0.5f + uy1 * 0.5f;
+      const float gvx = vx0 * 0.5f + vx1 * 0.5f, gvy = vy0 * 0.5f + vy1 * 0.5f;
+      const float div = gux + gvy;
+      const float sxx = 2.0f * mu * (gux - (1.0f / 3.0f) * div);
+      const float syy = 2.0f * mu * (gvy - (1.0f / 3.0f) * div);
+      const float sxy = mu * (guy + gvx);
+      acc[2] += -(double)(sxx * nx + sxy * ny);
+      acc[3] += -(double)(sxy * nx + syy * ny);
+    }
+  }
+  __shared__ double red[4][VT][32];
+#pragma unroll
+  for (int c = 0; c < 4; ++c) red[c][vg][lane] = acc[c];
+  __syncthreads();
+  if (vg == 0) {
+    for (int i = 1; i < VT; ++i)
+#pragma unroll
+      for (int c = 0; c < 4; ++c) acc[c] += red[c][i][lane];
+#pragma unroll
+    for (int c = 0; c < 4; ++c) out[((size_t)s * nf + f) * 4 + c] = acc[c];
+  }
 }
 
 // Ensemble moments of one level at its current state, FP64: Welford mean and

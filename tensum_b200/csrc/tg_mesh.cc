@@ -422,4 +422,35 @@ std::string build_tiles(HostLayout& L, int max_owned, int max_local, int max_edg
   return "";
 }
 
+std::string force_faces(const HostLayout& L, int n_forces, const int* n_tags, const int* tags, std::vector<int>& rec4,
+                        std::vector<int>& off) {
+  const int nbf = (int)L.rb_type.size();
+  rec4.clear();
+  off.assign(1, 0);
+  const int* t = tags;
+  for (int f = 0; f < n_forces; ++f) {
+    if (n_tags[f] < 1) return "a force needs at least one face tag (src/parameter.cc:652)";
+    // the condition the reference applies on every face of force f is that of bface[f] (src/force.cc:144-150)
+    int dq = -1, k0 = 0, k1 = 0;
+    for (int b = 0; b < nbf; ++b) {
+      bool mine = false;
+      for (int q = 0; q < n_tags[f]; ++q) mine = mine || L.rb_type[b] == t[q];
+      if (!mine) continue;
+      if (L.rb_dev[b] < 0) return "force faces must not be periodic";
+      if (f < nbf) {
+        dq = L.rb_dev[f];
+        const int dv0 = L.b_v0[L.rb_dev[b]], dv1 = L.b_v1[L.rb_dev[b]];
+        const int q0 = L.new_of_old[L.rb_v0[f]];
+        k0 = (q0 == dv0) ? 0 : 1;   // value slot: vertex 0 of bface[f] or not (src/bc.h:568-654 via the table)
+        k1 = (q0 == dv1) ? 0 : 1;
+      }
+      rec4.insert(rec4.end(), {L.rb_dev[b], dq, k0, k1});
+    }
+    if ((int)rec4.size() / 4 == off.back()) return "a force tag matches no boundary face";
+    off.push_back((int)rec4.size() / 4);
+    t += n_tags[f];
+  }
+  return "";
+}
+
 }  // namespace tg

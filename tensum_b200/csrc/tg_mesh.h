@@ -80,4 +80,12 @@ std::string build_layout(const tg_mesh& m, const tg_bc_table* bc, bool need_visc
 // vertices, max_local local vertices and max_edges edges each.
 std::string build_tiles(HostLayout& L, int max_owned, int max_local, int max_edges);
 
+// Face records of compute_forces (src/force.cc:116-219) for n_forces force
+// definitions (n_tags[f] face tags each, consecutive in `tags`): per face 4 ints
+// (device face index, the device index of bface[f] whose condition the
+// reference applies on every face of force f or -1, and the value slots that
+// condition uses at the face's two vertices); off[f] .. off[f+1] index force f.
+std::string force_faces(const HostLayout& L, int n_forces, const int* n_tags, const int* tags, std::vector<int>& rec4,
+                        std::vector<int>& off);
+
 }  // namespace tg

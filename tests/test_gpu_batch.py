@@ -144,9 +144,10 @@ def test_rejects_unsupported_setups():
     m, P = _problem(17)
     with pytest.raises(gpu.TensumError):
         batch.Batch([(P, 48)])                         # not a multiple of 32
-    m2 = cases.cylinder_mesh(6, 12, 0)
-    cfg = dict(flux="kepes_tecno_roe", reconstruct="minmod", final_time=1.0, time_stamps=1,
-               boundary={1: ("slip", {}), 2: ("outlet", {})})
-    P2 = abi.Problem(preproc.preprocess(m2), cfg)
+    m2, P2 = _problem(17, flux=("kep", "first"))
     with pytest.raises(gpu.TensumError):
-        batch.Batch([(P2, 32)])                        # not periodic
+        batch.Batch([(P2, 32)])                        # flux without a batched kernel
+    b = batch.Batch([(P, 32)])
+    with pytest.raises(gpu.TensumError) as e:
+        b.set_parameters(0, mu_ref=np.zeros(32))       # periodic Euler: nothing per sample
+    assert abi.STATUS[e.value.status] == "TG_NOT_SUPPORTED"
