@@ -25,7 +25,17 @@ Keys beyond the base contract:
 
     python bench.py --workload mc [--samples S] [--n 257] [--steps K]
 
-measures the Monte Carlo configuration instead: S Kelvin-Helmholtz samples
+    python bench.py --workload cylinder [--samples S] [--final-time T] [--outputs K] [--t-start T0]
+
+measures the surrogate control-variate configuration on the Navier-Stokes
+cylinder (128 x 256 O-mesh; Mach ~ U[0.15, 0.25], Re ~ U[80, 120], angle ~
+U[-2, 2] degrees): S batched FP32 solves to time T with the wall force at K
+output times, FP64 solves of a subset (several handles at once), a surrogate
+trained on the first --train solves, and the time to a 1 % relative standard
+error of the mean and of the variance of each QoI for plain FP64 MC, batched
+FP32 MC and batched FP32 with the control variate.
+
+--workload mc measures the Monte Carlo configuration instead: S Kelvin-Helmholtz samples
 (rnd rows, device-generated initial states) on an n x n mesh advanced together
 by the batched FP32 engine (KEPES-TeCNO-Rusanov, minmod), against the FP64
 per-sample path on the same GPU, with the QoI error of the FP32 members
@@ -68,8 +78,14 @@ def parse():
     ap.add_argument("--seed", type=int, default=0)
     ap.add_argument("--e2e-steps", type=int, default=10)
     ap.add_argument("--no-cpu-baseline", action="store_true")
-    ap.add_argument("--workload", default="single", choices=["single", "mc"])
-    ap.add_argument("--samples", type=int, default=4096, help="ensemble size of --workload mc")
+    ap.add_argument("--workload", default="single", choices=["single", "mc", "cylinder"])
+    ap.add_argument("--samples", type=int, default=None,
+                    help="ensemble size (--workload mc: 4096, --workload cylinder: 1024)")
+    ap.add_argument("--final-time", type=float, default=2.0, help="cylinder: run length of every sample")
+    ap.add_argument("--outputs", type=int, default=40, help="cylinder: force outputs over the run")
+    ap.add_argument("--t-start", type=float, default=1.0, help="cylinder: start of the QoI window")
+    ap.add_argument("--fp64-samples", type=int, default=32, help="cylinder: samples also run in FP64")
+    ap.add_argument("--train", type=int, default=256, help="cylinder: solver runs the surrogate is trained on")
     ap.add_argument("--no-mc", action="store_true", help="skip the Monte Carlo object of the default line")
     a = ap.parse_args()
     a.flux_list = [(f, r) for f, r in FLUXES if f in a.fluxes.split(",")]
@@ -501,7 +517,98 @@ def mc_line(n, S, K, W, seed):
 
 def run_mc(args):
     n = args.n if args.n != 1025 else 257
-    print(json.dumps(mc_line(n, args.samples, args.steps, max(3, args.warmup), args.seed)))
+    print(json.dumps(mc_line(n, args.samples or 4096, args.steps, max(3, args.warmup), args.seed)))
+    return 0
+
+
+def cylinder_line(S, T, n_out, t_start, n_fp64, n_train, K, seed, n_r=128, n_t=256):
+    """Surrogate control-variate MC on the Navier-Stokes cylinder (one GPU): the JSON object."""
+    import torch
+    from tensum_b200 import cases, cv, cylinder, mlp, preproc
+    torch.cuda.set_device(0)
+    m = cases.cylinder_mesh(n_r, n_t, seed)
+    V = m.n_vertex
+    g = preproc.preprocess(m)
+    X = cylinder.draw_inputs(S, seed)
+    with ClockSampler(0) as clk:
+        rb = cylinder.run_batched(g, m.coords, X, T, n_out, t_start, time_steps=K)
+    y = rb["y"]
+    r64 = cylinder.run_fp64(g, m.coords, X[:n_fp64], T, n_out, t_start)
+    y64 = r64["y"]
+    steps_per_sample = float(np.mean(r64["steps"]))
+    t_b = rb["wall_s"] / S
+    t_64 = r64["wall_s"] / n_fp64
+    err = np.abs(y[:n_fp64] - y64) / np.maximum(np.abs(y64), 1e-300)
+    mean_err = np.abs(y[:n_fp64].mean(0) - y64.mean(0)) / np.abs(y64.mean(0))
+    std_err = np.abs(y[:n_fp64].std(0, ddof=1) - y64.std(0, ddof=1)) / y64.std(0, ddof=1)
+
+    net = mlp.MLP(3, 3, seed=1)
+    torch.cuda.synchronize()
+    t0 = time.perf_counter()
+    net.fit(X[:n_train], y[:n_train], epochs=400, batch=64, lr=2e-3)
+    t_train = time.perf_counter() - t0
+    x_extra = cylinder.draw_inputs(1 << 20, 10 ** 7 + seed)
+    t0 = time.perf_counter()
+    g_extra = net.predict(x_extra, precision=1)
+    t_surr = time.perf_counter() - t0
+    g_ev = net.predict(X[n_train:], precision=1)
+    est = cv.estimate(y[n_train:], g_ev, g_extra)
+    ttr = {}
+    for rse in (0.01,):
+        n_plain_mean = cv.samples_for_rse(y[n_train:], None, rse)
+        n_cv_mean = cv.samples_for_rse(y[n_train:], g_ev, rse)
+        n_plain_var = cv.samples_for_rse_var(y[n_train:], None, rse)
+        n_cv_var = cv.samples_for_rse_var(y[n_train:], g_ev, rse)
+        n_plain = float(max(n_plain_mean.max(), n_plain_var.max()))
+        n_cv = float(max(n_cv_mean.max(), n_cv_var.max()))
+        t = {"plain_fp64_mc_s": n_plain * t_64, "batched_fp32_mc_s": n_plain * t_b,
+             "batched_fp32_cv_s": (n_train + n_cv) * t_b + t_train + t_surr}
+        ttr[f"rse_{rse:g}"] = dict(
+            t, samples_plain=n_plain, samples_cv=n_cv,
+            samples_by_qoi={"plain_mean": n_plain_mean.tolist(), "cv_mean": n_cv_mean.tolist(),
+                            "plain_var": n_plain_var.tolist(), "cv_var": n_cv_var.tolist()},
+            speedup_batched_vs_plain_fp64=t["plain_fp64_mc_s"] / t["batched_fp32_mc_s"],
+            speedup_cv_vs_plain_fp64=t["plain_fp64_mc_s"] / t["batched_fp32_cv_s"])
+    value = V * 3 * S * steps_per_sample / rb["wall_s"]
+    line = {"metric": "time to 1% RSE of the QoI mean and variance vs plain FP64 MC (cylinder, surrogate control variate)",
+            "value": value, "unit": "vertex-sample-stage updates/s", "n_gpus": 1, "steps": rb["steps"], "warmup": 0,
+            "ms_per_step": rb["ms_per_step"], "higher_is_better": True, "scaling": "weak", "vs_baseline": None,
+            "dtype": "f32 members, f64 geometry / log-mean series / forces / moments",
+            "data": "synthetic (seeded uncertain inputs, seeded O-mesh)",
+            "config": {"workload": f"navier-stokes cylinder {n_r}x{n_t} O-mesh, {S} samples, kepes_tecno_roe(minmod), "
+                                   f"ssprk3 cfl 0.8, t = 0 .. {T}, forces at {n_out} outputs, QoI window t >= {t_start}",
+                       "mesh_vertices": V, "samples": S, "final_time": T, "outputs": n_out, "t_start": t_start,
+                       "inputs": "mach U[0.15,0.25], re U[80,120], angle U[-2,2] deg",
+                       "l2": "working set > L2 (no flush needed)"},
+            "qoi": {"names": list(cylinder.NAMES), "fp64_subset": n_fp64,
+                    "fp32_vs_fp64_rel_err_max": err.max(0).tolist(), "fp32_vs_fp64_rel_err_mean": err.mean(0).tolist(),
+                    "subset_mean_rel_err": mean_err.tolist(), "subset_std_rel_err": std_err.tolist(),
+                    "ensemble_mean": y.mean(0).tolist(), "ensemble_std": y.std(0, ddof=1).tolist(),
+                    "strouhal": "no shedding cycle fits the window (shedding needs t of order 100)"},
+            "time_to_rse": dict(ttr, n_train=n_train, train_s=t_train, surrogate_evals=1 << 20,
+                                surrogate_eval_s=t_surr, fp64_sample_s=t_64, fp64_streams=r64["streams"],
+                                batched_sample_s=t_b,
+                                note="sample counts from the ensemble's variance and the control-variate residual "
+                                     "variance (mean and variance targets of all three QoIs); FP64 per-sample time "
+                                     "measured on the FP64 subset run as concurrent handles"),
+            "cv": {"gain": [float(x) for x in est["gain"]], "used": [bool(x) for x in est["used"]],
+                   "mean": est["mean"].tolist(), "plain_mean": est["plain_mean"].tolist(),
+                   "var": est["var"].tolist(), "plain_var": est["plain_var"].tolist(),
+                   "se_mean": est["se_mean"].tolist()},
+            "batched": {"wall_s": rb["wall_s"], "steps_issued": rb["steps"], "bad_samples": rb["bad"],
+                        "shape": rb["shape"], "device_value": V * 3 * S / (rb["ms_per_step"] / 1e3)},
+            "fp64": {"wall_s": r64["wall_s"], "steps_per_sample": steps_per_sample},
+            "gpu_launches": rb["kernels_per_step"] * rb["steps"], "clocks": clk.summary(), "impl": "ours",
+            "roofline": None,
+            "e2e": {"value": value, "unit": "vertex-sample-stage updates/s", "h2d_bytes_per_step": 0,
+                    "d2h_bytes_per_step": 0,
+                    "path": "tg_batch_advance + tg_batch_forces at every output time, wall clock"}}
+    return line
+
+
+def run_cylinder(args):
+    print(json.dumps(cylinder_line(args.samples or 1024, args.final_time, args.outputs, args.t_start, args.fp64_samples,
+                                   args.train, max(5, min(args.steps, 50)), args.seed)))
     return 0
 
 
@@ -513,6 +620,12 @@ def main():
                               "groups run one sample after another (see the single-solve reference arm)"}))
             return 0
         return run_mc(args)
+    if args.workload == "cylinder":
+        if args.impl == "reference":
+            print(json.dumps({"impl": "reference", "unavailable": "the reference has no batched ensemble path; its MC "
+                              "groups run one sample after another (see the single-solve reference arm)"}))
+            return 0
+        return run_cylinder(args)
     if args.impl == "reference":
         return run_reference(args)
     return run_ours(args)

@@ -80,3 +80,23 @@ def samples_for_rse(y, g=None, rse: float = 0.01) -> np.ndarray:
         _, _, _, _, beta = _cv(y, g, g)
         v = (y - beta * g).var(0, ddof=1)
     return np.ceil(v / (rse * mu) ** 2)
+
+
+def samples_for_rse_var(y, g=None, rse: float = 0.01) -> np.ndarray:
+    """Expensive samples needed for a relative standard error `rse` of the
+    variance estimate: Var((Y - E Y)^2) / (rse Var Y)^2 for plain MC; with the
+    surrogate, the squared deviations get (g - E g)^2 as their control
+    (unlimited surrogate budget), Var(Z - beta G) / (rse Var Y)^2."""
+    y = np.asarray(y, np.float64)
+    if y.ndim == 1:
+        y = y[:, None]
+    z = (y - y.mean(0)) ** 2
+    target = (rse * y.var(0, ddof=1)) ** 2
+    if g is None:
+        return np.ceil(z.var(0, ddof=1) / target)
+    g = np.asarray(g, np.float64)
+    if g.ndim == 1:
+        g = g[:, None]
+    gz = (g - g.mean(0)) ** 2
+    _, _, _, _, beta = _cv(z, gz, gz)
+    return np.ceil((z - beta * gz).var(0, ddof=1) / target)

@@ -49,3 +49,15 @@ def test_variance_estimate_and_sample_counts():
     n_mc = cv.samples_for_rse(y, None, 0.01)
     n_cv = cv.samples_for_rse(y, g, 0.01)
     assert np.all(n_cv < n_mc)
+
+
+def test_variance_sample_counts():
+    """Gaussian Y: Var((Y - mu)^2) = 2 sigma^4, so plain MC needs 2 / rse^2 samples
+    for the variance; a close surrogate needs far fewer."""
+    rng = np.random.default_rng(3)
+    x = rng.normal(size=200000)
+    y = 2.0 + 0.3 * x
+    n = cv.samples_for_rse_var(y, None, 0.01)[0]
+    assert abs(n / 20000.0 - 1.0) < 0.03
+    g = 2.0 + 0.3 * x + 0.01 * rng.normal(size=x.size)
+    assert cv.samples_for_rse_var(y, g, 0.01)[0] < n / 50
