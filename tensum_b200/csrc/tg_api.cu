@@ -193,7 +193,7 @@ size_t flux_smem(int flux, int recon, int lmax, int emax, int cmax) {
   }
 }
 
-typedef void (*TileGradKernel)(Params, MeshView, TileView, StateView, Scalars*, int, int, const int*);
+typedef void (*TileGradKernel)(Params, MeshView, TileView, StateView, Scalars*, int, int, const int*, int);
 TileGradKernel grad_kernel(bool first, bool grad) {
   if (first) return grad ? k_tile_grad<true, true> : k_tile_grad<true, false>;
   return k_tile_grad<false, true>;
@@ -213,10 +213,15 @@ StateView view(const tg_handle* h, int b) {
 
 // ---- phases (all enqueue on h->stream; `done` gates work inside graphs)
 // Gradients (when `grad`), plus at the first stage dt and U_old.
+// At a step's first stage with fuse_dt, the first-stage kernel runs when dt and
+// U_old are still to be formed, else a gradient-only launch (warm) takes its place.
 void enqueue_gradient(tg_handle* h, int b, bool first, bool grad, const int* done) {
   if (!first && !grad) return;
   grad_kernel(first, grad)<<<h->L.ntiles, kTileThreads, first ? h->smem_grad1 : h->smem_grad0, h->stream>>>(
-      h->prm, h->mv, h->tv, view(h, b), h->sc, h->L.lmax, h->L.emax, done);
+      h->prm, h->mv, h->tv, view(h, b), h->sc, h->L.lmax, h->L.emax, done, 0);
+  if (first && grad && h->prm.fuse_dt)
+    grad_kernel(false, true)<<<h->L.ntiles, kTileThreads, h->smem_grad0, h->stream>>>(
+        h->prm, h->mv, h->tv, view(h, b), h->sc, h->L.lmax, h->L.emax, done, 1);
 }
 
 // boundary-face and viscous contributions, gathered by the tiled flux kernel
@@ -292,6 +297,9 @@ void enqueue_step(tg_handle* h) {
   }
   k_step_end<<<1, 1, 0, h->stream>>>(h->ctl, h->sc, h->done);
 }
+
+// The state changed outside a captured step: the next step forms dt and U_old itself.
+void clear_dt_next(tg_handle* h) { cudaMemsetAsync(&h->sc->dt_next, 0, sizeof(int), h->stream); }
 
 tg_status sync(tg_handle* h) {
   TG_CUDA(h, cudaGetLastError());
@@ -491,6 +499,8 @@ tg_status tg_create(const tg_mesh* mesh, const tg_material* mat, const tg_bc_tab
   k.nd = mat->nd_active; k.visc = mat->visc_active; k.heat = mat->heat_active;
   k.liou = (opt->liou_fix && mat->flux_scheme == FLUX_TECNO_ROE) ? 1 : 0;
   k.strong = opt->bc_strong ? 1 : 0;
+  // strong conditions change the state after the last update; a fixed time step needs no dt
+  k.fuse_dt = (!k.strong && opt->time_step <= 0.0) ? 1 : 0;
 
   tg_status st;
 #define UP(vec, field) \
@@ -592,10 +602,11 @@ tg_status tg_create(const tg_mesh* mesh, const tg_material* mat, const tg_bc_tab
   c.min_residue = opt->min_residue; c.max_iter = opt->max_iter; c.final_time = opt->final_time; c.tinst = tip;
 
   h->kernels_per_flux = residual_kernels(h);
-  // step_begin + gradient/dt passes + per stage (boundary, viscous, tiled flux) + [store_old] + dt_final
-  // + norm_final + step_end
-  h->kernels_per_step = 1 + (1 + (h->grads_needed ? c.n_rks - 1 : 0)) + (k.liou ? 1 : 0) + (k.strong && h->mv.nsb > 0 ? c.n_rks : 0) + c.n_rks * residual_kernels(h) + (c.time_step > 0.0 ? 1 : 0) +
-                        1 + 1 + 1;
+  // step_begin + gradient/dt passes (+ the first stage's warm gradient launch) + per stage
+  // (boundary, viscous, tiled flux) + [store_old] + dt_final + norm_final + step_end
+  h->kernels_per_step = 1 + (1 + (h->grads_needed ? c.n_rks - 1 : 0)) + (h->grads_needed && k.fuse_dt ? 1 : 0) +
+                        (k.liou ? 1 : 0) + (k.strong && h->mv.nsb > 0 ? c.n_rks : 0) + c.n_rks * residual_kernels(h) +
+                        (c.time_step > 0.0 ? 1 : 0) + 1 + 1 + 1;
   if ((st = dev_alloc(h, 5 * nv, &h->raw)) != TG_OK) { tg_destroy(h); return st; }
   if ((st = dev_alloc(h, 1, &h->bad)) != TG_OK) { tg_destroy(h); return st; }
   if ((st = dev_upload(h, L.old_of_new, &h->old_of_new)) != TG_OK) { tg_destroy(h); return st; }
@@ -752,6 +763,7 @@ tg_status tg_update(tg_handle* h, int r) {
   enqueue_update(h, r, false, h->never);
   if (h->prm.strong && h->mv.nsb > 0)
     k_strong_bc<<<nblk(h->mv.nsb), kBlock, 0, h->stream>>>(h->mv, h->sv.P, h->never);
+  clear_dt_next(h);
   tg_status st = sync(h);
   if (st != TG_OK) return st;
   return check_bad(h);
@@ -876,7 +888,8 @@ tg_status tg_update_parameters(tg_handle* h, const tg_material* mat, const tg_bc
       TG_CUDA(h, cudaMemcpyAsync(const_cast<double*>(h->mv.b_val), L.b_val.data(), L.b_val.size() * sizeof(double),
                                  cudaMemcpyHostToDevice, h->stream));
   }
-  // the captured step holds the parameters by value
+  // dt depends on the material; the captured step holds the parameters by value
+  clear_dt_next(h);
   if (h->graph_exec) cudaGraphExecDestroy(h->graph_exec);
   if (h->graph) cudaGraphDestroy(h->graph);
   h->graph_exec = nullptr;

@@ -67,6 +67,11 @@ struct Scalars {
   int bad;
   unsigned long long dtmin_bits;
   int stop_counter;    // steps stop once counter exceeds it (output-time stepping)
+  // Set by a last-stage update that also formed dt, U_old and their minimum
+  // (dtmin_next) for the state it wrote; cleared whenever the state changes by
+  // any other route, so the next step's first stage then forms them itself.
+  int dt_next;
+  unsigned long long dtmin_next;
 };
 
 struct Control {
@@ -247,6 +252,14 @@ __global__ void k_viscous(Params k, MeshView m, StateView s, const int* __restri
   }
 }
 
+// |n| and the face spectral radius |u.n| + c |n| of the local time step
+// (src/fv.cc:1512-1580), with their multiply-adds written out so that every
+// kernel forming them rounds them the same way.
+__device__ __forceinline__ double face_area(double nx, double ny) { return sqrt(fma(nx, nx, ny * ny)); }
+__device__ __forceinline__ double face_radius(double u, double v, double nx, double ny, double c, double area) {
+  return fma(c, area, fabs(fma(u, nx, v * ny)));
+}
+
 __device__ __forceinline__ unsigned long long warp_min_u64(unsigned long long x) {
 #pragma unroll
   for (int o = 16; o > 0; o >>= 1) {
@@ -271,8 +284,8 @@ __global__ void k_dt(Params k, MeshView m, StateView s, Scalars* sc, const int* 
       int self = (ent & 1) ? m.e_b[e] : m.e_a[e];
       Prim q = load_prim(s.P, nv, self);
       double nx = m.e_nx[e], ny = m.e_ny[e];
-      double area = sqrt(nx * nx + ny * ny);
-      lam += (fabs(q.u * nx + q.v * ny) + sound_speed(k, q) * area) * 1.0;
+      double area = face_area(nx, ny);
+      lam += face_radius(q.u, q.v, nx, ny, sound_speed(k, q), area) * 1.0;
     }
     for (int j = m.cb_off[v]; j < m.cb_off[v + 1]; ++j) {
       int ent = m.cb_ent[j];
@@ -281,8 +294,8 @@ __global__ void k_dt(Params k, MeshView m, StateView s, Scalars* sc, const int* 
       int self = (idx & 1) ? m.b_v1[d] : m.b_v0[d];
       Prim q = load_prim(s.P, nv, self);
       double nx = m.b_nx[d], ny = m.b_ny[d];
-      double area = sqrt(nx * nx + ny * ny);
-      lam += 0.5 * (fabs(q.u * nx + q.v * ny) + sound_speed(k, q) * area);
+      double area = face_area(nx, ny);
+      lam += 0.5 * face_radius(q.u, q.v, nx, ny, sound_speed(k, q), area);
     }
     if (k.model == 1) {
       for (int j = m.ce_off[v]; j < m.ce_off[v + 1]; ++j) {
@@ -291,8 +304,8 @@ __global__ void k_dt(Params k, MeshView m, StateView s, Scalars* sc, const int* 
         int self = (ent & 1) ? m.e_b[e] : m.e_a[e];
         Prim q = load_prim(s.P, nv, self);
         double nx = m.e_nx[e], ny = m.e_ny[e];
-        double area = sqrt(nx * nx + ny * ny);
-        double dl = sqrt(m.e_dx[e] * m.e_dx[e] + m.e_dy[e] * m.e_dy[e]);
+        double area = face_area(nx, ny);
+        double dl = face_area(m.e_dx[e], m.e_dy[e]);
         lam += (viscosity(k, q.T) * area / dl / density(k, q)) * 1.0;
       }
     }
@@ -366,7 +379,9 @@ __global__ void k_step_begin(Control ctl, Scalars* sc, int* done) {
   bool go = sc->rtotal > ctl.min_residue && (ctl.time_mode == 1 || sc->iter < ctl.max_iter) &&
             sc->elapsed < ctl.final_time && sc->counter <= sc->stop_counter;
   *done = go ? 0 : 1;
-  sc->dtmin_bits = 0x7ff0000000000000ull;
+  if (!go) return;
+  sc->dtmin_bits = sc->dt_next ? sc->dtmin_next : 0x7ff0000000000000ull;
+  sc->dtmin_next = 0x7ff0000000000000ull;
 }
 
 // Global dt and the unsteady clamp to the next output time (src/fv.cc:1584-1618).
@@ -506,6 +521,8 @@ __global__ void k_norm_final(StateView s, int nblocks, int nv_total, Scalars* sc
   if (*done) return;
   __shared__ double red[4][kBlock];
   double acc[4] = {0.0, 0.0, 0.0, 0.0};
+  // unrolled so that several partials' loads are in flight before the ordered adds
+#pragma unroll 8
   for (int b = threadIdx.x; b < nblocks; b += blockDim.x)
 #pragma unroll
     for (int c = 0; c < 4; ++c) acc[c] += s.part[(size_t)b * 4 + c];

@@ -37,6 +37,7 @@ struct Params {
   int nd, visc, heat;
   int liou;       // Liou's carbuncle switch active (liou_fix with kepes_tecno_roe)
   int strong;     // bc_scheme strong
+  int fuse_dt;    // the last stage's update also forms the next step's local dt and U_old
 };
 
 struct Prim { double T, u, v, p; };
@@ -79,13 +80,16 @@ __device__ __forceinline__ double viscosity(const Params& k, double T) {   // sr
   return k.mu_ref;
 }
 
+// The energy's multiply-adds are written out so that every kernel that forms
+// U_old from a state (the first stage's pass, or the previous step's last
+// update) rounds it the same way.
 __device__ __forceinline__ Cons prim2con(const Params& k, const Prim& q) {   // src/material.h:501-513
   Cons c;
   double rho = density(k, q);
   c.r = rho;
   c.mx = q.u * rho;
   c.my = q.v * rho;
-  c.E = q.p / (k.gamma - 1.0) + 0.5 * (q.u * q.u + q.v * q.v) * rho;
+  c.E = fma(0.5 * fma(q.u, q.u, q.v * q.v), rho, q.p / (k.gamma - 1.0));
   return c;
 }
 

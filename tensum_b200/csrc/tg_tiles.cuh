@@ -106,11 +106,17 @@ __device__ __forceinline__ int list_entry(const unsigned int* sC, int j) {
 __host__ __device__ constexpr int grad_vertex_doubles(bool first) { return first ? 7 : 4; }
 __host__ __device__ constexpr int grad_edge_doubles(bool first) { return first ? 6 : 4; }
 
+// warm_only (gradient kernels at a step's first stage): runs only when the
+// previous step's last stage has already formed dt and U_old for this state,
+// the first-stage kernel (FIRST) only when it has not.
 template <bool FIRST, bool GRAD>
 __global__ void __launch_bounds__(kTileThreads, TG_GRAD_MINB) k_tile_grad(Params k, MeshView m, TileView t, StateView s,
                                                             Scalars* sc, int lmax, int emax,
-                                                            const int* __restrict__ done) {
+                                                            const int* __restrict__ done, int warm_only) {
   if (*done) return;
+  const bool warm = k.fuse_dt && sc->dt_next;
+  if ((FIRST && warm) || (warm_only && !warm)) return;
+  const bool dt_here = FIRST;
   extern __shared__ double sm[];
   const int tile = blockIdx.x;
   const int l0 = t.loff[tile], L = t.loff[tile + 1] - l0;
@@ -129,7 +135,7 @@ __global__ void __launch_bounds__(kTileThreads, TG_GRAD_MINB) k_tile_grad(Params
     if (GRAD)
 #pragma unroll
       for (int c = 0; c < 4; ++c) cp_async8(sW + c * L + i, s.W + (size_t)c * nv + g);
-    if (FIRST) {
+    if (dt_here) {
       cp_async8(sU + i, s.P + g);                              // T
       cp_async8(sU + L + i, s.P + (size_t)nv + g);             // u
       cp_async8(sU + 2 * L + i, s.P + (size_t)2 * nv + g);     // v
@@ -142,7 +148,7 @@ __global__ void __launch_bounds__(kTileThreads, TG_GRAD_MINB) k_tile_grad(Params
       cp_async8(sE + 2 * NE + le, t.g1x + e0 + le);
       cp_async8(sE + 3 * NE + le, t.g1y + e0 + le);
     }
-    if (FIRST) {
+    if (dt_here) {
       cp_async8(sE + 4 * NE + le, t.nx + e0 + le);
       cp_async8(sE + 5 * NE + le, t.ny + e0 + le);
     }
@@ -151,7 +157,7 @@ __global__ void __launch_bounds__(kTileThreads, TG_GRAD_MINB) k_tile_grad(Params
   const int cbase = stage_lists(t, vb, nown, sC, sO);
   cp_async_wait_all();
   __syncthreads();
-  if (FIRST) {
+  if (dt_here) {
     for (int i = threadIdx.x; i < L; i += blockDim.x) {
       Prim q;
       q.T = sU[i];
@@ -184,10 +190,10 @@ __global__ void __launch_bounds__(kTileThreads, TG_GRAD_MINB) k_tile_grad(Params
           acc[2 * c + 1] += gy * dW;
         }
       }
-      if (FIRST) {
+      if (dt_here) {
         double nx = sE[4 * NE + le], ny = sE[5 * NE + le];
-        double area = sqrt(nx * nx + ny * ny);
-        lam += (fabs(sU[L + self] * nx + sU[2 * L + self] * ny) + sU[self] * area) * 1.0;
+        double area = face_area(nx, ny);
+        lam += face_radius(sU[L + self], sU[2 * L + self], nx, ny, sU[self], area) * 1.0;
       }
     }
     for (int j = m.cb_off[v]; j < m.cb_off[v + 1]; ++j) {
@@ -201,13 +207,13 @@ __global__ void __launch_bounds__(kTileThreads, TG_GRAD_MINB) k_tile_grad(Params
           acc[2 * c] += m.b_nx[idx] * dW[c];
           acc[2 * c + 1] += m.b_ny[idx] * dW[c];
         }
-      } else if (FIRST && type == 0) {
+      } else if (dt_here && type == 0) {
         int d = idx >> 1;
         int selfg = (idx & 1) ? m.b_v1[d] : m.b_v0[d];
         Prim q = load_prim(s.P, nv, selfg);
         double nx = m.b_nx[d], ny = m.b_ny[d];
-        double area = sqrt(nx * nx + ny * ny);
-        lam += 0.5 * (fabs(q.u * nx + q.v * ny) + sound_speed(k, q) * area);
+        double area = face_area(nx, ny);
+        lam += 0.5 * face_radius(q.u, q.v, nx, ny, sound_speed(k, q), area);
       }
     }
     if (GRAD) {
@@ -215,7 +221,7 @@ __global__ void __launch_bounds__(kTileThreads, TG_GRAD_MINB) k_tile_grad(Params
 #pragma unroll
       for (int c = 0; c < 8; ++c) s.G[(size_t)c * nv + v] = acc[c] * f;
     }
-    if (FIRST) {
+    if (dt_here) {
       if (k.model == 1) {
         for (int j = j0; j < j1; ++j) {
           int ent = list_entry(sC, j);
@@ -226,9 +232,9 @@ __global__ void __launch_bounds__(kTileThreads, TG_GRAD_MINB) k_tile_grad(Params
           int ga = t.lv[l0 + la], gb = t.lv[l0 + lb];
           Prim q = load_prim(s.P, nv, selfg);
           double nx = sE[4 * NE + le], ny = sE[5 * NE + le];
-          double area = sqrt(nx * nx + ny * ny);
+          double area = face_area(nx, ny);
           double dx = t.x[gb] - t.x[ga], dy = t.y[gb] - t.y[ga];
-          double dl = sqrt(dx * dx + dy * dy);
+          double dl = face_area(dx, dy);
           lam += (viscosity(k, q.T) * area / dl / density(k, q)) * 1.0;
         }
       }
@@ -240,7 +246,7 @@ __global__ void __launch_bounds__(kTileThreads, TG_GRAD_MINB) k_tile_grad(Params
       s.Uold[v] = c.r; s.Uold[nv + v] = c.mx; s.Uold[2 * nv + v] = c.my; s.Uold[3 * nv + v] = c.E;
     }
   }
-  if (FIRST) {
+  if (dt_here) {
     bits = block_min_u64(bits);
     if (threadIdx.x == 0) atomicMin(&sc->dtmin_bits, bits);
   }
@@ -399,6 +405,10 @@ __global__ void __launch_bounds__(kTileThreads, (FLUX == FLUX_TECNO_ROE || FLUX 
   const int tid = threadIdx.x;
   const int v = vb + tid;
   double nrm[4] = {0.0, 0.0, 0.0, 0.0};
+  // last stage with fuse_dt: the next step's local dt and U_old from the new state
+  const bool next_dt = MODE == MODE_UPDATE && do_norm && k.fuse_dt;
+  unsigned long long dbits = 0x7ff0000000000000ull;
+  Prim qn;                                   // the owned vertex's new state (next_dt)
   if (tid < nown) {
     Prim q0;
     double uo[4], area = 0.0, w = 0.0, dtl = 0.0;
@@ -449,6 +459,61 @@ __global__ void __launch_bounds__(kTileThreads, (FLUX == FLUX_TECNO_ROE || FLUX 
       Wout[v] = e.f; Wout[nv + v] = e.vx; Wout[2 * nv + v] = e.vy; Wout[3 * nv + v] = e.l;
       bool ok = isfinite(q.T) && isfinite(q.u) && isfinite(q.v) && isfinite(q.p) && q.p > 0.0 && c.r > 0.0;
       if (!ok) atomicOr(&sc->bad, 1);
+      if (next_dt) qn = q;
+    }
+  }
+  if (next_dt) {
+    // compute_dt (src/fv.cc:1499-1598) and store_conserved_old (src/fv.cc:1626-1630) of
+    // the coming step, with the operands and order of k_tile_grad<true, *>: the tile's
+    // dual normals are staged over the consumed fluxes in one wave of copies
+    __syncthreads();
+    for (int le = threadIdx.x; le < NE; le += blockDim.x) {
+      cp_async8(sE + le, t.nx + e0 + le);
+      cp_async8(sE + NE + le, t.ny + e0 + le);
+    }
+    cp_async_wait_all();
+    __syncthreads();
+    if (tid < nown) {
+      const double cs = sound_speed(k, qn);
+      const int j0 = sO[tid] - cbase, j1 = sO[tid + 1] - cbase;
+      double lam = 0.0;
+      for (int j = j0; j < j1; ++j) {
+        const int le = list_entry(sC, j) >> 1;
+        const double nx = sE[le], ny = sE[NE + le];
+        const double ar = face_area(nx, ny);
+        lam += face_radius(qn.u, qn.v, nx, ny, cs, ar) * 1.0;
+      }
+      for (int j = m.cb_off[v]; j < m.cb_off[v + 1]; ++j) {
+        const int ent = m.cb_ent[j];
+        if ((ent & 3) != 0) continue;
+        const int d = ent >> 3;
+        const double nx = m.b_nx[d], ny = m.b_ny[d];
+        const double ar = face_area(nx, ny);
+        lam += 0.5 * face_radius(qn.u, qn.v, nx, ny, cs, ar);
+      }
+      if (k.model == 1) {
+        for (int j = j0; j < j1; ++j) {
+          const int le = list_entry(sC, j) >> 1;
+          const unsigned int ab = t.ab[e0 + le];
+          const int ga = t.lv[l0 + (int)(ab & 0xffff)], gb = t.lv[l0 + (int)(ab >> 16)];
+          const double nx = sE[le], ny = sE[NE + le];
+          const double ar = face_area(nx, ny);
+          const double dx = t.x[gb] - t.x[ga], dy = t.y[gb] - t.y[ga];
+          const double dl = face_area(dx, dy);
+          lam += (viscosity(k, qn.T) * ar / dl / density(k, qn)) * 1.0;
+        }
+      }
+      const double dtn = k.cfl * m.dcarea[v] / lam;
+      s.dt[v] = dtn;
+      dbits = (unsigned long long)__double_as_longlong(dtn);
+      if (!(dtn > 0.0)) dbits = 0x7ff0000000000000ull;
+      const Cons un = prim2con(k, qn);
+      s.Uold[v] = un.r; s.Uold[nv + v] = un.mx; s.Uold[2 * nv + v] = un.my; s.Uold[3 * nv + v] = un.E;
+    }
+    dbits = block_min_u64(dbits);
+    if (threadIdx.x == 0) {
+      atomicMin(&sc->dtmin_next, dbits);
+      if (blockIdx.x == 0) sc->dt_next = 1;
     }
   }
   if (MODE == MODE_UPDATE && do_norm) {
