@@ -235,6 +235,21 @@ tg_status tg_global(tg_handle* h, double* ke_out, double* entropy_out);
  * bc may be NULL (values kept).  The state is untouched. */
 tg_status tg_update_parameters(tg_handle* h, const tg_material* mat, const tg_bc_table* bc);
 
+/* Output at an output time (the writers of src/writer.cc:129-409,
+ * src/output_skin_friction.cc, src/output_heatflux.cc read primitive and dE):
+ * tg_output_begin snapshots the current state, as PrimVar records in the
+ * caller's vertex order, and optionally the entropy-variable gradients as the
+ * reference's dE records (n_vertex x 5 variables x (x, y, z)), on the device,
+ * then copies them into the caller's PINNED buffers on a side stream and
+ * returns; steps enqueued afterwards overlap the copy.  tg_output_wait blocks
+ * until the copy is complete.  grad_state selects which gradients the
+ * reference would hold: TG_GRAD_LAST_STAGE those of the last stage's input
+ * state (after a step; zero before any step), TG_GRAD_CURRENT those of the
+ * current state (after compute_forces of a Navier-Stokes run). */
+enum { TG_GRAD_LAST_STAGE = 0, TG_GRAD_CURRENT = 1 };
+tg_status tg_output_begin(tg_handle* h, double* prim_aos, double* dE_aos, int grad_state);
+tg_status tg_output_wait(tg_handle* h);
+
 /* compute_forces (src/force.cc:116-219) on the current state: for each force
  * f (its face tags are tags[sum n_tags[<f] .. +n_tags[f]), the integrals over
  * its boundary faces of the pressure force and, for Navier-Stokes, the viscous

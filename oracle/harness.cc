@@ -12,8 +12,15 @@
 // override before including the header (the reference files are untouched).
 //
 // Usage:
-//   tensum_harness <param.in> <case_dir> <ic.bin|-> <n_steps> <n_dump_steps> <out.bin>
+//   tensum_harness <param.in> <case_dir> <ic.bin|-> <n_steps> <n_dump_steps> <out.bin> [files]
 //   tensum_harness <param.in> <case_dir> mc 0 0 <out.bin>
+//
+// With "files" the loop makes the reference's own file output calls in
+// FiniteVolume::solve's order (src/fv.cc:2240-2343: output at t = 0, then per
+// step log_messages, compute_forces, compute_global, output at each output
+// time) into SAMPLE_*/ as the parameter file asks, output_restart after the
+// last step, and dumps the exact state and dE each output time wrote
+// (records o<k>_prim, o<k>_grad, o<k>_time) so the files can be regenerated.
 //
 // The "mc" form runs the reference's own Monte Carlo driver FiniteVolume::run
 // (src/fv.cc:2401-2492: per-sample extract_rnd_nos + initial condition with
@@ -213,6 +220,7 @@ int main(int argc, char* argv[]) {
 
   const long n_steps = std::atol(argv[4]);
   const long n_dump = std::atol(argv[5]);
+  const bool files = argc > 7 && std::strcmp(argv[7], "files") == 0;
   Dump dump(argv[6]);
 
   FiniteVolume fv(argv[1], argv[2]);
@@ -241,7 +249,19 @@ int main(int argc, char* argv[]) {
   dump_geometry(dump, fv.grid);
   dump.rec("prim0", prim_vec(fv.primitive));
 
-  // Mirrors FiniteVolume::solve (src/fv.cc:2273-2343) without file output.
+  auto dump_output = [&](int k) {
+    std::ostringstream tg;
+    tg << "o" << k << "_";
+    dump.rec(tg.str() + "prim", prim_vec(fv.primitive));
+    dump.rec(tg.str() + "grad", grad_vec(fv.dE));
+    dump.rec(tg.str() + "time", std::vector<double>(1, fv.elapsed_time));
+  };
+  if (files && fv.param.write_soln) {   // src/fv.cc:2240-2245
+    dump_output(fv.counter);
+    fv.output();
+  }
+
+  // Mirrors FiniteVolume::solve (src/fv.cc:2273-2343); file output only with "files".
   if (fv.counter == 0) fv.counter++;
   unsigned long iter = 0;
   fv.residual_norm_total = 1.0e20;
@@ -286,6 +306,22 @@ int main(int argc, char* argv[]) {
     }
     ++iter;
     step_s.push_back(std::chrono::duration<double>(std::chrono::steady_clock::now() - ts).count());
+    if (files) {   // src/fv.cc:2307-2343
+      fv.elapsed_time += fv.dt_global;
+      if (fv.param.write_log) fv.log_messages(iter);
+      fv.compute_forces(iter);
+      fv.compute_global(iter);
+      if (fv.time_instance_reached && fv.param.time_mode == "unsteady") {
+        if (fv.param.write_soln) {
+          dump_output(fv.counter);
+          fv.output();
+        }
+        fv.counter++;
+        fv.time_instance_reached = false;
+      }
+      if (fv.elapsed_time >= fv.param.final_time) { ++step; dump.rec("steps_run", std::vector<double>(1, (double)step)); break; }
+      continue;
+    }
     if (full && !fv.param.force_data.empty()) {
       // compute_forces follows every step in FiniteVolume::solve (src/fv.cc:2313)
       fv.compute_forces(iter);
@@ -306,6 +342,11 @@ int main(int argc, char* argv[]) {
     if (fv.elapsed_time >= fv.param.final_time) { ++step; dump.rec("steps_run", std::vector<double>(1, (double)step)); break; }
   }
   auto t1 = std::chrono::steady_clock::now();
+  if (files && fv.param.write_restart) {
+    fv.output_restart(iter);
+    dump.rec("restart_res0", std::vector<double>(1, fv.residual_norm_total0));
+    dump.rec("restart_counter", std::vector<double>(1, (double)fv.counter));
+  }
   dump.rec("wall_s", std::vector<double>(1, std::chrono::duration<double>(t1 - t0).count()));
   dump.rec("step_s", step_s);
   dump.rec("iters", std::vector<double>(1, (double)iter));

@@ -39,6 +39,8 @@ def param_text(cfg: dict) -> str:
     online_stat (bool), variables (extra moment variables, e.g. ["density"]).
     forces: {name: [face tags]} (integrals section, compute_forces).
     liou_fix (bool), bc_scheme ('weak' | 'strong').
+    Output keys: files (bool: solution, log, global and restart files),
+    surfaces (face tags of the surface files).
     """
     flux = cfg.get("flux", "kepes_tecno_roe")
     recon = cfg.get("reconstruct", "minmod")
@@ -63,6 +65,8 @@ def param_text(cfg: dict) -> str:
     force_text = "\n".join("   force\n   {\n      " + name + "   " + "   ".join(str(t) for t in tags) + "\n   }"
                            for name, tags in cfg.get("forces", {}).items())
     online = "yes" if cfg.get("online_stat", False) else "no"
+    files = "yes" if cfg.get("files", False) else "no"
+    surf_text = "\n".join(f"      {int(t)}" for t in cfg.get("surfaces", []))
     return f"""grid
 {{
    cell      median
@@ -159,12 +163,13 @@ output
    }}
    surfaces
    {{
+{surf_text}
    }}
-   restart               no
-   restart_frequency     100
-   log_output            no
-   soln_output           no
-   save_global           no
+   restart               {files}
+   restart_frequency     100000000
+   log_output            {files}
+   soln_output           {files}
+   save_global           {files}
    find_error            no
 }}
 """
@@ -223,6 +228,42 @@ def run_case(mesh, cfg: dict, prim0: np.ndarray | None, n_steps: int, n_dump: in
         if own:
             import shutil
             shutil.rmtree(wd, ignore_errors=True)
+
+
+def run_files(mesh, cfg: dict, prim0: np.ndarray | None, n_steps: int, timeout: float = 3600.0):
+    """Run the harness in its file-output mode: the reference writes its
+    solution, surface, log, force, global and restart files into SAMPLE_*/.
+    Returns (dump, {file name: text}) for the files of the sample directory."""
+    from tensum_b200.mesh import write_part_file
+
+    if not harness_available():
+        raise RuntimeError("oracle/_ref/tensum_harness is not built (make -C oracle ref)")
+    wd = tempfile.mkdtemp(prefix="tensum_files_")
+    try:
+        write_part_file(mesh, wd)
+        with open(os.path.join(wd, "param.in"), "w") as fh:
+            fh.write(param_text(dict(cfg, files=True)))
+        ic = "-"
+        if prim0 is not None:
+            ic = os.path.join(wd, "ic.bin")
+            np.ascontiguousarray(prim0, dtype="<f8").tofile(ic)
+        out = os.path.join(wd, "dump.bin")
+        r = subprocess.run([HARNESS, "param.in", ".", ic, str(n_steps), "0", out, "files"],
+                           cwd=wd, capture_output=True, text=True, timeout=timeout)
+        if r.returncode != 0 or not os.path.exists(out):
+            raise RuntimeError(f"reference harness failed ({r.returncode}):\n{r.stdout[-2000:]}\n{r.stderr[-2000:]}")
+        if "ERROR" in r.stdout or "assertion failed" in r.stdout:
+            raise RuntimeError("reference harness reported an error:\n" + r.stdout[-2000:])
+        texts = {}
+        for d in sorted(os.listdir(wd)):
+            if d.startswith("SAMPLE_") and os.path.isdir(os.path.join(wd, d)):
+                for name in sorted(os.listdir(os.path.join(wd, d))):
+                    with open(os.path.join(wd, d, name)) as fh:
+                        texts[name] = fh.read()
+        return read_dump(out), texts
+    finally:
+        import shutil
+        shutil.rmtree(wd, ignore_errors=True)
 
 
 def rnd_file_text(rows: dict) -> str:

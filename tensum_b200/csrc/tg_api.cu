@@ -72,6 +72,12 @@ struct tg_handle {
   int* bad = nullptr;                 // device flag of k_state_check
   cudaEvent_t raw_ready = nullptr;
   Stager stage;
+  // output snapshots (tg_output_begin / tg_output_wait)
+  double* snap = nullptr;             // 5 * nv: PrimVar records in the caller's order
+  double* snap_grad = nullptr;        // 15 * nv: dE records in the caller's order
+  cudaStream_t out_stream = nullptr;
+  cudaEvent_t snap_ready = nullptr, out_done = nullptr;
+  bool out_pending = false;
   // Monte Carlo moments: per output instance three [nvar][nv] arrays (fm, sm, m2)
   int mom_ninst = 0, mom_extras = 0, mom_nvar = 0;
   double* mom = nullptr;
@@ -646,6 +652,10 @@ tg_status tg_destroy(tg_handle* h) {
   }
   if (h->stage.slots) cudaFreeHost(h->stage.slots);
   if (h->raw_ready) cudaEventDestroy(h->raw_ready);
+  if (h->out_stream) cudaStreamSynchronize(h->out_stream);
+  if (h->snap_ready) cudaEventDestroy(h->snap_ready);
+  if (h->out_done) cudaEventDestroy(h->out_done);
+  if (h->out_stream) cudaStreamDestroy(h->out_stream);
   if (h->stream) cudaStreamDestroy(h->stream);
   delete h;
   return TG_OK;
@@ -895,6 +905,52 @@ tg_status tg_update_parameters(tg_handle* h, const tg_material* mat, const tg_bc
   h->graph_exec = nullptr;
   h->graph = nullptr;
   return sync(h);
+}
+
+tg_status tg_output_begin(tg_handle* h, double* prim_out, double* dE_out, int grad_state) {
+  if (!h || !prim_out) return fail(h, TG_INVALID_ARG, "NULL handle or output buffer");
+  if (grad_state != TG_GRAD_LAST_STAGE && grad_state != TG_GRAD_CURRENT)
+    return fail(h, TG_INVALID_ARG, "grad_state is TG_GRAD_LAST_STAGE or TG_GRAD_CURRENT");
+  if (!host_pinned(prim_out) || (dE_out && !host_pinned(dE_out)))
+    return fail(h, TG_INVALID_ARG, "tg_output_begin copies into pinned host memory; tg_get_state takes any buffer");
+  const int nv = h->L.nv;
+  tg_status st;
+  if (!h->snap && (st = dev_alloc(h, 5 * (size_t)nv, &h->snap)) != TG_OK) return st;
+  if (dE_out && !h->snap_grad && (st = dev_alloc(h, 15 * (size_t)nv, &h->snap_grad)) != TG_OK) return st;
+  if (!h->out_stream) {
+    TG_CUDA(h, cudaStreamCreateWithFlags(&h->out_stream, cudaStreamNonBlocking));
+    TG_CUDA(h, cudaEventCreateWithFlags(&h->snap_ready, cudaEventDisableTiming));
+    TG_CUDA(h, cudaEventCreateWithFlags(&h->out_done, cudaEventDisableTiming));
+  }
+  // the previous snapshot's copies finish before its buffers are written again
+  if (h->out_pending) TG_CUDA(h, cudaStreamWaitEvent(h->stream, h->out_done, 0));
+  k_state_out<<<nblk(nv), kBlock, 0, h->stream>>>(nv, h->Pb[0], h->old_of_new, h->snap);
+  if (dE_out) {
+    // the reference writes the dE of its last compute_gradients: the last stage's input
+    // state after a step, the current state after compute_forces of a Navier-Stokes run
+    const int last_in = h->ctl.scheme == 1 ? 1 : h->ctl.n_rks - 1;
+    enqueue_gradient(h, grad_state == TG_GRAD_CURRENT ? 0 : last_in, false, true, h->never);
+    k_grad_out<<<nblk(nv), kBlock, 0, h->stream>>>(nv, h->sv.G, h->old_of_new, h->snap_grad, h->sc,
+                                                    grad_state == TG_GRAD_LAST_STAGE ? 1 : 0);
+  }
+  TG_CUDA(h, cudaEventRecord(h->snap_ready, h->stream));
+  TG_CUDA(h, cudaStreamWaitEvent(h->out_stream, h->snap_ready, 0));
+  TG_CUDA(h, cudaMemcpyAsync(prim_out, h->snap, 5 * (size_t)nv * sizeof(double), cudaMemcpyDeviceToHost, h->out_stream));
+  if (dE_out)
+    TG_CUDA(h, cudaMemcpyAsync(dE_out, h->snap_grad, 15 * (size_t)nv * sizeof(double), cudaMemcpyDeviceToHost,
+                               h->out_stream));
+  TG_CUDA(h, cudaEventRecord(h->out_done, h->out_stream));
+  h->out_pending = true;
+  TG_CUDA(h, cudaGetLastError());
+  return TG_OK;
+}
+
+tg_status tg_output_wait(tg_handle* h) {
+  if (!h) return fail(h, TG_INVALID_ARG, "NULL handle");
+  if (!h->out_pending) return TG_OK;
+  h->out_pending = false;
+  TG_CUDA(h, cudaEventSynchronize(h->out_done));
+  return TG_OK;
 }
 
 tg_status tg_forces(tg_handle* h, int n_forces, const int* n_tags, const int* tags, double* out) {

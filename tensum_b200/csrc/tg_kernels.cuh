@@ -149,6 +149,27 @@ __global__ void k_state_out(int nv, const double* __restrict__ P, const int* __r
   q[0] = P[i]; q[1] = P[3 * (size_t)nv + i]; q[2] = P[nv + i]; q[3] = P[2 * (size_t)nv + i]; q[4] = 0.0;
 }
 
+// Device gradients G (V1, V2, V3, V5) x (x, y) -> the reference's dE records,
+// 5 variables x (x, y, z) per vertex in the caller's order (src/fv.h:148),
+// zero for the z components and for the fourth (z-momentum) variable.
+// zero_unstepped: all zero while no step has run since the state was set (the
+// reference zeroes dE when a sample starts, src/fv.cc:207-212).
+__global__ void k_grad_out(int nv, const double* __restrict__ G, const int* __restrict__ old_of_new,
+                           double* __restrict__ out, const Scalars* __restrict__ sc, int zero_unstepped) {
+  int i = blockIdx.x * blockDim.x + threadIdx.x;
+  if (i >= nv) return;
+  double* d = out + 15 * (size_t)old_of_new[i];
+  const int var_of[4] = {0, 1, 2, 4};
+#pragma unroll
+  for (int q = 0; q < 15; ++q) d[q] = 0.0;
+  if (zero_unstepped && sc->iter == 0) return;
+#pragma unroll
+  for (int c = 0; c < 4; ++c) {
+    d[3 * var_of[c]] = G[(size_t)(2 * c) * nv + i];
+    d[3 * var_of[c] + 1] = G[(size_t)(2 * c + 1) * nv + i];
+  }
+}
+
 // store_conserved_old (src/fv.cc:1626-1630)
 __global__ void k_store_old(Params k, MeshView m, StateView s, const int* __restrict__ done) {
   if (*done) return;

@@ -20,7 +20,8 @@ EXPORTS = ["tg_create", "tg_destroy", "tg_last_error", "tg_abi_version", "tg_set
            "tg_store_conserved_old", "tg_compute_dt", "tg_gradients", "tg_residual", "tg_update",
            "tg_residual_norm", "tg_end_step", "tg_step", "tg_global", "tg_stream", "tg_time_phase", "tg_query",
            "tg_advance", "tg_moments_init", "tg_moments_increment", "tg_moments_get", "tg_moments_export",
-           "tg_moments_merge", "tg_moments_merge_device", "tg_moments_finalize", "tg_forces", "tg_update_parameters"]
+           "tg_moments_merge", "tg_moments_merge_device", "tg_moments_finalize", "tg_forces", "tg_update_parameters",
+           "tg_output_begin", "tg_output_wait"]
 
 PHASE = {"gradient": 0, "flux": 1, "update": 2, "dt": 3, "step": 4}
 QUERY = {"n_vertex": 0, "n_edge": 1, "n_bface": 2, "kernels_per_step": 3, "device_bytes": 4, "kernels_per_flux": 5}
@@ -65,6 +66,8 @@ def load():
     L.tg_advance.argtypes = [vp, i, C.c_long, dp]
     L.tg_forces.argtypes = [vp, i, C.POINTER(i), C.POINTER(i), dp]
     L.tg_update_parameters.argtypes = [vp, vp, vp]
+    L.tg_output_begin.argtypes = [vp, dp, dp, i]
+    L.tg_output_wait.argtypes = [vp]
     L.tg_moments_init.argtypes = [vp, i, i]
     L.tg_moments_increment.argtypes = [vp, i, C.c_long]
     L.tg_moments_get.argtypes = [vp, i, dp, dp, dp]
@@ -174,6 +177,26 @@ class Solver:
         """Material constants and boundary values of `problem` (same mesh and schemes)."""
         self._keep = problem          # the ctypes structs point into its arrays
         self._chk(self.L.tg_update_parameters(self.h, C.byref(problem.material), C.byref(problem.bc)))
+
+    # ---- output snapshots (tg_output_begin / tg_output_wait)
+    GRAD_LAST_STAGE, GRAD_CURRENT = 0, 1
+
+    def output_buffers(self, with_gradients: bool = True):
+        """Pinned host buffers for output_begin: state (n_vertex, 5) and dE (n_vertex, 5, 3)."""
+        import torch
+        prim = torch.empty((self.nv, 5), dtype=torch.float64, pin_memory=True).numpy()
+        grad = torch.empty((self.nv, 5, 3), dtype=torch.float64, pin_memory=True).numpy() if with_gradients else None
+        return prim, grad
+
+    def output_begin(self, prim_out: np.ndarray, grad_out: np.ndarray | None = None,
+                     grad_state: int = GRAD_LAST_STAGE):
+        """Start copying the current state (and gradients) into pinned buffers;
+        later calls overlap the copy until output_wait."""
+        self._out_keep = (prim_out, grad_out)
+        self._chk(self.L.tg_output_begin(self.h, _d(prim_out), None if grad_out is None else _d(grad_out), grad_state))
+
+    def output_wait(self):
+        self._chk(self.L.tg_output_wait(self.h))
 
     def forces(self, forces: dict) -> np.ndarray:
         """compute_forces on the current state for {name: [face tags]} (in insertion

@@ -128,3 +128,25 @@ def build_mc_case(spec: dict = MC_CASE):
                samples=list(spec["samples"]), rnd_per_sample=cases.KH_RND_PER_SAMPLE, ic=kh_expressions(),
                variables=list(spec["variables"]))
     return m, cfg, rows
+
+
+# Output-file cases: the reference writes its files at every output time
+# (solution with derived variables, surfaces, skin friction and heat flux for
+# Navier-Stokes, logs, forces, global integrals, restart).
+OUTPUT_CASES = {
+    "out_cyl_ns": dict(_cyl("kepes_tecno_roe", "minmod", "ns", forces={"cyl": [1]}), steps=100000,
+                       final_time=0.02, time_stamps=2, surfaces=[1],
+                       variables=["mach", "density", "entropy", "vorticity"]),
+    "out_cyl_iso": dict(_cyl("kepes_tecno_rusanov", "minmod", "ns", bc="isothermal"), steps=100000,
+                        final_time=0.01, time_stamps=1, surfaces=[1, 2], variables=["entropy"]),
+    "out_sq_euler": dict(_sq("kepes_tecno_roe", "minmod"), steps=100000, final_time=0.05, time_stamps=2,
+                         variables=["vorticity", "mach"]),
+}
+
+
+def build_output_case(spec: dict):
+    """Mesh, configuration (with the output keys) and initial state of an output case."""
+    m, cfg, prim0 = build_case(spec)
+    cfg = dict(cfg, final_time=spec["final_time"], time_stamps=spec["time_stamps"],
+               variables=list(spec.get("variables", [])), surfaces=list(spec.get("surfaces", [])))
+    return m, cfg, prim0
