@@ -40,7 +40,7 @@ def param_text(cfg: dict) -> str:
     forces: {name: [face tags]} (integrals section, compute_forces).
     liou_fix (bool), bc_scheme ('weak' | 'strong').
     Output keys: files (bool: solution, log, global and restart files),
-    surfaces (face tags of the surface files).
+    surfaces (face tags of the surface files).  cell: 'median' | 'voronoi' dual cells.
     """
     flux = cfg.get("flux", "kepes_tecno_roe")
     recon = cfg.get("reconstruct", "minmod")
@@ -69,7 +69,7 @@ def param_text(cfg: dict) -> str:
     surf_text = "\n".join(f"      {int(t)}" for t in cfg.get("surfaces", []))
     return f"""grid
 {{
-   cell      median
+   cell      {cfg.get('cell', 'median')}
 }}
 
 numeric

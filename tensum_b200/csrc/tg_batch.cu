@@ -350,7 +350,7 @@ tg_status tg_batch_create(const tg_batch_level* levels, int n_levels, const tg_m
     for (int v = 0; v < L.nv; ++v) aw[v] = L.dcarea[v] * L.pweight[v];
     for (int e = 0; e < L.ne; ++e) {
       const double a = std::sqrt(L.e_nx[e] * L.e_nx[e] + L.e_ny[e] * L.e_ny[e]);
-      const double ia = 1.0 / a;
+      const double ia = a > 0.0 ? 1.0 / a : 0.0;   // gradient-only edges carry no flux
       ux[e] = L.e_nx[e] * ia; uy[e] = L.e_ny[e] * ia; ar[e] = a;
     }
 #define BU(vec, field) \

@@ -135,34 +135,58 @@ std::string build_layout(const tg_mesh& m, const tg_bc_table* bc, bool need_visc
                                   : 1.0 / 1.0;
   }
 
-  // ---- edges: every reference face, sorted by (lower vertex, upper vertex, face)
-  std::vector<int> eorder(nf);
+  // ---- edges: every reference face, plus each primal edge whose dual face the
+  // reference dropped for zero measure (Voronoi duals, src/grid_preproc.cc:633-647):
+  // those carry no flux (zero normal) but their P1 weights belong to the vertex
+  // gradients, which the reference forms cell by cell
+  std::vector<int> fvx(m.face_vertex, m.face_vertex + 2 * (size_t)nf);
+  std::vector<double> fnrm(m.face_normal, m.face_normal + 2 * (size_t)nf);
+  std::vector<int> flc(m.face_lcell, m.face_lcell + nf), frc(m.face_rcell, m.face_rcell + nf);
+  {
+    auto pkey = [](int a, int b) { return ((uint64_t)(uint32_t)std::min(a, b) << 32) | (uint32_t)std::max(a, b); };
+    std::unordered_map<uint64_t, int> seen;
+    seen.reserve(2 * (size_t)nf);
+    for (int f = 0; f < nf; ++f) seen.emplace(pkey(m.face_vertex[2 * f], m.face_vertex[2 * f + 1]), -1);
+    for (int c = 0; c < nc; ++c)
+      for (int k = 0; k < 3; ++k) {
+        const int a = m.cell_vertex[3 * c + k], b = m.cell_vertex[3 * c + (k + 1) % 3];
+        auto it = seen.find(pkey(a, b));
+        if (it == seen.end()) {
+          seen.emplace(pkey(a, b), (int)flc.size());
+          fvx.push_back(a); fvx.push_back(b);
+          fnrm.push_back(0.0); fnrm.push_back(0.0);
+          flc.push_back(c); frc.push_back(-1);
+        } else if (it->second >= 0) {
+          frc[it->second] = c;
+        }
+      }
+  }
+  const int nfa = (int)flc.size();
+  std::vector<int> eorder(nfa);
   std::iota(eorder.begin(), eorder.end(), 0);
-  auto lo = [&](int f) { return std::min(N[m.face_vertex[2 * f]], N[m.face_vertex[2 * f + 1]]); };
-  auto hi = [&](int f) { return std::max(N[m.face_vertex[2 * f]], N[m.face_vertex[2 * f + 1]]); };
+  auto lo = [&](int f) { return std::min(N[fvx[2 * f]], N[fvx[2 * f + 1]]); };
+  auto hi = [&](int f) { return std::max(N[fvx[2 * f]], N[fvx[2 * f + 1]]); };
   std::stable_sort(eorder.begin(), eorder.end(), [&](int a, int b) {
     int la = lo(a), lb = lo(b);
     if (la != lb) return la < lb;
     return hi(a) < hi(b);
   });
-  L.ne = nf;
-  L.e_a.resize(nf); L.e_b.resize(nf); L.e_face.resize(nf);
-  L.e_nx.resize(nf); L.e_ny.resize(nf); L.e_dx.resize(nf); L.e_dy.resize(nf);
-  L.e_g0x.assign(nf, 0.0); L.e_g0y.assign(nf, 0.0); L.e_g1x.assign(nf, 0.0); L.e_g1y.assign(nf, 0.0);
-  std::vector<int> edge_of_face(nf);
-  for (int e = 0; e < nf; ++e) {
+  L.ne = nfa;
+  L.e_a.resize(nfa); L.e_b.resize(nfa); L.e_face.resize(nfa);
+  L.e_nx.resize(nfa); L.e_ny.resize(nfa); L.e_dx.resize(nfa); L.e_dy.resize(nfa);
+  L.e_g0x.assign(nfa, 0.0); L.e_g0y.assign(nfa, 0.0); L.e_g1x.assign(nfa, 0.0); L.e_g1y.assign(nfa, 0.0);
+  for (int e = 0; e < nfa; ++e) {
     int f = eorder[e];
-    edge_of_face[f] = e;
-    int va = m.face_vertex[2 * f], vb = m.face_vertex[2 * f + 1];
+    int va = fvx[2 * f], vb = fvx[2 * f + 1];
     L.e_face[e] = f;
     L.e_a[e] = N[va];
     L.e_b[e] = N[vb];
-    L.e_nx[e] = m.face_normal[2 * f];
-    L.e_ny[e] = m.face_normal[2 * f + 1];
+    L.e_nx[e] = fnrm[2 * f];
+    L.e_ny[e] = fnrm[2 * f + 1];
     L.e_dx[e] = m.coords[2 * vb] - m.coords[2 * va];     // src/kepes_tecno_roe.cc:112
     L.e_dy[e] = m.coords[2 * vb + 1] - m.coords[2 * va + 1];
     // gradient weights: sum over the face's cells of the P1 normal of the other endpoint
-    int cells[2] = {m.face_lcell[f], m.face_rcell[f]};
+    int cells[2] = {flc[f], frc[f]};
     for (int q = 0; q < 2; ++q) {
       int c = cells[q];
       if (c < 0) continue;
@@ -189,9 +213,9 @@ std::string build_layout(const tg_mesh& m, const tg_bc_table* bc, bool need_visc
 
   // per reference vertex incident edges (in edge order)
   std::vector<std::vector<int>> inc(nv);
-  for (int e = 0; e < nf; ++e) {
-    inc[m.face_vertex[2 * L.e_face[e]]].push_back(e << 1);
-    inc[m.face_vertex[2 * L.e_face[e] + 1]].push_back((e << 1) | 1);
+  for (int e = 0; e < nfa; ++e) {
+    inc[fvx[2 * L.e_face[e]]].push_back(e << 1);
+    inc[fvx[2 * L.e_face[e] + 1]].push_back((e << 1) | 1);
   }
   L.ce_off.assign(nv + 1, 0);
   std::vector<int> g;
@@ -394,9 +418,10 @@ std::string build_tiles(HostLayout& L, int max_owned, int max_local, int max_edg
       L.te_nx.push_back(L.e_nx[e]); L.te_ny.push_back(L.e_ny[e]);
       L.te_g0x.push_back(L.e_g0x[e]); L.te_g0y.push_back(L.e_g0y[e]);
       L.te_g1x.push_back(L.e_g1x[e]); L.te_g1y.push_back(L.e_g1y[e]);
-      // src/material.cc:69 area = normal.norm(); src/kepec.cc:18 unit = normal * (1/area)
+      // src/material.cc:69 area = normal.norm(); src/kepec.cc:18 unit = normal * (1/area);
+      // a gradient-only edge (zero normal) gets a zero unit normal, so its flux is zero
       double area = std::sqrt(L.e_nx[e] * L.e_nx[e] + L.e_ny[e] * L.e_ny[e] + 0.0 * 0.0);
-      double ia = 1.0 / area;
+      double ia = area > 0.0 ? 1.0 / area : 0.0;
       L.te_ux.push_back(L.e_nx[e] * ia);
       L.te_uy.push_back(L.e_ny[e] * ia);
       L.te_ar.push_back(area);

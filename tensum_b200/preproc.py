@@ -13,6 +13,9 @@ geometry is bit-identical to the reference's on the same part file:
 
 * face / cell centroids: ``Vector::equ`` (src/vec.h:254-272), src/grid_preproc.cc:18-30, 156-170
 * cell area and median dual area: src/grid_preproc.cc:175-211, periodic sum src/reduce_dual_area.cc:18-133
+* Voronoi dual cells (``cell="voronoi"``): circumcentres with the small-face
+  fix and the boundary check, src/grid_preproc.cc:38-149; dual areas by the
+  polygon (shoelace) sum per cell corner, src/grid_preproc.cc:211-246
 * face orientation and dual normals: src/grid_preproc.cc:252-303
 * boundary-face outward normals: src/grid_preproc.cc:306-328
 * P1 basis normals: src/grid_preproc.cc:330-362
@@ -23,6 +26,7 @@ geometry is bit-identical to the reference's on the same part file:
 from __future__ import annotations
 
 import dataclasses
+import math
 
 import numpy as np
 
@@ -118,13 +122,83 @@ def _build_face_list(cells: np.ndarray, bfaces: np.ndarray):
     return face_vertex, face_type, face_lcell, face_rcell
 
 
-def preprocess(mesh: TriMesh, periodic_types=None) -> Geometry:
-    """Median-dual preprocessing of a single-partition mesh (2D, radius = 1).
+def _voronoi_centroids(x, y, cells, bcen, blc):
+    """Cell centres of the Voronoi dual (src/grid_preproc.cc:38-149): the
+    circumcentre, or the midpoint of the edge opposite a vertex whose weight
+    beta vanishes (an obtuse or nearly degenerate corner); a cell whose centre
+    falls on one of its boundary faces' centres takes the geometric centroid."""
+    n1, n2, n3 = cells[:, 0], cells[:, 1], cells[:, 2]
+    x1, y1, x2, y2, x3, y3 = x[n1], y[n1], x[n2], y[n2], x[n3], y[n3]
+    pw = np.frompyfunc(math.pow, 2, 1)        # libm pow(d, 2), as the reference calls it
+
+    def sq(d):
+        return pw(d, 2.0).astype(np.float64)
+
+    l1 = sq(x2 - x3) + sq(y2 - y3)
+    l2 = sq(x3 - x1) + sq(y3 - y1)
+    l3 = sq(x1 - x2) + sq(y1 - y2)
+    beta1 = np.where(0.0 < l2 + l3 - l1, l2 + l3 - l1, 0.0)   # std::max(0.0, .)
+    beta2 = np.where(0.0 < l3 + l1 - l2, l3 + l1 - l2, 0.0)
+    beta3 = np.where(0.0 < l1 + l2 - l3, l1 + l2 - l3, 0.0)
+    beta1 = np.where((beta1 < beta2 / 2.0) & (beta1 < beta3 / 2.0), 0.0, beta1)
+    beta2 = np.where((beta2 < beta3 / 2.0) & (beta2 < beta1 / 2.0), 0.0, beta2)
+    beta3 = np.where((beta3 < beta1 / 2.0) & (beta3 < beta2 / 2.0), 0.0, beta3)
+    det = (x2 - x1) * (y3 - y1) - (x3 - x1) * (y2 - y1)
+    b1 = 0.5 * ((x2 - x1) * (x2 + x1) + (y2 - y1) * (y2 + y1))
+    b2 = 0.5 * ((x3 - x1) * (x3 + x1) + (y3 - y1) * (y3 + y1))
+    with np.errstate(divide="ignore", invalid="ignore"):
+        xc = ((y3 - y1) * b1 - (y2 - y1) * b2) / det
+        yc = (-(x3 - x1) * b1 + (x2 - x1) * b2) / det
+    cx = np.where(beta1 == 0.0, 0.5 * (x2 + x3), np.where(beta2 == 0.0, 0.5 * (x3 + x1),
+                                                           np.where(beta3 == 0.0, 0.5 * (x1 + x2), xc)))
+    cy = np.where(beta1 == 0.0, 0.5 * (y2 + y3), np.where(beta2 == 0.0, 0.5 * (y3 + y1),
+                                                           np.where(beta3 == 0.0, 0.5 * (y1 + y2), yc)))
+    cen = np.stack([cx, cy], 1)
+    third = 1.0 / 3.0
+    for i in range(bcen.shape[0]):
+        c = blc[i]
+        dx = bcen[i, 0] * 1.0 + cen[c, 0] * (-1.0)
+        dy = bcen[i, 1] * 1.0 + cen[c, 1] * (-1.0)
+        if math.sqrt(dx * dx + dy * dy + 0.0 * 0.0) < 1.0e-14:
+            v0, v1, v2 = cells[c]
+            cen[c, 0] = x[v0] * third + x[v1] * third + x[v2] * third
+            cen[c, 1] = y[v0] * third + y[v1] * third + y[v2] * third
+    return cen
+
+
+def _polygon_dual_areas(x, y, cells, cen, V):
+    """Dual area per vertex as the reference sums it for non-median cells
+    (src/grid_preproc.cc:211-246): per cell corner n0, the polygon n0, mid(n0, n2),
+    cell centre, mid(n0, n1) by the shoelace formula, added in cell and corner order."""
+    C = cells.shape[0]
+    areas = np.empty((C, 3))
+    for j in range(3):
+        n0 = cells[:, j]
+        n1 = cells[:, 2] if j == 0 else cells[:, j - 1]
+        n2 = cells[:, 0] if j == 2 else cells[:, j + 1]
+        px = [x[n0], x[n0] * 0.5 + x[n2] * 0.5, cen[:, 0], x[n0] * 0.5 + x[n1] * 0.5, x[n0]]
+        py = [y[n0], y[n0] * 0.5 + y[n2] * 0.5, cen[:, 1], y[n0] * 0.5 + y[n1] * 0.5, y[n0]]
+        a = np.zeros(C)
+        for k in range(4):
+            a = a + (px[k] * py[k + 1] - px[k + 1] * py[k])
+        if np.any(a < 0.0):
+            raise ValueError("dual cell area is non-positive (src/grid_preproc.cc:237-241)")
+        areas[:, j] = a * 0.5
+    dc = np.zeros(V)
+    np.add.at(dc, cells.reshape(-1), areas.reshape(-1))
+    return dc
+
+
+def preprocess(mesh: TriMesh, periodic_types=None, cell: str = "median") -> Geometry:
+    """Dual-mesh preprocessing of a single-partition mesh (2D, radius = 1),
+    median or Voronoi dual cells (the grid section's ``cell`` entry).
 
     ``periodic_types``: boundary tags whose BC is ``periodic``.  Faces with
     such a tag keep their part-file periodic flag; all others are marked
     non-periodic, as src/read_part_mesh_file.cc:166-170 does.
     """
+    if cell not in ("median", "voronoi"):
+        raise ValueError(f"unknown dual cell type {cell!r}")
     coords = np.asarray(mesh.coords, np.float64)
     cells = np.asarray(mesh.cells, np.int64)
     bfaces = np.asarray(mesh.bfaces, np.int64)
@@ -142,8 +216,12 @@ def preprocess(mesh: TriMesh, periodic_types=None) -> Geometry:
         return np.stack([x[v0] * 0.5 + x[v1] * 0.5, y[v0] * 0.5 + y[v1] * 0.5], 1)
 
     c0, c1, c2 = cells[:, 0], cells[:, 1], cells[:, 2]
-    cen = np.stack([x[c0] * third + x[c1] * third + x[c2] * third,
-                    y[c0] * third + y[c1] * third + y[c2] * third], 1)
+    if cell == "voronoi":
+        B0 = bfaces.shape[0]
+        cen = _voronoi_centroids(x, y, cells, mid(bfaces[:, 0], bfaces[:, 1]), flc[:B0])
+    else:
+        cen = np.stack([x[c0] * third + x[c1] * third + x[c2] * third,
+                        y[c0] * third + y[c1] * third + y[c2] * third], 1)
 
     # cell area: l1 = v1 - v0, l2 = v2 - v0, area = 0.5 * (l1.x*l2.y - l1.y*l2.x)
     l1x = x[c1] * 1.0 + x[c0] * (-1.0)
@@ -160,12 +238,18 @@ def preprocess(mesh: TriMesh, periodic_types=None) -> Geometry:
     contrib_a = np.repeat(a3, 3)
     # np.add.at accumulates in index order, i.e. the reference's loop order
     np.add.at(mc, contrib_v, contrib_a)
+    dcv = _polygon_dual_areas(x, y, cells, cen, V) if cell == "voronoi" else None
     for s in mesh.periodic_sets:
         acc = 0.0
         for v in s:
             acc += mc[v] * 1.0
         mc[s] = acc
-    dc = mc.copy()
+        if dcv is not None:
+            acc = 0.0
+            for v in s:
+                acc += dcv[v] * 1.0
+            dcv[s] = acc
+    dc = mc.copy() if dcv is None else dcv
 
     # face orientation (src/grid_preproc.cc:256-277)
     fc = mid(fv[:, 0], fv[:, 1])
@@ -187,6 +271,11 @@ def preprocess(mesh: TriMesh, periodic_types=None) -> Geometry:
     dy = np.where(inter, dy + (cen[rc, 1] * 1.0 + fc[:, 1] * (-1.0)), dy)
     fnormal = np.stack([-dy, dx], 1)
     fmeasure = np.sqrt(fnormal[:, 0] * fnormal[:, 0] + fnormal[:, 1] * fnormal[:, 1] + 0.0)
+    if cell == "voronoi":
+        # remove_empty_faces (src/grid_preproc.cc:633-647): dual faces of zero measure go
+        keep = fmeasure > 0.0
+        fv, ftype, flc, frc = fv[keep], ftype[keep], flc[keep], frc[keep]
+        fnormal, fmeasure = fnormal[keep], fmeasure[keep]
 
     # boundary faces (copied from the face list before the flip above)
     B = bfaces.shape[0]

@@ -52,6 +52,9 @@ CASES = {
     "cyl_inlet_outlet_strong": _cyl("kepec", "first", "euler", bc="inlet_outlet", bc_scheme="strong"),
     "sq_roe_liou": _sq("kepes_tecno_roe", "minmod", ic="collide", liou_fix=True, cfl=0.3),
     "sq_roe_first_liou": _sq("kepes_tecno_roe", "first", n=11, ic="collide", liou_fix=True, steps=3, dump=3, cfl=0.3),
+    "sq_roe_minmod_voronoi": _sq("kepes_tecno_roe", "minmod", cell="voronoi"),
+    "sq_kepec_voronoi_long": _sq("kepec", "first", n=17, seed=13, steps=40, dump=0, cell="voronoi"),
+    "cyl_ns_voronoi": _cyl("kepes_tecno_roe", "minmod", "ns", cell="voronoi", forces={"cyl": [1]}),
 }
 
 
@@ -99,6 +102,8 @@ def build_case(spec: dict):
         cfg["liou_fix"] = True
     if "bc_scheme" in spec:
         cfg["bc_scheme"] = spec["bc_scheme"]
+    if "cell" in spec:
+        cfg["cell"] = spec["cell"]
     return m, cfg, prim0
 
 

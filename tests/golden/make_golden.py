@@ -32,14 +32,18 @@ OUT = os.path.dirname(os.path.abspath(__file__))
 def main():
     if not ref_runner.harness_available():
         raise SystemExit("oracle/_ref/tensum_harness missing: run `make -C oracle ref` first")
+    only = set(sys.argv[1:])
     for name, spec in CASES.items():
+        if only and name not in only:
+            continue
         mesh, cfg, prim0 = build_case(spec)
         d = ref_runner.run_case(mesh, cfg, prim0, spec["steps"], spec["dump_steps"])
         keep = {k: v for k, v in d.items() if k not in ("wall_s", "step_s")}   # timings are not fixtures
         keep["prim_in"] = prim0.ravel()
         np.savez_compressed(os.path.join(OUT, f"{name}.npz"), spec=np.array(json.dumps(spec)), **keep)
         print(name, "vertices", mesh.n_vertex, "records", len(keep))
-    make_mc()
+    if not only or "mc_kh" in only:
+        make_mc()
 
 
 def make_mc():

@@ -21,7 +21,7 @@ TOL_STATE_LONG = 1e-10
 
 
 def make_solver(mesh, cfg):
-    g = preproc.preprocess(mesh)
+    g = preproc.preprocess(mesh, cell=cfg.get("cell", "median"))
     P = abi.Problem(g, cfg)
     return gpu.Solver(P), P
 

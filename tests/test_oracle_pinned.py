@@ -15,7 +15,7 @@ import oracle as O
 @pytest.mark.parametrize("name", golden_names())
 def test_oracle_matches_reference_exactly(name):
     spec, mesh, cfg, prim0, d = load_golden(name)
-    g = preproc.preprocess(mesh)
+    g = preproc.preprocess(mesh, cell=cfg.get("cell", "median"))
     o = O.Oracle(abi.Problem(g, cfg))
     o.set_prim(prim0)
     if spec["dump_steps"] == 0:
@@ -45,10 +45,10 @@ def test_oracle_matches_reference_exactly(name):
             assert np.array_equal(o.forces(cfg["forces"]).ravel(), d[f"s{s}_force"]), f"forces step {s}"
 
 
-@pytest.mark.parametrize("name", ["sq_roe_minmod", "cyl_ns"])
+@pytest.mark.parametrize("name", ["sq_roe_minmod", "cyl_ns", "sq_roe_minmod_voronoi", "cyl_ns_voronoi"])
 def test_geometry_matches_reference_exactly(name):
     spec, mesh, cfg, prim0, d = load_golden(name)
-    g = preproc.preprocess(mesh)
+    g = preproc.preprocess(mesh, cell=cfg.get("cell", "median"))
     faces = d["faces"].reshape(-1, 8)
     assert np.array_equal(faces[:, :2].astype(int), g.face_vertex)
     assert np.array_equal(faces[:, 2].astype(int), g.face_type)
