@@ -28,7 +28,7 @@
 extern "C" {
 #endif
 
-#define TG_ABI_VERSION 2
+#define TG_ABI_VERSION 3
 
 typedef enum {
   TG_OK = 0,
@@ -78,7 +78,7 @@ typedef enum {
 
 /*
  * Mesh after Grid::preproc (src/grid_preproc.cc:1147-1194), one partition,
- * 2D (radius 1), median dual.  Field-by-field the members of Grid:
+ * median or Voronoi dual, planar or axisymmetric.  Field-by-field the members of Grid:
  *   coords        vertex[i].coord.{x,y}                      2*n_vertex
  *   dcarea/mcarea dual / median areas, periodic-summed        n_vertex
  *   cell_vertex   cell[c].vertex[0..2]                        3*n_cell
@@ -90,6 +90,10 @@ typedef enum {
  *   bface_*       bface[b]: vertex[0..1], type, normal.{x,y} (outward),
  *                 lcell, periodic flag.
  *   periodic_*    periodic_lists[i].P_ij as CSR (offsets n_periodic+1).
+ *   *_radius      vertex[i].radius, face[f].radius, cell[c].radius of an
+ *                 axisymmetric run (-axi, src/grid_preproc.cc:750-777: the x of
+ *                 the vertex, face centre and cell centre); all three NULL for
+ *                 a planar mesh (radius 1 everywhere).
  */
 typedef struct {
   int n_vertex;
@@ -115,6 +119,9 @@ typedef struct {
   int n_periodic;
   const int* periodic_offsets;
   const int* periodic_members;
+  const double* vertex_radius;
+  const double* face_radius;
+  const double* cell_radius;
 } tg_mesh;
 
 /* class Material, src/material.h:54-420 (data members). */

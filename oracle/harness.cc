@@ -27,6 +27,9 @@
 // pert(), solve with increment_moments at every output time, reduce_moments)
 // and dumps the reduced moments of every output time instance.
 //
+// With TENSUM_HARNESS_AXI set in the environment the reference runs axisymmetric
+// (its -axi option: radius = x).
+//
 // case_dir holds PARTITION/part_file_0.dat.  ic.bin (optional, "-" to use the
 // parameter file's initial condition) is n_vertex x 5 doubles in the reference
 // PrimVar memory order (T, p, u, v, w), indexed like the part file's active vertices.
@@ -159,6 +162,13 @@ void dump_geometry(Dump& d, const Grid& g) {
   d.rec("cell_nbr_bface", nbr);
   d.rec("faces", faces);
   d.rec("bfaces", bfaces);
+  std::vector<double> vr, fr, cr;
+  for (const auto& v : g.vertex) vr.push_back(v.radius);
+  for (const auto& f : g.face) fr.push_back(f.radius);
+  for (const auto& c : g.cell) cr.push_back(c.radius);
+  d.rec("vradius", vr);
+  d.rec("fradius", fr);
+  d.rec("cradius", cr);
   d.rec("dcarea", g.dcarea);
   d.rec("mcarea", g.mcarea);
   d.rec("periodic", periodic);
@@ -214,7 +224,8 @@ int main(int argc, char* argv[]) {
   NPART = 1;
   N_MC_GROUPS = 1;
   PERIODIC = false;
-  dim = two;
+  // the reference's -axi switch (src/process_command_line.cc:50-52), from the environment
+  dim = std::getenv("TENSUM_HARNESS_AXI") ? axi : two;
   debug = restart = preprocess = bounds = verbose = false;
   if (std::strcmp(argv[3], "mc") == 0) return run_mc(argv[1], argv[2], argv[6]);
 

@@ -41,6 +41,7 @@ def param_text(cfg: dict) -> str:
     liou_fix (bool), bc_scheme ('weak' | 'strong').
     Output keys: files (bool: solution, log, global and restart files),
     surfaces (face tags of the surface files).  cell: 'median' | 'voronoi' dual cells.
+    axisymmetric (bool): the run uses the reference's -axi option (radius = x).
     """
     flux = cfg.get("flux", "kepes_tecno_roe")
     recon = cfg.get("reconstruct", "minmod")
@@ -216,8 +217,12 @@ def run_case(mesh, cfg: dict, prim0: np.ndarray | None, n_steps: int, n_dump: in
             ic = os.path.join(wd, "ic.bin")
             np.ascontiguousarray(prim0, dtype="<f8").tofile(ic)
         out = os.path.join(wd, "dump.bin")
+        env = dict(os.environ)
+        env.pop("TENSUM_HARNESS_AXI", None)
+        if cfg.get("axisymmetric"):
+            env["TENSUM_HARNESS_AXI"] = "1"     # the reference's -axi option
         r = subprocess.run([HARNESS, "param.in", ".", ic, str(n_steps), str(n_dump), out],
-                           cwd=wd, capture_output=True, text=True, timeout=timeout)
+                           cwd=wd, capture_output=True, text=True, timeout=timeout, env=env)
         if r.returncode != 0 or not os.path.exists(out):
             raise RuntimeError(f"reference harness failed ({r.returncode}):\n{r.stdout[-2000:]}\n{r.stderr[-2000:]}")
         if "ERROR" in r.stdout or "assertion failed" in r.stdout:

@@ -31,7 +31,8 @@ class TgMesh(C.Structure):
                 ("face_lcell", ip), ("face_rcell", ip),
                 ("n_bface", C.c_int), ("bface_vertex", ip), ("bface_type", ip), ("bface_normal", dp),
                 ("bface_lcell", ip), ("bface_periodic", bp),
-                ("n_periodic", C.c_int), ("periodic_offsets", ip), ("periodic_members", ip)]
+                ("n_periodic", C.c_int), ("periodic_offsets", ip), ("periodic_members", ip),
+                ("vertex_radius", dp), ("face_radius", dp), ("cell_radius", dp)]
 
 
 class TgMaterial(C.Structure):
@@ -116,6 +117,10 @@ class Problem:
         m.n_periodic = len(g.periodic_sets)
         m.periodic_offsets = _p(arr(offs, np.int32), ip)
         m.periodic_members = _p(arr(mem if mem.size else np.zeros(1, np.int32), np.int32), ip)
+        if g.vertex_radius is not None:   # axisymmetric
+            m.vertex_radius = _p(arr(g.vertex_radius, np.float64), dp)
+            m.face_radius = _p(arr(g.face_radius, np.float64), dp)
+            m.cell_radius = _p(arr(g.cell_radius, np.float64), dp)
         self.mesh = m
 
         mat = TgMaterial()

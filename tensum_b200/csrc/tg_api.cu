@@ -507,6 +507,7 @@ tg_status tg_create(const tg_mesh* mesh, const tg_material* mat, const tg_bc_tab
   k.strong = opt->bc_strong ? 1 : 0;
   // strong conditions change the state after the last update; a fixed time step needs no dt
   k.fuse_dt = (!k.strong && opt->time_step <= 0.0) ? 1 : 0;
+  k.axi = h->L.axi ? 1 : 0;
 
   tg_status st;
 #define UP(vec, field) \
@@ -521,6 +522,7 @@ tg_status tg_create(const tg_mesh* mesh, const tg_material* mat, const tg_bc_tab
   UP(bf_face_nx, bf_face_nx) UP(bf_face_ny, bf_face_ny) UP(bf_face_v0, bf_face_v0) UP(bf_face_v1, bf_face_v1)
   UP(u_cell, u_cell) UP(c_v, c_v) UP(c_n, c_n) UP(c_inv2a, c_inv2a)
   UP(c_bf_off, c_bf_off) UP(c_bf, c_bf) UP(c_nbr_off, c_nbr_off) UP(c_nbr, c_nbr)
+  UP(v_r, v_r) UP(u_r, u_r)
   {
     // bc_scheme strong: which vertices a condition resets (slip, no-slip, pressure,
     // inlet) and in which face order, and which lie on no-slip faces
@@ -553,6 +555,7 @@ tg_status tg_create(const tg_mesh* mesh, const tg_material* mat, const tg_bc_tab
   UPT(t_vbeg, vbeg) UPT(t_loff, loff) UPT(t_eoff, eoff) UPT(lv, lv) UPT(te_ab, ab)
   UPT(te_nx, nx) UPT(te_ny, ny) UPT(te_g0x, g0x) UPT(te_g0y, g0y) UPT(te_g1x, g1x) UPT(te_g1y, g1y)
   UPT(cv_off, cv_off) UPT(cv_ent, cv_ent) UPT(x, x) UPT(y, y) UPT(te_ux, ux) UPT(te_uy, uy) UPT(te_ar, ar)
+  UPT(te_r, r)
 #undef UPT
   const size_t nv = L.nv;
   h->nblocks_v = nblk(L.nv);

@@ -334,6 +334,10 @@ tg_status tg_batch_create(const tg_batch_level* levels, int n_levels, const tg_m
       tg_batch_destroy(b);
       return bfail(nullptr, TG_INVALID_ARG, "every level needs a mesh and a positive multiple of 32 samples");
     }
+    if (levels[l].mesh->vertex_radius) {
+      tg_batch_destroy(b);
+      return bfail(nullptr, TG_NOT_SUPPORTED, "batched ensembles run planar meshes (no radii)");
+    }
     LevelHost& H = b->lh[l];
     std::string msg = build_layout(*levels[l].mesh, levels[l].bc, mat->model == 1, H.L);
     if (!msg.empty()) { tg_batch_destroy(b); return bfail(nullptr, TG_INVALID_ARG, msg); }

@@ -34,7 +34,15 @@ struct MeshView {
   const int* sflag;
   int nsb;
   const int *sb_v, *sb_off, *sb_ent;
+  // axisymmetric radii (src/grid_preproc.cc:750-777): per vertex and per viscous unit
+  const double *v_r, *u_r;
 };
+
+// Vertex radius of an axisymmetric run (1 when planar): update_solution divides
+// by radius x dual area (src/fv.cc:1646, 1671, 1685).
+__device__ __forceinline__ double vertex_radius(const Params& k, const MeshView& m, int v) {
+  return k.axi ? m.v_r[v] : 1.0;
+}
 
 // Device state, structure-of-arrays with component stride nv (or ne, nb ...).
 struct StateView {
@@ -479,7 +487,7 @@ __global__ void k_update(Params k, MeshView m, StateView s, Control ctl, Scalars
       nrm[0] = q0 * q0 * w; nrm[1] = q1 * q1 * w; nrm[2] = q2 * q2 * w; nrm[3] = q3 * q3 * w;
     }
     double dtv = (ctl.time_mode == 1 || ctl.time_step > 0.0) ? sc->dt_global : s.dt[i];
-    double factor = dtv / (1.0 * area);
+    double factor = dtv / (vertex_radius(k, m, i) * area);
     const double uo[4] = {s.Uold[i], s.Uold[nv + i], s.Uold[2 * nv + i], s.Uold[3 * nv + i]};
     Cons c = rk_stage(k, ctl, s, nv, i, r, load_prim(s.P, nv, i), uo, factor, R0, R1, R2, R3);
     Prim q = con2prim(k, c);

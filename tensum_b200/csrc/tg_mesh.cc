@@ -71,6 +71,9 @@ std::string build_layout(const tg_mesh& m, const tg_bc_table* bc, bool need_visc
   }
   for (int i = 0; i < nv; ++i)
     if (!(m.dcarea[i] > 0.0) || !(m.mcarea[i] > 0.0)) return "non-positive dual area";
+  const bool axi = m.vertex_radius || m.face_radius || m.cell_radius;
+  if (axi && !(m.vertex_radius && m.face_radius && m.cell_radius))
+    return "an axisymmetric mesh needs vertex, face and cell radii";
 
   // periodic sets -> set id per vertex
   std::vector<int> set_of(nv, -1);
@@ -123,6 +126,11 @@ std::string build_layout(const tg_mesh& m, const tg_bc_table* bc, bool need_visc
   for (int i = 0; i < nv; ++i) L.new_of_old[L.old_of_new[i]] = i;
   const std::vector<int>& N = L.new_of_old;
 
+  L.axi = axi;
+  if (axi) {
+    L.v_r.resize(nv);
+    for (int i = 0; i < nv; ++i) L.v_r[i] = m.vertex_radius[L.old_of_new[i]];
+  }
   L.dcarea.resize(nv); L.inv6mc.resize(nv); L.pweight.resize(nv); L.x.resize(nv); L.y.resize(nv);
   for (int i = 0; i < nv; ++i) {
     int o = L.old_of_new[i];
@@ -183,6 +191,7 @@ std::string build_layout(const tg_mesh& m, const tg_bc_table* bc, bool need_visc
     L.e_b[e] = N[vb];
     L.e_nx[e] = fnrm[2 * f];
     L.e_ny[e] = fnrm[2 * f + 1];
+    if (axi) L.e_r.push_back(f < nf ? m.face_radius[f] : 1.0);   // gradient-only edges carry no flux
     L.e_dx[e] = m.coords[2 * vb] - m.coords[2 * va];     // src/kepes_tecno_roe.cc:112
     L.e_dy[e] = m.coords[2 * vb + 1] - m.coords[2 * va + 1];
     // gradient weights: sum over the face's cells of the P1 normal of the other endpoint
@@ -321,6 +330,8 @@ std::string build_layout(const tg_mesh& m, const tg_bc_table* bc, bool need_visc
     L.n_int_cells = (int)L.u_cell.size();
     for (int d = 0; d < nb; ++d) L.u_cell.push_back(L.b_cell[d]);
     L.nvu = (int)L.u_cell.size();
+    if (axi)
+      for (int u = 0; u < L.nvu; ++u) L.u_r.push_back(m.cell_radius[L.u_cell[u]]);
     for (int u = 0; u < L.nvu; ++u) {
       int c = L.u_cell[u];
       for (int k = 0; k < 3; ++k) inc_b[m.cell_vertex[3 * c + k]].push_back(((3 * u + k) << 2) | 2);
@@ -358,7 +369,7 @@ std::string build_tiles(HostLayout& L, int max_owned, int max_local, int max_edg
   L.t_vbeg.clear(); L.t_loff.assign(1, 0); L.t_eoff.assign(1, 0); L.lv.clear();
   L.te_ab.clear(); L.te_nx.clear(); L.te_ny.clear();
   L.te_g0x.clear(); L.te_g0y.clear(); L.te_g1x.clear(); L.te_g1y.clear();
-  L.te_ux.clear(); L.te_uy.clear(); L.te_ar.clear();
+  L.te_ux.clear(); L.te_uy.clear(); L.te_ar.clear(); L.te_r.clear();
   L.cv_off.assign(nv + 1, 0);
   L.cv_ent.clear();
   L.lmax = L.emax = L.tmax = L.cmax = 0;
@@ -425,6 +436,7 @@ std::string build_tiles(HostLayout& L, int max_owned, int max_local, int max_edg
       L.te_ux.push_back(L.e_nx[e] * ia);
       L.te_uy.push_back(L.e_ny[e] * ia);
       L.te_ar.push_back(area);
+      if (L.axi) L.te_r.push_back(L.e_r[e]);
     }
     L.t_eoff.push_back((int)L.te_ab.size());
     for (int x = vb; x < v; ++x) {

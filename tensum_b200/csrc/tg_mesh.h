@@ -30,6 +30,10 @@ struct HostLayout {
   std::vector<int> new_of_old, old_of_new;
   // vertices (device order)
   std::vector<double> dcarea, inv6mc, pweight, x, y;
+  // axisymmetric radii (src/grid_preproc.cc:750-777; empty when planar): per vertex,
+  // per edge (its reference face's radius) and per viscous unit (its cell's radius)
+  bool axi = false;
+  std::vector<double> v_r, e_r, u_r;
   // edges
   std::vector<int> e_a, e_b, e_face;
   std::vector<double> e_nx, e_ny, e_dx, e_dy, e_g0x, e_g0y, e_g1x, e_g1y;
@@ -69,6 +73,7 @@ struct HostLayout {
   std::vector<uint32_t> te_ab;
   std::vector<double> te_nx, te_ny, te_g0x, te_g0y, te_g1x, te_g1y;
   std::vector<double> te_ux, te_uy, te_ar;   // n/|n| and |n|, as Material::num_flux forms them
+  std::vector<double> te_r;                  // the edge's radius (axisymmetric runs)
   std::vector<int> cv_off;
   std::vector<uint16_t> cv_ent;
 };

@@ -38,6 +38,7 @@ struct Params {
   int liou;       // Liou's carbuncle switch active (liou_fix with kepes_tecno_roe)
   int strong;     // bc_scheme strong
   int fuse_dt;    // the last stage's update also forms the next step's local dt and U_old
+  int axi;        // axisymmetric: residual contributions and the update weighted by radii
 };
 
 struct Prim { double T, u, v, p; };

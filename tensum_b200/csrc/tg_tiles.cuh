@@ -52,6 +52,7 @@ struct TileView {
   const unsigned int* ab;
   const double *nx, *ny, *g0x, *g0y, *g1x, *g1y;
   const double *ux, *uy, *ar;   // unit normal and |n| per tile edge
+  const double* r;              // radius per tile edge (axisymmetric runs)
   const int* cv_off;            // per vertex (nv + 1); cv_ent has an even length
   const unsigned short* cv_ent;
   const double *x, *y;          // vertex coordinates (device order)
@@ -397,6 +398,10 @@ __global__ void __launch_bounds__(kTileThreads, (FLUX == FLUX_TECNO_ROE || FLUX 
       dy = sX[L + lb] - sX[L + la];
     }
     Flx F = num_flux_unit<FLUX, RECON>(k, A, B, unx, uny, area, dx, dy, gl, gr, kRoe ? sS[la] + sS[lb] : 0);
+    if (k.axi) {   // residual[cl] += flux * r_f, residual[cr] -= flux * r_f (src/fv.cc:1095-1096)
+      const double rf = t.r[e0 + le];
+      F.m *= rf; F.x *= rf; F.y *= rf; F.e *= rf;
+    }
     sE[le] = F.m; sE[NE + le] = F.x; sE[2 * NE + le] = F.y; sE[3 * NE + le] = F.e;
   }
   __syncthreads();
@@ -432,12 +437,17 @@ __global__ void __launch_bounds__(kTileThreads, (FLUX == FLUX_TECNO_ROE || FLUX 
     for (int j = m.cb_off[v]; j < m.cb_off[v + 1]; ++j) {
       int ent = m.cb_ent[j];
       int type = ent & 3, idx = ent >> 2;
+      // axisymmetric weights (src/fv.cc:1151, 1187, 1226-1228, 1280-1282, 1315-1316): half the
+      // radius of the boundary-face vertex, of the viscous unit's cell, of the vertex
       if (type == 0) {
-        r0 += s.Fb[idx] * 0.5; r1 += s.Fb[n2 + idx] * 0.5; r2 += s.Fb[2 * n2 + idx] * 0.5; r3 += s.Fb[3 * n2 + idx] * 0.5;
+        const double w = k.axi ? 0.5 * m.v_r[(idx & 1) ? m.b_v1[idx >> 1] : m.b_v0[idx >> 1]] : 0.5;
+        r0 += s.Fb[idx] * w; r1 += s.Fb[n2 + idx] * w; r2 += s.Fb[2 * n2 + idx] * w; r3 += s.Fb[3 * n2 + idx] * w;
       } else if (type == 2 && k.model == 1) {
-        r1 += s.Fv[idx] * -(0.5 * 1.0); r2 += s.Fv[n3 + idx] * -(0.5 * 1.0); r3 += s.Fv[2 * n3 + idx] * -(0.5 * 1.0);
+        const double w = k.axi ? -(0.5 * m.u_r[idx / 3]) : -(0.5 * 1.0);
+        r1 += s.Fv[idx] * w; r2 += s.Fv[n3 + idx] * w; r3 += s.Fv[2 * n3 + idx] * w;
       } else if (type == 3 && k.model == 1) {
-        r1 += s.Fvb[idx] * 0.5; r2 += s.Fvb[m.nb + idx] * 0.5; r3 += s.Fvb[2 * m.nb + idx] * 0.5;
+        const double w = k.axi ? 0.5 * m.v_r[v] : 0.5;
+        r1 += s.Fvb[idx] * w; r2 += s.Fvb[m.nb + idx] * w; r3 += s.Fvb[2 * m.nb + idx] * w;
       }
     }
     // strong conditions: compute_residual_norm zeroes the no-slip momentum residual
@@ -451,7 +461,7 @@ __global__ void __launch_bounds__(kTileThreads, (FLUX == FLUX_TECNO_ROE || FLUX 
         nrm[0] = a0 * a0 * w; nrm[1] = a1 * a1 * w; nrm[2] = a2 * a2 * w; nrm[3] = a3 * a3 * w;
       }
       double dtv = (ctl.time_mode == 1 || ctl.time_step > 0.0) ? sc->dt_global : dtl;
-      double factor = dtv / (1.0 * area);
+      double factor = dtv / (vertex_radius(k, m, v) * area);
       Cons c = rk_stage(k, ctl, s, nv, v, r, q0, uo, factor, r0, r1, r2, r3);
       Prim q = con2prim(k, c);
       Ent e = prim2ent(k, q);

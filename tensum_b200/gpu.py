@@ -23,6 +23,7 @@ EXPORTS = ["tg_create", "tg_destroy", "tg_last_error", "tg_abi_version", "tg_set
            "tg_moments_merge", "tg_moments_merge_device", "tg_moments_finalize", "tg_forces", "tg_update_parameters",
            "tg_output_begin", "tg_output_wait"]
 
+ABI_VERSION = 3        # TG_ABI_VERSION of include/tensum_gpu.h
 PHASE = {"gradient": 0, "flux": 1, "update": 2, "dt": 3, "step": 4}
 QUERY = {"n_vertex": 0, "n_edge": 1, "n_bface": 2, "kernels_per_step": 3, "device_bytes": 4, "kernels_per_flux": 5}
 
@@ -79,6 +80,9 @@ def load():
         f = getattr(L, name)
         if name not in ("tg_last_error", "tg_abi_version"):
             f.restype = i
+    if L.tg_abi_version() != ABI_VERSION:
+        raise OSError(f"{LIB_PATH} has ABI version {L.tg_abi_version()}, this binding needs {ABI_VERSION}; "
+                      "rebuild it with `python -m tensum_b200.build`")
     _lib = L
     return L
 

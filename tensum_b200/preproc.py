@@ -54,6 +54,10 @@ class Geometry:
     dcarea: np.ndarray        # (V,) dual area (periodic-summed)
     mcarea: np.ndarray        # (V,) median area (periodic-summed)
     periodic_sets: list
+    # axisymmetric radii (src/grid_preproc.cc:750-777); None for a planar mesh
+    vertex_radius: np.ndarray | None = None   # (V,) vertex x
+    face_radius: np.ndarray | None = None     # (F,) face centre x
+    cell_radius: np.ndarray | None = None     # (C,) cell centre x (dual vertex)
 
     @property
     def n_vertex(self):
@@ -189,9 +193,10 @@ def _polygon_dual_areas(x, y, cells, cen, V):
     return dc
 
 
-def preprocess(mesh: TriMesh, periodic_types=None, cell: str = "median") -> Geometry:
-    """Dual-mesh preprocessing of a single-partition mesh (2D, radius = 1),
-    median or Voronoi dual cells (the grid section's ``cell`` entry).
+def preprocess(mesh: TriMesh, periodic_types=None, cell: str = "median", axisymmetric: bool = False) -> Geometry:
+    """Dual-mesh preprocessing of a single-partition mesh, median or Voronoi
+    dual cells (the grid section's ``cell`` entry), planar (radius 1) or
+    axisymmetric (the reference's -axi: radius = x, src/grid_preproc.cc:750-777).
 
     ``periodic_types``: boundary tags whose BC is ``periodic``.  Faces with
     such a tag keep their part-file periodic flag; all others are marked
@@ -297,9 +302,13 @@ def preprocess(mesh: TriMesh, periodic_types=None, cell: str = "median") -> Geom
         return np.stack([y[a] - y[b], -(x[a] - x[b])], 1)
     cnormal = np.stack([drn(c1, c2), drn(c2, c0), drn(c0, c1)], 1)
 
+    radii = {}
+    if axisymmetric:
+        radii = dict(vertex_radius=x.copy(), face_radius=mid(fv[:, 0], fv[:, 1])[:, 0].copy(),
+                     cell_radius=cen[:, 0].copy())
     return Geometry(coords=coords, cells=cells, cell_normal=cnormal, cell_area=area,
                     face_vertex=fv, face_type=ftype, face_normal=fnormal, face_measure=fmeasure,
                     face_lcell=flc, face_rcell=frc,
                     bface_vertex=bv, bface_type=bfaces[:, 2].copy(), bface_normal=bn,
                     bface_measure=bmeasure, bface_lcell=blc, bface_periodic=bper,
-                    dcarea=dc, mcarea=mc, periodic_sets=[list(s) for s in mesh.periodic_sets])
+                    dcarea=dc, mcarea=mc, periodic_sets=[list(s) for s in mesh.periodic_sets], **radii)

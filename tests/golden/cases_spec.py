@@ -1,6 +1,8 @@
 """Recipes of the golden-fixture cases (shared by the generator and the tests)."""
 from __future__ import annotations
 
+import dataclasses
+
 import numpy as np
 
 from tensum_b200 import cases, mesh as M
@@ -55,6 +57,11 @@ CASES = {
     "sq_roe_minmod_voronoi": _sq("kepes_tecno_roe", "minmod", cell="voronoi"),
     "sq_kepec_voronoi_long": _sq("kepec", "first", n=17, seed=13, steps=40, dump=0, cell="voronoi"),
     "cyl_ns_voronoi": _cyl("kepes_tecno_roe", "minmod", "ns", cell="voronoi", forces={"cyl": [1]}),
+    "sq_roe_minmod_axi": _sq("kepes_tecno_roe", "minmod", axi_shift=10.0),
+    "sq_kepec_axi_long": _sq("kepec", "first", n=17, seed=17, steps=40, dump=0, axi_shift=10.0),
+    "cyl_ns_axi": _cyl("kepes_tecno_roe", "minmod", "ns", axi_shift=50.0, forces={"cyl": [1]}),
+    "cyl_slip_axi_voronoi": _cyl("kepes_tecno_rusanov", "minmod", "euler", bc="slip", axi_shift=50.0,
+                                 cell="voronoi"),
 }
 
 
@@ -104,6 +111,10 @@ def build_case(spec: dict):
         cfg["bc_scheme"] = spec["bc_scheme"]
     if "cell" in spec:
         cfg["cell"] = spec["cell"]
+    if spec.get("axi_shift"):
+        # axisymmetric: radius = x, so the mesh is moved to x > 0 (the state moves with it)
+        m = dataclasses.replace(m, coords=m.coords + np.array([spec["axi_shift"], 0.0]), name=m.name + "_axi")
+        cfg["axisymmetric"] = True
     return m, cfg, prim0
 
 

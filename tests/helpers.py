@@ -32,3 +32,9 @@ def rel_l2(a, b):
     b = np.asarray(b, np.float64).ravel()
     n = np.linalg.norm(b)
     return float(np.linalg.norm(a - b) / n) if n > 0 else float(np.linalg.norm(a - b))
+
+
+def geometry(mesh, cfg):
+    """The preprocessed geometry a fixture's configuration asks for (dual cell type, axisymmetry)."""
+    from tensum_b200 import preproc
+    return preproc.preprocess(mesh, cell=cfg.get("cell", "median"), axisymmetric=cfg.get("axisymmetric", False))

@@ -8,7 +8,7 @@ through FMA contraction, summation order and last-ulp log/sqrt differences.
 import numpy as np
 import pytest
 
-from tests.helpers import golden_names, load_golden, rel_l2
+from tests.helpers import geometry, golden_names, load_golden, rel_l2
 from tensum_b200 import abi, cases, gpu, preproc
 from tensum_b200 import mesh as M
 import oracle as O
@@ -21,7 +21,7 @@ TOL_STATE_LONG = 1e-10
 
 
 def make_solver(mesh, cfg):
-    g = preproc.preprocess(mesh, cell=cfg.get("cell", "median"))
+    g = geometry(mesh, cfg)
     P = abi.Problem(g, cfg)
     return gpu.Solver(P), P
 

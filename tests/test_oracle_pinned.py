@@ -7,7 +7,7 @@ gradients, residual, updated primitive state and residual norms -- is equal.
 import numpy as np
 import pytest
 
-from tests.helpers import golden_names, load_golden
+from tests.helpers import geometry, golden_names, load_golden
 from tensum_b200 import abi, preproc
 import oracle as O
 
@@ -15,7 +15,7 @@ import oracle as O
 @pytest.mark.parametrize("name", golden_names())
 def test_oracle_matches_reference_exactly(name):
     spec, mesh, cfg, prim0, d = load_golden(name)
-    g = preproc.preprocess(mesh, cell=cfg.get("cell", "median"))
+    g = geometry(mesh, cfg)
     o = O.Oracle(abi.Problem(g, cfg))
     o.set_prim(prim0)
     if spec["dump_steps"] == 0:
@@ -45,10 +45,11 @@ def test_oracle_matches_reference_exactly(name):
             assert np.array_equal(o.forces(cfg["forces"]).ravel(), d[f"s{s}_force"]), f"forces step {s}"
 
 
-@pytest.mark.parametrize("name", ["sq_roe_minmod", "cyl_ns", "sq_roe_minmod_voronoi", "cyl_ns_voronoi"])
+@pytest.mark.parametrize("name", ["sq_roe_minmod", "cyl_ns", "sq_roe_minmod_voronoi", "cyl_ns_voronoi",
+                                  "cyl_ns_axi", "cyl_slip_axi_voronoi"])
 def test_geometry_matches_reference_exactly(name):
     spec, mesh, cfg, prim0, d = load_golden(name)
-    g = preproc.preprocess(mesh, cell=cfg.get("cell", "median"))
+    g = geometry(mesh, cfg)
     faces = d["faces"].reshape(-1, 8)
     assert np.array_equal(faces[:, :2].astype(int), g.face_vertex)
     assert np.array_equal(faces[:, 2].astype(int), g.face_type)
@@ -60,3 +61,7 @@ def test_geometry_matches_reference_exactly(name):
     assert np.array_equal(d["cell_area"], g.cell_area)
     assert np.array_equal(d["dcarea"], g.dcarea)
     assert np.array_equal(d["mcarea"], g.mcarea)
+    if cfg.get("axisymmetric"):   # vertex, face and cell radii (src/grid_preproc.cc:750-777)
+        assert np.array_equal(d["vradius"], g.vertex_radius)
+        assert np.array_equal(d["fradius"], g.face_radius)
+        assert np.array_equal(d["cradius"], g.cell_radius)
