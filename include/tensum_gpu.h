@@ -197,6 +197,18 @@ int tg_abi_version(void);
 /* primitive[] <- prim_aos (T,p,u,v,w per vertex: the PrimVar layout of src/primvar.h:17-18),
  * then entropy_var = prim2ent(primitive) (src/fv.cc:392-393).  Resets time to t0. */
 tg_status tg_set_state(tg_handle* h, const double* prim_aos, int n_vertex, double t0);
+/* Queue a new state (PrimVar records in the caller's order, from PINNED host
+ * memory, starting at time t0) and return at once: its copy to the device runs
+ * on a side stream while the handle keeps working, and the next tg_step or
+ * tg_advance takes it in before its first step, exactly as tg_set_state would
+ * (at most two states queued; they are taken in order).  The buffer must stay
+ * unchanged until that tg_step / tg_advance has returned.  A refused state
+ * (T <= 0 or p <= 0, src/fv.cc:388-389) is reported by that call as
+ * TG_INVALID_ARG, after its steps ran on the previous state.  tg_set_state
+ * drops queued states.  With tg_output_begin this lets a caller stream states
+ * in and results out while the device steps. */
+tg_status tg_set_state_async(tg_handle* h, const double* prim_aos, int n_vertex, double t0);
+
 /* prim_aos <- primitive[] (periodic copies receive their set's value). */
 tg_status tg_get_state(tg_handle* h, double* prim_aos, int n_vertex);
 

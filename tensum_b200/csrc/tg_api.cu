@@ -14,6 +14,7 @@
 #include <new>
 #include <string>
 #include <thread>
+#include <deque>
 #include <vector>
 
 #include "../../include/tensum_gpu.h"
@@ -78,6 +79,14 @@ struct tg_handle {
   cudaStream_t out_stream = nullptr;
   cudaEvent_t snap_ready = nullptr, out_done = nullptr;
   bool out_pending = false;
+  // asynchronous state input (tg_set_state_async): two staging buffers, a copy stream,
+  // and the queue of states (slot, start time) the next tg_step / tg_advance takes in order
+  double* in_stage[2] = {nullptr, nullptr};
+  cudaStream_t in_stream = nullptr;
+  cudaEvent_t in_done[2] = {nullptr, nullptr};
+  int in_next = 0;
+  std::deque<std::pair<int, double>> in_queue;
+  bool in_check = false;              // a queued state was taken in: its check is read after the step
   // Monte Carlo moments: per output instance three [nvar][nv] arrays (fm, sm, m2)
   int mom_ninst = 0, mom_extras = 0, mom_nvar = 0;
   double* mom = nullptr;
@@ -414,6 +423,52 @@ tg_status read_scalars(tg_handle* h, Scalars* out) {
   return sync(h);
 }
 
+// Step bookkeeping of a state that starts at time t0 (FiniteVolume::initialize_sample_run).
+Scalars fresh_scalars(const tg_handle* h, double t0) {
+  Scalars s;
+  std::memset(&s, 0, sizeof(s));
+  s.elapsed = t0;
+  s.rtotal = 1.0e20;
+  s.rtotal0 = 1.0;
+  s.counter = 1;
+  if (h->ctl.time_mode == 1) {
+    double dti = h->ctl.final_time / (h->ctl.ntinst - 1);
+    while (s.counter < h->ctl.ntinst - 1 && s.counter * dti <= t0) s.counter++;
+  }
+  s.dtmin_bits = 0x7ff0000000000000ull;
+  s.stop_counter = INT_MAX;
+  return s;
+}
+
+// The oldest state queued by tg_set_state_async becomes current, in stream order
+// after its copy, if k_state_check accepts it (read back by queued_input_refused).
+tg_status take_queued_input(tg_handle* h) {
+  if (h->in_queue.empty()) return TG_OK;
+  const int slot = h->in_queue.front().first;
+  const double t0 = h->in_queue.front().second;
+  h->in_queue.pop_front();
+  const int nv = h->L.nv;
+  TG_CUDA(h, cudaStreamWaitEvent(h->stream, h->in_done[slot], 0));
+  TG_CUDA(h, cudaMemsetAsync(h->bad, 0, sizeof(int), h->stream));
+  k_state_check<<<nblk(nv), kBlock, 0, h->stream>>>(nv, h->in_stage[slot], h->bad);
+  k_state_in<<<nblk(nv), kBlock, 0, h->stream>>>(nv, h->in_stage[slot], h->old_of_new, h->bad, h->sv.P);
+  k_prim2ent_checked<<<nblk(nv), kBlock, 0, h->stream>>>(h->prm, nv, h->sv.P, h->sv.W, h->bad);
+  k_scalars_set<<<1, 1, 0, h->stream>>>(h->sc, fresh_scalars(h, t0), h->bad);
+  h->in_check = true;
+  TG_CUDA(h, cudaGetLastError());
+  return TG_OK;
+}
+
+tg_status queued_input_refused(tg_handle* h) {
+  if (!h->in_check) return TG_OK;
+  h->in_check = false;
+  int bad = 0;
+  TG_CUDA(h, cudaMemcpy(&bad, h->bad, sizeof(int), cudaMemcpyDeviceToHost));
+  if (bad) return fail(h, TG_INVALID_ARG, "a state queued by tg_set_state_async was refused (T > 0 and p > 0, "
+                                           "src/fv.cc:388-389); the step ran on the previous state");
+  return TG_OK;
+}
+
 tg_status check_bad(tg_handle* h) {
   Scalars s;
   tg_status st = read_scalars(h, &s);
@@ -656,6 +711,10 @@ tg_status tg_destroy(tg_handle* h) {
   if (h->stage.slots) cudaFreeHost(h->stage.slots);
   if (h->raw_ready) cudaEventDestroy(h->raw_ready);
   if (h->out_stream) cudaStreamSynchronize(h->out_stream);
+  if (h->in_stream) cudaStreamSynchronize(h->in_stream);
+  for (int k = 0; k < 2; ++k)
+    if (h->in_done[k]) cudaEventDestroy(h->in_done[k]);
+  if (h->in_stream) cudaStreamDestroy(h->in_stream);
   if (h->snap_ready) cudaEventDestroy(h->snap_ready);
   if (h->out_done) cudaEventDestroy(h->out_done);
   if (h->out_stream) cudaStreamDestroy(h->out_stream);
@@ -668,6 +727,8 @@ tg_status tg_set_state(tg_handle* h, const double* prim, int n_vertex, double t0
   if (!h || !prim) return fail(h, TG_INVALID_ARG, "NULL argument");
   if (n_vertex != h->L.nv) return fail(h, TG_INVALID_ARG, "n_vertex does not match the mesh");
   const int nv = h->L.nv;
+  if (h->in_stream) TG_CUDA(h, cudaStreamSynchronize(h->in_stream));
+  h->in_queue.clear();                 // states queued by tg_set_state_async are dropped
   tg_status st = state_h2d(h, prim, 5 * (size_t)nv * sizeof(double));
   if (st != TG_OK) return st;
   TG_CUDA(h, cudaMemsetAsync(h->bad, 0, sizeof(int), h->stream));
@@ -678,20 +739,31 @@ tg_status tg_set_state(tg_handle* h, const double* prim, int n_vertex, double t0
   if ((st = sync(h)) != TG_OK) return st;
   if (bad) return fail(h, TG_INVALID_ARG, "state needs T > 0 and p > 0 (src/fv.cc:388-389)");
   k_prim2ent<<<nblk(nv), kBlock, 0, h->stream>>>(h->prm, nv, h->sv.P, h->sv.W);
-  Scalars s;
-  std::memset(&s, 0, sizeof(s));
-  s.elapsed = t0;
-  s.rtotal = 1.0e20;
-  s.rtotal0 = 1.0;
-  s.counter = 1;
-  if (h->ctl.time_mode == 1) {
-    double dti = h->ctl.final_time / (h->ctl.ntinst - 1);
-    while (s.counter < h->ctl.ntinst - 1 && s.counter * dti <= t0) s.counter++;
-  }
-  s.dtmin_bits = 0x7ff0000000000000ull;
-  s.stop_counter = INT_MAX;
+  const Scalars s = fresh_scalars(h, t0);
   TG_CUDA(h, cudaMemcpyAsync(h->sc, &s, sizeof(s), cudaMemcpyHostToDevice, h->stream));
   return sync(h);
+}
+
+tg_status tg_set_state_async(tg_handle* h, const double* prim, int n_vertex, double t0) {
+  if (!h || !prim) return fail(h, TG_INVALID_ARG, "NULL argument");
+  if (n_vertex != h->L.nv) return fail(h, TG_INVALID_ARG, "n_vertex does not match the mesh");
+  if (!host_pinned(prim)) return fail(h, TG_INVALID_ARG, "tg_set_state_async copies from pinned host memory");
+  if (h->in_queue.size() >= 2) return fail(h, TG_INVALID_ARG, "two states are queued already; step first");
+  const size_t bytes = 5 * (size_t)h->L.nv * sizeof(double);
+  tg_status st;
+  if (!h->in_stream) {
+    for (int k = 0; k < 2; ++k)
+      if ((st = dev_alloc(h, 5 * (size_t)h->L.nv, &h->in_stage[k])) != TG_OK) return st;
+    TG_CUDA(h, cudaStreamCreateWithFlags(&h->in_stream, cudaStreamNonBlocking));
+    for (int k = 0; k < 2; ++k) TG_CUDA(h, cudaEventCreateWithFlags(&h->in_done[k], cudaEventDisableTiming));
+  }
+  // a slot is rewritten only after the step that took its previous state in has returned
+  const int slot = h->in_next;
+  h->in_next ^= 1;
+  TG_CUDA(h, cudaMemcpyAsync(h->in_stage[slot], prim, bytes, cudaMemcpyHostToDevice, h->in_stream));
+  TG_CUDA(h, cudaEventRecord(h->in_done[slot], h->in_stream));
+  h->in_queue.emplace_back(slot, t0);
+  return TG_OK;
 }
 
 tg_status tg_get_state(tg_handle* h, double* prim, int n_vertex) {
@@ -812,10 +884,12 @@ tg_status tg_step(tg_handle* h, int n_steps, double* info4) {
   if (n_steps < 0) return fail(h, TG_INVALID_ARG, "n_steps < 0");
   tg_status st = capture_step_graph(h);
   if (st != TG_OK) return st;
+  if ((st = take_queued_input(h)) != TG_OK) return st;
   for (int i = 0; i < n_steps; ++i) TG_CUDA(h, cudaGraphLaunch(h->graph_exec, h->stream));
   Scalars s;
   st = read_scalars(h, &s);
   if (st != TG_OK) return st;
+  if ((st = queued_input_refused(h)) != TG_OK) return st;
   if (info4) { info4[0] = s.elapsed; info4[1] = s.dt_global; info4[2] = s.rtotal; info4[3] = (double)s.iter; }
   if (s.bad) return fail(h, TG_BAD_STATE, "non-finite or non-positive state produced by an update");
   return TG_OK;
@@ -854,10 +928,12 @@ tg_status tg_advance(tg_handle* h, int instance, long max_steps, double* info5) 
   if (max_steps < 0) return fail(h, TG_INVALID_ARG, "max_steps < 0");
   tg_status st = capture_step_graph(h);
   if (st != TG_OK) return st;
+  if ((st = take_queued_input(h)) != TG_OK) return st;
   int stop = instance;
   TG_CUDA(h, cudaMemcpyAsync(&h->sc->stop_counter, &stop, sizeof(int), cudaMemcpyHostToDevice, h->stream));
   Scalars s;
   if ((st = read_scalars(h, &s)) != TG_OK) return st;
+  if ((st = queued_input_refused(h)) != TG_OK) return st;
   long launched = 0;
   while (launched < max_steps && !s.bad && s.counter <= instance && !run_over(h, s)) {
     const long chunk = std::min<long>(16, max_steps - launched);

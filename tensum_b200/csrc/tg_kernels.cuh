@@ -157,6 +157,21 @@ __global__ void k_state_out(int nv, const double* __restrict__ P, const int* __r
   q[0] = P[i]; q[1] = P[3 * (size_t)nv + i]; q[2] = P[nv + i]; q[3] = P[2 * (size_t)nv + i]; q[4] = 0.0;
 }
 
+// A state handed in asynchronously (tg_set_state_async) becomes current only if
+// k_state_check accepted it: its entropy variables and fresh step bookkeeping.
+__global__ void k_prim2ent_checked(Params k, int nv, const double* __restrict__ P, double* __restrict__ W,
+                                   const int* __restrict__ bad) {
+  int i = blockIdx.x * blockDim.x + threadIdx.x;
+  if (i >= nv || *bad) return;
+  Ent e = prim2ent(k, load_prim(P, nv, i));
+  W[i] = e.f; W[nv + i] = e.vx; W[2 * nv + i] = e.vy; W[3 * nv + i] = e.l;
+}
+
+__global__ void k_scalars_set(Scalars* sc, Scalars s0, const int* __restrict__ bad) {
+  if (*bad) return;
+  *sc = s0;
+}
+
 // Device gradients G (V1, V2, V3, V5) x (x, y) -> the reference's dE records,
 // 5 variables x (x, y, z) per vertex in the caller's order (src/fv.h:148),
 // zero for the z components and for the fourth (z-momentum) variable.

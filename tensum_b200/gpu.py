@@ -21,7 +21,7 @@ EXPORTS = ["tg_create", "tg_destroy", "tg_last_error", "tg_abi_version", "tg_set
            "tg_residual_norm", "tg_end_step", "tg_step", "tg_global", "tg_stream", "tg_time_phase", "tg_query",
            "tg_advance", "tg_moments_init", "tg_moments_increment", "tg_moments_get", "tg_moments_export",
            "tg_moments_merge", "tg_moments_merge_device", "tg_moments_finalize", "tg_forces", "tg_update_parameters",
-           "tg_output_begin", "tg_output_wait"]
+           "tg_output_begin", "tg_output_wait", "tg_set_state_async"]
 
 ABI_VERSION = 3        # TG_ABI_VERSION of include/tensum_gpu.h
 PHASE = {"gradient": 0, "flux": 1, "update": 2, "dt": 3, "step": 4}
@@ -69,6 +69,7 @@ def load():
     L.tg_update_parameters.argtypes = [vp, vp, vp]
     L.tg_output_begin.argtypes = [vp, dp, dp, i]
     L.tg_output_wait.argtypes = [vp]
+    L.tg_set_state_async.argtypes = [vp, dp, i, C.c_double]
     L.tg_moments_init.argtypes = [vp, i, i]
     L.tg_moments_increment.argtypes = [vp, i, C.c_long]
     L.tg_moments_get.argtypes = [vp, i, dp, dp, dp]
@@ -123,6 +124,14 @@ class Solver:
     def set_state(self, prim: np.ndarray, t0: float = 0.0):
         prim = np.ascontiguousarray(prim, np.float64)
         self._chk(self.L.tg_set_state(self.h, _d(prim), self.nv, t0))
+
+    def set_state_async(self, prim: np.ndarray, t0: float = 0.0):
+        """Queue a state from pinned host memory (see output_buffers); the next
+        step() / advance() takes it in.  Keep the buffer unchanged until then."""
+        if prim.dtype != np.float64 or not prim.flags.c_contiguous or prim.shape != (self.nv, 5):
+            raise ValueError("prim must be a C-contiguous float64 array of shape (n_vertex, 5)")
+        self._in_keep = getattr(self, "_in_keep", [])[-1:] + [prim]
+        self._chk(self.L.tg_set_state_async(self.h, _d(prim), self.nv, t0))
 
     def get_state(self, out: np.ndarray | None = None) -> np.ndarray:
         """The state as (n_vertex, 5) PrimVar records; written into `out` when given
