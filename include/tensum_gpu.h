@@ -419,6 +419,38 @@ typedef enum {
 } tg_batch_query_key;
 tg_status tg_batch_query(tg_batch* b, int key, double* out);
 
+/* ---- parameter-file expressions evaluated on the device (no counterpart in
+ *      the reference, which evaluates its fparser expressions on the host, per
+ *      vertex: src/ic.h:79-104, src/bc.h:568-654) ----------------------------- */
+/* An expression in the parameter file's syntax (fparser: + - * / % ^, unary -
+ * and !, comparisons with fparser's 1e-12 tolerance, & |, the real functions,
+ * if(c, a, b)) of x, y, t with pi, the named constants given here (the
+ * constants section) and pert(type, x, y, p) (src/perturb.cc:16-208), compiled
+ * once on the host.  tg_expr_eval evaluates it on the host for one point and
+ * one sample's random numbers (the rnd-file row, src/fv.cc:502-551). */
+typedef struct tg_expr tg_expr;
+tg_status tg_expr_create(const char* text, int n_const, const char* const* names, const double* values,
+                         tg_expr** out);
+tg_status tg_expr_destroy(tg_expr* e);
+const char* tg_expr_last_error(void);
+tg_status tg_expr_eval(const tg_expr* e, double x, double y, double t, const double* rnd, int n_rnd, double* out);
+/* InitialCondition::value on the device: fields[0..4] give temperature,
+ * x/y/z velocity and pressure (a NULL z velocity is 0); the state of every
+ * vertex is evaluated at t = 0 with the random numbers rnd[0 .. n_rnd) and
+ * then taken in as tg_set_state takes a state (checked, clocks at t0). */
+tg_status tg_set_state_expr(tg_handle* h, const tg_expr* const* fields, const double* rnd, int n_rnd, double t0);
+/* The same for every sample of a level, sample s with random numbers
+ * rnd_rows[s * n_rnd ..]; clocks restart at t = 0.  A sample whose state has
+ * T <= 0 or p <= 0 somewhere makes the call fail (TG_INVALID_ARG) and leaves
+ * the level's states undefined until they are set again. */
+tg_status tg_batch_set_state_expr(tg_batch* b, int level, const tg_expr* const* fields, const double* rnd_rows,
+                                  int n_rnd);
+/* Per-sample boundary values of the faces with boundary tag `tag`
+ * (BoundaryCondition expressions evaluated at each face vertex at time t):
+ * fields as above, a NULL entry keeps that variable's current values. */
+tg_status tg_batch_set_bc_expr(tg_batch* b, int level, int tag, const tg_expr* const* fields, const double* rnd_rows,
+                               int n_rnd, double t);
+
 /* ---- surrogate network (no counterpart in the reference) ---------------- */
 /* The multilayer perceptron din -> 64 -> 64 -> 64 -> dout (GELU) used as the
  * control variate of the multi-fidelity Monte Carlo estimator: FP32 training

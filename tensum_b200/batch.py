@@ -48,11 +48,13 @@ def _lib():
         L.tg_batch_set_parameters.argtypes = [vp, i, dp, dp]
         L.tg_batch_set_uniform.argtypes = [vp, i, dp]
         L.tg_batch_forces.argtypes = [vp, i, i, ip, ip, dp]
+        L.tg_batch_set_state_expr.argtypes = [vp, i, C.POINTER(vp), dp, i]
+        L.tg_batch_set_bc_expr.argtypes = [vp, i, i, C.POINTER(vp), dp, i, C.c_double]
         for n in ("tg_batch_create", "tg_batch_destroy", "tg_batch_set_state", "tg_batch_get_state",
                   "tg_batch_set_kh", "tg_batch_advance", "tg_batch_clock", "tg_batch_moments",
                   "tg_batch_set_shape", "tg_batch_tune", "tg_batch_time_steps", "tg_batch_stream",
                   "tg_batch_query", "tg_batch_integrals", "tg_batch_set_parameters", "tg_batch_set_uniform",
-                  "tg_batch_forces"):
+                  "tg_batch_forces", "tg_batch_set_state_expr", "tg_batch_set_bc_expr"):
             getattr(L, n).restype = i
         _bound = True
     return L
@@ -129,6 +131,23 @@ class Batch:
         prim = np.ascontiguousarray(prim, np.float64)
         assert prim.shape == (self.S[level], 5)
         self._chk(self.L.tg_batch_set_uniform(self.h, level, _d(prim)))
+
+    def set_state_expr(self, level: int, fields, rnd_rows=None):
+        """Every sample's initial state from expressions (gpu.expr_fields), sample s
+        with random numbers rnd_rows[s], evaluated on the device."""
+        S = self.S[level]
+        r = np.ascontiguousarray(rnd_rows if rnd_rows is not None else np.zeros((S, 0)), np.float64)
+        assert r.shape[0] == S
+        self._chk(self.L.tg_batch_set_state_expr(self.h, level, gpu.expr_array(fields), _d(r) if r.size else None,
+                                                 r.shape[1]))
+
+    def set_bc_expr(self, level: int, tag: int, fields, rnd_rows=None, t: float = 0.0):
+        """Per-sample boundary values of the faces of `tag` from expressions (None keeps a variable)."""
+        S = self.S[level]
+        r = np.ascontiguousarray(rnd_rows if rnd_rows is not None else np.zeros((S, 0)), np.float64)
+        assert r.shape[0] == S
+        self._chk(self.L.tg_batch_set_bc_expr(self.h, level, tag, gpu.expr_array(fields), _d(r) if r.size else None,
+                                              r.shape[1], t))
 
     def forces(self, level: int, forces: dict) -> np.ndarray:
         """(S, n_forces, 4): compute_forces of every sample for {name: [face tags]}."""

@@ -18,7 +18,7 @@ CSRC = os.path.join(HERE, "csrc")
 LIB = os.path.join(HERE, "libtensum_b200.so")
 ARCH = ["-gencode", "arch=compute_100a,code=sm_100a"]
 
-SOURCES = ["tg_api.cu", "tg_mesh.cc", "tg_noalloc.cu", "tg_batch.cu", "tg_mlp.cu"]
+SOURCES = ["tg_api.cu", "tg_mesh.cc", "tg_noalloc.cu", "tg_batch.cu", "tg_mlp.cu", "tg_expr.cu"]
 
 
 def nvcc() -> str:

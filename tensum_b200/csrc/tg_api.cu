@@ -19,6 +19,7 @@
 
 #include "../../include/tensum_gpu.h"
 #include "tg_kernels.cuh"
+#include "tg_expr.cuh"
 #include "tg_tiles.cuh"
 #include "tg_mesh.h"
 
@@ -502,6 +503,42 @@ void enqueue_phase(tg_handle* h, int phase) {
   }
 }
 
+// InitialCondition::value (src/ic.h:79-104) at every vertex, on the device, written
+// as PrimVar records in the caller's order into the state staging buffer.
+__global__ void k_state_expr(int nv, const double* __restrict__ x, const double* __restrict__ y,
+                             const int* __restrict__ old_of_new, expr::Field5 f, const double* __restrict__ rnd,
+                             int nrnd, double* __restrict__ raw, int* __restrict__ err) {
+  const int i = blockIdx.x * blockDim.x + threadIdx.x;
+  if (i >= nv) return;
+  int e = 0;
+  const double xv = x[i], yv = y[i];
+  double* q = raw + 5 * (size_t)old_of_new[i];
+  q[0] = expr::eval5(f, 0, xv, yv, 0.0, rnd, nrnd, &e);   // temperature
+  q[2] = expr::eval5(f, 1, xv, yv, 0.0, rnd, nrnd, &e);   // x velocity
+  q[3] = expr::eval5(f, 2, xv, yv, 0.0, rnd, nrnd, &e);   // y velocity
+  q[4] = expr::eval5(f, 3, xv, yv, 0.0, rnd, nrnd, &e);   // z velocity
+  q[1] = expr::eval5(f, 4, xv, yv, 0.0, rnd, nrnd, &e);   // pressure
+  if (e) atomicOr(err, e);
+}
+
+// The state in the staging buffer (PrimVar records, caller's order) becomes
+// current if every vertex passes the reference's check, with fresh bookkeeping.
+tg_status take_raw_state(tg_handle* h, double t0) {
+  const int nv = h->L.nv;
+  tg_status st;
+  TG_CUDA(h, cudaMemsetAsync(h->bad, 0, sizeof(int), h->stream));
+  k_state_check<<<nblk(nv), kBlock, 0, h->stream>>>(nv, h->raw, h->bad);
+  k_state_in<<<nblk(nv), kBlock, 0, h->stream>>>(nv, h->raw, h->old_of_new, h->bad, h->sv.P);
+  int bad = 0;
+  TG_CUDA(h, cudaMemcpyAsync(&bad, h->bad, sizeof(int), cudaMemcpyDeviceToHost, h->stream));
+  if ((st = sync(h)) != TG_OK) return st;
+  if (bad) return fail(h, TG_INVALID_ARG, "state needs T > 0 and p > 0 (src/fv.cc:388-389)");
+  k_prim2ent<<<nblk(nv), kBlock, 0, h->stream>>>(h->prm, nv, h->sv.P, h->sv.W);
+  const Scalars s = fresh_scalars(h, t0);
+  TG_CUDA(h, cudaMemcpyAsync(h->sc, &s, sizeof(s), cudaMemcpyHostToDevice, h->stream));
+  return sync(h);
+}
+
 extern "C" {
 
 int tg_abi_version(void) { return TG_ABI_VERSION; }
@@ -726,23 +763,49 @@ tg_status tg_destroy(tg_handle* h) {
 tg_status tg_set_state(tg_handle* h, const double* prim, int n_vertex, double t0) {
   if (!h || !prim) return fail(h, TG_INVALID_ARG, "NULL argument");
   if (n_vertex != h->L.nv) return fail(h, TG_INVALID_ARG, "n_vertex does not match the mesh");
-  const int nv = h->L.nv;
   if (h->in_stream) TG_CUDA(h, cudaStreamSynchronize(h->in_stream));
   h->in_queue.clear();                 // states queued by tg_set_state_async are dropped
-  tg_status st = state_h2d(h, prim, 5 * (size_t)nv * sizeof(double));
+  tg_status st = state_h2d(h, prim, 5 * (size_t)h->L.nv * sizeof(double));
   if (st != TG_OK) return st;
-  TG_CUDA(h, cudaMemsetAsync(h->bad, 0, sizeof(int), h->stream));
-  k_state_check<<<nblk(nv), kBlock, 0, h->stream>>>(nv, h->raw, h->bad);
-  k_state_in<<<nblk(nv), kBlock, 0, h->stream>>>(nv, h->raw, h->old_of_new, h->bad, h->sv.P);
-  int bad = 0;
-  TG_CUDA(h, cudaMemcpyAsync(&bad, h->bad, sizeof(int), cudaMemcpyDeviceToHost, h->stream));
-  if ((st = sync(h)) != TG_OK) return st;
-  if (bad) return fail(h, TG_INVALID_ARG, "state needs T > 0 and p > 0 (src/fv.cc:388-389)");
-  k_prim2ent<<<nblk(nv), kBlock, 0, h->stream>>>(h->prm, nv, h->sv.P, h->sv.W);
-  const Scalars s = fresh_scalars(h, t0);
-  TG_CUDA(h, cudaMemcpyAsync(h->sc, &s, sizeof(s), cudaMemcpyHostToDevice, h->stream));
-  return sync(h);
+  return take_raw_state(h, t0);
 }
+
+tg_status tg_set_state_expr(tg_handle* h, const tg_expr* const* fields, const double* rnd, int n_rnd, double t0) {
+  if (!h || !fields) return fail(h, TG_INVALID_ARG, "NULL argument");
+  for (int c = 0; c < 5; ++c)
+    if (c != 3 && !fields[c]) return fail(h, TG_INVALID_ARG, "temperature, velocity and pressure expressions are needed");
+  if (n_rnd < 0 || (n_rnd > 0 && !rnd)) return fail(h, TG_INVALID_ARG, "bad random numbers");
+  if (h->in_stream) TG_CUDA(h, cudaStreamSynchronize(h->in_stream));
+  h->in_queue.clear();
+  std::vector<int> code, off;
+  std::vector<double> k;
+  expr::pack5(fields, nullptr, code, off, k);
+  int *dcode = nullptr, *doff = nullptr, *derr = nullptr;
+  double *dk = nullptr, *drnd = nullptr;
+  cudaError_t e = cudaMalloc((void**)&dcode, code.size() * sizeof(int));
+  if (e == cudaSuccess) e = cudaMalloc((void**)&doff, off.size() * sizeof(int));
+  if (e == cudaSuccess) e = cudaMalloc((void**)&dk, std::max<size_t>(1, k.size()) * sizeof(double));
+  if (e == cudaSuccess) e = cudaMalloc((void**)&drnd, std::max(1, n_rnd) * sizeof(double));
+  if (e == cudaSuccess) e = cudaMalloc((void**)&derr, sizeof(int));
+  if (e == cudaSuccess) e = cudaMemcpyAsync(dcode, code.data(), code.size() * sizeof(int), cudaMemcpyHostToDevice, h->stream);
+  if (e == cudaSuccess) e = cudaMemcpyAsync(doff, off.data(), off.size() * sizeof(int), cudaMemcpyHostToDevice, h->stream);
+  if (e == cudaSuccess && !k.empty()) e = cudaMemcpyAsync(dk, k.data(), k.size() * sizeof(double), cudaMemcpyHostToDevice, h->stream);
+  if (e == cudaSuccess && n_rnd > 0) e = cudaMemcpyAsync(drnd, rnd, n_rnd * sizeof(double), cudaMemcpyHostToDevice, h->stream);
+  if (e == cudaSuccess) e = cudaMemsetAsync(derr, 0, sizeof(int), h->stream);
+  int err = 0;
+  if (e == cudaSuccess) {
+    const int nv = h->L.nv;
+    k_state_expr<<<nblk(nv), kBlock, 0, h->stream>>>(nv, h->tv.x, h->tv.y, h->old_of_new, expr::Field5{dcode, doff, dk},
+                                                     drnd, n_rnd, h->raw, derr);
+    e = cudaMemcpyAsync(&err, derr, sizeof(int), cudaMemcpyDeviceToHost, h->stream);
+    if (e == cudaSuccess) e = cudaStreamSynchronize(h->stream);
+  }
+  cudaFree(dcode); cudaFree(doff); cudaFree(dk); cudaFree(drnd); cudaFree(derr);
+  if (e != cudaSuccess) return fail(h, TG_CUDA_ERROR, cudaGetErrorString(e));
+  if (err) return fail(h, TG_INVALID_ARG, "pert: unknown type or random-number index out of range");
+  return take_raw_state(h, t0);
+}
+
 
 tg_status tg_set_state_async(tg_handle* h, const double* prim, int n_vertex, double t0) {
   if (!h || !prim) return fail(h, TG_INVALID_ARG, "NULL argument");

@@ -603,6 +603,89 @@ tg_status tg_batch_forces(tg_batch* b, int level, int n_forces, const int* n_tag
   return TG_OK;
 }
 
+namespace {
+
+// Device copies of five packed programs and the samples' random numbers.
+struct ExprUpload {
+  int *code = nullptr, *off = nullptr, *err = nullptr;
+  double *k = nullptr, *rnd = nullptr;
+  ~ExprUpload() { cudaFree(code); cudaFree(off); cudaFree(err); cudaFree(k); cudaFree(rnd); }
+  cudaError_t load(const tg_expr* const* fields, const double* rnd_rows, size_t n_rnd_total, cudaStream_t st) {
+    std::vector<int> c, o;
+    std::vector<double> kk;
+    expr::pack5(fields, nullptr, c, o, kk);
+    cudaError_t e = cudaMalloc((void**)&code, c.size() * sizeof(int));
+    if (e == cudaSuccess) e = cudaMalloc((void**)&off, o.size() * sizeof(int));
+    if (e == cudaSuccess) e = cudaMalloc((void**)&k, std::max<size_t>(1, kk.size()) * sizeof(double));
+    if (e == cudaSuccess) e = cudaMalloc((void**)&rnd, std::max<size_t>(1, n_rnd_total) * sizeof(double));
+    if (e == cudaSuccess) e = cudaMalloc((void**)&err, sizeof(int));
+    if (e == cudaSuccess) e = cudaMemcpyAsync(code, c.data(), c.size() * sizeof(int), cudaMemcpyHostToDevice, st);
+    if (e == cudaSuccess) e = cudaMemcpyAsync(off, o.data(), o.size() * sizeof(int), cudaMemcpyHostToDevice, st);
+    if (e == cudaSuccess && !kk.empty()) e = cudaMemcpyAsync(k, kk.data(), kk.size() * sizeof(double), cudaMemcpyHostToDevice, st);
+    if (e == cudaSuccess && n_rnd_total) e = cudaMemcpyAsync(rnd, rnd_rows, n_rnd_total * sizeof(double), cudaMemcpyHostToDevice, st);
+    if (e == cudaSuccess) e = cudaMemsetAsync(err, 0, sizeof(int), st);
+    return e;
+  }
+  expr::Field5 view() const { return expr::Field5{code, off, k}; }
+};
+
+}  // namespace
+
+tg_status tg_batch_set_state_expr(tg_batch* b, int level, const tg_expr* const* fields, const double* rnd_rows,
+                                  int n_rnd) {
+  if (!b || !fields || level < 0 || level >= b->nlev) return bfail(b, TG_INVALID_ARG, "bad level or NULL fields");
+  for (int c = 0; c < 5; ++c)
+    if (c != 3 && !fields[c]) return bfail(b, TG_INVALID_ARG, "temperature, velocity and pressure expressions are needed");
+  const Level& V = b->B.lev[level];
+  if (n_rnd < 0 || (n_rnd > 0 && !rnd_rows)) return bfail(b, TG_INVALID_ARG, "bad random numbers");
+  ExprUpload up;
+  cudaError_t e = up.load(fields, rnd_rows, (size_t)V.S * n_rnd, b->stream);
+  int err = 0;
+  if (e == cudaSuccess) {
+    const long long t = (long long)V.m.nv * V.S;
+    kb_ic_expr<<<(unsigned)((t + 255) / 256), 256, 0, b->stream>>>(V, b->prm, up.view(), up.rnd, n_rnd, up.err);
+    e = cudaMemcpyAsync(&err, up.err, sizeof(int), cudaMemcpyDeviceToHost, b->stream);
+    if (e == cudaSuccess) e = cudaStreamSynchronize(b->stream);
+  }
+  if (e != cudaSuccess) return bfail(b, TG_CUDA_ERROR, cudaGetErrorString(e));
+  if (err & 8) return bfail(b, TG_INVALID_ARG, "an initial state has T <= 0 or p <= 0 (src/fv.cc:388-389)");
+  if (err) return bfail(b, TG_INVALID_ARG, "pert: unknown type or random-number index out of range");
+  return reset_clock(b, level, 0, V.S);
+}
+
+tg_status tg_batch_set_bc_expr(tg_batch* b, int level, int tag, const tg_expr* const* fields, const double* rnd_rows,
+                               int n_rnd, double t) {
+  if (!b || !fields || level < 0 || level >= b->nlev) return bfail(b, TG_INVALID_ARG, "bad level or NULL fields");
+  const Level& V = b->B.lev[level];
+  const HostLayout& L = b->lh[level].L;
+  if (!V.bval) return bfail(b, TG_NOT_SUPPORTED, "a periodic Euler level has no boundary values");
+  if (n_rnd < 0 || (n_rnd > 0 && !rnd_rows)) return bfail(b, TG_INVALID_ARG, "bad random numbers");
+  int mask = 0;
+  for (int c = 0; c < 5; ++c) mask |= fields[c] ? (1 << c) : 0;
+  std::vector<int> btag(std::max(L.nb, 1), INT_MIN);
+  bool any = false;
+  for (size_t f = 0; f < L.rb_type.size(); ++f)
+    if (L.rb_dev[f] >= 0) { btag[L.rb_dev[f]] = L.rb_type[f]; any = any || L.rb_type[f] == tag; }
+  if (!any) return bfail(b, TG_INVALID_ARG, "no non-periodic boundary face has this tag");
+  ExprUpload up;
+  int* dtag = nullptr;
+  cudaError_t e = up.load(fields, rnd_rows, (size_t)V.S * n_rnd, b->stream);
+  if (e == cudaSuccess) e = cudaMalloc((void**)&dtag, btag.size() * sizeof(int));
+  if (e == cudaSuccess) e = cudaMemcpyAsync(dtag, btag.data(), btag.size() * sizeof(int), cudaMemcpyHostToDevice, b->stream);
+  int err = 0;
+  if (e == cudaSuccess) {
+    const long long n = 2LL * L.nb * V.S;
+    kb_bc_expr<<<(unsigned)((n + 255) / 256), 256, 0, b->stream>>>(V, up.view(), mask, dtag, tag, up.rnd, n_rnd, t,
+                                                                   up.err);
+    e = cudaMemcpyAsync(&err, up.err, sizeof(int), cudaMemcpyDeviceToHost, b->stream);
+    if (e == cudaSuccess) e = cudaStreamSynchronize(b->stream);
+  }
+  cudaFree(dtag);
+  if (e != cudaSuccess) return bfail(b, TG_CUDA_ERROR, cudaGetErrorString(e));
+  if (err) return bfail(b, TG_INVALID_ARG, "pert: unknown type or random-number index out of range");
+  return TG_OK;
+}
+
 tg_status tg_batch_set_kh(tg_batch* b, int level, const double* rows, int n_rnd) {
   if (!b || !rows || level < 0 || level >= b->nlev || n_rnd < 2 || n_rnd % 2)
     return bfail(b, TG_INVALID_ARG, "bad level, NULL rows or odd row length");

@@ -25,6 +25,7 @@
 
 #include <cstdint>
 
+#include "tg_expr.cuh"
 #include "tg_physics.cuh"
 
 namespace tg {
@@ -966,6 +967,57 @@ __global__ void __launch_bounds__(32 * VT) kb_forces(Level L, BParams k, const i
 #pragma unroll
     for (int c = 0; c < 4; ++c) out[((size_t)s * nf + f) * 4 + c] = acc[c];
   }
+}
+
+// Initial states from parameter-file expressions (InitialCondition::value,
+// src/ic.h:79-104) per (vertex, sample), sample s with random numbers
+// rnd[s * nrnd ..]; evaluated in FP64, stored as the FP32 record.  err: bit 8 a
+// state with T <= 0 or p <= 0 (or not finite), lower bits pert errors.
+__global__ void kb_ic_expr(Level L, BParams k, expr::Field5 f, const double* __restrict__ rnd, int nrnd,
+                           int* __restrict__ err) {
+  const long long t = blockIdx.x * (long long)blockDim.x + threadIdx.x;
+  if (t >= (long long)L.m.nv * L.S) return;
+  const int v = (int)(t / L.S), s = (int)(t % L.S);
+  const double x = L.m.x[v], y = L.m.y[v];
+  const double* row = rnd + (size_t)s * nrnd;
+  int e = 0;
+  const double T = expr::eval5(f, 0, x, y, 0.0, row, nrnd, &e);
+  const double u = expr::eval5(f, 1, x, y, 0.0, row, nrnd, &e);
+  const double vv = expr::eval5(f, 2, x, y, 0.0, row, nrnd, &e);
+  const double p = expr::eval5(f, 4, x, y, 0.0, row, nrnd, &e);
+  if (!(T > 0.0) || !(p > 0.0) || !isfinite(u) || !isfinite(vv) || !isfinite(T) || !isfinite(p)) e |= 8;
+  if (e) { atomicOr(err, e); return; }
+  const double g = (double)k.gamma;
+  const double rho = p / ((double)k.R * T);
+  const double beta = rho / (2.0 * p);
+  const double sent = log(p) - g * log(rho);
+  const double V1 = (g - sent) / (g - 1.0) - (u * u + vv * vv) * beta;
+  float* q = L.Q[0] + rows(v, kQ, L.P) + s;
+  q[0] = (float)u;
+  q[L.P] = (float)vv;
+  q[2 * L.P] = (float)p;
+  q[3 * L.P] = (float)V1;
+  q[4 * L.P] = (float)(-2.0 * beta);
+}
+
+// Per-sample boundary values of the faces of one boundary tag from expressions
+// (BoundaryCondition at each face vertex, time t): variable c of the record
+// (T, u, v, w, p) is written where bit c of mask is set.
+__global__ void kb_bc_expr(Level L, expr::Field5 f, int mask, const int* __restrict__ btag, int tag,
+                           const double* __restrict__ rnd, int nrnd, double t, int* __restrict__ err) {
+  const long long i = blockIdx.x * (long long)blockDim.x + threadIdx.x;
+  if (i >= 2LL * L.m.nb * L.S) return;
+  const int slot = (int)(i / L.S), s = (int)(i % L.S);
+  const int d = slot >> 1, q = slot & 1;
+  if (btag[d] != tag) return;
+  const int vtx = q ? L.m.b_v1[d] : L.m.b_v0[d];
+  const double x = L.m.x[vtx], y = L.m.y[vtx];
+  const double* row = rnd + (size_t)s * nrnd;
+  int e = 0;
+  float* val = L.bval + rows(d, 10, L.P) + 5 * q * L.P + s;
+  for (int c = 0; c < 5; ++c)
+    if ((mask >> c) & 1) val[c * L.P] = (float)expr::eval5(f, c, x, y, t, row, nrnd, &e);
+  if (e) atomicOr(err, e);
 }
 
 // Ensemble moments of one level at its current state, FP64: Welford mean and

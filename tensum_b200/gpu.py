@@ -21,7 +21,8 @@ EXPORTS = ["tg_create", "tg_destroy", "tg_last_error", "tg_abi_version", "tg_set
            "tg_residual_norm", "tg_end_step", "tg_step", "tg_global", "tg_stream", "tg_time_phase", "tg_query",
            "tg_advance", "tg_moments_init", "tg_moments_increment", "tg_moments_get", "tg_moments_export",
            "tg_moments_merge", "tg_moments_merge_device", "tg_moments_finalize", "tg_forces", "tg_update_parameters",
-           "tg_output_begin", "tg_output_wait", "tg_set_state_async"]
+           "tg_output_begin", "tg_output_wait", "tg_set_state_async", "tg_expr_create", "tg_expr_destroy",
+           "tg_expr_last_error", "tg_expr_eval", "tg_set_state_expr"]
 
 ABI_VERSION = 3        # TG_ABI_VERSION of include/tensum_gpu.h
 PHASE = {"gradient": 0, "flux": 1, "update": 2, "dt": 3, "step": 4}
@@ -70,6 +71,12 @@ def load():
     L.tg_output_begin.argtypes = [vp, dp, dp, i]
     L.tg_output_wait.argtypes = [vp]
     L.tg_set_state_async.argtypes = [vp, dp, i, C.c_double]
+    L.tg_expr_create.argtypes = [C.c_char_p, i, C.POINTER(C.c_char_p), dp, C.POINTER(vp)]
+    L.tg_expr_destroy.argtypes = [vp]
+    L.tg_expr_last_error.argtypes = []
+    L.tg_expr_last_error.restype = C.c_char_p
+    L.tg_expr_eval.argtypes = [vp, C.c_double, C.c_double, C.c_double, dp, i, dp]
+    L.tg_set_state_expr.argtypes = [vp, C.POINTER(vp), dp, i, C.c_double]
     L.tg_moments_init.argtypes = [vp, i, i]
     L.tg_moments_increment.argtypes = [vp, i, C.c_long]
     L.tg_moments_get.argtypes = [vp, i, dp, dp, dp]
@@ -79,7 +86,7 @@ def load():
     L.tg_moments_finalize.argtypes = [vp, i, C.c_long]
     for name in EXPORTS:
         f = getattr(L, name)
-        if name not in ("tg_last_error", "tg_abi_version"):
+        if name not in ("tg_last_error", "tg_abi_version", "tg_expr_last_error"):
             f.restype = i
     if L.tg_abi_version() != ABI_VERSION:
         raise OSError(f"{LIB_PATH} has ABI version {L.tg_abi_version()}, this binding needs {ABI_VERSION}; "
@@ -90,6 +97,53 @@ def load():
 
 def _d(a: np.ndarray):
     return a.ctypes.data_as(C.POINTER(C.c_double))
+
+
+class Expr:
+    """A parameter-file expression of (x, y, t) compiled for host and device
+    evaluation (tg_expr_*): fparser syntax, pi, the given named constants and
+    pert(type, x, y, p) over a sample's random numbers."""
+
+    def __init__(self, text: str, constants: dict | None = None):
+        self.L = load()
+        consts = dict(constants or {})
+        names = (C.c_char_p * max(1, len(consts)))(*[k.encode() for k in consts])
+        vals = np.array(list(consts.values()) or [0.0], np.float64)
+        h = C.c_void_p()
+        st = self.L.tg_expr_create(text.encode(), len(consts), names, _d(vals), C.byref(h))
+        if st != 0:
+            raise TensumError(st, self.L.tg_expr_last_error().decode())
+        self.h = h
+        self.text = text
+
+    def __del__(self):
+        try:
+            if getattr(self, "h", None):
+                self.L.tg_expr_destroy(self.h)
+                self.h = None
+        except Exception:
+            pass
+
+    def __call__(self, x: float, y: float, t: float = 0.0, rnd=None) -> float:
+        r = np.ascontiguousarray(rnd if rnd is not None else np.zeros(1), np.float64)
+        out = C.c_double()
+        st = self.L.tg_expr_eval(self.h, float(x), float(y), float(t), _d(r), 0 if rnd is None else r.size,
+                                 C.byref(out))
+        if st != 0:
+            raise TensumError(st, self.L.tg_expr_last_error().decode())
+        return out.value
+
+
+def expr_fields(ic: dict, constants: dict | None = None):
+    """Five Expr (temperature, x/y/z velocity, pressure; z velocity may be absent)
+    from {variable: expression} as the initial_condition section names them."""
+    names = ("temperature", "xvelocity", "yvelocity", "zvelocity", "pressure")
+    return [Expr(ic[n], constants) if n in ic else None for n in names]
+
+
+def expr_array(fields):
+    vp = C.c_void_p
+    return (vp * 5)(*[f.h if f is not None else None for f in fields])
 
 
 class Solver:
@@ -132,6 +186,12 @@ class Solver:
             raise ValueError("prim must be a C-contiguous float64 array of shape (n_vertex, 5)")
         self._in_keep = getattr(self, "_in_keep", [])[-1:] + [prim]
         self._chk(self.L.tg_set_state_async(self.h, _d(prim), self.nv, t0))
+
+    def set_state_expr(self, fields, rnd=None, t0: float = 0.0):
+        """The initial condition evaluated on the device from expr_fields(...)
+        with one sample's random numbers, taken in as set_state takes a state."""
+        r = np.ascontiguousarray(rnd if rnd is not None else np.zeros(1), np.float64)
+        self._chk(self.L.tg_set_state_expr(self.h, expr_array(fields), _d(r), 0 if rnd is None else r.size, t0))
 
     def get_state(self, out: np.ndarray | None = None) -> np.ndarray:
         """The state as (n_vertex, 5) PrimVar records; written into `out` when given

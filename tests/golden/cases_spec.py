@@ -166,3 +166,29 @@ def build_output_case(spec: dict):
     cfg = dict(cfg, final_time=spec["final_time"], time_stamps=spec["time_stamps"],
                variables=list(spec.get("variables", [])), surfaces=list(spec.get("surfaces", [])))
     return m, cfg, prim0
+
+
+# Expression case: an initial condition using every pert type, comparisons,
+# logic, if-free functions and a named constant, evaluated by the reference's
+# own fparser for two samples' random numbers.
+EXPR_CASE = dict(n=17, seed=4, samples=[0, 1], rnd_seed_base=300, n_rnd=8, constants={"c1": 0.0125},
+                 ic={"temperature": "1.0 + 0.1*sin(2*pi*x/10)*cos(pi*y/7) + 0.02*pert(1,x,y/10+0.5,0.8)"
+                                    " + 0.01*(x<0 & y>0)",
+                     "xvelocity": "0.3*tanh(y) - 0.1*exp(-(x^2+y^2)/4) + 0.05*pert(3,x,(y+5)/10,0.6)"
+                                  " + 0.01*((abs(x)>=2) - (abs(x)<2))",
+                     "yvelocity": "0.2*pert(2,x,(x+5)/10,0.9) + 0.1*atan2(y,x+0.5)/pi + 0.01*floor(x) + c1*x",
+                     "zvelocity": "0.0",
+                     "pressure": "1 + 0.05*sqrt(x^2+y^2) + 0.01*pert(4,x,y,3) + 0.001*(x%3)"
+                                 " + 0.02*(x>=0 | y<=-1) + 0.003*max(x,y) - 0.002*min(x,y)"
+                                 " + 0.01*log(2+cosh(0.1*x)) + 0.004*!(x>1)"})
+
+
+def build_expr_case(spec: dict = EXPR_CASE):
+    """Mesh, reference configuration and per-sample random rows of the expression case."""
+    m = cases.vortex_mesh(spec["n"], spec["seed"])
+    r = np.random.default_rng(spec["rnd_seed_base"])
+    rows = {s: r.uniform(0.05, 1.0, spec["n_rnd"]) for s in spec["samples"]}
+    cfg = dict(flux="kepes_tecno_roe", reconstruct="minmod", boundary=dict(PERIODIC4), final_time=1.0,
+               time_stamps=1, cfl=0.8, samples=list(spec["samples"]), rnd_per_sample=spec["n_rnd"],
+               ic=dict(spec["ic"]), constants=dict(spec["constants"]))
+    return m, cfg, rows

@@ -23,7 +23,7 @@ ROOT = os.path.dirname(os.path.dirname(os.path.dirname(os.path.abspath(__file__)
 sys.path.insert(0, ROOT)
 sys.path.insert(0, os.path.join(ROOT, "oracle"))
 
-from tests.golden.cases_spec import build_mc_case, MC_CASE, CASES, build_case  # noqa: E402
+from tests.golden.cases_spec import build_mc_case, MC_CASE, CASES, build_case, EXPR_CASE, build_expr_case  # noqa: E402
 import ref_runner  # noqa: E402
 
 OUT = os.path.dirname(os.path.abspath(__file__))
@@ -44,6 +44,21 @@ def main():
         print(name, "vertices", mesh.n_vertex, "records", len(keep))
     if not only or "mc_kh" in only:
         make_mc()
+    if not only or "expr_ic" in only:
+        make_expr()
+
+
+def make_expr():
+    """expr_ic.npz: initial states the reference evaluates with its fparser from
+    the expression case's parameter file, one per sample's random numbers."""
+    mesh, cfg, rows = build_expr_case()
+    ics = []
+    for s in cfg["samples"]:
+        one = ref_runner.run_case(mesh, dict(cfg, samples=[s]), None, 0, 0, rnd_rows=rows)
+        ics.append(one["prim0"].reshape(-1, 5))
+    np.savez_compressed(os.path.join(OUT, "expr_ic.npz"), spec=np.array(json.dumps(EXPR_CASE)), ics=np.stack(ics),
+                        rows=np.stack([rows[s] for s in cfg["samples"]]))
+    print("expr_ic vertices", mesh.n_vertex, "samples", len(ics))
 
 
 def make_mc():

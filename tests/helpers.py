@@ -12,10 +12,10 @@ GOLDEN = os.path.join(ROOT, "tests", "golden")
 
 
 def golden_names():
-    """Single-solve fixtures (the Monte Carlo fixtures mc_*.npz and the output-file
-    fixtures out_*.npz have their own tests)."""
+    """Single-solve fixtures (the Monte Carlo fixtures mc_*.npz, the output-file
+    fixtures out_*.npz and the expression fixture expr_*.npz have their own tests)."""
     return sorted(os.path.basename(p)[:-4] for p in glob.glob(os.path.join(GOLDEN, "*.npz"))
-                  if not os.path.basename(p).startswith(("mc_", "out_")))
+                  if not os.path.basename(p).startswith(("mc_", "out_", "expr_")))
 
 
 def load_golden(name):
