@@ -26,23 +26,23 @@
 #include "tg_kernels.cuh"
 
 #ifndef TG_TILE_OWNED
-#define TG_TILE_OWNED 256      // owned vertices per tile (<= kTileThreads)
+#define TG_TILE_OWNED 128      // owned vertices per tile (<= kTileThreads)
 #endif
 #ifndef TG_TILE_LCAP
-#define TG_TILE_LCAP 448       // local (owned + halo) vertices per tile
+#define TG_TILE_LCAP 256       // local (owned + halo) vertices per tile
 #endif
 #ifndef TG_TILE_ECAP
-#define TG_TILE_ECAP 1152      // edges per tile
+#define TG_TILE_ECAP 512       // edges per tile
 #endif
 // resident flux CTAs per SM the register budget is sized for: TeCNO fluxes / central fluxes
 #ifndef TG_FLUX_MINB
-#define TG_FLUX_MINB 2
+#define TG_FLUX_MINB 4
 #endif
 #ifndef TG_FLUX_MINB_CENTRAL
-#define TG_FLUX_MINB_CENTRAL 3
+#define TG_FLUX_MINB_CENTRAL 6
 #endif
 #ifndef TG_GRAD_MINB
-#define TG_GRAD_MINB 3         // resident gradient / dt CTAs per SM the register budget is sized for
+#define TG_GRAD_MINB 6         // resident gradient / dt CTAs per SM the register budget is sized for
 #endif
 
 namespace tg {
@@ -58,7 +58,10 @@ struct TileView {
   const double *x, *y;          // vertex coordinates (device order)
 };
 
-constexpr int kTileThreads = 256;
+#ifndef TG_TILE_THREADS
+#define TG_TILE_THREADS 128    // threads per tile CTA (>= TG_TILE_OWNED)
+#endif
+constexpr int kTileThreads = TG_TILE_THREADS;
 
 // ---- asynchronous global -> shared copies (sm_80+ cp.async)
 __device__ __forceinline__ void cp_async8(void* smem, const void* gmem) {

@@ -14,7 +14,8 @@ import numpy as np
 from . import abi
 
 HERE = os.path.dirname(os.path.abspath(__file__))
-LIB_PATH = os.path.join(HERE, "libtensum_b200.so")
+# TENSUM_B200_LIB selects another build of the library (e.g. one with other tile sizes)
+LIB_PATH = os.environ.get("TENSUM_B200_LIB") or os.path.join(HERE, "libtensum_b200.so")
 
 EXPORTS = ["tg_create", "tg_destroy", "tg_last_error", "tg_abi_version", "tg_set_state", "tg_get_state",
            "tg_store_conserved_old", "tg_compute_dt", "tg_gradients", "tg_residual", "tg_update",
