@@ -66,8 +66,11 @@ struct tg_handle {
   int nblocks_v = 0;
   bool viscous = false;
   bool grads_needed = false;
-  cudaGraph_t graph = nullptr;
+  cudaGraph_t graph = nullptr;                 // a step that forms its own dt (any state)
   cudaGraphExec_t graph_exec = nullptr;
+  cudaGraph_t wgraph = nullptr;                // a step whose dt the previous step formed
+  cudaGraphExec_t wgraph_exec = nullptr;
+  bool cold = true;                            // the next step may not find dt_next set
   // state transfers: PrimVar records in the caller's order on the device
   double* raw = nullptr;              // 5 * nv doubles
   const int* old_of_new = nullptr;    // device copy of the vertex permutation
@@ -289,8 +292,11 @@ void enqueue_norm_final(tg_handle* h, int nblocks, bool use_sc_iter, long long i
 
 // One iteration of FiniteVolume::solve's loop on the rotating buffers:
 // stage r reads buffer r and writes buffer (r+1)%3, so the step ends in buffer 0.
-void enqueue_step(tg_handle* h) {
-  k_step_begin<<<1, 1, 0, h->stream>>>(h->ctl, h->sc, h->done);
+// The last stage's update also forms the residual norms and ends the iteration
+// (its last block).  warm: the previous step's last update formed this step's dt
+// and U_old (dt_next set), so the first-stage dt pass and k_dt_final are left out.
+void enqueue_step(tg_handle* h, bool warm) {
+  k_step_begin<<<1, 1, 0, h->stream>>>(h->ctl, h->sc, h->done, warm ? 1 : 0);
   // stage r reads buffer bin and writes bout: ssprk3 0->1->2->0, rk4 0->1->2->1->0,
   // so a step always ends in buffer 0 and no stage writes the buffer it reads
   const int rk4_in[4] = {0, 1, 2, 1}, rk4_out[4] = {1, 2, 1, 0};
@@ -300,22 +306,40 @@ void enqueue_step(tg_handle* h) {
     if (first && h->ctl.time_step > 0.0) {
       k_store_old<<<nblk(h->mv.nv), kBlock, 0, h->stream>>>(h->prm, h->mv, view(h, 0), h->done);
       enqueue_gradient(h, bin, false, h->grads_needed, h->done);
+    } else if (first && warm) {
+      enqueue_gradient(h, bin, false, h->grads_needed, h->done);
     } else {
       enqueue_gradient(h, bin, first, h->grads_needed, h->done);   // first stage: + dt, U_old
     }
-    if (first) k_dt_final<<<1, 1, 0, h->stream>>>(h->ctl, h->sc, h->done);
+    if (first && !warm) k_dt_final<<<1, 1, 0, h->stream>>>(h->ctl, h->sc, h->done);
     if (first) enqueue_ssw(h, h->done);
     enqueue_boundary(h, bin, h->done);
     enqueue_tile_flux(h, bin, MODE_UPDATE, r, last, bout, h->done);
     if (h->prm.strong && h->mv.nsb > 0)
       k_strong_bc<<<nblk(h->mv.nsb), kBlock, 0, h->stream>>>(h->mv, h->Pb[bout], h->done);
-    if (last) enqueue_norm_final(h, h->L.ntiles, true, 0, h->done);
   }
-  k_step_end<<<1, 1, 0, h->stream>>>(h->ctl, h->sc, h->done);
+}
+
+// The captured step to replay: the warm one once the host has seen the previous
+// step form dt and U_old for the current state (cold is cleared only then).
+cudaGraphExec_t step_graph(const tg_handle* h) {
+  return (h->prm.fuse_dt && !h->cold && h->wgraph_exec) ? h->wgraph_exec : h->graph_exec;
+}
+
+void drop_graphs(tg_handle* h) {
+  if (h->graph_exec) cudaGraphExecDestroy(h->graph_exec);
+  if (h->graph) cudaGraphDestroy(h->graph);
+  if (h->wgraph_exec) cudaGraphExecDestroy(h->wgraph_exec);
+  if (h->wgraph) cudaGraphDestroy(h->wgraph);
+  h->graph_exec = h->wgraph_exec = nullptr;
+  h->graph = h->wgraph = nullptr;
 }
 
 // The state changed outside a captured step: the next step forms dt and U_old itself.
-void clear_dt_next(tg_handle* h) { cudaMemsetAsync(&h->sc->dt_next, 0, sizeof(int), h->stream); }
+void clear_dt_next(tg_handle* h) {
+  cudaMemsetAsync(&h->sc->dt_next, 0, sizeof(int), h->stream);
+  h->cold = true;
+}
 
 tg_status sync(tg_handle* h) {
   TG_CUDA(h, cudaGetLastError());
@@ -456,6 +480,7 @@ tg_status take_queued_input(tg_handle* h) {
   k_prim2ent_checked<<<nblk(nv), kBlock, 0, h->stream>>>(h->prm, nv, h->sv.P, h->sv.W, h->bad);
   k_scalars_set<<<1, 1, 0, h->stream>>>(h->sc, fresh_scalars(h, t0), h->bad);
   h->in_check = true;
+  h->cold = true;
   TG_CUDA(h, cudaGetLastError());
   return TG_OK;
 }
@@ -482,11 +507,14 @@ tg_status check_bad(tg_handle* h) {
 
 tg_status capture_step_graph(tg_handle* h) {
   if (h->graph_exec) return TG_OK;
-  TG_CUDA(h, cudaStreamBeginCapture(h->stream, cudaStreamCaptureModeThreadLocal));
-  enqueue_step(h);
-  cudaError_t e = cudaStreamEndCapture(h->stream, &h->graph);
-  if (e != cudaSuccess) return fail(h, TG_CUDA_ERROR, std::string("graph capture: ") + cudaGetErrorString(e));
-  TG_CUDA(h, cudaGraphInstantiate(&h->graph_exec, h->graph, 0));
+  for (int w = 0; w < (h->prm.fuse_dt ? 2 : 1); ++w) {
+    cudaGraph_t* g = w ? &h->wgraph : &h->graph;
+    TG_CUDA(h, cudaStreamBeginCapture(h->stream, cudaStreamCaptureModeThreadLocal));
+    enqueue_step(h, w == 1);
+    cudaError_t e = cudaStreamEndCapture(h->stream, g);
+    if (e != cudaSuccess) return fail(h, TG_CUDA_ERROR, std::string("graph capture: ") + cudaGetErrorString(e));
+    TG_CUDA(h, cudaGraphInstantiate(w ? &h->wgraph_exec : &h->graph_exec, *g, 0));
+  }
   return TG_OK;
 }
 
@@ -499,7 +527,7 @@ void enqueue_phase(tg_handle* h, int phase) {
       break;
     case TG_PHASE_UPDATE: enqueue_update(h, 1, false, h->never); break;
     case TG_PHASE_DT: enqueue_dt(h, h->never); break;
-    default: cudaGraphLaunch(h->graph_exec, h->stream); break;
+    default: cudaGraphLaunch(step_graph(h), h->stream); break;
   }
 }
 
@@ -536,6 +564,7 @@ tg_status take_raw_state(tg_handle* h, double t0) {
   k_prim2ent<<<nblk(nv), kBlock, 0, h->stream>>>(h->prm, nv, h->sv.P, h->sv.W);
   const Scalars s = fresh_scalars(h, t0);
   TG_CUDA(h, cudaMemcpyAsync(h->sc, &s, sizeof(s), cudaMemcpyHostToDevice, h->stream));
+  h->cold = true;
   return sync(h);
 }
 
@@ -703,11 +732,16 @@ tg_status tg_create(const tg_mesh* mesh, const tg_material* mat, const tg_bc_tab
   c.min_residue = opt->min_residue; c.max_iter = opt->max_iter; c.final_time = opt->final_time; c.tinst = tip;
 
   h->kernels_per_flux = residual_kernels(h);
-  // step_begin + gradient/dt passes (+ the first stage's warm gradient launch) + per stage
-  // (boundary, viscous, tiled flux) + [store_old] + dt_final + norm_final + step_end
-  h->kernels_per_step = 1 + (1 + (h->grads_needed ? c.n_rks - 1 : 0)) + (h->grads_needed && k.fuse_dt ? 1 : 0) +
-                        (k.liou ? 1 : 0) + (k.strong && h->mv.nsb > 0 ? c.n_rks : 0) + c.n_rks * residual_kernels(h) +
-                        (c.time_step > 0.0 ? 1 : 0) + 1 + 1 + 1;
+  // launches of a replayed step: step_begin + gradient passes + per stage (boundary,
+  // viscous, tiled flux; the last also forms the norms and ends the step) + Liou /
+  // strong-condition kernels; a step that forms its own dt adds the first-stage dt
+  // pass (and its gradient-only twin) and dt_final, a fixed time step store_old.
+  // The count is that of the steady state: warm steps when the next dt is fused.
+  const int tail = (k.liou ? 1 : 0) + (k.strong && h->mv.nsb > 0 ? c.n_rks : 0) + c.n_rks * residual_kernels(h);
+  const int grads = h->grads_needed ? c.n_rks : 0;
+  if (k.fuse_dt) h->kernels_per_step = 1 + grads + tail;
+  else if (c.time_step > 0.0) h->kernels_per_step = 1 + 1 + grads + 1 + tail;
+  else h->kernels_per_step = 1 + (h->grads_needed ? c.n_rks : 1) + 1 + tail;
   if ((st = dev_alloc(h, 5 * nv, &h->raw)) != TG_OK) { tg_destroy(h); return st; }
   if ((st = dev_alloc(h, 1, &h->bad)) != TG_OK) { tg_destroy(h); return st; }
   if ((st = dev_upload(h, L.old_of_new, &h->old_of_new)) != TG_OK) { tg_destroy(h); return st; }
@@ -733,8 +767,7 @@ tg_status tg_create(const tg_mesh* mesh, const tg_material* mat, const tg_bc_tab
 
 tg_status tg_destroy(tg_handle* h) {
   if (!h) return TG_OK;
-  if (h->graph_exec) cudaGraphExecDestroy(h->graph_exec);
-  if (h->graph) cudaGraphDestroy(h->graph);
+  drop_graphs(h);
   if (h->stream) cudaStreamSynchronize(h->stream);
   for (void* p : h->allocs) cudaFree(p);
   if (h->mom) cudaFree(h->mom);
@@ -948,10 +981,12 @@ tg_status tg_step(tg_handle* h, int n_steps, double* info4) {
   tg_status st = capture_step_graph(h);
   if (st != TG_OK) return st;
   if ((st = take_queued_input(h)) != TG_OK) return st;
-  for (int i = 0; i < n_steps; ++i) TG_CUDA(h, cudaGraphLaunch(h->graph_exec, h->stream));
+  const cudaGraphExec_t g = step_graph(h);
+  for (int i = 0; i < n_steps; ++i) TG_CUDA(h, cudaGraphLaunch(g, h->stream));
   Scalars s;
   st = read_scalars(h, &s);
   if (st != TG_OK) return st;
+  h->cold = !s.dt_next;
   if ((st = queued_input_refused(h)) != TG_OK) return st;
   if (info4) { info4[0] = s.elapsed; info4[1] = s.dt_global; info4[2] = s.rtotal; info4[3] = (double)s.iter; }
   if (s.bad) return fail(h, TG_BAD_STATE, "non-finite or non-positive state produced by an update");
@@ -1000,9 +1035,11 @@ tg_status tg_advance(tg_handle* h, int instance, long max_steps, double* info5) 
   long launched = 0;
   while (launched < max_steps && !s.bad && s.counter <= instance && !run_over(h, s)) {
     const long chunk = std::min<long>(16, max_steps - launched);
-    for (long i = 0; i < chunk; ++i) TG_CUDA(h, cudaGraphLaunch(h->graph_exec, h->stream));
+    const cudaGraphExec_t g = step_graph(h);
+    for (long i = 0; i < chunk; ++i) TG_CUDA(h, cudaGraphLaunch(g, h->stream));
     launched += chunk;
     if ((st = read_scalars(h, &s)) != TG_OK) return st;
+    h->cold = !s.dt_next;
   }
   stop = INT_MAX;
   TG_CUDA(h, cudaMemcpyAsync(&h->sc->stop_counter, &stop, sizeof(int), cudaMemcpyHostToDevice, h->stream));
@@ -1042,10 +1079,7 @@ tg_status tg_update_parameters(tg_handle* h, const tg_material* mat, const tg_bc
   }
   // dt depends on the material; the captured step holds the parameters by value
   clear_dt_next(h);
-  if (h->graph_exec) cudaGraphExecDestroy(h->graph_exec);
-  if (h->graph) cudaGraphDestroy(h->graph);
-  h->graph_exec = nullptr;
-  h->graph = nullptr;
+  drop_graphs(h);
   return sync(h);
 }
 

@@ -80,6 +80,7 @@ struct Scalars {
   // any other route, so the next step's first stage then forms them itself.
   int dt_next;
   unsigned long long dtmin_next;
+  unsigned int blocks_done;   // blocks of the last stage's launch that have written their norm partials
 };
 
 struct Control {
@@ -418,19 +419,8 @@ __global__ void k_strong_zero_res(MeshView m, StateView s) {
   s.R[2 * (size_t)m.nv + v] = 0.0;
 }
 
-__global__ void k_step_begin(Control ctl, Scalars* sc, int* done) {
-  // unsteady runs never advance the iteration bound (term_iter stays 0, src/fv.cc:2266-2268)
-  bool go = sc->rtotal > ctl.min_residue && (ctl.time_mode == 1 || sc->iter < ctl.max_iter) &&
-            sc->elapsed < ctl.final_time && sc->counter <= sc->stop_counter;
-  *done = go ? 0 : 1;
-  if (!go) return;
-  sc->dtmin_bits = sc->dt_next ? sc->dtmin_next : 0x7ff0000000000000ull;
-  sc->dtmin_next = 0x7ff0000000000000ull;
-}
-
 // Global dt and the unsteady clamp to the next output time (src/fv.cc:1584-1618).
-__global__ void k_dt_final(Control ctl, Scalars* sc, const int* __restrict__ done) {
-  if (*done) return;
+__device__ __forceinline__ void dt_final(const Control& ctl, Scalars* sc) {
   double dtg;
   if (ctl.time_step > 0.0) {
     dtg = ctl.time_step;
@@ -447,6 +437,64 @@ __global__ void k_dt_final(Control ctl, Scalars* sc, const int* __restrict__ don
     }
   }
   sc->dt_global = dtg;
+}
+
+__global__ void k_dt_final(Control ctl, Scalars* sc, const int* __restrict__ done) {
+  if (*done) return;
+  dt_final(ctl, sc);
+}
+
+// Start of a solve-loop iteration: the loop condition, and the running dt
+// minimum -- the previous step's last update already formed it for this state
+// when dt_next is set.  warm (a step captured without the first-stage dt pass,
+// launched only when dt_next is set): the dt clamp happens here too.
+__global__ void k_step_begin(Control ctl, Scalars* sc, int* done, int warm) {
+  // unsteady runs never advance the iteration bound (term_iter stays 0, src/fv.cc:2266-2268)
+  bool go = sc->rtotal > ctl.min_residue && (ctl.time_mode == 1 || sc->iter < ctl.max_iter) &&
+            sc->elapsed < ctl.final_time && sc->counter <= sc->stop_counter;
+  *done = go ? 0 : 1;
+  if (!go) return;
+  sc->dtmin_bits = sc->dt_next ? sc->dtmin_next : 0x7ff0000000000000ull;
+  sc->dtmin_next = 0x7ff0000000000000ull;
+  if (warm) dt_final(ctl, sc);
+}
+
+// Residual norms from the per-block partials (src/fv.cc:1846-1876) and the end
+// of the solve-loop iteration (src/fv.cc:2307-2343), by one block of `threads`
+// threads (red: 4 * threads doubles of shared memory).
+__device__ __forceinline__ void norm_and_step_end(const StateView& s, int nblocks, int nv_total, Scalars* sc,
+                                                  const Control& ctl, double* red, int threads) {
+  double acc[4] = {0.0, 0.0, 0.0, 0.0};
+#pragma unroll 8
+  for (int b = threadIdx.x; b < nblocks; b += threads)
+#pragma unroll
+    for (int c = 0; c < 4; ++c) acc[c] += __ldcg(s.part + (size_t)b * 4 + c);
+#pragma unroll
+  for (int c = 0; c < 4; ++c) red[c * threads + threadIdx.x] = acc[c];
+  __syncthreads();
+  for (int o = threads / 2; o > 0; o >>= 1) {
+    if ((int)threadIdx.x < o)
+#pragma unroll
+      for (int c = 0; c < 4; ++c) red[c * threads + threadIdx.x] += red[c * threads + threadIdx.x + o];
+    __syncthreads();
+  }
+  if (threadIdx.x == 0) {
+    double n0 = sqrt(red[0]) / nv_total, n1 = sqrt(red[threads]) / nv_total;
+    double n2 = sqrt(red[2 * threads]) / nv_total, n3 = sqrt(red[3 * threads]) / nv_total;
+    double total = sqrt(n0 * n0 + (n1 * n1 + n2 * n2 + 0.0) + n3 * n3);
+    if (sc->iter == 0) {
+      sc->rtotal0 = total;
+      if (sc->rtotal0 == 0.0) sc->rtotal0 = 1.0;
+    }
+    sc->rnorm[0] = n0; sc->rnorm[1] = n1; sc->rnorm[2] = n2; sc->rnorm[3] = n3;
+    sc->rtotal = total / sc->rtotal0;
+    sc->iter += 1;
+    sc->elapsed += sc->dt_global;
+    if (sc->reached && ctl.time_mode == 1) {
+      sc->counter += 1;
+      sc->reached = 0;
+    }
+  }
 }
 
 // update_solution for SSP-RK3 (src/fv.cc:1641-1652), fused with the residual-norm

@@ -545,6 +545,18 @@ __global__ void __launch_bounds__(kTileThreads, (FLUX == FLUX_TECNO_ROE || FLUX 
     if (threadIdx.x == 0)
 #pragma unroll
       for (int c = 0; c < 4; ++c) s.part[(size_t)blockIdx.x * 4 + c] = red[c * kTileThreads];
+    // the last block to finish forms the norms and ends the step
+    __shared__ int last;
+    if (threadIdx.x == 0) {
+      __threadfence();
+      last = atomicAdd(&sc->blocks_done, 1u) == gridDim.x - 1;
+    }
+    __syncthreads();
+    if (last) {
+      __threadfence();
+      norm_and_step_end(s, gridDim.x, nv, sc, ctl, red, kTileThreads);
+      if (threadIdx.x == 0) sc->blocks_done = 0;
+    }
   }
 }
 
