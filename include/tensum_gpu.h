@@ -28,7 +28,7 @@
 extern "C" {
 #endif
 
-#define TG_ABI_VERSION 3
+#define TG_ABI_VERSION 4
 
 typedef enum {
   TG_OK = 0,
@@ -335,9 +335,61 @@ typedef enum {
   TG_Q_N_BFACE = 2,
   TG_Q_KERNELS_PER_STEP = 3,   /* kernel launches in one tg_step step        */
   TG_Q_DEVICE_BYTES = 4,       /* device memory owned by the handle          */
-  TG_Q_KERNELS_PER_PHASE = 5   /* launches of one TG_PHASE_FLUX call         */
+  TG_Q_KERNELS_PER_PHASE = 5,  /* launches of one TG_PHASE_FLUX call         */
+  TG_Q_N_TILES = 6             /* vertex tiles (CTAs of one tiled pass)      */
 } tg_query_key;
 tg_status tg_query(tg_handle* h, int key, double* out);
+
+/* ---- domain decomposition of one mesh -----------------------------------
+ * Replaces the reference's MPI partitions of one mesh (read_part_mesh_file.cc,
+ * the shared-vertex residual and gradient sums of src/reduce_residual.cc:14-104
+ * and src/fv.cc:827-1030, the dt minimum of src/fv.cc:1602 and the norm sum of
+ * src/reduce_res_norm.cc:25).  The vertices, in the solver's Hilbert order,
+ * are cut into n_parts contiguous ranges; a partition owns one range and holds as
+ * ghosts every vertex its owned vertices' gather lists reach.  Each vertex is
+ * computed only by its owner, in the one-partition order, so any partition count
+ * gives the one-partition result bit for bit.  Inviscid runs with weak boundary
+ * conditions (no strong conditions, no Liou fix).  One process per GPU, each with
+ * its partition handle, is the intended use; the exchange is the caller's (NCCL
+ * all-to-all and all-gather over NVLink, or device copies in one process).
+ *
+ * A step, every call enqueued on the handle's stream (tg_stream), no host wait:
+ *   tg_part_begin
+ *   for each stage r:  tg_part_gradients(r), exchange TG_HALO_GRAD,
+ *                      tg_part_flux(r),      exchange TG_HALO_STATE
+ *   tg_part_export, all-gather of the 5-word records in partition order, tg_part_import
+ * An exchange of a field: tg_part_pack into the send buffer (8 doubles per
+ * vertex, peers in ascending order, send_counts[q] vertices for peer q), the
+ * all-to-all, tg_part_unpack from the receive buffer (recv_counts[q] vertices
+ * from peer q, peers ascending).  After tg_set_state (the whole mesh's records):
+ * tg_part_prime, then the scalar exchange, before the first tg_part_begin. */
+enum { TG_HALO_STATE = 0, TG_HALO_GRAD = 1 };
+
+/* Host only (no device): the plan of partition `part`.  out4 = {n_owned, n_ghost,
+ * n_send, n_recv}; the optional arrays receive the caller indices of the
+ * partition's vertices (owned first, n_owned + n_ghost), the per-peer counts
+ * (n_parts each) and the local positions of the send / receive entries. */
+tg_status tg_part_plan(const tg_mesh* mesh, const tg_bc_table* bc, int n_parts, int part, int* out4, int* local,
+                       int* send_counts, int* recv_counts, int* send_idx, int* recv_idx);
+tg_status tg_part_create(const tg_mesh* mesh, const tg_material* mat, const tg_bc_table* bc, const tg_options* opt,
+                         int n_parts, int part, tg_handle** out);
+/* out6 = {n_parts, part, n_owned, n_ghost, n_send, n_recv}; counts per peer. */
+tg_status tg_part_info(tg_handle* h, int* out6, int* send_counts, int* recv_counts);
+/* Local dt and U_old of the owned vertices of a new state (the first-stage dt pass). */
+tg_status tg_part_prime(tg_handle* h);
+tg_status tg_part_begin(tg_handle* h);
+tg_status tg_part_gradients(tg_handle* h, int stage);
+/* Boundary and edge fluxes and the stage update; the last stage also forms the
+ * next step's local dt and U_old and this partition's residual-norm sums. */
+tg_status tg_part_flux(tg_handle* h, int stage);
+tg_status tg_part_pack(tg_handle* h, int field, void* dev_send);
+tg_status tg_part_unpack(tg_handle* h, int field, const void* dev_recv);
+/* 5 x 8 bytes: the dt minimum (bits) and the four residual-norm sums. */
+tg_status tg_part_export(tg_handle* h, void* dev_out);
+/* n_parts x 5 x 8 bytes in partition order: every partition forms the same dt and norms. */
+tg_status tg_part_import(tg_handle* h, const void* dev_all);
+/* Waits for the stream; info4 = {elapsed, dt, relative residual, iteration}. */
+tg_status tg_part_scalars(tg_handle* h, double* info4);
 
 /* ---- batched FP32 ensembles (no counterpart in the reference, which runs
  *      one sample after another per MC group, src/fv.cc:2440-2456) ------- */

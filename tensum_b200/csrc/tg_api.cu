@@ -98,6 +98,18 @@ struct tg_handle {
   size_t device_bytes = 0;
   int kernels_per_step = 0;
   int kernels_per_flux = 0;
+  int n_caller = 0;           // PrimVar records in the caller's state arrays (the whole mesh)
+  // domain decomposition (tg_part_create): one partition of a mesh, ghosts filled by the
+  // caller's halo exchange (tg_part_pack / tg_part_unpack)
+  struct {
+    int n_parts = 0, part = 0, n_owned = 0, n_send = 0, n_recv = 0;
+    std::vector<int> send_off, recv_off;
+    const int* send_idx = nullptr;       // device: local ids of owned vertices, per peer
+    const int* recv_idx = nullptr;       // device: local ids of ghosts, per peer
+    int cur = 0;                         // state buffer the last flux phase wrote
+    bool norms_pending = false;          // a step ended since the last tg_part_import
+    double* out = nullptr;               // device: owned PrimVar records (tg_get_state)
+  } part;
 };
 
 namespace {
@@ -147,6 +159,10 @@ inline int nblk(int n) { return (n + kBlock - 1) / kBlock; }
 
 // ---- kernel dispatch over (flux, reconstruction)
 typedef void (*BfluxKernel)(Params, MeshView, StateView, const int*);
+// Entry points that step or read the whole mesh: a partition handle steps through tg_part_*.
+#define TG_WHOLE_MESH(h) \
+  if ((h) && (h)->part.n_parts > 0) return fail((h), TG_NOT_SUPPORTED, "a partition handle steps through tg_part_*");
+
 typedef void (*TileFluxKernel)(Params, MeshView, TileView, StateView, Control, Scalars*, int, int, double*, double*,
                                int, int, const int*);
 
@@ -210,6 +226,17 @@ size_t flux_smem(int flux, int recon, int lmax, int emax, int cmax) {
     case FLUX_ROE_EC: return tile_flux_smem_t<FLUX_ROE_EC, RECON_FIRST>(lmax, emax, cmax);
     default: return tile_flux_smem_t<FLUX_AVG, RECON_FIRST>(lmax, emax, cmax);
   }
+}
+
+// The dynamic shared-memory limit is an attribute of the kernel, shared by every
+// handle in the process: it is only ever raised, so a later handle with smaller
+// tiles does not lower it below what an earlier handle's launches need.
+cudaError_t raise_smem(const void* f, size_t bytes) {
+  cudaFuncAttributes a;
+  cudaError_t e = cudaFuncGetAttributes(&a, f);
+  if (e != cudaSuccess) return e;
+  if ((size_t)a.maxDynamicSharedSizeBytes >= bytes) return cudaSuccess;
+  return cudaFuncSetAttribute(f, cudaFuncAttributeMaxDynamicSharedMemorySize, (int)bytes);
 }
 
 typedef void (*TileGradKernel)(Params, MeshView, TileView, StateView, Scalars*, int, int, const int*, int);
@@ -552,10 +579,10 @@ __global__ void k_state_expr(int nv, const double* __restrict__ x, const double*
 // The state in the staging buffer (PrimVar records, caller's order) becomes
 // current if every vertex passes the reference's check, with fresh bookkeeping.
 tg_status take_raw_state(tg_handle* h, double t0) {
-  const int nv = h->L.nv;
+  const int nv = h->L.nv, nc = h->n_caller;   // a partition checks every record, takes its local ones
   tg_status st;
   TG_CUDA(h, cudaMemsetAsync(h->bad, 0, sizeof(int), h->stream));
-  k_state_check<<<nblk(nv), kBlock, 0, h->stream>>>(nv, h->raw, h->bad);
+  k_state_check<<<nblk(nc), kBlock, 0, h->stream>>>(nc, h->raw, h->bad);
   k_state_in<<<nblk(nv), kBlock, 0, h->stream>>>(nv, h->raw, h->old_of_new, h->bad, h->sv.P);
   int bad = 0;
   TG_CUDA(h, cudaMemcpyAsync(&bad, h->bad, sizeof(int), cudaMemcpyDeviceToHost, h->stream));
@@ -577,8 +604,9 @@ const char* tg_last_error(const tg_handle* h) {
   return g_last_error.c_str();
 }
 
-tg_status tg_create(const tg_mesh* mesh, const tg_material* mat, const tg_bc_table* bc, const tg_options* opt,
-                    tg_handle** out) {
+// tg_create (n_parts = 0) and tg_part_create (partition `part` of n_parts).
+static tg_status create_handle(const tg_mesh* mesh, const tg_material* mat, const tg_bc_table* bc,
+                               const tg_options* opt, int n_parts, int part, tg_handle** out) {
   if (!out) return fail(nullptr, TG_INVALID_ARG, "out is NULL");
   *out = nullptr;
   if (!mesh || !mat || !opt) return fail(nullptr, TG_INVALID_ARG, "mesh, material or options is NULL");
@@ -596,6 +624,9 @@ tg_status tg_create(const tg_mesh* mesh, const tg_material* mat, const tg_bc_tab
   if (opt->time_mode == TG_UNSTEADY && opt->n_time_stamps <= 0)
     return fail(nullptr, TG_INVALID_ARG, "unsteady runs need n_time_stamps > 0");
   if (!(opt->cfl > 0.0) && !(opt->time_step > 0.0)) return fail(nullptr, TG_INVALID_ARG, "cfl or time_step must be > 0");
+  if (n_parts > 0 && (mat->model == 1 || opt->bc_strong || (opt->liou_fix && mat->flux_scheme == FLUX_TECNO_ROE)))
+    return fail(nullptr, TG_NOT_SUPPORTED,
+                "partitioned runs are inviscid with weak boundary conditions and without the Liou fix");
 
   tg_handle* h = new (std::nothrow) tg_handle();
   if (!h) return fail(nullptr, TG_INVALID_ARG, "out of host memory");
@@ -605,6 +636,17 @@ tg_status tg_create(const tg_mesh* mesh, const tg_material* mat, const tg_bc_tab
   if (!msg.empty()) {
     delete h;
     return fail(nullptr, TG_INVALID_ARG, msg);
+  }
+  h->n_caller = h->L.nv;
+  PartPlan plan;
+  if (n_parts > 0) {
+    HostLayout G = std::move(h->L);
+    msg = plan_partition(G, n_parts, part, plan);
+    if (msg.empty()) msg = restrict_layout(G, plan, h->L);
+    if (!msg.empty()) {
+      delete h;
+      return fail(nullptr, TG_INVALID_ARG, msg);
+    }
   }
   msg = build_tiles(h->L, TG_TILE_OWNED, TG_TILE_LCAP, TG_TILE_ECAP);
   if (!msg.empty()) {
@@ -696,16 +738,13 @@ tg_status tg_create(const tg_mesh* mesh, const tg_material* mat, const tg_bc_tab
   h->smem_grad1 = tile_grad_smem(L.lmax, L.emax, L.cmax, true);
   h->smem_flux = flux_smem(mat->flux_scheme, mat->reconstruct_scheme, L.lmax, L.emax, L.cmax);
   {
-    cudaError_t ea = cudaFuncSetAttribute(grad_kernel(true, true), cudaFuncAttributeMaxDynamicSharedMemorySize,
-                                          (int)h->smem_grad1);
-    cudaError_t ea2 = cudaFuncSetAttribute(grad_kernel(true, false), cudaFuncAttributeMaxDynamicSharedMemorySize,
-                                           (int)h->smem_grad1);
-    cudaError_t eb = cudaFuncSetAttribute(grad_kernel(false, true), cudaFuncAttributeMaxDynamicSharedMemorySize,
-                                          (int)h->smem_grad0);
-    cudaError_t ec = cudaFuncSetAttribute(tile_kernel(mat->flux_scheme, mat->reconstruct_scheme, MODE_UPDATE),
-                                          cudaFuncAttributeMaxDynamicSharedMemorySize, (int)h->smem_flux);
-    cudaError_t ed = cudaFuncSetAttribute(tile_kernel(mat->flux_scheme, mat->reconstruct_scheme, MODE_RESIDUAL),
-                                          cudaFuncAttributeMaxDynamicSharedMemorySize, (int)h->smem_flux);
+    cudaError_t ea = raise_smem((const void*)grad_kernel(true, true), h->smem_grad1);
+    cudaError_t ea2 = raise_smem((const void*)grad_kernel(true, false), h->smem_grad1);
+    cudaError_t eb = raise_smem((const void*)grad_kernel(false, true), h->smem_grad0);
+    cudaError_t ec = raise_smem((const void*)tile_kernel(mat->flux_scheme, mat->reconstruct_scheme, MODE_UPDATE),
+                                h->smem_flux);
+    cudaError_t ed = raise_smem((const void*)tile_kernel(mat->flux_scheme, mat->reconstruct_scheme, MODE_RESIDUAL),
+                                h->smem_flux);
     if (ea != cudaSuccess || ea2 != cudaSuccess || eb != cudaSuccess || ec != cudaSuccess || ed != cudaSuccess) {
       tg_destroy(h);
       return fail(nullptr, TG_CUDA_ERROR, "tile kernels need more shared memory than the device allows");
@@ -742,12 +781,12 @@ tg_status tg_create(const tg_mesh* mesh, const tg_material* mat, const tg_bc_tab
   if (k.fuse_dt) h->kernels_per_step = 1 + grads + tail;
   else if (c.time_step > 0.0) h->kernels_per_step = 1 + 1 + grads + 1 + tail;
   else h->kernels_per_step = 1 + (h->grads_needed ? c.n_rks : 1) + 1 + tail;
-  if ((st = dev_alloc(h, 5 * nv, &h->raw)) != TG_OK) { tg_destroy(h); return st; }
+  if ((st = dev_alloc(h, 5 * (size_t)h->n_caller, &h->raw)) != TG_OK) { tg_destroy(h); return st; }
   if ((st = dev_alloc(h, 1, &h->bad)) != TG_OK) { tg_destroy(h); return st; }
   if ((st = dev_upload(h, L.old_of_new, &h->old_of_new)) != TG_OK) { tg_destroy(h); return st; }
   {
     Stager& S = h->stage;
-    const size_t bytes = 5 * nv * sizeof(double);
+    const size_t bytes = 5 * (size_t)h->n_caller * sizeof(double);
     S.lanes = (int)std::max<size_t>(1, std::min<size_t>(Stager::kMaxLanes, bytes / (2 * Stager::kSlot)));
     cudaError_t ep = cudaMallocHost((void**)&S.slots, 2 * (size_t)S.lanes * Stager::kSlot);
     for (int t = 0; t < S.lanes && ep == cudaSuccess; ++t) {
@@ -757,12 +796,27 @@ tg_status tg_create(const tg_mesh* mesh, const tg_material* mat, const tg_bc_tab
     if (ep == cudaSuccess) ep = cudaEventCreateWithFlags(&h->raw_ready, cudaEventDisableTiming);
     if (ep != cudaSuccess) { tg_destroy(h); return fail(nullptr, TG_CUDA_ERROR, cudaGetErrorString(ep)); }
   }
+  if (n_parts > 0) {
+    auto& P = h->part;
+    P.n_parts = n_parts; P.part = part; P.n_owned = plan.n_owned;
+    P.send_off = plan.send_off; P.recv_off = plan.recv_off;
+    P.n_send = (int)plan.send_idx.size(); P.n_recv = (int)plan.recv_idx.size();
+    if ((st = dev_upload(h, plan.send_idx, &P.send_idx)) != TG_OK) { tg_destroy(h); return st; }
+    if ((st = dev_upload(h, plan.recv_idx, &P.recv_idx)) != TG_OK) { tg_destroy(h); return st; }
+    if ((st = dev_alloc(h, 5 * (size_t)std::max(1, P.n_owned), &P.out)) != TG_OK) { tg_destroy(h); return st; }
+    c.part = 1;
+  }
   cudaError_t e = cudaStreamCreateWithFlags(&h->stream, cudaStreamNonBlocking);
   if (e != cudaSuccess) { tg_destroy(h); return fail(nullptr, TG_CUDA_ERROR, cudaGetErrorString(e)); }
   e = cudaDeviceSynchronize();
   if (e != cudaSuccess) { tg_destroy(h); return fail(nullptr, TG_CUDA_ERROR, cudaGetErrorString(e)); }
   *out = h;
   return TG_OK;
+}
+
+tg_status tg_create(const tg_mesh* mesh, const tg_material* mat, const tg_bc_table* bc, const tg_options* opt,
+                    tg_handle** out) {
+  return create_handle(mesh, mat, bc, opt, 0, 0, out);
 }
 
 tg_status tg_destroy(tg_handle* h) {
@@ -795,15 +849,18 @@ tg_status tg_destroy(tg_handle* h) {
 
 tg_status tg_set_state(tg_handle* h, const double* prim, int n_vertex, double t0) {
   if (!h || !prim) return fail(h, TG_INVALID_ARG, "NULL argument");
-  if (n_vertex != h->L.nv) return fail(h, TG_INVALID_ARG, "n_vertex does not match the mesh");
+  if (n_vertex != h->n_caller) return fail(h, TG_INVALID_ARG, "n_vertex does not match the mesh");
   if (h->in_stream) TG_CUDA(h, cudaStreamSynchronize(h->in_stream));
   h->in_queue.clear();                 // states queued by tg_set_state_async are dropped
-  tg_status st = state_h2d(h, prim, 5 * (size_t)h->L.nv * sizeof(double));
+  tg_status st = state_h2d(h, prim, 5 * (size_t)h->n_caller * sizeof(double));
   if (st != TG_OK) return st;
+  h->part.cur = 0;
+  h->part.norms_pending = false;
   return take_raw_state(h, t0);
 }
 
 tg_status tg_set_state_expr(tg_handle* h, const tg_expr* const* fields, const double* rnd, int n_rnd, double t0) {
+  TG_WHOLE_MESH(h)
   if (!h || !fields) return fail(h, TG_INVALID_ARG, "NULL argument");
   for (int c = 0; c < 5; ++c)
     if (c != 3 && !fields[c]) return fail(h, TG_INVALID_ARG, "temperature, velocity and pressure expressions are needed");
@@ -841,6 +898,7 @@ tg_status tg_set_state_expr(tg_handle* h, const tg_expr* const* fields, const do
 
 
 tg_status tg_set_state_async(tg_handle* h, const double* prim, int n_vertex, double t0) {
+  TG_WHOLE_MESH(h)
   if (!h || !prim) return fail(h, TG_INVALID_ARG, "NULL argument");
   if (n_vertex != h->L.nv) return fail(h, TG_INVALID_ARG, "n_vertex does not match the mesh");
   if (!host_pinned(prim)) return fail(h, TG_INVALID_ARG, "tg_set_state_async copies from pinned host memory");
@@ -864,7 +922,20 @@ tg_status tg_set_state_async(tg_handle* h, const double* prim, int n_vertex, dou
 
 tg_status tg_get_state(tg_handle* h, double* prim, int n_vertex) {
   if (!h || !prim) return fail(h, TG_INVALID_ARG, "NULL argument");
-  if (n_vertex != h->L.nv) return fail(h, TG_INVALID_ARG, "n_vertex does not match the mesh");
+  if (n_vertex != h->n_caller) return fail(h, TG_INVALID_ARG, "n_vertex does not match the mesh");
+  if (h->part.n_parts > 0) {
+    // a partition writes the records of the vertices it owns and leaves the others
+    const int n = h->part.n_owned;
+    std::vector<double> rec(5 * (size_t)n);
+    k_part_state_out<<<nblk(std::max(1, n)), kBlock, 0, h->stream>>>(n, h->L.nv, h->Pb[h->part.cur], h->part.out);
+    TG_CUDA(h, cudaGetLastError());
+    TG_CUDA(h, cudaMemcpyAsync(rec.data(), h->part.out, rec.size() * sizeof(double), cudaMemcpyDeviceToHost,
+                               h->stream));
+    tg_status st = sync(h);
+    if (st != TG_OK) return st;
+    for (int i = 0; i < n; ++i) std::memcpy(prim + 5 * (size_t)h->L.old_of_new[i], &rec[5 * (size_t)i], 5 * sizeof(double));
+    return TG_OK;
+  }
   const int nv = h->L.nv;
   k_state_out<<<nblk(nv), kBlock, 0, h->stream>>>(nv, h->sv.P, h->old_of_new, h->raw);
   TG_CUDA(h, cudaGetLastError());
@@ -872,12 +943,14 @@ tg_status tg_get_state(tg_handle* h, double* prim, int n_vertex) {
 }
 
 tg_status tg_store_conserved_old(tg_handle* h) {
+  TG_WHOLE_MESH(h)
   if (!h) return fail(h, TG_INVALID_ARG, "NULL handle");
   k_store_old<<<nblk(h->mv.nv), kBlock, 0, h->stream>>>(h->prm, h->mv, view(h, 0), h->never);
   return sync(h);
 }
 
 tg_status tg_compute_dt(tg_handle* h, double* dt_global_out, double* dt_out) {
+  TG_WHOLE_MESH(h)
   if (!h) return fail(h, TG_INVALID_ARG, "NULL handle");
   unsigned long long inf = 0x7ff0000000000000ull;
   TG_CUDA(h, cudaMemcpyAsync(&h->sc->dtmin_bits, &inf, sizeof(inf), cudaMemcpyHostToDevice, h->stream));
@@ -916,6 +989,7 @@ static tg_status copy_grad_out(tg_handle* h, double* dE_out) {
 }
 
 tg_status tg_gradients(tg_handle* h, double* dE_out) {
+  TG_WHOLE_MESH(h)
   if (!h) return fail(h, TG_INVALID_ARG, "NULL handle");
   enqueue_gradient(h, 0, false, true, h->never);
   tg_status st = sync(h);
@@ -924,6 +998,7 @@ tg_status tg_gradients(tg_handle* h, double* dE_out) {
 }
 
 tg_status tg_residual(tg_handle* h, double* res_out) {
+  TG_WHOLE_MESH(h)
   if (!h) return fail(h, TG_INVALID_ARG, "NULL handle");
   enqueue_residual(h, h->never);
   tg_status st = sync(h);
@@ -939,6 +1014,7 @@ tg_status tg_residual(tg_handle* h, double* res_out) {
 }
 
 tg_status tg_update(tg_handle* h, int r) {
+  TG_WHOLE_MESH(h)
   if (!h) return fail(h, TG_INVALID_ARG, "NULL handle");
   if (r < 0 || r >= h->ctl.n_rks) return fail(h, TG_INVALID_ARG, "stage index out of range for the time scheme");
   enqueue_update(h, r, false, h->never);
@@ -951,6 +1027,7 @@ tg_status tg_update(tg_handle* h, int r) {
 }
 
 tg_status tg_residual_norm(tg_handle* h, long iter, double* out6) {
+  TG_WHOLE_MESH(h)
   if (!h) return fail(h, TG_INVALID_ARG, "NULL handle");
   if (h->prm.strong) k_strong_zero_res<<<h->nblocks_v, kBlock, 0, h->stream>>>(h->mv, h->sv);
   k_norm_part<<<h->nblocks_v, kBlock, 0, h->stream>>>(h->mv, h->sv, h->never);
@@ -966,6 +1043,7 @@ tg_status tg_residual_norm(tg_handle* h, long iter, double* out6) {
 }
 
 tg_status tg_end_step(tg_handle* h, double* info4) {
+  TG_WHOLE_MESH(h)
   if (!h) return fail(h, TG_INVALID_ARG, "NULL handle");
   k_step_end<<<1, 1, 0, h->stream>>>(h->ctl, h->sc, h->never);
   Scalars s;
@@ -976,6 +1054,7 @@ tg_status tg_end_step(tg_handle* h, double* info4) {
 }
 
 tg_status tg_step(tg_handle* h, int n_steps, double* info4) {
+  TG_WHOLE_MESH(h)
   if (!h) return fail(h, TG_INVALID_ARG, "NULL handle");
   if (n_steps < 0) return fail(h, TG_INVALID_ARG, "n_steps < 0");
   tg_status st = capture_step_graph(h);
@@ -1022,6 +1101,7 @@ tg_status mom_check(tg_handle* h, int instance) {
 extern "C" {
 
 tg_status tg_advance(tg_handle* h, int instance, long max_steps, double* info5) {
+  TG_WHOLE_MESH(h)
   if (!h) return fail(h, TG_INVALID_ARG, "NULL handle");
   if (max_steps < 0) return fail(h, TG_INVALID_ARG, "max_steps < 0");
   tg_status st = capture_step_graph(h);
@@ -1053,6 +1133,7 @@ tg_status tg_advance(tg_handle* h, int instance, long max_steps, double* info5) 
 }
 
 tg_status tg_update_parameters(tg_handle* h, const tg_material* mat, const tg_bc_table* bc) {
+  TG_WHOLE_MESH(h)
   if (!h || !mat) return fail(h, TG_INVALID_ARG, "NULL handle or material");
   Params& k = h->prm;
   if (mat->model != k.model || mat->flux_scheme != k.flux || mat->reconstruct_scheme != k.recon ||
@@ -1084,6 +1165,7 @@ tg_status tg_update_parameters(tg_handle* h, const tg_material* mat, const tg_bc
 }
 
 tg_status tg_output_begin(tg_handle* h, double* prim_out, double* dE_out, int grad_state) {
+  TG_WHOLE_MESH(h)
   if (!h || !prim_out) return fail(h, TG_INVALID_ARG, "NULL handle or output buffer");
   if (grad_state != TG_GRAD_LAST_STAGE && grad_state != TG_GRAD_CURRENT)
     return fail(h, TG_INVALID_ARG, "grad_state is TG_GRAD_LAST_STAGE or TG_GRAD_CURRENT");
@@ -1130,6 +1212,7 @@ tg_status tg_output_wait(tg_handle* h) {
 }
 
 tg_status tg_forces(tg_handle* h, int n_forces, const int* n_tags, const int* tags, double* out) {
+  TG_WHOLE_MESH(h)
   if (!h || n_forces < 1 || !n_tags || !tags || !out) return fail(h, TG_INVALID_ARG, "bad force specification");
   std::vector<int> rec4, off;
   const std::string msg = force_faces(h->L, n_forces, n_tags, tags, rec4, off);
@@ -1162,6 +1245,7 @@ tg_status tg_forces(tg_handle* h, int n_forces, const int* n_tags, const int* ta
 }
 
 tg_status tg_moments_init(tg_handle* h, int n_instances, int extras) {
+  TG_WHOLE_MESH(h)
   if (!h) return fail(h, TG_INVALID_ARG, "NULL handle");
   if (n_instances < 1 || extras < 0 || extras > 15) return fail(h, TG_INVALID_ARG, "bad moment layout");
   if (h->mom) { cudaFree(h->mom); h->mom = nullptr; }
@@ -1270,6 +1354,7 @@ tg_status tg_moments_finalize(tg_handle* h, int instance, long n) {
 }
 
 tg_status tg_global(tg_handle* h, double* ke, double* ent) {
+  TG_WHOLE_MESH(h)
   if (!h) return fail(h, TG_INVALID_ARG, "NULL handle");
   k_global<<<h->nblocks_v, kBlock, 0, h->stream>>>(h->prm, h->mv, view(h, 0));
   std::vector<double> part(4 * (size_t)h->nblocks_v);
@@ -1290,6 +1375,7 @@ tg_status tg_stream(tg_handle* h, void** out) {
 }
 
 tg_status tg_time_phase(tg_handle* h, int phase, int reps, double* ms) {
+  TG_WHOLE_MESH(h)
   if (!h || !ms || reps <= 0 || phase < 0 || phase > 4) return fail(h, TG_INVALID_ARG, "bad argument");
   if (phase == TG_PHASE_STEP) {
     tg_status st = capture_step_graph(h);
@@ -1323,8 +1409,179 @@ tg_status tg_query(tg_handle* h, int key, double* out) {
     case TG_Q_KERNELS_PER_STEP: *out = h->kernels_per_step; break;
     case TG_Q_DEVICE_BYTES: *out = (double)h->device_bytes; break;
     case TG_Q_KERNELS_PER_PHASE: *out = h->kernels_per_flux; break;
+    case TG_Q_N_TILES: *out = h->L.ntiles; break;
     default: return fail(h, TG_INVALID_ARG, "unknown query key");
   }
+  return TG_OK;
+}
+
+// ---- domain decomposition
+
+tg_status tg_part_plan(const tg_mesh* mesh, const tg_bc_table* bc, int n_parts, int part, int* out4, int* local,
+                       int* send_counts, int* recv_counts, int* send_idx, int* recv_idx) {
+  if (!mesh || !out4) return fail(nullptr, TG_INVALID_ARG, "NULL argument");
+  HostLayout G;
+  std::string msg = build_layout(*mesh, bc, false, G);
+  PartPlan P;
+  if (msg.empty()) msg = plan_partition(G, n_parts, part, P);
+  if (!msg.empty()) return fail(nullptr, TG_INVALID_ARG, msg);
+  out4[0] = P.n_owned;
+  out4[1] = (int)P.local.size() - P.n_owned;
+  out4[2] = (int)P.send_idx.size();
+  out4[3] = (int)P.recv_idx.size();
+  if (local)
+    for (size_t i = 0; i < P.local.size(); ++i) local[i] = G.old_of_new[P.local[i]];
+  for (int q = 0; q < n_parts; ++q) {
+    if (send_counts) send_counts[q] = P.send_off[q + 1] - P.send_off[q];
+    if (recv_counts) recv_counts[q] = P.recv_off[q + 1] - P.recv_off[q];
+  }
+  if (send_idx) std::copy(P.send_idx.begin(), P.send_idx.end(), send_idx);
+  if (recv_idx) std::copy(P.recv_idx.begin(), P.recv_idx.end(), recv_idx);
+  return TG_OK;
+}
+
+tg_status tg_part_create(const tg_mesh* mesh, const tg_material* mat, const tg_bc_table* bc, const tg_options* opt,
+                         int n_parts, int part, tg_handle** out) {
+  if (n_parts < 1 || part < 0 || part >= n_parts) return fail(nullptr, TG_INVALID_ARG, "partition index out of range");
+  return create_handle(mesh, mat, bc, opt, n_parts, part, out);
+}
+
+}  // extern "C"
+
+namespace {
+
+tg_status part_check(tg_handle* h) {
+  if (!h) return fail(h, TG_INVALID_ARG, "NULL handle");
+  if (h->part.n_parts == 0) return fail(h, TG_INVALID_ARG, "not a partition handle (tg_part_create)");
+  return TG_OK;
+}
+
+// buffers stage r reads and writes (as enqueue_step rotates them)
+void stage_buffers(const tg_handle* h, int r, int* bin, int* bout) {
+  const int rk4_in[4] = {0, 1, 2, 1}, rk4_out[4] = {1, 2, 1, 0};
+  *bin = h->ctl.scheme == 1 ? rk4_in[r] : r;
+  *bout = h->ctl.scheme == 1 ? rk4_out[r] : (r + 1) % 3;
+}
+
+tg_status launched(tg_handle* h) {
+  TG_CUDA(h, cudaGetLastError());
+  return TG_OK;
+}
+
+}  // namespace
+
+extern "C" {
+
+tg_status tg_part_info(tg_handle* h, int* out6, int* send_counts, int* recv_counts) {
+  tg_status st = part_check(h);
+  if (st != TG_OK) return st;
+  if (!out6) return fail(h, TG_INVALID_ARG, "NULL argument");
+  const auto& P = h->part;
+  out6[0] = P.n_parts; out6[1] = P.part; out6[2] = P.n_owned; out6[3] = h->L.nv - P.n_owned;
+  out6[4] = P.n_send; out6[5] = P.n_recv;
+  for (int q = 0; q < P.n_parts; ++q) {
+    if (send_counts) send_counts[q] = P.send_off[q + 1] - P.send_off[q];
+    if (recv_counts) recv_counts[q] = P.recv_off[q + 1] - P.recv_off[q];
+  }
+  return TG_OK;
+}
+
+tg_status tg_part_prime(tg_handle* h) {
+  tg_status st = part_check(h);
+  if (st != TG_OK) return st;
+  if (h->prm.fuse_dt) {
+    grad_kernel(true, false)<<<h->L.ntiles, kTileThreads, h->smem_grad1, h->stream>>>(
+        h->prm, h->mv, h->tv, view(h, 0), h->sc, h->L.lmax, h->L.emax, h->never, 0);
+    k_part_primed<<<1, 1, 0, h->stream>>>(h->sc);
+  }
+  h->cold = false;
+  return launched(h);
+}
+
+tg_status tg_part_begin(tg_handle* h) {
+  tg_status st = part_check(h);
+  if (st != TG_OK) return st;
+  if (h->cold) return fail(h, TG_INVALID_ARG, "tg_part_prime and the scalar exchange come first after a new state");
+  k_step_begin<<<1, 1, 0, h->stream>>>(h->ctl, h->sc, h->done, 1);
+  if (h->ctl.time_step > 0.0) k_store_old<<<nblk(h->mv.nv), kBlock, 0, h->stream>>>(h->prm, h->mv, view(h, 0), h->done);
+  return launched(h);
+}
+
+tg_status tg_part_gradients(tg_handle* h, int r) {
+  tg_status st = part_check(h);
+  if (st != TG_OK) return st;
+  if (r < 0 || r >= h->ctl.n_rks) return fail(h, TG_INVALID_ARG, "stage out of range");
+  int bin, bout;
+  stage_buffers(h, r, &bin, &bout);
+  enqueue_gradient(h, bin, false, h->grads_needed, h->done);
+  return launched(h);
+}
+
+tg_status tg_part_flux(tg_handle* h, int r) {
+  tg_status st = part_check(h);
+  if (st != TG_OK) return st;
+  if (r < 0 || r >= h->ctl.n_rks) return fail(h, TG_INVALID_ARG, "stage out of range");
+  int bin, bout;
+  stage_buffers(h, r, &bin, &bout);
+  const bool last = r == h->ctl.n_rks - 1;
+  enqueue_boundary(h, bin, h->done);
+  enqueue_tile_flux(h, bin, MODE_UPDATE, r, last, bout, h->done);
+  h->part.cur = bout;
+  if (last) h->part.norms_pending = true;
+  return launched(h);
+}
+
+tg_status tg_part_pack(tg_handle* h, int field, void* dev_send) {
+  tg_status st = part_check(h);
+  if (st != TG_OK) return st;
+  if (field != TG_HALO_STATE && field != TG_HALO_GRAD) return fail(h, TG_INVALID_ARG, "unknown halo field");
+  const int n = h->part.n_send, nv = h->L.nv;
+  if (n == 0) return TG_OK;
+  if (!dev_send) return fail(h, TG_INVALID_ARG, "NULL send buffer");
+  const double* A = field == TG_HALO_STATE ? h->Pb[h->part.cur] : h->sv.G;
+  const double* B = field == TG_HALO_STATE ? h->Wb[h->part.cur] : h->sv.G + 4 * (size_t)nv;
+  k_halo_pack<<<nblk(8 * n), kBlock, 0, h->stream>>>(n, h->part.send_idx, nv, A, B, (double*)dev_send);
+  return launched(h);
+}
+
+tg_status tg_part_unpack(tg_handle* h, int field, const void* dev_recv) {
+  tg_status st = part_check(h);
+  if (st != TG_OK) return st;
+  if (field != TG_HALO_STATE && field != TG_HALO_GRAD) return fail(h, TG_INVALID_ARG, "unknown halo field");
+  const int n = h->part.n_recv, nv = h->L.nv;
+  if (n == 0) return TG_OK;
+  if (!dev_recv) return fail(h, TG_INVALID_ARG, "NULL receive buffer");
+  double* A = field == TG_HALO_STATE ? h->Pb[h->part.cur] : h->sv.G;
+  double* B = field == TG_HALO_STATE ? h->Wb[h->part.cur] : h->sv.G + 4 * (size_t)nv;
+  k_halo_unpack<<<nblk(8 * n), kBlock, 0, h->stream>>>(n, h->part.recv_idx, nv, A, B, (const double*)dev_recv);
+  return launched(h);
+}
+
+tg_status tg_part_export(tg_handle* h, void* dev_out) {
+  tg_status st = part_check(h);
+  if (st != TG_OK) return st;
+  if (!dev_out) return fail(h, TG_INVALID_ARG, "NULL buffer");
+  k_part_export<<<1, 1, 0, h->stream>>>(h->sc, (unsigned long long*)dev_out);
+  return launched(h);
+}
+
+tg_status tg_part_import(tg_handle* h, const void* dev_all) {
+  tg_status st = part_check(h);
+  if (st != TG_OK) return st;
+  if (!dev_all) return fail(h, TG_INVALID_ARG, "NULL buffer");
+  k_part_import<<<1, 1, 0, h->stream>>>(h->sc, (const unsigned long long*)dev_all, h->part.n_parts, h->n_caller,
+                                        h->part.norms_pending ? 1 : 0);
+  h->part.norms_pending = false;
+  return launched(h);
+}
+
+tg_status tg_part_scalars(tg_handle* h, double* info4) {
+  tg_status st = part_check(h);
+  if (st != TG_OK) return st;
+  Scalars s;
+  if ((st = read_scalars(h, &s)) != TG_OK) return st;
+  if (info4) { info4[0] = s.elapsed; info4[1] = s.dt_global; info4[2] = s.rtotal; info4[3] = (double)s.iter; }
+  if (s.bad) return fail(h, TG_BAD_STATE, "non-finite or non-positive state produced by an update");
   return TG_OK;
 }
 

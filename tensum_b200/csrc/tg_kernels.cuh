@@ -81,6 +81,7 @@ struct Scalars {
   int dt_next;
   unsigned long long dtmin_next;
   unsigned int blocks_done;   // blocks of the last stage's launch that have written their norm partials
+  double rsq[4];              // a partition's residual-norm sums of its last step, before the exchange
 };
 
 struct Control {
@@ -93,6 +94,7 @@ struct Control {
   long long max_iter;
   double final_time;
   const double* tinst;
+  int part;            // a partition of a decomposed mesh: norms wait for the other partitions' sums
 };
 
 __device__ __forceinline__ Prim load_prim(const double* P, int nv, int i) {
@@ -459,6 +461,20 @@ __global__ void k_step_begin(Control ctl, Scalars* sc, int* done, int warm) {
   if (warm) dt_final(ctl, sc);
 }
 
+// Residual norms from the weighted squared sums of the whole mesh (src/fv.cc:1846-1876);
+// the first iteration's total becomes the reference for the relative residual.
+__device__ __forceinline__ void set_norms(Scalars* sc, const double* sum4, int nv_total, bool first) {
+  double n0 = sqrt(sum4[0]) / nv_total, n1 = sqrt(sum4[1]) / nv_total;
+  double n2 = sqrt(sum4[2]) / nv_total, n3 = sqrt(sum4[3]) / nv_total;
+  double total = sqrt(n0 * n0 + (n1 * n1 + n2 * n2 + 0.0) + n3 * n3);
+  if (first) {
+    sc->rtotal0 = total;
+    if (sc->rtotal0 == 0.0) sc->rtotal0 = 1.0;
+  }
+  sc->rnorm[0] = n0; sc->rnorm[1] = n1; sc->rnorm[2] = n2; sc->rnorm[3] = n3;
+  sc->rtotal = total / sc->rtotal0;
+}
+
 // Residual norms from the per-block partials (src/fv.cc:1846-1876) and the end
 // of the solve-loop iteration (src/fv.cc:2307-2343), by one block of `threads`
 // threads (red: 4 * threads doubles of shared memory).
@@ -479,15 +495,13 @@ __device__ __forceinline__ void norm_and_step_end(const StateView& s, int nblock
     __syncthreads();
   }
   if (threadIdx.x == 0) {
-    double n0 = sqrt(red[0]) / nv_total, n1 = sqrt(red[threads]) / nv_total;
-    double n2 = sqrt(red[2 * threads]) / nv_total, n3 = sqrt(red[3 * threads]) / nv_total;
-    double total = sqrt(n0 * n0 + (n1 * n1 + n2 * n2 + 0.0) + n3 * n3);
-    if (sc->iter == 0) {
-      sc->rtotal0 = total;
-      if (sc->rtotal0 == 0.0) sc->rtotal0 = 1.0;
+    const double sum4[4] = {red[0], red[threads], red[2 * threads], red[3 * threads]};
+    if (ctl.part) {
+#pragma unroll
+      for (int c = 0; c < 4; ++c) sc->rsq[c] = sum4[c];
+    } else {
+      set_norms(sc, sum4, nv_total, sc->iter == 0);
     }
-    sc->rnorm[0] = n0; sc->rnorm[1] = n1; sc->rnorm[2] = n2; sc->rnorm[3] = n3;
-    sc->rtotal = total / sc->rtotal0;
     sc->iter += 1;
     sc->elapsed += sc->dt_global;
     if (sc->reached && ctl.time_mode == 1) {
@@ -797,6 +811,67 @@ __global__ void k_moments_scale(size_t n, double fact3, double fact4, double* __
   if (j >= n) return;
   m2[j] *= fact3;
   sm[j] *= fact4;
+}
+
+// ---- domain decomposition (tg_part_*): halo exchange and the exchanged step scalars
+
+// Packs 8 doubles per listed vertex (components 0-3 of A, then 0-3 of B: the P and W
+// of a state buffer, or the two halves of the gradient array) into out[8 * i + c].
+__global__ void k_halo_pack(int n, const int* __restrict__ idx, int nv, const double* __restrict__ A,
+                            const double* __restrict__ B, double* __restrict__ out) {
+  const int i = blockIdx.x * blockDim.x + threadIdx.x;
+  if (i >= 8 * n) return;
+  const int v = idx[i >> 3], c = i & 7;
+  out[i] = c < 4 ? A[(size_t)c * nv + v] : B[(size_t)(c - 4) * nv + v];
+}
+
+__global__ void k_halo_unpack(int n, const int* __restrict__ idx, int nv, double* __restrict__ A,
+                              double* __restrict__ B, const double* __restrict__ in) {
+  const int i = blockIdx.x * blockDim.x + threadIdx.x;
+  if (i >= 8 * n) return;
+  const int v = idx[i >> 3], c = i & 7;
+  if (c < 4) A[(size_t)c * nv + v] = in[i];
+  else B[(size_t)(c - 4) * nv + v] = in[i];
+}
+
+// After the first-stage dt pass of tg_part_prime: its minimum is the next step's.
+__global__ void k_part_primed(Scalars* sc) {
+  sc->dtmin_next = sc->dtmin_bits;
+  sc->dtmin_bits = 0x7ff0000000000000ull;
+  sc->dt_next = 1;
+}
+
+// A partition's contribution to the step exchange: its running dt minimum (as
+// bits; positive doubles order like their bit patterns) and its residual-norm sums.
+__global__ void k_part_export(const Scalars* sc, unsigned long long* out) {
+  out[0] = sc->dtmin_next;
+#pragma unroll
+  for (int c = 0; c < 4; ++c) out[1 + c] = (unsigned long long)__double_as_longlong(sc->rsq[c]);
+}
+
+// All partitions' contributions, combined in partition order so every partition
+// forms the same dt and norms: the dt minimum of the whole mesh and, after a
+// step, the norms over the whole mesh with nv_total its vertex count (the
+// reference's MPI reductions, src/fv.cc:1602, src/reduce_res_norm.cc:25).
+__global__ void k_part_import(Scalars* sc, const unsigned long long* __restrict__ all, int n_parts, int nv_total,
+                              int norms) {
+  unsigned long long m = all[0];
+  double sum4[4] = {0.0, 0.0, 0.0, 0.0};
+  for (int q = 0; q < n_parts; ++q) {
+    m = all[5 * q] < m ? all[5 * q] : m;
+#pragma unroll
+    for (int c = 0; c < 4; ++c) sum4[c] += __longlong_as_double((long long)all[5 * q + 1 + c]);
+  }
+  sc->dtmin_next = m;
+  if (norms) set_norms(sc, sum4, nv_total, sc->iter == 1);
+}
+
+// Owned vertices of a partition -> PrimVar records in local order (tg_get_state).
+__global__ void k_part_state_out(int n, int nv, const double* __restrict__ P, double* __restrict__ out) {
+  const int i = blockIdx.x * blockDim.x + threadIdx.x;
+  if (i >= n) return;
+  double* q = out + 5 * (size_t)i;
+  q[0] = P[i]; q[1] = P[3 * (size_t)nv + i]; q[2] = P[nv + i]; q[3] = P[2 * (size_t)nv + i]; q[4] = 0.0;
 }
 
 }  // namespace tg

@@ -365,6 +365,7 @@ std::string build_layout(const tg_mesh& m, const tg_bc_table* bc, bool need_visc
 
 std::string build_tiles(HostLayout& L, int max_owned, int max_local, int max_edges) {
   const int nv = L.nv;
+  const int n_own = L.n_owned >= 0 ? L.n_owned : nv;   // tiles cover the owned vertices only
   if (max_owned <= 0 || max_local > 65535 || max_edges > 32767) return "bad tile limits";
   L.t_vbeg.clear(); L.t_loff.assign(1, 0); L.t_eoff.assign(1, 0); L.lv.clear();
   L.te_ab.clear(); L.te_nx.clear(); L.te_ny.clear();
@@ -377,13 +378,13 @@ std::string build_tiles(HostLayout& L, int max_owned, int max_local, int max_edg
   std::vector<int> vloc(nv, -1), eloc(L.ne, -1);
   std::vector<int> tv, te;  // current tile's local vertices / edges (global ids)
   int v = 0;
-  while (v < nv) {
+  while (v < n_own) {
     int vb = v;
     tv.clear();
     te.clear();
     // greedily add owned vertices while the neighbourhood fits
     int nown = 0;
-    while (v < nv && nown < max_owned) {
+    while (v < n_own && nown < max_owned) {
       // tentative: count new edges and new local vertices of vertex v
       int add_e = 0, add_v = (vloc[v] < 0) ? 1 : 0;
       std::vector<int> new_halo;
@@ -453,9 +454,155 @@ std::string build_tiles(HostLayout& L, int max_owned, int max_local, int max_edg
     for (int x : order) vloc[x] = -1;
     for (int e : te) eloc[e] = -1;
   }
-  L.t_vbeg.push_back(nv);
+  L.t_vbeg.push_back(n_own);
+  for (int x = n_own; x < nv; ++x) L.cv_off[x + 1] = L.cv_off[x];   // ghosts: empty lists
   L.ntiles = (int)L.t_vbeg.size() - 1;
   if (L.cv_ent.size() & 1) L.cv_ent.push_back(0);   // the lists are staged in whole 4-byte words
+  return "";
+}
+
+namespace {
+
+// Device ids a vertex's gather lists read: edge endpoints (periodic partners'
+// edges included) and the vertices of its boundary faces.
+template <class F>
+void for_each_reach(const HostLayout& G, int v, F&& f) {
+  for (int j = G.ce_off[v]; j < G.ce_off[v + 1]; ++j) {
+    const int e = G.ce_ent[j] >> 1;
+    f(G.e_a[e]);
+    f(G.e_b[e]);
+  }
+  for (int j = G.cb_off[v]; j < G.cb_off[v + 1]; ++j) {
+    const int ent = G.cb_ent[j], type = ent & 3, idx = ent >> 2;
+    const int d = type == 0 ? idx >> 1 : idx;
+    if (type == 0 || type == 1 || type == 3) { f(G.b_v0[d]); f(G.b_v1[d]); }
+  }
+}
+
+int owner_of(const std::vector<int>& v0, int v) {
+  return (int)(std::upper_bound(v0.begin(), v0.end(), v) - v0.begin()) - 1;
+}
+
+// Ghosts of partition q: vertices outside its range that its owned vertices reach.
+std::vector<int> ghosts_of(const HostLayout& G, const std::vector<int>& v0, int q) {
+  std::vector<int> g;
+  for (int v = v0[q]; v < v0[q + 1]; ++v)
+    for_each_reach(G, v, [&](int x) { if (x < v0[q] || x >= v0[q + 1]) g.push_back(x); });
+  std::sort(g.begin(), g.end());
+  g.erase(std::unique(g.begin(), g.end()), g.end());
+  return g;
+}
+
+}  // namespace
+
+std::string plan_partition(const HostLayout& G, int n_parts, int part, PartPlan& P) {
+  if (n_parts < 1 || part < 0 || part >= n_parts) return "partition index out of range";
+  if (n_parts > G.nv) return "more partitions than vertices";
+  if (G.nvu > 0) return "viscous runs are not partitioned";
+  P = PartPlan();
+  P.n_parts = n_parts;
+  P.part = part;
+  P.v0.resize(n_parts + 1);
+  for (int q = 0; q <= n_parts; ++q) P.v0[q] = (int)((long long)q * G.nv / n_parts);
+  const int a = P.v0[part], b = P.v0[part + 1];
+  P.n_owned = b - a;
+  const std::vector<int> mine = ghosts_of(G, P.v0, part);
+  P.local.resize(P.n_owned);
+  for (int v = a; v < b; ++v) P.local[v - a] = v;
+  P.local.insert(P.local.end(), mine.begin(), mine.end());
+  // receive lists: my ghosts grouped by owner (ascending device id within each)
+  P.recv_off.assign(n_parts + 1, 0);
+  {
+    std::vector<std::vector<int>> by(n_parts);
+    for (size_t i = 0; i < mine.size(); ++i) by[owner_of(P.v0, mine[i])].push_back(P.n_owned + (int)i);
+    for (int q = 0; q < n_parts; ++q) {
+      P.recv_idx.insert(P.recv_idx.end(), by[q].begin(), by[q].end());
+      P.recv_off[q + 1] = (int)P.recv_idx.size();
+    }
+  }
+  // send lists: for each peer, my owned vertices among its ghosts (ascending)
+  P.send_off.assign(n_parts + 1, 0);
+  for (int q = 0; q < n_parts; ++q) {
+    if (q != part)
+      for (int x : ghosts_of(G, P.v0, q))
+        if (x >= a && x < b) P.send_idx.push_back(x - a);
+    P.send_off[q + 1] = (int)P.send_idx.size();
+  }
+  return "";
+}
+
+std::string restrict_layout(const HostLayout& G, const PartPlan& P, HostLayout& L) {
+  const int nloc = (int)P.local.size(), nown = P.n_owned;
+  L = HostLayout();
+  L.nv = nloc;
+  L.n_owned = nown;
+  std::vector<int> lid(G.nv, -1);
+  for (int i = 0; i < nloc; ++i) lid[P.local[i]] = i;
+  L.old_of_new.resize(nloc);
+  L.axi = G.axi;
+  for (int i = 0; i < nloc; ++i) {
+    const int g = P.local[i];
+    L.old_of_new[i] = G.old_of_new[g];
+    L.dcarea.push_back(G.dcarea[g]); L.inv6mc.push_back(G.inv6mc[g]); L.pweight.push_back(G.pweight[g]);
+    L.x.push_back(G.x[g]); L.y.push_back(G.y[g]);
+    if (G.axi) L.v_r.push_back(G.v_r[g]);
+  }
+  // edges and boundary faces the owned vertices' lists use, in the global order
+  std::vector<int> edges, faces;
+  for (int v = P.v0[P.part]; v < P.v0[P.part + 1]; ++v) {
+    for (int j = G.ce_off[v]; j < G.ce_off[v + 1]; ++j) edges.push_back(G.ce_ent[j] >> 1);
+    for (int j = G.cb_off[v]; j < G.cb_off[v + 1]; ++j) {
+      const int ent = G.cb_ent[j], type = ent & 3, idx = ent >> 2;
+      if (type == 2) return "viscous units are not partitioned";
+      faces.push_back(type == 0 ? idx >> 1 : idx);
+    }
+  }
+  std::sort(edges.begin(), edges.end());
+  edges.erase(std::unique(edges.begin(), edges.end()), edges.end());
+  std::sort(faces.begin(), faces.end());
+  faces.erase(std::unique(faces.begin(), faces.end()), faces.end());
+  std::vector<int> elid(G.ne, -1), blid(G.nb, -1);
+  L.ne = (int)edges.size();
+  for (int i = 0; i < L.ne; ++i) {
+    const int e = edges[i];
+    elid[e] = i;
+    if (lid[G.e_a[e]] < 0 || lid[G.e_b[e]] < 0) return "partition edge endpoint is not local";
+    L.e_a.push_back(lid[G.e_a[e]]); L.e_b.push_back(lid[G.e_b[e]]); L.e_face.push_back(G.e_face[e]);
+    L.e_nx.push_back(G.e_nx[e]); L.e_ny.push_back(G.e_ny[e]); L.e_dx.push_back(G.e_dx[e]); L.e_dy.push_back(G.e_dy[e]);
+    L.e_g0x.push_back(G.e_g0x[e]); L.e_g0y.push_back(G.e_g0y[e]);
+    L.e_g1x.push_back(G.e_g1x[e]); L.e_g1y.push_back(G.e_g1y[e]);
+    if (G.axi) L.e_r.push_back(G.e_r[e]);
+  }
+  L.nb = (int)faces.size();
+  for (int i = 0; i < L.nb; ++i) {
+    const int d = faces[i];
+    blid[d] = i;
+    if (lid[G.b_v0[d]] < 0 || lid[G.b_v1[d]] < 0) return "partition boundary-face vertex is not local";
+    L.b_v0.push_back(lid[G.b_v0[d]]); L.b_v1.push_back(lid[G.b_v1[d]]);
+    L.b_kind.push_back(G.b_kind[d]); L.b_adiab.push_back(G.b_adiab[d]); L.b_cell.push_back(G.b_cell[d]);
+    L.b_nx.push_back(G.b_nx[d]); L.b_ny.push_back(G.b_ny[d]);
+    L.b_val.insert(L.b_val.end(), G.b_val.begin() + (size_t)d * 10, G.b_val.begin() + (size_t)d * 10 + 10);
+    L.bf_face_nx.push_back(G.bf_face_nx[d]); L.bf_face_ny.push_back(G.bf_face_ny[d]);
+    L.bf_face_v0.push_back(std::max(0, lid[G.bf_face_v0[d]])); L.bf_face_v1.push_back(std::max(0, lid[G.bf_face_v1[d]]));
+  }
+  // owned vertices keep their lists, entry for entry; ghosts have none
+  L.ce_off.assign(nloc + 1, 0);
+  L.cb_off.assign(nloc + 1, 0);
+  for (int i = 0; i < nown; ++i) {
+    const int v = P.local[i];
+    for (int j = G.ce_off[v]; j < G.ce_off[v + 1]; ++j) {
+      const int ent = G.ce_ent[j];
+      L.ce_ent.push_back((elid[ent >> 1] << 1) | (ent & 1));
+    }
+    for (int j = G.cb_off[v]; j < G.cb_off[v + 1]; ++j) {
+      const int ent = G.cb_ent[j], type = ent & 3, idx = ent >> 2;
+      const int nidx = type == 0 ? ((blid[idx >> 1] << 1) | (idx & 1)) : blid[idx];
+      L.cb_ent.push_back((nidx << 2) | type);
+    }
+    L.ce_off[i + 1] = (int)L.ce_ent.size();
+    L.cb_off[i + 1] = (int)L.cb_ent.size();
+  }
+  for (int i = nown; i < nloc; ++i) { L.ce_off[i + 1] = L.ce_off[i]; L.cb_off[i + 1] = L.cb_off[i]; }
   return "";
 }
 

@@ -69,6 +69,9 @@ struct HostLayout {
   // vertices' gather list in tile-local edge indices, (local_edge << 1) | side,
   // in exactly the order of ce_ent, so the tiled kernels sum in the same order.
   int ntiles = 0, lmax = 0, emax = 0, tmax = 0, cmax = 0;  // cmax: gather entries per tile
+  // A partition's layout owns vertices [0, n_owned) only; the rest are ghosts that
+  // the halo exchange fills (no tiles, no gather lists).  -1: every vertex is owned.
+  int n_owned = -1;
   std::vector<int> t_vbeg, t_loff, t_eoff, lv;
   std::vector<uint32_t> te_ab;
   std::vector<double> te_nx, te_ny, te_g0x, te_g0y, te_g1x, te_g1y;
@@ -84,6 +87,30 @@ std::string build_layout(const tg_mesh& m, const tg_bc_table* bc, bool need_visc
 // Splits the (already built) layout into tiles of at most max_owned owned
 // vertices, max_local local vertices and max_edges edges each.
 std::string build_tiles(HostLayout& L, int max_owned, int max_local, int max_edges);
+
+// Domain decomposition of one mesh into n_parts partitions: partition q owns the
+// device-order vertex range [v0[q], v0[q+1]) and holds as ghosts every other vertex
+// its owned vertices' gather lists reach (edge endpoints, periodic partners'
+// neighbours, boundary-face vertices).  Each vertex is computed by its owner only,
+// with the gather lists and their order unchanged, so a partitioned solve repeats
+// the one-partition solve bit for bit; the reference's partitions instead sum
+// partial residuals and gradients of shared vertices across processes
+// (src/reduce_residual.cc:14-104, src/fv.cc:827-1030).
+struct PartPlan {
+  int n_parts = 0, part = 0;
+  std::vector<int> v0;                 // n_parts + 1 range starts in the device order
+  std::vector<int> local;              // device ids of this partition's vertices: owned, then ghosts ascending
+  int n_owned = 0;
+  // per peer q (offsets n_parts + 1): local ids of the owned vertices q holds as
+  // ghosts, and local ids of the ghosts q owns, both in ascending device order, so
+  // a sender's list and the receiver's list pair up entry by entry
+  std::vector<int> send_off, send_idx, recv_off, recv_idx;
+};
+
+// Builds partition `part` of `n_parts` from the full layout.  Viscous units and
+// strong-condition lists are not split (the caller refuses those runs).
+std::string plan_partition(const HostLayout& G, int n_parts, int part, PartPlan& P);
+std::string restrict_layout(const HostLayout& G, const PartPlan& P, HostLayout& out);
 
 // Face records of compute_forces (src/force.cc:116-219) for n_forces force
 // definitions (n_tags[f] face tags each, consecutive in `tags`): per face 4 ints

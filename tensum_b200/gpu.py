@@ -23,11 +23,14 @@ EXPORTS = ["tg_create", "tg_destroy", "tg_last_error", "tg_abi_version", "tg_set
            "tg_advance", "tg_moments_init", "tg_moments_increment", "tg_moments_get", "tg_moments_export",
            "tg_moments_merge", "tg_moments_merge_device", "tg_moments_finalize", "tg_forces", "tg_update_parameters",
            "tg_output_begin", "tg_output_wait", "tg_set_state_async", "tg_expr_create", "tg_expr_destroy",
-           "tg_expr_last_error", "tg_expr_eval", "tg_set_state_expr"]
+           "tg_expr_last_error", "tg_expr_eval", "tg_set_state_expr", "tg_part_plan", "tg_part_create",
+           "tg_part_info", "tg_part_prime", "tg_part_begin", "tg_part_gradients", "tg_part_flux", "tg_part_pack",
+           "tg_part_unpack", "tg_part_export", "tg_part_import", "tg_part_scalars"]
 
-ABI_VERSION = 3        # TG_ABI_VERSION of include/tensum_gpu.h
+ABI_VERSION = 4        # TG_ABI_VERSION of include/tensum_gpu.h
 PHASE = {"gradient": 0, "flux": 1, "update": 2, "dt": 3, "step": 4}
-QUERY = {"n_vertex": 0, "n_edge": 1, "n_bface": 2, "kernels_per_step": 3, "device_bytes": 4, "kernels_per_flux": 5}
+QUERY = {"n_vertex": 0, "n_edge": 1, "n_bface": 2, "kernels_per_step": 3, "device_bytes": 4, "kernels_per_flux": 5,
+         "n_tiles": 6}
 
 _lib = None
 
@@ -85,6 +88,19 @@ def load():
     L.tg_moments_merge.argtypes = [vp, i, C.c_long, C.c_long, dp, dp, dp]
     L.tg_moments_merge_device.argtypes = [vp, i, C.c_long, C.c_long, vp]
     L.tg_moments_finalize.argtypes = [vp, i, C.c_long]
+    ip = C.POINTER(i)
+    L.tg_part_plan.argtypes = [vp, vp, i, i, ip, ip, ip, ip, ip, ip]
+    L.tg_part_create.argtypes = [vp, vp, vp, vp, i, i, C.POINTER(vp)]
+    L.tg_part_info.argtypes = [vp, ip, ip, ip]
+    for name in ("tg_part_prime", "tg_part_begin"):
+        getattr(L, name).argtypes = [vp]
+    L.tg_part_gradients.argtypes = [vp, i]
+    L.tg_part_flux.argtypes = [vp, i]
+    L.tg_part_pack.argtypes = [vp, i, vp]
+    L.tg_part_unpack.argtypes = [vp, i, vp]
+    L.tg_part_export.argtypes = [vp, vp]
+    L.tg_part_import.argtypes = [vp, vp]
+    L.tg_part_scalars.argtypes = [vp, dp]
     for name in EXPORTS:
         f = getattr(L, name)
         if name not in ("tg_last_error", "tg_abi_version", "tg_expr_last_error"):

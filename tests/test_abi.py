@@ -31,7 +31,7 @@ def test_library_exports_every_declared_symbol():
 
 def test_abi_version():
     lib = gpu.load()
-    assert lib.tg_abi_version() == gpu.ABI_VERSION == 3
+    assert lib.tg_abi_version() == gpu.ABI_VERSION == 4
 
 
 @pytest.mark.skipif(gpu.load() is None, reason="library not loadable")

@@ -1,0 +1,147 @@
+"""Domain decomposition on the device: a mesh cut into partitions steps to the
+same bits as the one-partition solve.
+
+Each partition handle owns a range of the Hilbert-ordered vertices, computes
+them with the unchanged gather lists and exchanges ghost states and gradients
+after every phase (all partitions on one GPU here, exchanged by device copies;
+across GPUs the same calls run with NCCL).  The reference instead sums the
+partial residuals and gradients of shared vertices across MPI ranks
+(src/reduce_residual.cc:14-104, src/fv.cc:827-1030), which reorders sums with
+the partition count; owner-computes does not, so the comparison is bitwise.
+"""
+import numpy as np
+import pytest
+
+from tensum_b200 import abi, cases, gpu, partition, preproc
+
+pytestmark = pytest.mark.gpu
+
+
+def _kh_problem(n, flux, recon, **extra):
+    g = preproc.preprocess(cases.kh_mesh(n, 0))
+    cfg = dict(flux=flux, reconstruct=recon, boundary={t: ("periodic", {}) for t in (1, 2, 3, 4)},
+               final_time=1e9, time_stamps=1, cfl=0.8, **extra)
+    a, phi = cases.kh_coefficients(3)
+    return abi.Problem(g, cfg), cases.kh_ic(g.coords, a, phi)
+
+
+def _cyl_problem(flux="kepes_tecno_roe", recon="minmod"):
+    m = cases.cylinder_mesh(12, 24, 0)
+    g = preproc.preprocess(m)
+    T, u, v, p = cases.cylinder_freestream(0.3, 1.0)
+    far = {"temperature": T, "xvelocity": u, "yvelocity": v, "zvelocity": 0.0, "pressure": p}
+    cfg = dict(flux=flux, reconstruct=recon, model="euler", boundary={1: ("slip", {}), 2: ("farfield", far)},
+               final_time=1e9, time_stamps=1, cfl=0.8)
+    return abi.Problem(g, cfg), cases.cylinder_ic(g.coords, 0.3, 1.0)
+
+
+def _one_partition(P, ic, steps):
+    s = gpu.Solver(P)
+    s.set_state(ic)
+    info = s.step(steps)
+    out = s.get_state()
+    s.close()
+    return out, info
+
+
+@pytest.mark.parametrize("flux,recon,n_parts", [("kepes_tecno_rusanov", "minmod", 2),
+                                                ("kepes_tecno_rusanov", "minmod", 3),
+                                                ("kep", "first", 4),
+                                                ("roe_ec", "first", 2)])
+def test_periodic_partitions_match_one_partition(flux, recon, n_parts):
+    P, ic = _kh_problem(33, flux, recon)
+    want, winfo = _one_partition(P, ic, 6)
+    ps = partition.PartitionedSolver(P, n_parts)
+    ps.set_state(ic)
+    info = ps.step(6)
+    got = ps.get_state()
+    assert np.array_equal(got, want)
+    assert info[0] == winfo[0] and info[1] == winfo[1] and info[3] == winfo[3]   # elapsed, dt, iterations
+    assert abs(info[2] - winfo[2]) <= 1e-12 * abs(winfo[2])                      # norms: sums regrouped
+    for p in ps.parts:                                                             # every partition agrees
+        assert np.array_equal(p.scalars()[:2], info[:2])
+    ps.close()
+
+
+@pytest.mark.parametrize("n_parts", [1, 2, 5])
+def test_boundary_partitions_match_one_partition(n_parts):
+    P, ic = _cyl_problem()
+    want, winfo = _one_partition(P, ic, 5)
+    ps = partition.PartitionedSolver(P, n_parts)
+    ps.set_state(ic)
+    info = ps.step(5)
+    assert np.array_equal(ps.get_state(), want)
+    assert info[1] == winfo[1]
+    ps.close()
+
+
+def test_rk4_and_fixed_time_step():
+    for extra in (dict(time_scheme="rk4"), dict(time_step=2e-4)):
+        P, ic = _kh_problem(17, "kepes_tecno_roe", "minmod", **extra)
+        want, winfo = _one_partition(P, ic, 4)
+        ps = partition.PartitionedSolver(P, 3)
+        ps.set_state(ic, 0.0)
+        info = ps.step(4)
+        assert np.array_equal(ps.get_state(), want), extra
+        assert info[0] == winfo[0]
+        ps.close()
+
+
+def test_restart_from_a_new_state():
+    """A new state mid-run takes the partitions back through prime and the dt exchange."""
+    P, ic = _kh_problem(17, "kepes_tecno_rusanov", "minmod")
+    ps = partition.PartitionedSolver(P, 2)
+    ps.set_state(ic)
+    ps.step(3)
+    mid = ps.get_state()
+    ps.set_state(mid, 0.5)
+    ps.step(2)
+    got = ps.get_state()
+    s = gpu.Solver(P)
+    s.set_state(mid, 0.5)
+    s.step(2)
+    assert np.array_equal(got, s.get_state())
+
+
+def test_partition_handles_refuse_whole_mesh_calls():
+    P, ic = _kh_problem(17, "kep", "first")
+    p = partition.Partition(P, 2, 0)
+    p.set_state(ic)
+    for call in (lambda: p._call("tg_step", 1, None), lambda: p._call("tg_advance", 1, 1, None)):
+        with pytest.raises(gpu.TensumError) as e:
+            call()
+        assert abi.STATUS[e.value.status] == "TG_NOT_SUPPORTED"
+    with pytest.raises(gpu.TensumError) as e:
+        p.begin()                                   # prime and the dt exchange come first
+    assert abi.STATUS[e.value.status] == "TG_INVALID_ARG"
+    p.close()
+    m = cases.cylinder_mesh(8, 16, 0)
+    ns = abi.Problem(preproc.preprocess(m), cases.cylinder_config(0.2, 100.0, 0.0, 1.0, 1))
+    with pytest.raises(gpu.TensumError) as e:
+        partition.Partition(ns, 2, 0)
+    assert abi.STATUS[e.value.status] == "TG_NOT_SUPPORTED"
+
+
+def test_torch_distributed_path_on_one_rank():
+    """DistPartitionedSolver over a one-rank NCCL group: the collectives run on the
+    partition's stream and the result is the one-partition solve."""
+    import datetime
+    import socket
+
+    import torch.distributed as dist
+    with socket.socket() as s:
+        s.bind(("127.0.0.1", 0))
+        port = s.getsockname()[1]
+    dist.init_process_group("nccl", init_method=f"tcp://127.0.0.1:{port}", rank=0, world_size=1,
+                            timeout=datetime.timedelta(seconds=60))
+    try:
+        P, ic = _kh_problem(17, "kepes_tecno_rusanov", "minmod")
+        want, winfo = _one_partition(P, ic, 3)
+        d = partition.DistPartitionedSolver(P, device=0)
+        d.set_state(ic)
+        info = d.step(3)
+        assert np.array_equal(d.get_state(), want)
+        assert info[1] == winfo[1]
+        d.part.close()
+    finally:
+        dist.destroy_process_group()
