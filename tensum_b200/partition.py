@@ -289,13 +289,18 @@ def run_step(parts, exchange):
 
 class PartitionedSolver:
     """One mesh in n_parts partitions, all driven by this process (devices[q]
-    holds partition q; by default all on cuda:0)."""
+    holds partition q; by default all on cuda:0).  With every partition on one
+    device the step -- phases, halo copies and scalar exchange of all partitions
+    -- is captured once as a CUDA graph and replayed (graph=True), so issuing a
+    step costs one launch however many partitions there are."""
 
-    def __init__(self, problem: abi.Problem, n_parts: int, devices=None):
+    def __init__(self, problem: abi.Problem, n_parts: int, devices=None, graph: bool = True):
         devices = devices or [0] * n_parts
         self.nv = problem.geom.n_vertex
         self.parts = [Partition(problem, n_parts, q, devices[q]) for q in range(n_parts)]
         self.exchange = LocalExchange(self.parts)
+        self.graph = graph and len(set(devices)) == 1
+        self._graph = None
 
     def set_state(self, prim: np.ndarray, t0: float = 0.0):
         for p in self.parts:
@@ -304,9 +309,47 @@ class PartitionedSolver:
             p.prime()
         self.exchange.scalars()
 
-    def step(self, n: int) -> np.ndarray:
-        for _ in range(n):
+    def _fresh_events(self):
+        import torch
+        for p in self.parts:
+            p.done = torch.cuda.Event()
+
+    def _capture(self):
+        """Record one step: the partitions' streams fork from the capture stream
+        and join it again, so the graph orders every partition's work."""
+        import torch
+        dev = self.parts[0].device
+        cap = torch.cuda.Stream(device=dev)
+        g = torch.cuda.CUDAGraph()
+        torch.cuda.synchronize(dev)
+        self._fresh_events()          # no wait on events recorded outside the capture
+        with torch.cuda.graph(g, stream=cap):
+            fork = torch.cuda.Event()
+            fork.record(cap)
+            for p in self.parts:
+                p.stream.wait_event(fork)
             run_step(self.parts, self.exchange)
+            for p in self.parts:
+                ev = torch.cuda.Event()
+                ev.record(p.stream)
+                cap.wait_event(ev)
+        self._fresh_events()
+        self._graph, self._cap = g, cap
+
+    def step(self, n: int) -> np.ndarray:
+        if self.graph:
+            import torch
+            dev = self.parts[0].device
+            if self._graph is None:
+                self._capture()
+            torch.cuda.synchronize(dev)            # the partitions' streams hold set_state / prime
+            with torch.cuda.stream(self._cap):
+                for _ in range(n):
+                    self._graph.replay()
+            torch.cuda.synchronize(dev)
+        else:
+            for _ in range(n):
+                run_step(self.parts, self.exchange)
         info = [p.scalars() for p in self.parts]
         return info[0]
 

@@ -44,14 +44,15 @@ def _one_partition(P, ic, steps):
     return out, info
 
 
+@pytest.mark.parametrize("graph", [True, False])
 @pytest.mark.parametrize("flux,recon,n_parts", [("kepes_tecno_rusanov", "minmod", 2),
                                                 ("kepes_tecno_rusanov", "minmod", 3),
                                                 ("kep", "first", 4),
                                                 ("roe_ec", "first", 2)])
-def test_periodic_partitions_match_one_partition(flux, recon, n_parts):
+def test_periodic_partitions_match_one_partition(flux, recon, n_parts, graph):
     P, ic = _kh_problem(33, flux, recon)
     want, winfo = _one_partition(P, ic, 6)
-    ps = partition.PartitionedSolver(P, n_parts)
+    ps = partition.PartitionedSolver(P, n_parts, graph=graph)
     ps.set_state(ic)
     info = ps.step(6)
     got = ps.get_state()
@@ -92,7 +93,7 @@ def test_restart_from_a_new_state():
     P, ic = _kh_problem(17, "kepes_tecno_rusanov", "minmod")
     ps = partition.PartitionedSolver(P, 2)
     ps.set_state(ic)
-    ps.step(3)
+    ps.step(3)                  # captures the step graph; the restart replays it
     mid = ps.get_state()
     ps.set_state(mid, 0.5)
     ps.step(2)
