@@ -34,15 +34,18 @@
 #ifndef TG_TILE_ECAP
 #define TG_TILE_ECAP 512       // edges per tile
 #endif
-// resident flux CTAs per SM the register budget is sized for: TeCNO fluxes / central fluxes
+// resident flux CTAs per SM the register budget is sized for: TeCNO fluxes / central fluxes.
+// Measured at KH 1025^2: 7 central / gradient CTAs (72 / 70 registers, a 48-byte spill in
+// the update-mode central kernels) beat 6 (80 / 74 registers) by 5% a step, 8 (64
+// registers, 100+ bytes of spills) lose; 5 TeCNO CTAs spill and lose.
 #ifndef TG_FLUX_MINB
 #define TG_FLUX_MINB 4
 #endif
 #ifndef TG_FLUX_MINB_CENTRAL
-#define TG_FLUX_MINB_CENTRAL 6
+#define TG_FLUX_MINB_CENTRAL 7
 #endif
 #ifndef TG_GRAD_MINB
-#define TG_GRAD_MINB 6         // resident gradient / dt CTAs per SM the register budget is sized for
+#define TG_GRAD_MINB 7         // resident gradient / dt CTAs per SM the register budget is sized for
 #endif
 
 namespace tg {
