@@ -35,6 +35,13 @@ trained on the first --train solves, and the time to a 1 % relative standard
 error of the mean and of the variance of each QoI for plain FP64 MC, batched
 FP32 MC and batched FP32 with the control variate.
 
+    python bench.py --workload partitioned [--parts 1,2,4] [--steps K]
+
+times the domain-decomposed single solve (tensum_b200.partition) on the same
+Kelvin-Helmholtz workload: every partition on this one GPU, halos exchanged by
+device copies, the whole step of all partitions replayed as one CUDA graph,
+against the one-partition step, per flux and partition count.
+
 --workload mc measures the Monte Carlo configuration instead: S Kelvin-Helmholtz samples
 (rnd rows, device-generated initial states) on an n x n mesh advanced together
 by the batched FP32 engine (KEPES-TeCNO-Rusanov, minmod), against the FP64
@@ -78,7 +85,7 @@ def parse():
     ap.add_argument("--seed", type=int, default=0)
     ap.add_argument("--e2e-steps", type=int, default=20)
     ap.add_argument("--no-cpu-baseline", action="store_true")
-    ap.add_argument("--workload", default="single", choices=["single", "mc", "cylinder"])
+    ap.add_argument("--workload", default="single", choices=["single", "mc", "cylinder", "partitioned"])
     ap.add_argument("--samples", type=int, default=None,
                     help="ensemble size (--workload mc: 4096, --workload cylinder: 1024)")
     ap.add_argument("--final-time", type=float, default=2.0, help="cylinder: run length of every sample")
@@ -87,6 +94,7 @@ def parse():
     ap.add_argument("--fp64-samples", type=int, default=32, help="cylinder: samples also run in FP64")
     ap.add_argument("--train", type=int, default=256, help="cylinder: solver runs the surrogate is trained on")
     ap.add_argument("--no-mc", action="store_true", help="skip the Monte Carlo object of the default line")
+    ap.add_argument("--parts", default="1,2,4", help="partitioned: partition counts")
     a = ap.parse_args()
     a.flux_list = [(f, r) for f, r in FLUXES if f in a.fluxes.split(",")]
     return a
@@ -642,8 +650,55 @@ def run_cylinder(args):
     return 0
 
 
+def run_partitioned(args):
+    """The domain-decomposed solve (all partitions on this GPU) against the one-partition step."""
+    import torch
+    from tensum_b200 import abi, gpu, partition, preproc
+    m, prim0 = workload(args)
+    g = preproc.preprocess(m)
+    parts = [int(x) for x in args.parts.split(",")]
+    steps = max(5, min(args.steps, 100))
+    V = g.n_vertex
+    one, per, ghosts = {}, {str(n): {} for n in parts}, {}
+    for flux, recon in args.flux_list:
+        P = abi.Problem(g, flux_cfg(flux, recon))
+        s = gpu.Solver(P)
+        s.set_state(prim0)
+        s.step(max(3, args.warmup))
+        one[flux] = s.time_phase("step", steps)
+        s.close()
+        for n in parts:
+            ps = partition.PartitionedSolver(P, n)
+            ps.set_state(prim0)
+            ps.step(max(3, args.warmup))
+            per[str(n)][flux] = ps.time_steps(steps)
+            ghosts[str(n)] = max(p.n_ghost for p in ps.parts) / max(p.n_owned for p in ps.parts)
+            ps.close()
+        torch.cuda.synchronize()
+    nmax = str(max(parts))
+    total_ms = sum(per[nmax].values())
+    line = {"metric": "vertex-stage updates/s (one mesh in partitions, all on one GPU)",
+            "value": len(per[nmax]) * V * 3 / (total_ms / 1e3), "unit": UNIT, "n_gpus": 1, "steps": steps,
+            "higher_is_better": True, "dtype": "f64", "data": "synthetic (seeded mesh and field)",
+            "config": {"workload": f"kelvin-helmholtz periodic {args.n}x{args.n}, ssprk3 cfl 0.8, fp64, "
+                                   f"partitions {args.parts} on one GPU, step captured as one CUDA graph",
+                       "fluxes": [f for f, _ in args.flux_list]},
+            "one_partition_ms_per_step": {k: round(v, 4) for k, v in one.items()},
+            "partitioned_ms_per_step": {n: {k: round(v, 4) for k, v in d.items()} for n, d in per.items()},
+            "ghost_fraction": {n: round(v, 4) for n, v in ghosts.items()},
+            "command": "python bench.py --workload partitioned --parts " + args.parts}
+    print(json.dumps(line))
+    return 0
+
+
 def main():
     args = parse()
+    if args.workload == "partitioned":
+        if args.impl == "reference":
+            print(json.dumps({"impl": "reference", "unavailable": "the reference partitions through METIS part files "
+                              "and MPI; its single-process run is the single-solve reference arm"}))
+            return 0
+        return run_partitioned(args)
     if args.workload == "mc":
         if args.impl == "reference":
             print(json.dumps({"impl": "reference", "unavailable": "the reference has no batched ensemble path; its MC "

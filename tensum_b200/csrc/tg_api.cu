@@ -71,6 +71,7 @@ struct tg_handle {
   cudaGraph_t wgraph = nullptr;                // a step whose dt the previous step formed
   cudaGraphExec_t wgraph_exec = nullptr;
   bool cold = true;                            // the next step may not find dt_next set
+  bool w_partial[3] = {false, false, false};   // a step left only V5 in this buffer's W (refresh_w)
   // state transfers: PrimVar records in the caller's order on the device
   double* raw = nullptr;              // 5 * nv doubles
   const int* old_of_new = nullptr;    // device copy of the vertex permutation
@@ -282,6 +283,21 @@ void enqueue_tile_flux(tg_handle* h, int b, int mode, int r, bool norm, int bout
   tile_kernel(h->prm.flux, h->prm.recon, mode)<<<h->L.ntiles, kTileThreads, h->smem_flux, h->stream>>>(
       h->prm, h->mv, h->tv, view(h, b), h->ctl, h->sc, r, norm ? 1 : 0, h->Pb[bout], h->Wb[bout], h->L.lmax,
       h->L.emax, done);
+}
+
+// Inviscid central-flux steps without strong conditions store only V5 of the entropy
+// variables (w3_only in k_tile_flux).  Steps mark the buffers they wrote; before
+// gradients are formed outside a step, a marked buffer gets all four back from P.
+void mark_steps(tg_handle* h) {
+  const bool central = h->prm.flux != FLUX_TECNO_ROE && h->prm.flux != FLUX_TECNO_RUSANOV;
+  if (central && h->prm.model == 0 && !h->prm.strong)
+    for (int b = 0; b < 3; ++b) h->w_partial[b] = true;
+}
+
+void refresh_w(tg_handle* h, int b) {
+  if (!h->w_partial[b]) return;
+  k_prim2ent<<<nblk(h->mv.nv), kBlock, 0, h->stream>>>(h->prm, h->mv.nv, h->Pb[b], h->Wb[b]);
+  h->w_partial[b] = false;
 }
 
 int residual_kernels(const tg_handle* h) {
@@ -505,6 +521,7 @@ tg_status take_queued_input(tg_handle* h) {
   k_state_check<<<nblk(nv), kBlock, 0, h->stream>>>(nv, h->in_stage[slot], h->bad);
   k_state_in<<<nblk(nv), kBlock, 0, h->stream>>>(nv, h->in_stage[slot], h->old_of_new, h->bad, h->sv.P);
   k_prim2ent_checked<<<nblk(nv), kBlock, 0, h->stream>>>(h->prm, nv, h->sv.P, h->sv.W, h->bad);
+  h->w_partial[0] = false;
   k_scalars_set<<<1, 1, 0, h->stream>>>(h->sc, fresh_scalars(h, t0), h->bad);
   h->in_check = true;
   h->cold = true;
@@ -554,7 +571,10 @@ void enqueue_phase(tg_handle* h, int phase) {
       break;
     case TG_PHASE_UPDATE: enqueue_update(h, 1, false, h->never); break;
     case TG_PHASE_DT: enqueue_dt(h, h->never); break;
-    default: cudaGraphLaunch(step_graph(h), h->stream); break;
+    default:
+      cudaGraphLaunch(step_graph(h), h->stream);
+      mark_steps(h);
+      break;
   }
 }
 
@@ -589,6 +609,7 @@ tg_status take_raw_state(tg_handle* h, double t0) {
   if ((st = sync(h)) != TG_OK) return st;
   if (bad) return fail(h, TG_INVALID_ARG, "state needs T > 0 and p > 0 (src/fv.cc:388-389)");
   k_prim2ent<<<nblk(nv), kBlock, 0, h->stream>>>(h->prm, nv, h->sv.P, h->sv.W);
+  h->w_partial[0] = false;
   const Scalars s = fresh_scalars(h, t0);
   TG_CUDA(h, cudaMemcpyAsync(h->sc, &s, sizeof(s), cudaMemcpyHostToDevice, h->stream));
   h->cold = true;
@@ -991,6 +1012,7 @@ static tg_status copy_grad_out(tg_handle* h, double* dE_out) {
 tg_status tg_gradients(tg_handle* h, double* dE_out) {
   TG_WHOLE_MESH(h)
   if (!h) return fail(h, TG_INVALID_ARG, "NULL handle");
+  refresh_w(h, 0);
   enqueue_gradient(h, 0, false, true, h->never);
   tg_status st = sync(h);
   if (st != TG_OK || !dE_out) return st;
@@ -1018,6 +1040,7 @@ tg_status tg_update(tg_handle* h, int r) {
   if (!h) return fail(h, TG_INVALID_ARG, "NULL handle");
   if (r < 0 || r >= h->ctl.n_rks) return fail(h, TG_INVALID_ARG, "stage index out of range for the time scheme");
   enqueue_update(h, r, false, h->never);
+  h->w_partial[0] = false;                   // k_update stores all four entropy variables
   if (h->prm.strong && h->mv.nsb > 0)
     k_strong_bc<<<nblk(h->mv.nsb), kBlock, 0, h->stream>>>(h->mv, h->sv.P, h->never);
   clear_dt_next(h);
@@ -1062,6 +1085,7 @@ tg_status tg_step(tg_handle* h, int n_steps, double* info4) {
   if ((st = take_queued_input(h)) != TG_OK) return st;
   const cudaGraphExec_t g = step_graph(h);
   for (int i = 0; i < n_steps; ++i) TG_CUDA(h, cudaGraphLaunch(g, h->stream));
+  if (n_steps > 0) mark_steps(h);
   Scalars s;
   st = read_scalars(h, &s);
   if (st != TG_OK) return st;
@@ -1117,6 +1141,7 @@ tg_status tg_advance(tg_handle* h, int instance, long max_steps, double* info5) 
     const long chunk = std::min<long>(16, max_steps - launched);
     const cudaGraphExec_t g = step_graph(h);
     for (long i = 0; i < chunk; ++i) TG_CUDA(h, cudaGraphLaunch(g, h->stream));
+    mark_steps(h);
     launched += chunk;
     if ((st = read_scalars(h, &s)) != TG_OK) return st;
     h->cold = !s.dt_next;
@@ -1187,6 +1212,7 @@ tg_status tg_output_begin(tg_handle* h, double* prim_out, double* dE_out, int gr
     // the reference writes the dE of its last compute_gradients: the last stage's input
     // state after a step, the current state after compute_forces of a Navier-Stokes run
     const int last_in = h->ctl.scheme == 1 ? 1 : h->ctl.n_rks - 1;
+    refresh_w(h, grad_state == TG_GRAD_CURRENT ? 0 : last_in);
     enqueue_gradient(h, grad_state == TG_GRAD_CURRENT ? 0 : last_in, false, true, h->never);
     k_grad_out<<<nblk(nv), kBlock, 0, h->stream>>>(nv, h->sv.G, h->old_of_new, h->snap_grad, h->sc,
                                                     grad_state == TG_GRAD_LAST_STAGE ? 1 : 0);
@@ -1270,8 +1296,12 @@ tg_status tg_moments_increment(tg_handle* h, int instance, long k) {
     // fluxes needed gradients
     Scalars s;
     if ((st = read_scalars(h, &s)) != TG_OK) return st;
-    if (s.iter == 0) enqueue_gradient(h, 0, false, true, h->never);
-    else if (!h->grads_needed) enqueue_gradient(h, 2, false, true, h->never);
+    if (s.iter == 0) {
+      enqueue_gradient(h, 0, false, true, h->never);
+    } else if (!h->grads_needed) {
+      refresh_w(h, 2);
+      enqueue_gradient(h, 2, false, true, h->never);
+    }
   }
   k_moments_increment<<<nblk(h->L.nv), kBlock, 0, h->stream>>>(h->prm, h->L.nv, h->sv.P, h->sv.G, h->mom_extras,
                                                                  h->mom_nvar, (long long)k, mom_array(h, instance, 0),

@@ -104,6 +104,12 @@ __device__ __forceinline__ Prim con2prim(const Params& k, const Cons& c) {   // 
   return q;
 }
 
+// V5 = -2 beta of prim2ent alone, with its operations (no logarithm).
+__device__ __forceinline__ double prim2ent_v5(const Params& k, const Prim& q) {
+  double beta = density(k, q) / (2 * q.p);
+  return -2 * beta;
+}
+
 __device__ __forceinline__ Ent prim2ent(const Params& k, const Prim& q) {   // src/material.h:534-546
   Ent e;
   double rho = density(k, q);

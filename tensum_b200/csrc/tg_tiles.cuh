@@ -318,6 +318,15 @@ __device__ __forceinline__ VRec load_vrec(const double* sV, int L, int i) {
   return q;
 }
 
+// Whether a stage update stores only V5 of the entropy variables: the central fluxes
+// read no other, and an inviscid run forms no gradients inside its steps.  Strong
+// conditions keep all four: they reset P after the update and leave the entropy
+// variables of the reset vertices as the update formed them, as the reference does.
+template <int FLUX>
+__device__ __forceinline__ bool w3_only(const Params& k) {
+  return FLUX != FLUX_TECNO_ROE && FLUX != FLUX_TECNO_RUSANOV && k.model == 0 && !k.strong;
+}
+
 template <int FLUX, int RECON, int MODE>
 __global__ void __launch_bounds__(kTileThreads, (FLUX == FLUX_TECNO_ROE || FLUX == FLUX_TECNO_RUSANOV)
                                                     ? TG_FLUX_MINB : TG_FLUX_MINB_CENTRAL)
@@ -470,9 +479,15 @@ __global__ void __launch_bounds__(kTileThreads, (FLUX == FLUX_TECNO_ROE || FLUX 
       double factor = dtv / (vertex_radius(k, m, v) * area);
       Cons c = rk_stage(k, ctl, s, nv, v, r, q0, uo, factor, r0, r1, r2, r3);
       Prim q = con2prim(k, c);
-      Ent e = prim2ent(k, q);
       Pout[v] = q.T; Pout[nv + v] = q.u; Pout[2 * nv + v] = q.v; Pout[3 * nv + v] = q.p;
-      Wout[v] = e.f; Wout[nv + v] = e.vx; Wout[2 * nv + v] = e.vy; Wout[3 * nv + v] = e.l;
+      if (w3_only<FLUX>(k)) {
+        // inviscid central fluxes read only V5 = -2 beta: the other entropy variables
+        // (two logarithms) are formed from P by whatever later needs them (refresh_w)
+        Wout[3 * nv + v] = prim2ent_v5(k, q);
+      } else {
+        Ent e = prim2ent(k, q);
+        Wout[v] = e.f; Wout[nv + v] = e.vx; Wout[2 * nv + v] = e.vy; Wout[3 * nv + v] = e.l;
+      }
       bool ok = isfinite(q.T) && isfinite(q.u) && isfinite(q.v) && isfinite(q.p) && q.p > 0.0 && c.r > 0.0;
       if (!ok) atomicOr(&sc->bad, 1);
       if (next_dt) qn = q;

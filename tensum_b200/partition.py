@@ -353,6 +353,24 @@ class PartitionedSolver:
         info = [p.scalars() for p in self.parts]
         return info[0]
 
+    def time_steps(self, n: int) -> float:
+        """Device time of n replayed steps (CUDA events on the graph's stream), ms per step."""
+        import torch
+        if not self.graph:
+            raise ValueError("time_steps replays the captured step (graph=True, one device)")
+        dev = self.parts[0].device
+        if self._graph is None:
+            self._capture()
+        torch.cuda.synchronize(dev)
+        a, b = torch.cuda.Event(enable_timing=True), torch.cuda.Event(enable_timing=True)
+        a.record(self._cap)
+        with torch.cuda.stream(self._cap):
+            for _ in range(n):
+                self._graph.replay()
+        b.record(self._cap)
+        b.synchronize()
+        return a.elapsed_time(b) / n
+
     def get_state(self) -> np.ndarray:
         out = np.zeros((self.nv, 5))
         for p in self.parts:

@@ -5,7 +5,7 @@ output time wrote are kept next to them.
 Needs the reference tree and a built oracle/_ref/tensum_harness (``make -C
 oracle ref``); run from the repository root:
 
-    python tests/golden/make_output_golden.py
+    python tests/golden/make_output_golden.py [case ...]
 
 Tests regenerate every file with tensum_b200.writer from the kept arrays and
 compare the text byte for byte, and compare device snapshots with the arrays.
@@ -31,7 +31,9 @@ OUT = os.path.dirname(os.path.abspath(__file__))
 def main():
     if not ref_runner.harness_available():
         raise SystemExit("oracle/_ref/tensum_harness missing: run `make -C oracle ref` first")
-    for name, spec in OUTPUT_CASES.items():
+    names = sys.argv[1:] or list(OUTPUT_CASES)
+    for name in names:
+        spec = OUTPUT_CASES[name]
         mesh, cfg, prim0 = build_output_case(spec)
         d, texts = ref_runner.run_files(mesh, cfg, prim0, spec["steps"])
         keep = {k: v for k, v in d.items() if k.startswith("o") or k in (
