@@ -146,3 +146,21 @@ def test_torch_distributed_path_on_one_rank():
         d.part.close()
     finally:
         dist.destroy_process_group()
+
+
+@pytest.mark.parametrize("name", ["sq_roe_minmod_voronoi", "sq_kepec_axi_long", "cyl_slip_axi_voronoi"])
+def test_voronoi_and_axisymmetric_partitions(name):
+    """Voronoi duals (gradient-only edges) and axisymmetric radii go with the
+    partition's edges and vertices: partitions repeat the one-partition solve,
+    which the fixture pins to the reference."""
+    from tests.golden.cases_spec import CASES, build_case
+    from tests.helpers import geometry
+    mesh, cfg, prim0 = build_case(CASES[name])
+    P = abi.Problem(geometry(mesh, cfg), dict(cfg, final_time=1e9, time_stamps=1))
+    want, winfo = _one_partition(P, prim0, 4)
+    ps = partition.PartitionedSolver(P, 3)
+    ps.set_state(prim0)
+    info = ps.step(4)
+    assert np.array_equal(ps.get_state(), want)
+    assert info[1] == winfo[1]
+    ps.close()
