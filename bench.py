@@ -95,6 +95,7 @@ def parse():
     ap.add_argument("--train", type=int, default=256, help="cylinder: solver runs the surrogate is trained on")
     ap.add_argument("--no-mc", action="store_true", help="skip the Monte Carlo object of the default line")
     ap.add_argument("--parts", default="1,2,4", help="partitioned: partition counts")
+    ap.add_argument("--throughput-only", action="store_true", help="mc: the ensemble's stepping alone")
     a = ap.parse_args()
     a.flux_list = [(f, r) for f, r in FLUXES if f in a.fluxes.split(",")]
     return a
@@ -433,8 +434,9 @@ def run_ours(args):
 MC_BYTES_PER_VSS = 187.0   # FP32 batched compulsory bytes per vertex-sample-stage (state, U_old, gradients)
 
 
-def mc_line(n, S, K, W, seed):
-    """Batched FP32 ensemble throughput and time to QoI error (one GPU): the JSON object."""
+def mc_line(n, S, K, W, seed, throughput_only=False):
+    """Batched FP32 ensemble throughput and time to QoI error (one GPU): the JSON object
+    (throughput_only: the graph-replayed steps alone, e.g. for a profiler)."""
     import torch
     from tensum_b200 import abi, batch, cases, cv, gpu, mlp, preproc
     torch.cuda.set_device(0)
@@ -458,6 +460,12 @@ def mc_line(n, S, K, W, seed):
     launches = int(b.query("kernels_per_step")) * K
     del b
     peak, peak_kind = measured_peaks()
+    if throughput_only:
+        return {"metric": "vertex-sample-stage updates/s (FP32 ensemble)", "value": value,
+                "unit": "vertex-sample-stage updates/s", "ms_per_step": ms / K, "steps": K, "gpu_launches": launches,
+                "config": {"workload": f"kelvin-helmholtz {n}x{n} periodic ensemble of {S} samples, "
+                                       "kepes_tecno_rusanov(minmod), ssprk3, fp32 members", "shape": shape},
+                "clocks": clk.summary()}
 
     # FP64 per-sample path on the same mesh
     s64 = gpu.Solver(P_long)
@@ -555,7 +563,8 @@ def mc_line(n, S, K, W, seed):
 
 def run_mc(args):
     n = args.n if args.n != 1025 else 257
-    print(json.dumps(mc_line(n, args.samples or 4096, args.steps, max(3, args.warmup), args.seed)))
+    print(json.dumps(mc_line(n, args.samples or 4096, args.steps, max(3, args.warmup), args.seed,
+                             throughput_only=args.throughput_only)))
     return 0
 
 
