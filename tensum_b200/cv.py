@@ -12,7 +12,7 @@ It is unbiased for any fixed beta because E[g(X)] = E[g(X')]; estimating beta
 from the same N pairs adds an O(1/N) bias that the plain estimate bounds.  Its
 variance is Var(Y - beta g)/N + beta^2 Var(g)/M against Var(Y)/N for plain MC.
 Plain MC is both the fallback (used whenever the control variate does not
-reduce the estimated variance) and the judge: every result reports the plain
+reduce the estimated variance) and the yardstick: every result reports the plain
 estimate and the variance ratio next to the multi-fidelity one.  The surrogate
 never replaces the solver.  The variance of Y is estimated the same way from
 the second moment E[Y^2] with g^2 as its control.
