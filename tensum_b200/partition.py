@@ -383,25 +383,52 @@ class PartitionedSolver:
 
 
 class DistPartitionedSolver:
-    """This rank's partition of one mesh (rank r of the group holds partition r)."""
+    """This rank's partition of one mesh (rank r of the group holds partition r).
+    With graph=True (NCCL groups) the step -- phases and collectives -- is captured
+    once as a CUDA graph on the partition's stream and replayed; every rank captures
+    and replays the same sequence."""
 
-    def __init__(self, problem: abi.Problem, group=None, device: int | None = None):
+    def __init__(self, problem: abi.Problem, group=None, device: int | None = None, graph: bool = False):
         import torch
         import torch.distributed as dist
         n_parts, part = dist.get_world_size(group), dist.get_rank(group)
         self.part = Partition(problem, n_parts, part, torch.cuda.current_device() if device is None else device)
         self.exchange = DistExchange(self.part, group)
         self.nv = problem.geom.n_vertex
+        self.graph = graph
+        self._graph = None
 
     def set_state(self, prim: np.ndarray, t0: float = 0.0):
         self.part.set_state(prim, t0)
         self.part.prime()
         self.exchange.scalars()
 
+    def _capture(self):
+        import torch
+        p = self.part
+        torch.cuda.synchronize(p.device)
+        g = torch.cuda.CUDAGraph()
+        with torch.cuda.graph(g, stream=p.stream):
+            run_step([p], self.exchange)
+        self._graph = g
+
     def step(self, n: int) -> np.ndarray:
-        for _ in range(n):
-            run_step([self.part], self.exchange)
+        if self.graph:
+            import torch
+            if self._graph is None:
+                self._capture()
+            with torch.cuda.stream(self.part.stream):
+                for _ in range(n):
+                    self._graph.replay()
+        else:
+            for _ in range(n):
+                run_step([self.part], self.exchange)
         return self.part.scalars()
+
+    def close(self):
+        """Releases the captured graph (it holds the collectives) before the handle."""
+        self._graph = None
+        self.part.close()
 
     def get_state(self, out: np.ndarray | None = None) -> np.ndarray:
         """The records this rank owns, written into `out` (others left as they are)."""

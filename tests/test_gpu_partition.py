@@ -123,9 +123,11 @@ def test_partition_handles_refuse_whole_mesh_calls():
     assert abi.STATUS[e.value.status] == "TG_NOT_SUPPORTED"
 
 
-def test_torch_distributed_path_on_one_rank():
+@pytest.mark.parametrize("graph", [False, True])
+def test_torch_distributed_path_on_one_rank(graph):
     """DistPartitionedSolver over a one-rank NCCL group: the collectives run on the
-    partition's stream and the result is the one-partition solve."""
+    partition's stream (eagerly, or captured with the phases as one CUDA graph) and
+    the result is the one-partition solve."""
     import datetime
     import socket
 
@@ -138,12 +140,12 @@ def test_torch_distributed_path_on_one_rank():
     try:
         P, ic = _kh_problem(17, "kepes_tecno_rusanov", "minmod")
         want, winfo = _one_partition(P, ic, 3)
-        d = partition.DistPartitionedSolver(P, device=0)
+        d = partition.DistPartitionedSolver(P, device=0, graph=graph)
         d.set_state(ic)
         info = d.step(3)
         assert np.array_equal(d.get_state(), want)
         assert info[1] == winfo[1]
-        d.part.close()
+        d.close()
     finally:
         dist.destroy_process_group()
 
