@@ -378,6 +378,8 @@ class PartitionedSolver:
         return out
 
     def close(self):
+        """Releases the captured graph (it names the handles' memory), then the handles."""
+        self._graph = None
         for p in self.parts:
             p.close()
 
