@@ -668,7 +668,7 @@ def run_partitioned(args):
     parts = [int(x) for x in args.parts.split(",")]
     steps = max(5, min(args.steps, 100))
     V = g.n_vertex
-    one, per, ghosts = {}, {str(n): {} for n in parts}, {}
+    one, per, seq, ghosts, frontier = {}, {str(n): {} for n in parts}, {str(n): {} for n in parts}, {}, {}
     for flux, recon in args.flux_list:
         P = abi.Problem(g, flux_cfg(flux, recon))
         s = gpu.Solver(P)
@@ -677,12 +677,14 @@ def run_partitioned(args):
         one[flux] = s.time_phase("step", steps)
         s.close()
         for n in parts:
-            ps = partition.PartitionedSolver(P, n)
-            ps.set_state(prim0)
-            ps.step(max(3, args.warmup))
-            per[str(n)][flux] = ps.time_steps(steps)
-            ghosts[str(n)] = max(p.n_ghost for p in ps.parts) / max(p.n_owned for p in ps.parts)
-            ps.close()
+            for overlap in (True, False):
+                ps = partition.PartitionedSolver(P, n, overlap=overlap)
+                ps.set_state(prim0)
+                ps.step(max(3, args.warmup))
+                (per if overlap else seq)[str(n)][flux] = ps.time_steps(steps)
+                ghosts[str(n)] = max(p.n_ghost for p in ps.parts) / max(p.n_owned for p in ps.parts)
+                frontier[str(n)] = sum(p.n_frontier for p in ps.parts) / sum(p.n_tiles for p in ps.parts)
+                ps.close()
         torch.cuda.synchronize()
     nmax = str(max(parts))
     total_ms = sum(per[nmax].values())
@@ -690,11 +692,14 @@ def run_partitioned(args):
             "value": len(per[nmax]) * V * 3 / (total_ms / 1e3), "unit": UNIT, "n_gpus": 1, "steps": steps,
             "higher_is_better": True, "dtype": "f64", "data": "synthetic (seeded mesh and field)",
             "config": {"workload": f"kelvin-helmholtz periodic {args.n}x{args.n}, ssprk3 cfl 0.8, fp64, "
-                                   f"partitions {args.parts} on one GPU, step captured as one CUDA graph",
+                                   f"partitions {args.parts} on one GPU, step captured as one CUDA graph, "
+                                   "exchanges overlapped with the interior tiles (and, beside it, not)",
                        "fluxes": [f for f, _ in args.flux_list]},
             "one_partition_ms_per_step": {k: round(v, 4) for k, v in one.items()},
             "partitioned_ms_per_step": {n: {k: round(v, 4) for k, v in d.items()} for n, d in per.items()},
+            "partitioned_no_overlap_ms_per_step": {n: {k: round(v, 4) for k, v in d.items()} for n, d in seq.items()},
             "ghost_fraction": {n: round(v, 4) for n, v in ghosts.items()},
+            "frontier_tile_fraction": {n: round(v, 4) for n, v in frontier.items()},
             "command": "python bench.py --workload partitioned --parts " + args.parts}
     print(json.dumps(line))
     return 0

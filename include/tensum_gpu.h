@@ -355,15 +355,21 @@ tg_status tg_query(tg_handle* h, int key, double* out);
  *
  * A step, every call enqueued on the handle's stream (tg_stream), no host wait:
  *   tg_part_begin
- *   for each stage r:  tg_part_gradients(r), exchange TG_HALO_GRAD,
- *                      tg_part_flux(r),      exchange TG_HALO_STATE
+ *   for each stage r:  tg_part_gradients(r, TG_TILES_ALL), exchange TG_HALO_GRAD,
+ *                      tg_part_flux(r, TG_TILES_ALL),      exchange TG_HALO_STATE
  *   tg_part_export, all-gather of the 5-word records in partition order, tg_part_import
+ * The tiles are ordered frontier first (tiles that read a ghost), interior after; the
+ * interior tiles need no ghost, so each exchange can overlap them:
+ *   gradients(r, INTERIOR) | finish STATE | gradients(r, FRONTIER) | start GRAD |
+ *   flux(r, INTERIOR) | finish GRAD | flux(r, FRONTIER) | start STATE
+ * (without gradients: flux(r, INTERIOR) | finish STATE | flux(r, FRONTIER) | start STATE).
  * An exchange of a field: tg_part_pack into the send buffer (8 doubles per
  * vertex, peers in ascending order, send_counts[q] vertices for peer q), the
  * all-to-all, tg_part_unpack from the receive buffer (recv_counts[q] vertices
  * from peer q, peers ascending).  After tg_set_state (the whole mesh's records):
  * tg_part_prime, then the scalar exchange, before the first tg_part_begin. */
 enum { TG_HALO_STATE = 0, TG_HALO_GRAD = 1 };
+enum { TG_TILES_ALL = 0, TG_TILES_FRONTIER = 1, TG_TILES_INTERIOR = 2 };
 
 /* Host only (no device): the plan of partition `part`.  out4 = {n_owned, n_ghost,
  * n_send, n_recv}; the optional arrays receive the caller indices of the
@@ -373,15 +379,18 @@ tg_status tg_part_plan(const tg_mesh* mesh, const tg_bc_table* bc, int n_parts, 
                        int* send_counts, int* recv_counts, int* send_idx, int* recv_idx);
 tg_status tg_part_create(const tg_mesh* mesh, const tg_material* mat, const tg_bc_table* bc, const tg_options* opt,
                          int n_parts, int part, tg_handle** out);
-/* out6 = {n_parts, part, n_owned, n_ghost, n_send, n_recv}; counts per peer. */
-tg_status tg_part_info(tg_handle* h, int* out6, int* send_counts, int* recv_counts);
+/* out8 = {n_parts, part, n_owned, n_ghost, n_send, n_recv, n_tiles, n_frontier_tiles};
+ * counts per peer. */
+tg_status tg_part_info(tg_handle* h, int* out8, int* send_counts, int* recv_counts);
 /* Local dt and U_old of the owned vertices of a new state (the first-stage dt pass). */
 tg_status tg_part_prime(tg_handle* h);
 tg_status tg_part_begin(tg_handle* h);
-tg_status tg_part_gradients(tg_handle* h, int stage);
+/* tiles: TG_TILES_ALL, or TG_TILES_FRONTIER and TG_TILES_INTERIOR in either order. */
+tg_status tg_part_gradients(tg_handle* h, int stage, int tiles);
 /* Boundary and edge fluxes and the stage update; the last stage also forms the
- * next step's local dt and U_old and this partition's residual-norm sums. */
-tg_status tg_part_flux(tg_handle* h, int stage);
+ * next step's local dt and U_old and this partition's residual-norm sums.  tiles:
+ * TG_TILES_ALL, or TG_TILES_INTERIOR followed by TG_TILES_FRONTIER. */
+tg_status tg_part_flux(tg_handle* h, int stage, int tiles);
 tg_status tg_part_pack(tg_handle* h, int field, void* dev_send);
 tg_status tg_part_unpack(tg_handle* h, int field, const void* dev_recv);
 /* 5 x 8 bytes: the dt minimum (bits) and the four residual-norm sums. */

@@ -108,6 +108,7 @@ struct tg_handle {
     const int* send_idx = nullptr;       // device: local ids of owned vertices, per peer
     const int* recv_idx = nullptr;       // device: local ids of ghosts, per peer
     int cur = 0;                         // state buffer the last flux phase wrote
+    int n_frontier = 0;                  // tiles that read ghosts: tile order [0, n_frontier), interior after
     bool norms_pending = false;          // a step ended since the last tg_part_import
     double* out = nullptr;               // device: owned PrimVar records (tg_get_state)
   } part;
@@ -262,13 +263,22 @@ StateView view(const tg_handle* h, int b) {
 // Gradients (when `grad`), plus at the first stage dt and U_old.
 // At a step's first stage with fuse_dt, the first-stage kernel runs when dt and
 // U_old are still to be formed, else a gradient-only launch (warm) takes its place.
-void enqueue_gradient(tg_handle* h, int b, bool first, bool grad, const int* done) {
+// Tiles [base, base + count) of the handle's tile order (all tiles by default).
+TileView tiles(const tg_handle* h, int base) {
+  TileView v = h->tv;
+  v.base = base;
+  return v;
+}
+
+void enqueue_gradient(tg_handle* h, int b, bool first, bool grad, const int* done, int base = 0, int count = -1) {
   if (!first && !grad) return;
-  grad_kernel(first, grad)<<<h->L.ntiles, kTileThreads, first ? h->smem_grad1 : h->smem_grad0, h->stream>>>(
-      h->prm, h->mv, h->tv, view(h, b), h->sc, h->L.lmax, h->L.emax, done, 0);
+  if (count < 0) count = h->L.ntiles;
+  if (count == 0) return;
+  grad_kernel(first, grad)<<<count, kTileThreads, first ? h->smem_grad1 : h->smem_grad0, h->stream>>>(
+      h->prm, h->mv, tiles(h, base), view(h, b), h->sc, h->L.lmax, h->L.emax, done, 0);
   if (first && grad && h->prm.fuse_dt)
-    grad_kernel(false, true)<<<h->L.ntiles, kTileThreads, h->smem_grad0, h->stream>>>(
-        h->prm, h->mv, h->tv, view(h, b), h->sc, h->L.lmax, h->L.emax, done, 1);
+    grad_kernel(false, true)<<<count, kTileThreads, h->smem_grad0, h->stream>>>(
+        h->prm, h->mv, tiles(h, base), view(h, b), h->sc, h->L.lmax, h->L.emax, done, 1);
 }
 
 // boundary-face and viscous contributions, gathered by the tiled flux kernel
@@ -279,9 +289,12 @@ void enqueue_boundary(tg_handle* h, int b, const int* done) {
   if (h->viscous) k_viscous<<<nblk(h->mv.nvu), kBlock, 0, h->stream>>>(h->prm, h->mv, view(h, b), done);
 }
 
-void enqueue_tile_flux(tg_handle* h, int b, int mode, int r, bool norm, int bout, const int* done) {
-  tile_kernel(h->prm.flux, h->prm.recon, mode)<<<h->L.ntiles, kTileThreads, h->smem_flux, h->stream>>>(
-      h->prm, h->mv, h->tv, view(h, b), h->ctl, h->sc, r, norm ? 1 : 0, h->Pb[bout], h->Wb[bout], h->L.lmax,
+void enqueue_tile_flux(tg_handle* h, int b, int mode, int r, bool norm, int bout, const int* done, int base = 0,
+                       int count = -1) {
+  if (count < 0) count = h->L.ntiles;
+  if (count == 0) return;
+  tile_kernel(h->prm.flux, h->prm.recon, mode)<<<count, kTileThreads, h->smem_flux, h->stream>>>(
+      h->prm, h->mv, tiles(h, base), view(h, b), h->ctl, h->sc, r, norm ? 1 : 0, h->Pb[bout], h->Wb[bout], h->L.lmax,
       h->L.emax, done);
 }
 
@@ -741,6 +754,9 @@ static tg_status create_handle(const tg_mesh* mesh, const tg_material* mat, cons
   UPT(cv_off, cv_off) UPT(cv_ent, cv_ent) UPT(x, x) UPT(y, y) UPT(te_ux, ux) UPT(te_uy, uy) UPT(te_ar, ar)
   UPT(te_r, r)
 #undef UPT
+  h->tv.order = nullptr;
+  h->tv.base = 0;
+  h->tv.total = L.ntiles;
   const size_t nv = L.nv;
   h->nblocks_v = nblk(L.nv);
 #define AL(field, n) \
@@ -825,6 +841,17 @@ static tg_status create_handle(const tg_mesh* mesh, const tg_material* mat, cons
     if ((st = dev_upload(h, plan.send_idx, &P.send_idx)) != TG_OK) { tg_destroy(h); return st; }
     if ((st = dev_upload(h, plan.recv_idx, &P.recv_idx)) != TG_OK) { tg_destroy(h); return st; }
     if ((st = dev_alloc(h, 5 * (size_t)std::max(1, P.n_owned), &P.out)) != TG_OK) { tg_destroy(h); return st; }
+    // frontier tiles (some local vertex is a ghost) first, then the interior ones, so a
+    // driver can run the interior while a halo exchange is in flight
+    std::vector<int> order, interior;
+    for (int t = 0; t < L.ntiles; ++t) {
+      bool ghost = false;
+      for (int i = L.t_loff[t]; i < L.t_loff[t + 1] && !ghost; ++i) ghost = L.lv[i] >= plan.n_owned;
+      (ghost ? order : interior).push_back(t);
+    }
+    P.n_frontier = (int)order.size();
+    order.insert(order.end(), interior.begin(), interior.end());
+    if ((st = dev_upload(h, order, &h->tv.order)) != TG_OK) { tg_destroy(h); return st; }
     c.part = 1;
   }
   cudaError_t e = cudaStreamCreateWithFlags(&h->stream, cudaStreamNonBlocking);
@@ -1502,13 +1529,13 @@ tg_status launched(tg_handle* h) {
 
 extern "C" {
 
-tg_status tg_part_info(tg_handle* h, int* out6, int* send_counts, int* recv_counts) {
+tg_status tg_part_info(tg_handle* h, int* out8, int* send_counts, int* recv_counts) {
   tg_status st = part_check(h);
   if (st != TG_OK) return st;
-  if (!out6) return fail(h, TG_INVALID_ARG, "NULL argument");
+  if (!out8) return fail(h, TG_INVALID_ARG, "NULL argument");
   const auto& P = h->part;
-  out6[0] = P.n_parts; out6[1] = P.part; out6[2] = P.n_owned; out6[3] = h->L.nv - P.n_owned;
-  out6[4] = P.n_send; out6[5] = P.n_recv;
+  out8[0] = P.n_parts; out8[1] = P.part; out8[2] = P.n_owned; out8[3] = h->L.nv - P.n_owned;
+  out8[4] = P.n_send; out8[5] = P.n_recv; out8[6] = h->L.ntiles; out8[7] = P.n_frontier;
   for (int q = 0; q < P.n_parts; ++q) {
     if (send_counts) send_counts[q] = P.send_off[q + 1] - P.send_off[q];
     if (recv_counts) recv_counts[q] = P.recv_off[q + 1] - P.recv_off[q];
@@ -1537,27 +1564,52 @@ tg_status tg_part_begin(tg_handle* h) {
   return launched(h);
 }
 
-tg_status tg_part_gradients(tg_handle* h, int r) {
+}  // extern "C"
+
+namespace {
+
+// The tiles a stage call covers: all, the frontier [0, n_frontier) or the interior.
+tg_status part_tiles(tg_handle* h, int which, int* base, int* count) {
+  const int nf = h->part.n_frontier, nt = h->L.ntiles;
+  switch (which) {
+    case TG_TILES_ALL: *base = 0; *count = nt; return TG_OK;
+    case TG_TILES_FRONTIER: *base = 0; *count = nf; return TG_OK;
+    case TG_TILES_INTERIOR: *base = nf; *count = nt - nf; return TG_OK;
+    default: return fail(h, TG_INVALID_ARG, "unknown tile set");
+  }
+}
+
+}  // namespace
+
+extern "C" {
+
+tg_status tg_part_gradients(tg_handle* h, int r, int which) {
   tg_status st = part_check(h);
   if (st != TG_OK) return st;
   if (r < 0 || r >= h->ctl.n_rks) return fail(h, TG_INVALID_ARG, "stage out of range");
-  int bin, bout;
+  int bin, bout, base, count;
+  if ((st = part_tiles(h, which, &base, &count)) != TG_OK) return st;
   stage_buffers(h, r, &bin, &bout);
-  enqueue_gradient(h, bin, false, h->grads_needed, h->done);
+  enqueue_gradient(h, bin, false, h->grads_needed, h->done, base, count);
   return launched(h);
 }
 
-tg_status tg_part_flux(tg_handle* h, int r) {
+tg_status tg_part_flux(tg_handle* h, int r, int which) {
   tg_status st = part_check(h);
   if (st != TG_OK) return st;
   if (r < 0 || r >= h->ctl.n_rks) return fail(h, TG_INVALID_ARG, "stage out of range");
-  int bin, bout;
+  int bin, bout, base, count;
+  if ((st = part_tiles(h, which, &base, &count)) != TG_OK) return st;
   stage_buffers(h, r, &bin, &bout);
   const bool last = r == h->ctl.n_rks - 1;
-  enqueue_boundary(h, bin, h->done);
-  enqueue_tile_flux(h, bin, MODE_UPDATE, r, last, bout, h->done);
-  h->part.cur = bout;
-  if (last) h->part.norms_pending = true;
+  // boundary-face sides depend only on their own vertex's state: the faces are formed with
+  // the interior (or all) tiles, and the frontier tiles, launched after, gather them too
+  if (which != TG_TILES_FRONTIER) enqueue_boundary(h, bin, h->done);
+  enqueue_tile_flux(h, bin, MODE_UPDATE, r, last, bout, h->done, base, count);
+  if (which != TG_TILES_INTERIOR) {
+    h->part.cur = bout;
+    if (last) h->part.norms_pending = true;
+  }
   return launched(h);
 }
 

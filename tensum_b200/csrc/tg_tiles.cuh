@@ -59,7 +59,16 @@ struct TileView {
   const int* cv_off;            // per vertex (nv + 1); cv_ent has an even length
   const unsigned short* cv_ent;
   const double *x, *y;          // vertex coordinates (device order)
+  // a launch over part of the tiles (a partition's frontier or interior tiles): block b
+  // works on tile order[base + b]; total counts the tiles of every launch of the pass.
+  // order == NULL: block b works on tile b and the launch covers all total tiles.
+  const int* order;
+  int base, total;
 };
+
+__device__ __forceinline__ int tile_of_block(const TileView& t) {
+  return t.order ? t.order[t.base + blockIdx.x] : (int)blockIdx.x;
+}
 
 #ifndef TG_TILE_THREADS
 #define TG_TILE_THREADS 128    // threads per tile CTA (>= TG_TILE_OWNED)
@@ -125,7 +134,7 @@ __global__ void __launch_bounds__(kTileThreads, TG_GRAD_MINB) k_tile_grad(Params
   if ((FIRST && warm) || (warm_only && !warm)) return;
   const bool dt_here = FIRST;
   extern __shared__ double sm[];
-  const int tile = blockIdx.x;
+  const int tile = tile_of_block(t);
   const int l0 = t.loff[tile], L = t.loff[tile + 1] - l0;
   const int e0 = t.eoff[tile], NE = t.eoff[tile + 1] - e0;
   const int vb = t.vbeg[tile], nown = t.vbeg[tile + 1] - vb;
@@ -336,7 +345,7 @@ __global__ void __launch_bounds__(kTileThreads, (FLUX == FLUX_TECNO_ROE || FLUX 
   if (*done) return;
   extern __shared__ double sm[];
   typedef VLayout<FLUX> Y;
-  const int tile = blockIdx.x;
+  const int tile = tile_of_block(t);
   const int l0 = t.loff[tile], L = t.loff[tile + 1] - l0;
   const int e0 = t.eoff[tile], NE = t.eoff[tile + 1] - e0;
   const int vb = t.vbeg[tile], nown = t.vbeg[tile + 1] - vb;
@@ -562,17 +571,17 @@ __global__ void __launch_bounds__(kTileThreads, (FLUX == FLUX_TECNO_ROE || FLUX 
     }
     if (threadIdx.x == 0)
 #pragma unroll
-      for (int c = 0; c < 4; ++c) s.part[(size_t)blockIdx.x * 4 + c] = red[c * kTileThreads];
+      for (int c = 0; c < 4; ++c) s.part[(size_t)(t.base + blockIdx.x) * 4 + c] = red[c * kTileThreads];
     // the last block to finish forms the norms and ends the step
     __shared__ int last;
     if (threadIdx.x == 0) {
       __threadfence();
-      last = atomicAdd(&sc->blocks_done, 1u) == gridDim.x - 1;
+      last = atomicAdd(&sc->blocks_done, 1u) == (unsigned)t.total - 1;
     }
     __syncthreads();
     if (last) {
       __threadfence();
-      norm_and_step_end(s, gridDim.x, nv, sc, ctl, red, kTileThreads);
+      norm_and_step_end(s, t.total, nv, sc, ctl, red, kTileThreads);
       if (threadIdx.x == 0) sc->blocks_done = 0;
     }
   }

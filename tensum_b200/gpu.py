@@ -94,8 +94,8 @@ def load():
     L.tg_part_info.argtypes = [vp, ip, ip, ip]
     for name in ("tg_part_prime", "tg_part_begin"):
         getattr(L, name).argtypes = [vp]
-    L.tg_part_gradients.argtypes = [vp, i]
-    L.tg_part_flux.argtypes = [vp, i]
+    L.tg_part_gradients.argtypes = [vp, i, i]
+    L.tg_part_flux.argtypes = [vp, i, i]
     L.tg_part_pack.argtypes = [vp, i, vp]
     L.tg_part_unpack.argtypes = [vp, i, vp]
     L.tg_part_export.argtypes = [vp, vp]

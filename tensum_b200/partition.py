@@ -34,6 +34,7 @@ import numpy as np
 from . import abi, gpu
 
 HALO_STATE, HALO_GRAD = 0, 1
+TILES_ALL, TILES_FRONTIER, TILES_INTERIOR = 0, 1, 2
 WIDTH = 8        # doubles per vertex in a halo record
 REC = 5          # 8-byte words per partition in the scalar exchange
 _ip = C.POINTER(C.c_int)
@@ -88,11 +89,12 @@ class Partition:
             if st != 0:
                 raise gpu.TensumError(st, self.L.tg_last_error(None).decode())
             self.h = h
-            info = np.zeros(6, np.int32)
+            info = np.zeros(8, np.int32)
             self.send_counts = np.zeros(n_parts, np.int32)
             self.recv_counts = np.zeros(n_parts, np.int32)
             self._chk(self.L.tg_part_info(self.h, _i(info), _i(self.send_counts), _i(self.recv_counts)))
-            self.n_parts, self.part, self.n_owned, self.n_ghost, self.n_send, self.n_recv = (int(x) for x in info)
+            (self.n_parts, self.part, self.n_owned, self.n_ghost, self.n_send, self.n_recv, self.n_tiles,
+             self.n_frontier) = (int(x) for x in info)
             self.send_off = np.concatenate([[0], np.cumsum(self.send_counts)]) * WIDTH
             self.recv_off = np.concatenate([[0], np.cumsum(self.recv_counts)]) * WIDTH
             f64 = dict(dtype=torch.float64, device=self.device)
@@ -104,6 +106,8 @@ class Partition:
             self._chk(self.L.tg_stream(self.h, C.byref(sp)))
             self.stream = torch.cuda.ExternalStream(sp.value, device=self.device)
             self.done = torch.cuda.Event()      # the exchange buffers of this partition are free again
+            self.cstream = torch.cuda.Stream(device=self.device)   # copies of the local exchange
+            self.copied = torch.cuda.Event()    # this partition's receive buffer is filled
         self.n_rks = 4 if problem.options.time_scheme == 1 else 3
         self.grads = needs_gradients(problem)
 
@@ -151,11 +155,11 @@ class Partition:
     def begin(self):
         self._call("tg_part_begin")
 
-    def gradients(self, r: int):
-        self._call("tg_part_gradients", r)
+    def gradients(self, r: int, tiles: int = TILES_ALL):
+        self._call("tg_part_gradients", r, tiles)
 
-    def flux(self, r: int):
-        self._call("tg_part_flux", r)
+    def flux(self, r: int, tiles: int = TILES_ALL):
+        self._call("tg_part_flux", r, tiles)
 
     def pack(self, field: int):
         self._call("tg_part_pack", field, C.c_void_p(self.send.data_ptr()))
@@ -177,44 +181,54 @@ class Partition:
 
 
 class LocalExchange:
-    """All partitions in this process: each receiver copies its peers' send
-    segments into its receive buffer on its own stream after the senders' pack
-    (CUDA events), and a sender packs again only after every receiver is done."""
+    """All partitions in this process.  start(): each sender packs on its stream; each
+    receiver's copy stream waits for the senders' packs and copies their segments into
+    its receive buffer.  finish(): the receiver's stream waits for its copies and
+    unpacks.  Work enqueued between the two (interior tiles) overlaps the copies.  A
+    sender packs again only after every receiver has copied, and a receive buffer is
+    refilled only after its unpack."""
 
     def __init__(self, parts):
         self.parts = parts
 
-    def halo(self, field: int):
+    def start(self, field: int):
         import torch
+        evs = []
         for p in self.parts:
             for q in self.parts:
                 if q is not p:
-                    p.stream.wait_event(q.done)
+                    p.stream.wait_event(q.copied)
             p.pack(field)
-        evs = []
-        for p in self.parts:
             ev = torch.cuda.Event()
             ev.record(p.stream)
             evs.append(ev)
-        for q in self.parts:
-            with torch.cuda.stream(q.stream):
+        for q, own in zip(self.parts, evs):
+            q.cstream.wait_event(own)          # joins the copy stream to q's work (and to a capture)
+            q.cstream.wait_event(q.done)
+            with torch.cuda.stream(q.cstream):
                 for p, ev in zip(self.parts, evs):
                     n = int(q.recv_counts[p.part]) * WIDTH
                     if p is q or n == 0:
                         continue
-                    q.stream.wait_event(ev)
+                    q.cstream.wait_event(ev)
                     a, b = int(p.send_off[q.part]), int(q.recv_off[p.part])
                     q.recv[b:b + n].copy_(p.send[a:a + n], non_blocking=True)
+            q.copied.record(q.cstream)
+
+    def finish(self, field: int):
+        for q in self.parts:
+            q.stream.wait_event(q.copied)
             q.unpack(field)
             q.done.record(q.stream)
+
+    def halo(self, field: int):
+        self.start(field)
+        self.finish(field)
 
     def scalars(self):
         import torch
         evs = []
         for p in self.parts:
-            for q in self.parts:
-                if q is not p:
-                    p.stream.wait_event(q.done)
             p.export()
             ev = torch.cuda.Event()
             ev.record(p.stream)
@@ -225,7 +239,12 @@ class LocalExchange:
                     q.stream.wait_event(ev)
                     q.sc_all[p.part * REC:(p.part + 1) * REC].copy_(p.sc_out, non_blocking=True)
             q.import_()
-            q.done.record(q.stream)
+        for p in self.parts:                  # sc_out is written again only after every copy
+            for q in self.parts:
+                if q is not p:
+                    ev = torch.cuda.Event()
+                    ev.record(q.stream)
+                    p.stream.wait_event(ev)
 
 
 class DistTransport:
@@ -237,11 +256,12 @@ class DistTransport:
         self.dist = dist
         self.group = group
 
-    def alltoall(self, send, recv, send_counts, recv_counts, width: int = WIDTH):
-        self.dist.all_to_all_single(recv[:int(np.sum(recv_counts)) * width] if recv.numel() else recv,
-                                    send[:int(np.sum(send_counts)) * width] if send.numel() else send,
-                                    [int(c) * width for c in recv_counts], [int(c) * width for c in send_counts],
-                                    group=self.group)
+    def alltoall(self, send, recv, send_counts, recv_counts, width: int = WIDTH, async_op: bool = False):
+        return self.dist.all_to_all_single(recv[:int(np.sum(recv_counts)) * width] if recv.numel() else recv,
+                                           send[:int(np.sum(send_counts)) * width] if send.numel() else send,
+                                           [int(c) * width for c in recv_counts],
+                                           [int(c) * width for c in send_counts], group=self.group,
+                                           async_op=async_op)
 
     def allgather(self, mine, everyone):
         self.dist.all_gather_into_tensor(everyone, mine, group=self.group)
@@ -254,13 +274,24 @@ class DistExchange:
         self.p = part
         self.t = DistTransport(group)
 
-    def halo(self, field: int):
+    def start(self, field: int):
+        """Pack and launch the all-to-all; work enqueued before finish() overlaps it."""
         import torch
         p = self.p
         p.pack(field)
         with torch.cuda.stream(p.stream):
-            self.t.alltoall(p.send, p.recv, p.send_counts, p.recv_counts)
-        p.unpack(field)
+            self.work = self.t.alltoall(p.send, p.recv, p.send_counts, p.recv_counts, async_op=True)
+
+    def finish(self, field: int):
+        import torch
+        with torch.cuda.stream(self.p.stream):
+            self.work.wait()
+        self.work = None
+        self.p.unpack(field)
+
+    def halo(self, field: int):
+        self.start(field)
+        self.finish(field)
 
     def scalars(self):
         import torch
@@ -271,19 +302,49 @@ class DistExchange:
         p.import_()
 
 
-def run_step(parts, exchange):
-    """One time step of every partition in `parts` with `exchange` as transport."""
+def run_step(parts, exchange, overlap: bool = True):
+    """One time step of every partition in `parts` with `exchange` as transport.  With
+    overlap, each exchange runs while the interior tiles (no ghost among their
+    vertices) compute: gradients(I) | finish STATE | gradients(F) | start GRAD |
+    flux(I) | finish GRAD | flux(F) | start STATE (the first stage finds no exchange
+    in flight; the last stage's completes before the scalar exchange)."""
     n_rks, grads = parts[0].n_rks, parts[0].grads
     for p in parts:
         p.begin()
+    if not overlap:
+        for r in range(n_rks):
+            if grads:
+                for p in parts:
+                    p.gradients(r)
+                exchange.halo(HALO_GRAD)
+            for p in parts:
+                p.flux(r)
+            exchange.halo(HALO_STATE)
+        exchange.scalars()
+        return
+    pending = False
     for r in range(n_rks):
         if grads:
             for p in parts:
-                p.gradients(r)
-            exchange.halo(HALO_GRAD)
+                p.gradients(r, TILES_INTERIOR)
+            if pending:
+                exchange.finish(HALO_STATE)
+            for p in parts:
+                p.gradients(r, TILES_FRONTIER)
+            exchange.start(HALO_GRAD)
+            for p in parts:
+                p.flux(r, TILES_INTERIOR)
+            exchange.finish(HALO_GRAD)
+        else:
+            for p in parts:
+                p.flux(r, TILES_INTERIOR)
+            if pending:
+                exchange.finish(HALO_STATE)
         for p in parts:
-            p.flux(r)
-        exchange.halo(HALO_STATE)
+            p.flux(r, TILES_FRONTIER)
+        exchange.start(HALO_STATE)
+        pending = True
+    exchange.finish(HALO_STATE)
     exchange.scalars()
 
 
@@ -292,10 +353,12 @@ class PartitionedSolver:
     holds partition q; by default all on cuda:0).  With every partition on one
     device the step -- phases, halo copies and scalar exchange of all partitions
     -- is captured once as a CUDA graph and replayed (graph=True), so issuing a
-    step costs one launch however many partitions there are."""
+    step costs one launch however many partitions there are.  overlap: the copies
+    run on side streams while the interior tiles compute (run_step)."""
 
-    def __init__(self, problem: abi.Problem, n_parts: int, devices=None, graph: bool = True):
+    def __init__(self, problem: abi.Problem, n_parts: int, devices=None, graph: bool = True, overlap: bool = True):
         devices = devices or [0] * n_parts
+        self.overlap = overlap
         self.nv = problem.geom.n_vertex
         self.parts = [Partition(problem, n_parts, q, devices[q]) for q in range(n_parts)]
         self.exchange = LocalExchange(self.parts)
@@ -313,6 +376,7 @@ class PartitionedSolver:
         import torch
         for p in self.parts:
             p.done = torch.cuda.Event()
+            p.copied = torch.cuda.Event()
 
     def _capture(self):
         """Record one step: the partitions' streams fork from the capture stream
@@ -328,7 +392,7 @@ class PartitionedSolver:
             fork.record(cap)
             for p in self.parts:
                 p.stream.wait_event(fork)
-            run_step(self.parts, self.exchange)
+            run_step(self.parts, self.exchange, self.overlap)
             for p in self.parts:
                 ev = torch.cuda.Event()
                 ev.record(p.stream)
@@ -349,7 +413,7 @@ class PartitionedSolver:
             torch.cuda.synchronize(dev)
         else:
             for _ in range(n):
-                run_step(self.parts, self.exchange)
+                run_step(self.parts, self.exchange, self.overlap)
         info = [p.scalars() for p in self.parts]
         return info[0]
 
@@ -390,7 +454,8 @@ class DistPartitionedSolver:
     once as a CUDA graph on the partition's stream and replayed; every rank captures
     and replays the same sequence."""
 
-    def __init__(self, problem: abi.Problem, group=None, device: int | None = None, graph: bool = False):
+    def __init__(self, problem: abi.Problem, group=None, device: int | None = None, graph: bool = False,
+                 overlap: bool = True):
         import torch
         import torch.distributed as dist
         n_parts, part = dist.get_world_size(group), dist.get_rank(group)
@@ -398,6 +463,7 @@ class DistPartitionedSolver:
         self.exchange = DistExchange(self.part, group)
         self.nv = problem.geom.n_vertex
         self.graph = graph
+        self.overlap = overlap
         self._graph = None
 
     def set_state(self, prim: np.ndarray, t0: float = 0.0):
@@ -411,7 +477,7 @@ class DistPartitionedSolver:
         torch.cuda.synchronize(p.device)
         g = torch.cuda.CUDAGraph()
         with torch.cuda.graph(g, stream=p.stream):
-            run_step([p], self.exchange)
+            run_step([p], self.exchange, self.overlap)
         self._graph = g
 
     def step(self, n: int) -> np.ndarray:
@@ -424,7 +490,7 @@ class DistPartitionedSolver:
                     self._graph.replay()
         else:
             for _ in range(n):
-                run_step([self.part], self.exchange)
+                run_step([self.part], self.exchange, self.overlap)
         return self.part.scalars()
 
     def close(self):

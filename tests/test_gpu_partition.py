@@ -44,15 +44,15 @@ def _one_partition(P, ic, steps):
     return out, info
 
 
-@pytest.mark.parametrize("graph", [True, False])
+@pytest.mark.parametrize("graph,overlap", [(True, True), (False, True), (True, False), (False, False)])
 @pytest.mark.parametrize("flux,recon,n_parts", [("kepes_tecno_rusanov", "minmod", 2),
                                                 ("kepes_tecno_rusanov", "minmod", 3),
                                                 ("kep", "first", 4),
                                                 ("roe_ec", "first", 2)])
-def test_periodic_partitions_match_one_partition(flux, recon, n_parts, graph):
+def test_periodic_partitions_match_one_partition(flux, recon, n_parts, graph, overlap):
     P, ic = _kh_problem(33, flux, recon)
     want, winfo = _one_partition(P, ic, 6)
-    ps = partition.PartitionedSolver(P, n_parts, graph=graph)
+    ps = partition.PartitionedSolver(P, n_parts, graph=graph, overlap=overlap)
     ps.set_state(ic)
     info = ps.step(6)
     got = ps.get_state()
@@ -123,8 +123,8 @@ def test_partition_handles_refuse_whole_mesh_calls():
     assert abi.STATUS[e.value.status] == "TG_NOT_SUPPORTED"
 
 
-@pytest.mark.parametrize("graph", [False, True])
-def test_torch_distributed_path_on_one_rank(graph):
+@pytest.mark.parametrize("graph,overlap", [(False, False), (False, True), (True, False), (True, True)])
+def test_torch_distributed_path_on_one_rank(graph, overlap):
     """DistPartitionedSolver over a one-rank NCCL group: the collectives run on the
     partition's stream (eagerly, or captured with the phases as one CUDA graph) and
     the result is the one-partition solve."""
@@ -140,7 +140,7 @@ def test_torch_distributed_path_on_one_rank(graph):
     try:
         P, ic = _kh_problem(17, "kepes_tecno_rusanov", "minmod")
         want, winfo = _one_partition(P, ic, 3)
-        d = partition.DistPartitionedSolver(P, device=0, graph=graph)
+        d = partition.DistPartitionedSolver(P, device=0, graph=graph, overlap=overlap)
         d.set_state(ic)
         info = d.step(3)
         assert np.array_equal(d.get_state(), want)
@@ -166,3 +166,17 @@ def test_voronoi_and_axisymmetric_partitions(name):
     assert np.array_equal(ps.get_state(), want)
     assert info[1] == winfo[1]
     ps.close()
+
+
+def test_frontier_tiles_are_the_ones_reading_ghosts():
+    """The tile order puts the tiles with a ghost among their vertices first; a single
+    partition has none, a mesh cut in two keeps interior tiles."""
+    P, ic = _kh_problem(65, "kep", "first")
+    for n in (1, 2, 4):
+        parts = [partition.Partition(P, n, q) for q in range(n)]
+        for p in parts:
+            assert 0 <= p.n_frontier <= p.n_tiles
+            assert (p.n_frontier == 0) == (n == 1)
+            if n == 2:
+                assert p.n_frontier < p.n_tiles
+            p.close()
