@@ -147,3 +147,64 @@ def test_exchange_over_gloo_fills_every_ghost(tmp_path, world):
     # the fixed-order reduction k_part_import applies: minimum dt, summed norms
     assert rec[:, 0].min() == 0.25 / world
     assert rec[:, 4].sum() == sum(4.0 * r for r in range(world))
+
+
+class _Part:
+    """Records the phases run_step issues (stands in for a partition handle)."""
+
+    def __init__(self, log, grads, n_rks=3):
+        self.log, self.grads, self.n_rks = log, grads, n_rks
+
+    def begin(self):
+        self.log.append("begin")
+
+    def gradients(self, r, tiles=partition.TILES_ALL):
+        self.log.append(f"grad{r}:{tiles}")
+
+    def flux(self, r, tiles=partition.TILES_ALL):
+        self.log.append(f"flux{r}:{tiles}")
+
+
+class _Exchange:
+    def __init__(self, log):
+        self.log = log
+
+    def start(self, field):
+        self.log.append(f"start:{field}")
+
+    def finish(self, field):
+        self.log.append(f"finish:{field}")
+
+    def halo(self, field):
+        self.log.append(f"halo:{field}")
+
+    def scalars(self):
+        self.log.append("scalars")
+
+
+@pytest.mark.parametrize("grads", [True, False])
+def test_overlap_schedule_keeps_every_dependency(grads):
+    """Interior tiles run while an exchange is in flight; frontier tiles and the next
+    exchange of a field only after the previous one finished; the last state
+    exchange completes before the step's scalar exchange."""
+    log = []
+    partition.run_step([_Part(log, grads)], _Exchange(log), overlap=True)
+    I, F = partition.TILES_INTERIOR, partition.TILES_FRONTIER
+    S, G = partition.HALO_STATE, partition.HALO_GRAD
+    want = ["begin"]
+    for r in range(3):
+        if grads:
+            want += [f"grad{r}:{I}"] + ([f"finish:{S}"] if r else []) + [f"grad{r}:{F}", f"start:{G}",
+                                                                           f"flux{r}:{I}", f"finish:{G}"]
+        else:
+            want += [f"flux{r}:{I}"] + ([f"finish:{S}"] if r else [])
+        want += [f"flux{r}:{F}", f"start:{S}"]
+    want += [f"finish:{S}", "scalars"]
+    assert log == want
+    log.clear()
+    partition.run_step([_Part(log, grads)], _Exchange(log), overlap=False)
+    A = partition.TILES_ALL
+    want = ["begin"]
+    for r in range(3):
+        want += ([f"grad{r}:{A}", f"halo:{G}"] if grads else []) + [f"flux{r}:{A}", f"halo:{S}"]
+    assert log == want + ["scalars"]
