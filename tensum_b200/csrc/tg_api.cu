@@ -191,27 +191,27 @@ BfluxKernel bflux_kernel(int flux, int recon) {
   }
 }
 
-template <int F, int M>
+template <int F, int M, bool O>
 TileFluxKernel pick_tile(int recon) {
   switch (recon) {
-    case RECON_FIRST: return k_tile_flux<F, RECON_FIRST, M>;
-    case RECON_SECOND: return k_tile_flux<F, RECON_SECOND, M>;
-    case RECON_SECOND_MUSCL: return k_tile_flux<F, RECON_SECOND_MUSCL, M>;
-    case RECON_VAN_ALBADA: return k_tile_flux<F, RECON_VAN_ALBADA, M>;
-    case RECON_TVD_MINMOD: return k_tile_flux<F, RECON_TVD_MINMOD, M>;
-    case RECON_TVB_MINMOD: return k_tile_flux<F, RECON_TVB_MINMOD, M>;
-    default: return k_tile_flux<F, RECON_ENO2, M>;
+    case RECON_FIRST: return k_tile_flux<F, RECON_FIRST, M, O>;
+    case RECON_SECOND: return k_tile_flux<F, RECON_SECOND, M, O>;
+    case RECON_SECOND_MUSCL: return k_tile_flux<F, RECON_SECOND_MUSCL, M, O>;
+    case RECON_VAN_ALBADA: return k_tile_flux<F, RECON_VAN_ALBADA, M, O>;
+    case RECON_TVD_MINMOD: return k_tile_flux<F, RECON_TVD_MINMOD, M, O>;
+    case RECON_TVB_MINMOD: return k_tile_flux<F, RECON_TVB_MINMOD, M, O>;
+    default: return k_tile_flux<F, RECON_ENO2, M, O>;
   }
 }
-template <int M>
+template <int M, bool O>
 TileFluxKernel tile_kernel_m(int flux, int recon) {
   switch (flux) {
-    case FLUX_TECNO_ROE: return pick_tile<FLUX_TECNO_ROE, M>(recon);
-    case FLUX_TECNO_RUSANOV: return pick_tile<FLUX_TECNO_RUSANOV, M>(recon);
-    case FLUX_KEPEC: return k_tile_flux<FLUX_KEPEC, RECON_FIRST, M>;
-    case FLUX_KEP: return k_tile_flux<FLUX_KEP, RECON_FIRST, M>;
-    case FLUX_ROE_EC: return k_tile_flux<FLUX_ROE_EC, RECON_FIRST, M>;
-    default: return k_tile_flux<FLUX_AVG, RECON_FIRST, M>;
+    case FLUX_TECNO_ROE: return pick_tile<FLUX_TECNO_ROE, M, O>(recon);
+    case FLUX_TECNO_RUSANOV: return pick_tile<FLUX_TECNO_RUSANOV, M, O>(recon);
+    case FLUX_KEPEC: return k_tile_flux<FLUX_KEPEC, RECON_FIRST, M, O>;
+    case FLUX_KEP: return k_tile_flux<FLUX_KEP, RECON_FIRST, M, O>;
+    case FLUX_ROE_EC: return k_tile_flux<FLUX_ROE_EC, RECON_FIRST, M, O>;
+    default: return k_tile_flux<FLUX_AVG, RECON_FIRST, M, O>;
   }
 }
 size_t flux_smem(int flux, int recon, int lmax, int emax, int cmax) {
@@ -242,13 +242,18 @@ cudaError_t raise_smem(const void* f, size_t bytes) {
 }
 
 typedef void (*TileGradKernel)(Params, MeshView, TileView, StateView, Scalars*, int, int, const int*, int);
-TileGradKernel grad_kernel(bool first, bool grad) {
+// ord: a partition's launches over its tile order (frontier / interior), whose
+// gradient and flux + update kernels are separate instantiations (ORD), so the
+// whole-mesh kernels stay exactly as they are
+TileGradKernel grad_kernel(bool first, bool grad, bool ord = false) {
   if (first) return grad ? k_tile_grad<true, true> : k_tile_grad<true, false>;
-  return k_tile_grad<false, true>;
+  return ord ? k_tile_grad<false, true, true> : k_tile_grad<false, true>;
 }
 
-TileFluxKernel tile_kernel(int flux, int recon, int mode) {
-  return mode == MODE_UPDATE ? tile_kernel_m<MODE_UPDATE>(flux, recon) : tile_kernel_m<MODE_RESIDUAL>(flux, recon);
+TileFluxKernel tile_kernel(int flux, int recon, int mode, bool ord = false) {
+  if (ord) return tile_kernel_m<MODE_UPDATE, true>(flux, recon);
+  return mode == MODE_UPDATE ? tile_kernel_m<MODE_UPDATE, false>(flux, recon)
+                             : tile_kernel_m<MODE_RESIDUAL, false>(flux, recon);
 }
 
 // state view of buffer b (the three P/W buffers rotate through the stages)
@@ -274,7 +279,8 @@ void enqueue_gradient(tg_handle* h, int b, bool first, bool grad, const int* don
   if (!first && !grad) return;
   if (count < 0) count = h->L.ntiles;
   if (count == 0) return;
-  grad_kernel(first, grad)<<<count, kTileThreads, first ? h->smem_grad1 : h->smem_grad0, h->stream>>>(
+  const bool ord = h->tv.order != nullptr && !first;   // first-stage passes cover all tiles unordered
+  grad_kernel(first, grad, ord)<<<count, kTileThreads, first ? h->smem_grad1 : h->smem_grad0, h->stream>>>(
       h->prm, h->mv, tiles(h, base), view(h, b), h->sc, h->L.lmax, h->L.emax, done, 0);
   if (first && grad && h->prm.fuse_dt)
     grad_kernel(false, true)<<<count, kTileThreads, h->smem_grad0, h->stream>>>(
@@ -293,7 +299,8 @@ void enqueue_tile_flux(tg_handle* h, int b, int mode, int r, bool norm, int bout
                        int count = -1) {
   if (count < 0) count = h->L.ntiles;
   if (count == 0) return;
-  tile_kernel(h->prm.flux, h->prm.recon, mode)<<<count, kTileThreads, h->smem_flux, h->stream>>>(
+  const bool ord = h->tv.order != nullptr && mode == MODE_UPDATE;
+  tile_kernel(h->prm.flux, h->prm.recon, mode, ord)<<<count, kTileThreads, h->smem_flux, h->stream>>>(
       h->prm, h->mv, tiles(h, base), view(h, b), h->ctl, h->sc, r, norm ? 1 : 0, h->Pb[bout], h->Wb[bout], h->L.lmax,
       h->L.emax, done);
 }
@@ -852,6 +859,12 @@ static tg_status create_handle(const tg_mesh* mesh, const tg_material* mat, cons
     P.n_frontier = (int)order.size();
     order.insert(order.end(), interior.begin(), interior.end());
     if ((st = dev_upload(h, order, &h->tv.order)) != TG_OK) { tg_destroy(h); return st; }
+    if (raise_smem((const void*)grad_kernel(false, true, true), h->smem_grad0) != cudaSuccess ||
+        raise_smem((const void*)tile_kernel(mat->flux_scheme, mat->reconstruct_scheme, MODE_UPDATE, true),
+                   h->smem_flux) != cudaSuccess) {
+      tg_destroy(h);
+      return fail(nullptr, TG_CUDA_ERROR, "tile kernels need more shared memory than the device allows");
+    }
     c.part = 1;
   }
   cudaError_t e = cudaStreamCreateWithFlags(&h->stream, cudaStreamNonBlocking);

@@ -59,15 +59,16 @@ struct TileView {
   const int* cv_off;            // per vertex (nv + 1); cv_ent has an even length
   const unsigned short* cv_ent;
   const double *x, *y;          // vertex coordinates (device order)
-  // a launch over part of the tiles (a partition's frontier or interior tiles): block b
-  // works on tile order[base + b]; total counts the tiles of every launch of the pass.
-  // order == NULL: block b works on tile b and the launch covers all total tiles.
+  // ordered launches (ORD kernels: a partition's frontier or interior tiles): block b
+  // works on tile order[base + b], and total counts the tiles of every launch of the
+  // pass; the other kernels work on tile blockIdx.x over one launch of all tiles
   const int* order;
   int base, total;
 };
 
+template <bool ORD>
 __device__ __forceinline__ int tile_of_block(const TileView& t) {
-  return t.order ? t.order[t.base + blockIdx.x] : (int)blockIdx.x;
+  return ORD ? t.order[t.base + blockIdx.x] : (int)blockIdx.x;
 }
 
 #ifndef TG_TILE_THREADS
@@ -125,7 +126,7 @@ __host__ __device__ constexpr int grad_edge_doubles(bool first) { return first ?
 // warm_only (gradient kernels at a step's first stage): runs only when the
 // previous step's last stage has already formed dt and U_old for this state,
 // the first-stage kernel (FIRST) only when it has not.
-template <bool FIRST, bool GRAD>
+template <bool FIRST, bool GRAD, bool ORD = false>
 __global__ void __launch_bounds__(kTileThreads, TG_GRAD_MINB) k_tile_grad(Params k, MeshView m, TileView t, StateView s,
                                                             Scalars* sc, int lmax, int emax,
                                                             const int* __restrict__ done, int warm_only) {
@@ -134,7 +135,7 @@ __global__ void __launch_bounds__(kTileThreads, TG_GRAD_MINB) k_tile_grad(Params
   if ((FIRST && warm) || (warm_only && !warm)) return;
   const bool dt_here = FIRST;
   extern __shared__ double sm[];
-  const int tile = tile_of_block(t);
+  const int tile = tile_of_block<ORD>(t);
   const int l0 = t.loff[tile], L = t.loff[tile + 1] - l0;
   const int e0 = t.eoff[tile], NE = t.eoff[tile + 1] - e0;
   const int vb = t.vbeg[tile], nown = t.vbeg[tile + 1] - vb;
@@ -336,7 +337,7 @@ __device__ __forceinline__ bool w3_only(const Params& k) {
   return FLUX != FLUX_TECNO_ROE && FLUX != FLUX_TECNO_RUSANOV && k.model == 0 && !k.strong;
 }
 
-template <int FLUX, int RECON, int MODE>
+template <int FLUX, int RECON, int MODE, bool ORD = false>
 __global__ void __launch_bounds__(kTileThreads, (FLUX == FLUX_TECNO_ROE || FLUX == FLUX_TECNO_RUSANOV)
                                                     ? TG_FLUX_MINB : TG_FLUX_MINB_CENTRAL)
     k_tile_flux(Params k, MeshView m, TileView t, StateView s, Control ctl, Scalars* sc, int r, int do_norm,
@@ -345,7 +346,7 @@ __global__ void __launch_bounds__(kTileThreads, (FLUX == FLUX_TECNO_ROE || FLUX 
   if (*done) return;
   extern __shared__ double sm[];
   typedef VLayout<FLUX> Y;
-  const int tile = tile_of_block(t);
+  const int tile = tile_of_block<ORD>(t);
   const int l0 = t.loff[tile], L = t.loff[tile + 1] - l0;
   const int e0 = t.eoff[tile], NE = t.eoff[tile + 1] - e0;
   const int vb = t.vbeg[tile], nown = t.vbeg[tile + 1] - vb;
@@ -571,17 +572,17 @@ __global__ void __launch_bounds__(kTileThreads, (FLUX == FLUX_TECNO_ROE || FLUX 
     }
     if (threadIdx.x == 0)
 #pragma unroll
-      for (int c = 0; c < 4; ++c) s.part[(size_t)(t.base + blockIdx.x) * 4 + c] = red[c * kTileThreads];
+      for (int c = 0; c < 4; ++c) s.part[(size_t)((ORD ? t.base : 0) + blockIdx.x) * 4 + c] = red[c * kTileThreads];
     // the last block to finish forms the norms and ends the step
     __shared__ int last;
     if (threadIdx.x == 0) {
       __threadfence();
-      last = atomicAdd(&sc->blocks_done, 1u) == (unsigned)t.total - 1;
+      last = atomicAdd(&sc->blocks_done, 1u) == (ORD ? (unsigned)t.total : gridDim.x) - 1;
     }
     __syncthreads();
     if (last) {
       __threadfence();
-      norm_and_step_end(s, t.total, nv, sc, ctl, red, kTileThreads);
+      norm_and_step_end(s, ORD ? t.total : (int)gridDim.x, nv, sc, ctl, red, kTileThreads);
       if (threadIdx.x == 0) sc->blocks_done = 0;
     }
   }
