@@ -15,7 +15,9 @@ one-partition solve bit for bit.  A step is
 where halo(field) packs 8 doubles per shared vertex, moves them with an
 all-to-all and unpacks them into the ghost slots, and scalars all-gathers each
 partition's dt minimum and norm sums so every partition forms the same dt and
-norms.  Two transports implement the exchange:
+norms.  With overlap (the default) every phase runs as two launches, the interior
+tiles (no ghost among their vertices) while an exchange is in flight and the
+frontier tiles after it landed (run_step).  Two transports implement the exchange:
 
 * :class:`LocalExchange` -- all partitions in this process, device copies
   ordered by CUDA events (one GPU, or several GPUs driven by one process);
