@@ -547,7 +547,12 @@ tg_status tg_mlp_predict(tg_mlp* m, const float* X, int n, float* Y, int precisi
  * and no cudaMalloc/cudaFree: its scratch is a fixed 64 KiB device array in
  * the library, held by every GPU that loads it until exit.
  *   res_dev     device array n_vertex x 5, the reference's Flux layout
- *               (mass, mx, my, mz, energy); the z component is ignored
+ *               (mass, mx, my, mz, energy); the z component is ignored.  With
+ *               strong boundary conditions the caller passes the residual
+ *               with the no-slip momentum already zeroed, as
+ *               compute_residual_norm zeroes it first (src/fv.cc:1807-1819)
+ *               and as tg_residual returns it; the entry point sums what it
+ *               is given
  *   dcarea_dev  device array n_vertex, dual areas
  *   weight_dev  device array n_vertex, 1/|P_i| for periodic vertices, else 1
  *   total0      normaliser; <= 0 marks the first iteration (total becomes it)
@@ -556,8 +561,15 @@ tg_status tg_mlp_predict(tg_mlp* m, const float* X, int n, float* Y, int precisi
  *   stream      cudaStream_t (NULL = default stream); the call is
  *               asynchronous on it.
  * n_vertex must be at most TG_NOALLOC_MAX_VERTICES (TG_INVALID_ARG otherwise).
+ * The norms are those of one whole mesh: each component is divided by
+ * n_vertex, so the entry point serves single-partition meshes.  (The
+ * reference's partitioned norm weights shared vertices by 1/nbs and divides by
+ * the global vertex count, src/fv.cc:1830-1859; per-partition calls do not
+ * give it.)
  * The first call on each device looks up the scratch array's device address,
- * so make it before any stream capture that should contain later calls.
+ * so make it before any stream capture that should contain later calls.  The
+ * address is kept for the life of the process: do not call the entry point
+ * on a device after cudaDeviceReset on it.
  * All calls share the scratch array: calls whose kernels overlap on the GPU
  * (e.g. on two streams) race and may return wrong norms.
  * On failure tg_noalloc_last_error() describes the problem. */

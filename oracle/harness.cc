@@ -235,6 +235,12 @@ int main(int argc, char* argv[]) {
   Dump dump(argv[6]);
 
   FiniteVolume fv(argv[1], argv[2]);
+  // Material::second_muscl (src/material.h:99, src/reconstruct.cc:46-64) has no
+  // keyword in the parameter reader (src/parameter.cc:113-140); with
+  // TENSUM_HARNESS_RECON=second_muscl the file names "second" and the scheme is
+  // switched here, after the reader ran.
+  if (const char* rc = std::getenv("TENSUM_HARNESS_RECON"))
+    if (std::strcmp(rc, "second_muscl") == 0) fv.param.material.reconstruct_scheme = Material::second_muscl;
   fv.grid.read(fv.param);
   fv.create_force_face_list();
   fv.initialize();

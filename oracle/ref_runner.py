@@ -20,7 +20,7 @@ import numpy as np
 HERE = os.path.dirname(os.path.abspath(__file__))
 HARNESS = os.path.join(HERE, "_ref", "tensum_harness")
 
-RECON_NAMES = {"first", "second", "minmod", "tvb_minmod", "eno2", "van_albada"}
+RECON_NAMES = {"first", "second", "second_muscl", "minmod", "tvb_minmod", "eno2", "van_albada"}
 FLUX_NAMES = {"kepes_tecno_roe", "kepes_tecno_rusanov", "kepec", "kep", "roe_ec", "simple_avg"}
 
 
@@ -46,7 +46,9 @@ def param_text(cfg: dict) -> str:
     flux = cfg.get("flux", "kepes_tecno_roe")
     recon = cfg.get("reconstruct", "minmod")
     assert flux in FLUX_NAMES and recon in RECON_NAMES
-    rec = f"      method   {recon}\n"
+    # second_muscl has no parameter-file keyword: the file names "second" and the
+    # harness switches the scheme (TENSUM_HARNESS_RECON, set by run_case)
+    rec = f"      method   {'second' if recon == 'second_muscl' else recon}\n"
     if recon == "tvb_minmod":
         rec += f"      M_value  {cfg.get('tvb_M', 1.0):.17g}\n"
     model = cfg.get("model", "euler")
@@ -219,8 +221,11 @@ def run_case(mesh, cfg: dict, prim0: np.ndarray | None, n_steps: int, n_dump: in
         out = os.path.join(wd, "dump.bin")
         env = dict(os.environ)
         env.pop("TENSUM_HARNESS_AXI", None)
+        env.pop("TENSUM_HARNESS_RECON", None)
         if cfg.get("axisymmetric"):
             env["TENSUM_HARNESS_AXI"] = "1"     # the reference's -axi option
+        if cfg.get("reconstruct") == "second_muscl":
+            env["TENSUM_HARNESS_RECON"] = "second_muscl"
         r = subprocess.run([HARNESS, "param.in", ".", ic, str(n_steps), str(n_dump), out],
                            cwd=wd, capture_output=True, text=True, timeout=timeout, env=env)
         if r.returncode != 0 or not os.path.exists(out):

@@ -34,6 +34,10 @@ CASES = {
     "sq_roe_vanalbada": _sq("kepes_tecno_roe", "van_albada"),
     "sq_roe_tvb": _sq("kepes_tecno_roe", "tvb_minmod", tvb_M=1.0),
     "sq_roe_eno2": _sq("kepes_tecno_roe", "eno2"),
+    # unlimited MUSCL, kappa = 1/3 (src/reconstruct.cc:46-64; no parameter-file keyword)
+    "sq_roe_muscl": _sq("kepes_tecno_roe", "second_muscl"),
+    "sq_rusanov_muscl_long": _sq("kepes_tecno_rusanov", "second_muscl", n=17, seed=19, steps=40, dump=0),
+    "cyl_ns_muscl": _cyl("kepes_tecno_roe", "second_muscl", "ns"),
     "sq_roe_evmod": _sq("kepes_tecno_roe", "minmod", ev_alpha=0.3, ev_beta=0.2),
     "sq_kh_rusanov": _sq("kepes_tecno_rusanov", "minmod", n=11, seed=5, ic="kh"),
     "vortex17_long": _sq("kepes_tecno_roe", "minmod", n=17, seed=7, steps=60, dump=0),

@@ -85,3 +85,43 @@ def test_noalloc_rejects_oversized_input():
     st = lib.tg_residual_norm_noalloc(p, p, p, 268435456 + 1, 0.0, p, None)
     assert st == 4
     assert b"TG_NOALLOC_MAX_VERTICES" in lib.tg_noalloc_last_error()
+
+
+def _bind():
+    lib = gpu.load()
+    lib.tg_residual_norm_noalloc.argtypes = [C.c_void_p] * 3 + [C.c_int, C.c_double, C.c_void_p, C.c_void_p]
+    lib.tg_residual_norm_noalloc.restype = C.c_int
+    lib.tg_noalloc_last_error.restype = C.c_char_p
+    return lib
+
+
+def test_noalloc_strided_blocks_match_numpy():
+    """Above 2048 blocks x 256 threads (524,288 vertices) the grid is capped and
+    every thread strides over several vertices: compare with the formula in numpy."""
+    lib = _bind()
+    nv = 900_001
+    rng = np.random.default_rng(7)
+    res = rng.standard_normal((nv, 5))
+    area = rng.uniform(0.5, 2.0, nv)
+    w = np.where(rng.uniform(size=nv) < 0.01, 0.5, 1.0)
+    q = res[:, [0, 1, 2, 4]] / area[:, None]
+    n = np.sqrt((q * q * w[:, None]).sum(axis=0)) / nv
+    total = np.sqrt(n[0] ** 2 + (n[1] ** 2 + n[2] ** 2 + 0.0) + n[3] ** 2)
+    for _ in range(2):
+        got = _noalloc(lib, res, area, w, 0.0)
+        assert rel_l2(got[:4], n) <= TOL
+        assert abs(got[5] - total) <= TOL * total and got[4] == 1.0
+
+
+def test_noalloc_zero_residual_and_null_buffer():
+    lib = _bind()
+    nv = 1000
+    got = _noalloc(lib, np.zeros((nv, 5)), np.ones(nv), np.ones(nv), 0.0)
+    # a zero first-iteration total makes the normaliser 1 (src/fv.cc:1860-1873)
+    assert got[5] == 1.0 and got[4] == 0.0 and np.all(got[:4] == 0.0)
+    import torch
+    t = torch.zeros(8, dtype=torch.float64, device="cuda")
+    p = C.c_void_p(t.data_ptr())
+    assert lib.tg_residual_norm_noalloc(None, p, p, 4, 0.0, p, None) == 4
+    assert lib.tg_residual_norm_noalloc(p, p, p, 4, 0.0, None, None) == 4
+    assert b"NULL" in lib.tg_noalloc_last_error()
