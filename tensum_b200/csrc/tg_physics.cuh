@@ -163,6 +163,14 @@ __device__ __forceinline__ double reconstructed_jump(double d, double gl, double
   }
 }
 
+// Whether reconstructed_jump<RECON> is positively homogeneous of degree one in
+// (d, gl, gr): van Albada's 1e-14 regularisation and the TVB threshold M h^2
+// carry their own scale.
+template <int RECON>
+__host__ __device__ constexpr bool recon_homogeneous() {
+  return RECON != RECON_VAN_ALBADA && RECON != RECON_TVB_MINMOD;
+}
+
 // Material::reconstruct (src/reconstruct.cc:139-188) for one component.
 template <int RECON>
 __device__ __forceinline__ void reconstruct1(double l, double r, double gl, double gr, double h, double M,
@@ -245,12 +253,32 @@ __device__ __forceinline__ VRec make_vrec_w(const Params& k, double u, double v,
   return r;
 }
 
+// The averages the KEPEC and TeCNO fluxes share: the density log mean, the
+// inverse of the beta log mean and p = (rho_l + rho_r) / (2 (beta_l + beta_r)),
+// from two reciprocals and one division instead of five divisions: the
+// beta sum's reciprocal serves beta's log-mean ratio f, 1/beta_ln and p.
+__device__ __forceinline__ double logavg_F_of(double f, double a, double b) {
+  double u = f * f;
+  if (u < 1.0e-2) {
+    double u2 = u * u;
+    double u3 = u2 * u;
+    return 1.0 + u * (1.0 / 3.0) + u2 * (1.0 / 5.0) + u3 * (1.0 / 7.0);
+  }
+  return log(b / a) / 2.0 / f;
+}
+__device__ __forceinline__ void shared_means(const VRec& L, const VRec& R, double& rho, double& ibeta, double& p) {
+  const double sr = L.rho + R.rho, sb = L.beta + R.beta;
+  const double isr = 1.0 / sr, isb = 1.0 / sb;
+  rho = 0.5 * sr / logavg_F_of((R.rho - L.rho) * isr, L.rho, R.rho);
+  ibeta = logavg_F_of((R.beta - L.beta) * isb, L.beta, R.beta) * (2.0 * isb);
+  p = 0.5 * sr * isb;
+}
+
 __device__ __forceinline__ Flx kepec_flux(const Params& k, const VRec& L, const VRec& R, double unx, double uny) {
   // src/kepec.cc:10-38; 1/((gamma-1) beta_ln) is formed from 1/beta_ln directly
-  double rho = logavg(L.rho, R.rho);
+  double rho, ibeta, p;
+  shared_means(L, R, rho, ibeta, p);
   double vel2 = 0.5 * ((L.u * L.u + L.v * L.v) + (R.u * R.u + R.v * R.v));
-  double ibeta = inv_logavg(L.beta, R.beta);
-  double p = 0.5 * (L.rho + R.rho) / (L.beta + R.beta);
   double vx = L.u * 0.5 + R.u * 0.5, vy = L.v * 0.5 + R.v * 0.5;
   double vn = vx * unx + vy * uny;
   Flx F;
@@ -325,10 +353,9 @@ template <int ROE, int RECON>
 __device__ __forceinline__ Flx tecno_flux(const Params& k, const VRec& L, const VRec& Rp, double unx, double uny,
                                           double dx, double dy, const double* dEl, const double* dEr, int ssw = 0) {
   const double g = k.gamma;
-  double rho = logavg(L.rho, Rp.rho);
-  double ibeta = inv_logavg(L.beta, Rp.beta);    // 1 / beta_ln
+  double rho, ibeta, p;                          // rho_ln, 1 / beta_ln, p
+  shared_means(L, Rp, rho, ibeta, p);
   double a = sqrt(0.5 * g * ibeta);
-  double p = 0.5 * (L.rho + Rp.rho) / (L.beta + Rp.beta);
   double vx = L.u * 0.5 + Rp.u * 0.5, vy = L.v * 0.5 + Rp.v * 0.5;
   double vn = vx * unx + vy * uny;
   // central KEPEC part (src/kepec.cc:25-34) from the log means computed above
@@ -343,8 +370,63 @@ __device__ __forceinline__ Flx tecno_flux(const Params& k, const VRec& L, const 
   if (!k.nd) return F;
 
   double vsq = vx * vx + vy * vy;
-  double H = a * a / (g - 1.0) + 0.5 * vsq;
   double v1 = vx * uny - vy * unx;
+  if (recon_homogeneous<RECON>()) {
+    // The reconstructions whose limiter is positively homogeneous of degree one
+    // (phi(s x, s y) = s phi(x, y) for s > 0: first, second, MUSCL, minmod, ENO2)
+    // commute with the scaling S of the eigenvectors: the dissipation
+    // S (Lambda jump(S R0^T V)) equals S^2 (Lambda jump(R0^T V)) with
+    // S0^2 = rho/(2 gamma), S1^2 = (gamma - 1) rho/gamma, S2^2 = p.  The
+    // unscaled form needs one square root per edge (a) instead of three.
+    const double aa = 0.5 * g * ibeta;            // a^2
+    const double H2 = aa * k.inv_gm1 + 0.5 * vsq;
+    auto RT0 = [&](const double* x, double* z) {
+      double A = x[0] + vx * x[1] + vy * x[2];
+      double B = unx * x[1] + uny * x[2] + vn * x[3];
+      double C = A + H2 * x[3];
+      z[0] = C - a * B;
+      z[1] = A + (0.5 * vsq) * x[3];
+      z[2] = uny * x[1] - unx * x[2] + v1 * x[3];
+      z[3] = C + a * B;
+    };
+    double Lam[4];
+    if (ROE) {
+      double vnl = L.u * unx + L.v * uny, vnr = Rp.u * unx + Rp.v * uny;
+      double l2 = fabs(vn);
+      Lam[0] = (1 + k.ev_beta) * fabs(vn - a) + k.ev_alpha * fabs((vnl - L.a) - (vnr - Rp.a));
+      Lam[1] = l2;
+      Lam[2] = ssw > 0 ? dmax_(l2, a) : l2;
+      Lam[3] = (1 + k.ev_beta) * fabs(vn + a) + k.ev_alpha * fabs((vnl + L.a) - (vnr + Rp.a));
+    } else {
+      double lr = fabs(vn) + a;                  // a >= 0
+      Lam[0] = Lam[1] = Lam[2] = Lam[3] = lr;
+    }
+    double dV[4] = {Rp.V1 - L.V1, 2 * Rp.u * Rp.beta - 2 * L.u * L.beta, 2 * Rp.v * Rp.beta - 2 * L.v * L.beta,
+                    -2 * Rp.beta - -2 * L.beta};
+    double gl[4], gr[4];
+#pragma unroll
+    for (int i = 0; i < 4; ++i) {
+      gl[i] = dEl[2 * i] * dx + dEl[2 * i + 1] * dy;
+      gr[i] = dEr[2 * i] * dx + dEr[2 * i + 1] * dy;
+    }
+    double d[4], sgl[4], sgr[4];
+    RT0(dV, d);
+    RT0(gl, sgl);
+    RT0(gr, sgr);
+    double q[4];
+#pragma unroll
+    for (int i = 0; i < 4; ++i) q[i] = Lam[i] * reconstructed_jump<RECON>(d[i], sgl[i], sgr[i], 0.0, 0.0);
+    const double s01 = rho * k.inv_gamma;
+    q[0] *= 0.5 * s01; q[1] *= (g - 1.0) * s01; q[2] *= p; q[3] *= 0.5 * s01;
+    double sum = q[0] + q[1] + q[3], dif = q[3] - q[0];
+    F.m -= 0.5 * sum;
+    F.x -= 0.5 * (vx * sum + a * unx * dif + uny * q[2]);
+    F.y -= 0.5 * (vy * sum + a * uny * dif - unx * q[2]);
+    F.e -= 0.5 * (H2 * (q[0] + q[3]) + a * vn * dif + (0.5 * vsq) * q[1] + v1 * q[2]);
+    return F;
+  }
+  // van Albada and TVB minmod: the scaled form of the reference
+  double H = a * a / (g - 1.0) + 0.5 * vsq;
   double const1 = sqrt(rho * k.inv_gamma);
   double psqrt = sqrt(p);
   double S0 = sqrt(0.5) * const1, S1 = k.sqrt_gm1 * const1, S2 = psqrt;
