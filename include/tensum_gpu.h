@@ -317,6 +317,10 @@ tg_status tg_moments_finalize(tg_handle* h, int instance, long n);
  * caller can bracket calls with its own CUDA events. */
 tg_status tg_stream(tg_handle* h, void** stream_out);
 
+/* ---- measurement hooks: extensions with no counterpart in the reference ----
+ * tg_time_phase, tg_query and tg_batch_time_steps exist for benchmarks and
+ * tests (device time of one phase, layout facts); a drop-in caller does not
+ * need them. */
 typedef enum {
   TG_PHASE_GRADIENT = 0,   /* compute_gradients                                   */
   TG_PHASE_FLUX = 1,       /* inviscid + viscous fluxes and residual assembly     */
@@ -336,7 +340,9 @@ typedef enum {
   TG_Q_KERNELS_PER_STEP = 3,   /* kernel launches in one tg_step step        */
   TG_Q_DEVICE_BYTES = 4,       /* device memory owned by the handle          */
   TG_Q_KERNELS_PER_PHASE = 5,  /* launches of one TG_PHASE_FLUX call         */
-  TG_Q_N_TILES = 6             /* vertex tiles (CTAs of one tiled pass)      */
+  TG_Q_N_TILES = 6,            /* vertex tiles (CTAs of one tiled pass)      */
+  TG_Q_RESIDUAL_NORM0 = 7      /* residual_norm_total0, the normaliser of the */
+                               /* relative norm (restart files, src/writer.cc) */
 } tg_query_key;
 tg_status tg_query(tg_handle* h, int key, double* out);
 
@@ -466,7 +472,8 @@ tg_status tg_batch_integrals(tg_batch* b, int level, double* out);
  * fastest; ms_out (may be NULL) gets one time per shape. */
 tg_status tg_batch_set_shape(tg_batch* b, int shape);
 tg_status tg_batch_tune(tg_batch* b, int steps, int* shape_out, double* ms_out);
-/* Device time per step over `steps` steps (the batch advances). */
+/* Device time per step over `steps` steps (the batch advances).  A measurement
+ * hook with no counterpart in the reference, like tg_time_phase. */
 tg_status tg_batch_time_steps(tg_batch* b, int steps, double* ms_per_step);
 tg_status tg_batch_stream(tg_batch* b, void** stream_out);
 typedef enum {

@@ -665,9 +665,11 @@ static tg_status create_handle(const tg_mesh* mesh, const tg_material* mat, cons
   if (opt->time_mode == TG_UNSTEADY && opt->n_time_stamps <= 0)
     return fail(nullptr, TG_INVALID_ARG, "unsteady runs need n_time_stamps > 0");
   if (!(opt->cfl > 0.0) && !(opt->time_step > 0.0)) return fail(nullptr, TG_INVALID_ARG, "cfl or time_step must be > 0");
-  if (n_parts > 0 && (mat->model == 1 || opt->bc_strong || (opt->liou_fix && mat->flux_scheme == FLUX_TECNO_ROE)))
-    return fail(nullptr, TG_NOT_SUPPORTED,
-                "partitioned runs are inviscid with weak boundary conditions and without the Liou fix");
+  // strong conditions reset the state after the last update, so dt could not come from
+  // it (fuse_dt) and would need an exchange inside the step; the Liou switch of a ghost
+  // depends on edges the partition does not hold
+  if (n_parts > 0 && (opt->bc_strong || (opt->liou_fix && mat->flux_scheme == FLUX_TECNO_ROE)))
+    return fail(nullptr, TG_NOT_SUPPORTED, "partitioned runs use weak boundary conditions and no Liou fix");
 
   tg_handle* h = new (std::nothrow) tg_handle();
   if (!h) return fail(nullptr, TG_INVALID_ARG, "out of host memory");
@@ -1480,6 +1482,13 @@ tg_status tg_query(tg_handle* h, int key, double* out) {
     case TG_Q_DEVICE_BYTES: *out = (double)h->device_bytes; break;
     case TG_Q_KERNELS_PER_PHASE: *out = h->kernels_per_flux; break;
     case TG_Q_N_TILES: *out = h->L.ntiles; break;
+    case TG_Q_RESIDUAL_NORM0: {
+      Scalars s;
+      const tg_status st = read_scalars(h, &s);
+      if (st != TG_OK) return st;
+      *out = s.rtotal0;
+      break;
+    }
     default: return fail(h, TG_INVALID_ARG, "unknown query key");
   }
   return TG_OK;
