@@ -474,8 +474,17 @@ void for_each_reach(const HostLayout& G, int v, F&& f) {
   }
   for (int j = G.cb_off[v]; j < G.cb_off[v + 1]; ++j) {
     const int ent = G.cb_ent[j], type = ent & 3, idx = ent >> 2;
+    if (type == 2) {   // a viscous unit: the vertices of its cell (and of its cell's boundary faces)
+      const int c = G.u_cell[idx / 3];
+      for (int k = 0; k < 3; ++k) f(G.c_v[3 * (size_t)c + k]);
+      continue;
+    }
     const int d = type == 0 ? idx >> 1 : idx;
-    if (type == 0 || type == 1 || type == 3) { f(G.b_v0[d]); f(G.b_v1[d]); }
+    f(G.b_v0[d]); f(G.b_v1[d]);
+    if (G.nvu > 0) {   // the face's boundary unit reads its cell
+      const int c = G.b_cell[d];
+      for (int k = 0; k < 3; ++k) f(G.c_v[3 * (size_t)c + k]);
+    }
   }
 }
 
@@ -498,7 +507,6 @@ std::vector<int> ghosts_of(const HostLayout& G, const std::vector<int>& v0, int 
 std::string plan_partition(const HostLayout& G, int n_parts, int part, PartPlan& P) {
   if (n_parts < 1 || part < 0 || part >= n_parts) return "partition index out of range";
   if (n_parts > G.nv) return "more partitions than vertices";
-  if (G.nvu > 0) return "viscous runs are not partitioned";
   P = PartPlan();
   P.n_parts = n_parts;
   P.part = part;
@@ -547,20 +555,38 @@ std::string restrict_layout(const HostLayout& G, const PartPlan& P, HostLayout& 
     L.x.push_back(G.x[g]); L.y.push_back(G.y[g]);
     if (G.axi) L.v_r.push_back(G.v_r[g]);
   }
-  // edges and boundary faces the owned vertices' lists use, in the global order
-  std::vector<int> edges, faces;
+  // edges, boundary faces and interior viscous units the owned vertices' lists use,
+  // in the global order
+  std::vector<int> edges, faces, iunits;
   for (int v = P.v0[P.part]; v < P.v0[P.part + 1]; ++v) {
     for (int j = G.ce_off[v]; j < G.ce_off[v + 1]; ++j) edges.push_back(G.ce_ent[j] >> 1);
     for (int j = G.cb_off[v]; j < G.cb_off[v + 1]; ++j) {
       const int ent = G.cb_ent[j], type = ent & 3, idx = ent >> 2;
-      if (type == 2) return "viscous units are not partitioned";
-      faces.push_back(type == 0 ? idx >> 1 : idx);
+      if (type == 2) {
+        const int u = idx / 3;
+        if (u < G.n_int_cells) iunits.push_back(u);
+        else faces.push_back(u - G.n_int_cells);   // a boundary unit belongs to its face
+      } else {
+        faces.push_back(type == 0 ? idx >> 1 : idx);
+      }
+    }
+  }
+  if (G.nvu > 0) {
+    // every local boundary face gets its boundary unit, which reads the boundary faces of
+    // the face's cell (its gradient corrections and boundary states): those join the set
+    const size_t n0 = faces.size();
+    for (size_t i = 0; i < n0; ++i) {
+      const int c = G.b_cell[faces[i]];
+      for (int j = G.c_bf_off[c]; j < G.c_bf_off[c + 1]; ++j) faces.push_back(G.c_bf[j]);
+      for (int j = G.c_nbr_off[c]; j < G.c_nbr_off[c + 1]; ++j) faces.push_back(G.c_nbr[j]);
     }
   }
   std::sort(edges.begin(), edges.end());
   edges.erase(std::unique(edges.begin(), edges.end()), edges.end());
   std::sort(faces.begin(), faces.end());
   faces.erase(std::unique(faces.begin(), faces.end()), faces.end());
+  std::sort(iunits.begin(), iunits.end());
+  iunits.erase(std::unique(iunits.begin(), iunits.end()), iunits.end());
   std::vector<int> elid(G.ne, -1), blid(G.nb, -1);
   L.ne = (int)edges.size();
   for (int i = 0; i < L.ne; ++i) {
@@ -585,6 +611,56 @@ std::string restrict_layout(const HostLayout& G, const PartPlan& P, HostLayout& 
     L.bf_face_nx.push_back(G.bf_face_nx[d]); L.bf_face_ny.push_back(G.bf_face_ny[d]);
     L.bf_face_v0.push_back(std::max(0, lid[G.bf_face_v0[d]])); L.bf_face_v1.push_back(std::max(0, lid[G.bf_face_v1[d]]));
   }
+  // viscous units: the interior units the owned vertices gather, then one boundary unit per
+  // local boundary face in local face order (the device's unit numbering); their cells
+  // with local vertex and face ids
+  std::vector<int> ulid(G.nvu, -1);
+  if (G.nvu > 0) {
+    std::vector<int> units = iunits;
+    for (int d : faces) units.push_back(G.n_int_cells + d);
+    L.n_int_cells = (int)iunits.size();
+    L.nvu = (int)units.size();
+    std::vector<int> clid;
+    std::vector<int> cells;
+    for (int u : units) cells.push_back(G.u_cell[u]);
+    std::vector<int> ucell_sorted = cells;
+    std::sort(ucell_sorted.begin(), ucell_sorted.end());
+    ucell_sorted.erase(std::unique(ucell_sorted.begin(), ucell_sorted.end()), ucell_sorted.end());
+    const int ncl = (int)ucell_sorted.size();
+    L.c_bf_off.assign(ncl + 1, 0);
+    L.c_nbr_off.assign(ncl + 1, 0);
+    for (int i = 0; i < ncl; ++i) {
+      const int c = ucell_sorted[i];
+      for (int k = 0; k < 3; ++k) {
+        const int x = lid[G.c_v[3 * (size_t)c + k]];
+        if (x < 0) return "partition viscous-cell vertex is not local";
+        L.c_v.push_back(x);
+      }
+      for (int k = 0; k < 6; ++k) L.c_n.push_back(G.c_n[6 * (size_t)c + k]);
+      L.c_inv2a.push_back(G.c_inv2a[c]);
+      for (int j = G.c_bf_off[c]; j < G.c_bf_off[c + 1]; ++j) {
+        if (blid[G.c_bf[j]] < 0) return "partition viscous-cell boundary face is not local";
+        L.c_bf.push_back(blid[G.c_bf[j]]);
+      }
+      for (int j = G.c_nbr_off[c]; j < G.c_nbr_off[c + 1]; ++j) {
+        if (blid[G.c_nbr[j]] < 0) return "partition viscous-cell boundary face is not local";
+        L.c_nbr.push_back(blid[G.c_nbr[j]]);
+      }
+      L.c_bf_off[i + 1] = (int)L.c_bf.size();
+      L.c_nbr_off[i + 1] = (int)L.c_nbr.size();
+    }
+    for (size_t i = 0; i < units.size(); ++i) {
+      ulid[units[i]] = (int)i;
+      const int c = (int)(std::lower_bound(ucell_sorted.begin(), ucell_sorted.end(), cells[i]) - ucell_sorted.begin());
+      L.u_cell.push_back(c);
+      if (G.axi) L.u_r.push_back(G.u_r[units[i]]);
+    }
+    for (int d : faces)
+      if (lid[G.bf_face_v0[d]] < 0 || lid[G.bf_face_v1[d]] < 0) return "partition viscous boundary vertex is not local";
+    for (int i = 0; i < L.nb; ++i)   // the boundary faces' cells in the local cell numbering
+      L.b_cell[i] = (int)(std::lower_bound(ucell_sorted.begin(), ucell_sorted.end(), G.b_cell[faces[i]]) -
+                          ucell_sorted.begin());
+  }
   // owned vertices keep their lists, entry for entry; ghosts have none
   L.ce_off.assign(nloc + 1, 0);
   L.cb_off.assign(nloc + 1, 0);
@@ -596,7 +672,8 @@ std::string restrict_layout(const HostLayout& G, const PartPlan& P, HostLayout& 
     }
     for (int j = G.cb_off[v]; j < G.cb_off[v + 1]; ++j) {
       const int ent = G.cb_ent[j], type = ent & 3, idx = ent >> 2;
-      const int nidx = type == 0 ? ((blid[idx >> 1] << 1) | (idx & 1)) : blid[idx];
+      const int nidx = type == 0 ? ((blid[idx >> 1] << 1) | (idx & 1))
+                       : type == 2 ? 3 * ulid[idx / 3] + idx % 3 : blid[idx];
       L.cb_ent.push_back((nidx << 2) | type);
     }
     L.ce_off[i + 1] = (int)L.ce_ent.size();

@@ -107,8 +107,10 @@ struct PartPlan {
   std::vector<int> send_off, send_idx, recv_off, recv_idx;
 };
 
-// Builds partition `part` of `n_parts` from the full layout.  Viscous units and
-// strong-condition lists are not split (the caller refuses those runs).
+// Builds partition `part` of `n_parts` from the full layout.  A partition holds the
+// viscous units its owned vertices gather (interior cells) and one per local boundary
+// face, with their cells renumbered.  Strong-condition lists are not split (the caller
+// refuses those runs).
 std::string plan_partition(const HostLayout& G, int n_parts, int part, PartPlan& P);
 std::string restrict_layout(const HostLayout& G, const PartPlan& P, HostLayout& out);
 

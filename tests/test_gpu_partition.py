@@ -117,9 +117,9 @@ def test_partition_handles_refuse_whole_mesh_calls():
     assert abi.STATUS[e.value.status] == "TG_INVALID_ARG"
     p.close()
     m = cases.cylinder_mesh(8, 16, 0)
-    ns = abi.Problem(preproc.preprocess(m), cases.cylinder_config(0.2, 100.0, 0.0, 1.0, 1))
+    strong = abi.Problem(preproc.preprocess(m), dict(cases.cylinder_config(0.2, 100.0, 0.0, 1.0, 1), bc_scheme="strong"))
     with pytest.raises(gpu.TensumError) as e:
-        partition.Partition(ns, 2, 0)
+        partition.Partition(strong, 2, 0)
     assert abi.STATUS[e.value.status] == "TG_NOT_SUPPORTED"
 
 
@@ -180,3 +180,61 @@ def test_frontier_tiles_are_the_ones_reading_ghosts():
             if n == 2:
                 assert p.n_frontier < p.n_tiles
             p.close()
+
+
+@pytest.mark.parametrize("name,n_parts", [("cyl_ns", 2), ("cyl_ns", 3), ("cyl_ns", 4), ("cyl_ns_isothermal", 3),
+                                          ("cyl_ns_rusanov_va", 2), ("cyl_ns_axi", 3), ("cyl_ns_voronoi", 2),
+                                          ("cyl_ns_rk4", 3)])
+def test_navier_stokes_partitions_match_one_partition_and_oracle(name, n_parts):
+    """Navier-Stokes meshes with walls and far field: each partition computes the
+    viscous units its owned vertices gather (interior cells) and the boundary units
+    of its boundary faces from its owned and ghost states (src/fv.cc:1197-1461 splits
+    them over MPI partitions and sums shared vertices, src/reduce_residual.cc:14-104).
+    The partitioned solve repeats the one-partition solve bit for bit, and both
+    follow the oracle."""
+    from tests.golden.cases_spec import CASES, build_case
+    from tests.helpers import geometry, rel_l2
+    import oracle as O
+    mesh, cfg, prim0 = build_case(CASES[name])
+    P = abi.Problem(geometry(mesh, cfg), dict(cfg, final_time=1e9, time_stamps=1))
+    want, winfo = _one_partition(P, prim0, 6)
+    ps = partition.PartitionedSolver(P, n_parts)
+    ps.set_state(prim0)
+    info = ps.step(6)
+    got = ps.get_state()
+    assert np.array_equal(got, want)
+    assert info[1] == winfo[1]
+    ps.close()
+    o = O.Oracle(P)
+    o.set_prim(prim0)
+    o.step(6)
+    assert rel_l2(got, o.get_prim()) <= 1e-10
+
+
+@pytest.mark.parametrize("graph,overlap", [(True, True), (False, False)])
+def test_navier_stokes_cylinder_partitions_over_many_steps(graph, overlap):
+    """The 16 x 32 Navier-Stokes cylinder (adiabatic wall, far field) in 3 partitions
+    over 25 steps: bit-identical to one partition and within 1e-10 of the oracle."""
+    from tests.helpers import rel_l2
+    import oracle as O
+    from tensum_b200 import mesh as M
+    m = M.annulus(16, 32, 0.5, 20.0, 0.05, seed=2)
+    prim0 = cases.cylinder_ic(m.coords)
+    prim0[:, 3] += 0.02 * np.cos(m.coords[:, 0])
+    cfg = dict(flux="kepes_tecno_roe", reconstruct="minmod", model="ns", mu_ref=0.002,
+               boundary={1: ("noslip", {"xvelocity": 0.0, "yvelocity": 0.0, "zvelocity": 0.0}),
+                         2: ("farfield", {"temperature": 1 / 1.4, "xvelocity": 0.2, "yvelocity": 0.0,
+                                          "zvelocity": 0.0, "pressure": 1 / 1.4})},
+               final_time=1e9, time_stamps=1, cfl=0.8)
+    P = abi.Problem(preproc.preprocess(m), cfg)
+    want, _ = _one_partition(P, prim0, 25)
+    ps = partition.PartitionedSolver(P, 3, graph=graph, overlap=overlap)
+    ps.set_state(prim0)
+    ps.step(25)
+    got = ps.get_state()
+    ps.close()
+    assert np.array_equal(got, want)
+    o = O.Oracle(P)
+    o.set_prim(prim0)
+    o.step(25)
+    assert rel_l2(got, o.get_prim()) <= 1e-10

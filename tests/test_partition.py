@@ -32,7 +32,12 @@ def _cyl():
                                                    boundary={1: ("slip", {}), 2: ("farfield", far)}))
 
 
-@pytest.mark.parametrize("make", [_kh, _cyl])
+def _cyl_ns():
+    m = cases.cylinder_mesh(8, 16, 0)
+    return abi.Problem(preproc.preprocess(m), cases.cylinder_config(0.2, 100.0, 0.0, 1.0, 1))
+
+
+@pytest.mark.parametrize("make", [_kh, _cyl, _cyl_ns])
 @pytest.mark.parametrize("n_parts", [1, 2, 3, 5])
 def test_plans_cover_and_pair(make, n_parts):
     P = make()
@@ -111,7 +116,7 @@ def _worker(rank, world, port, out_dir):
     os.environ["MASTER_PORT"] = str(port)
     dist.init_process_group("gloo", rank=rank, world_size=world, timeout=datetime.timedelta(seconds=60))
     try:
-        P = _cyl() if world == 3 else _kh(17)
+        P = {2: _kh(17), 3: _cyl(), 4: _cyl_ns()}[world]
         p = partition.plan(P, world, rank)
         n_own, local = p["n_owned"], p["local"]
         rec = np.full((len(local), partition.WIDTH), np.nan)
@@ -134,7 +139,7 @@ def _worker(rank, world, port, out_dir):
         dist.destroy_process_group()
 
 
-@pytest.mark.parametrize("world", [2, 3])
+@pytest.mark.parametrize("world", [2, 3, 4])
 def test_exchange_over_gloo_fills_every_ghost(tmp_path, world):
     import torch.multiprocessing as tmp
     tmp.start_processes(_worker, args=(world, _free_port(), str(tmp_path)), nprocs=world, join=True,
