@@ -159,11 +159,11 @@ __device__ __forceinline__ float fjump(float d, float gl, float gr) {
 
 // KEPEC central flux (src/kepec.cc:10-38) on a unit normal.
 __device__ __forceinline__ FFlx fkepec(const BParams& k, const FRec& L, const FRec& R, float unx, float uny,
-                                       float& rho_ln, float& ibeta) {
+                                       float& rho_ln, float& ibeta, float& p) {
   // __fdividef: at most 2 ulp for the magnitudes of densities and beta
   rho_ln = __fdividef(0.5f * (L.rho + R.rho), logavg_F_mixed(L.rho, R.rho));
   ibeta = __fdividef(logavg_F_mixed(L.beta, R.beta), 0.5f * (L.beta + R.beta));
-  const float p = __fdividef(0.5f * (L.rho + R.rho), L.beta + R.beta);
+  p = __fdividef(0.5f * (L.rho + R.rho), L.beta + R.beta);
   const float vx = 0.5f * (L.u + R.u), vy = 0.5f * (L.v + R.v);
   const float vn = vx * unx + vy * uny;
   const float vel2 = 0.5f * ((L.u * L.u + L.v * L.v) + (R.u * R.u + R.v * R.v));
@@ -177,28 +177,31 @@ __device__ __forceinline__ FFlx fkepec(const BParams& k, const FRec& L, const FR
 
 // KEPES-TeCNO (src/kepes_tecno_roe.cc:11-173, src/kepes_tecno_rusanov.cc:11-164):
 // KEPEC minus 0.5 R Lambda (Z_ji - Z_ij), R applied through its column structure.
+// First order and minmod are positively homogeneous of degree one, so the
+// eigenvector scaling S enters only squared: S (Lambda jump(S R0^T V)) =
+// S^2 (Lambda jump(R0^T V)), S0^2 = rho/(2 gamma), S1^2 = (gamma-1) rho/gamma,
+// S2^2 = p, without their square roots.
 template <int ROE, int RECON>
 __device__ __forceinline__ FFlx ftecno(const BParams& k, const FRec& L, const FRec& R, float unx, float uny, float dx,
                                        float dy, const float* gL, const float* gR) {
-  float rho, ibeta;
-  FFlx F = fkepec(k, L, R, unx, uny, rho, ibeta);
-  const float a = sqrtf(0.5f * k.gamma * ibeta);
-  const float p = __fdividef(0.5f * (L.rho + R.rho), L.beta + R.beta);
+  static_assert(RECON == RECON_FIRST || RECON == RECON_TVD_MINMOD, "ensembles run first order or minmod");
+  float rho, ibeta, p;
+  FFlx F = fkepec(k, L, R, unx, uny, rho, ibeta, p);
+  const float aa = 0.5f * k.gamma * ibeta;             // a^2
+  const float a = sqrtf(aa);
   const float vx = 0.5f * (L.u + R.u), vy = 0.5f * (L.v + R.v);
   const float vn = vx * unx + vy * uny;
   const float vsq = vx * vx + vy * vy;
-  const float H = a * a * k.inv_gm1 + 0.5f * vsq;
+  const float H = aa * k.inv_gm1 + 0.5f * vsq;
   const float v1 = vx * uny - vy * unx;
-  const float c1 = sqrtf(rho * k.inv_gamma);
-  const float S0 = 0.70710678118654752f * c1, S1 = k.sqrt_gm1 * c1, S2 = sqrtf(p);
   auto RT = [&](const float* x, float* z) {
     const float A = x[0] + vx * x[1] + vy * x[2];
     const float B = unx * x[1] + uny * x[2] + vn * x[3];
     const float C = A + H * x[3];
-    z[0] = S0 * (C - a * B);
-    z[1] = S1 * (A + (0.5f * vsq) * x[3]);
-    z[2] = S2 * (uny * x[1] - unx * x[2] + v1 * x[3]);
-    z[3] = S0 * (C + a * B);
+    z[0] = C - a * B;
+    z[1] = A + (0.5f * vsq) * x[3];
+    z[2] = uny * x[1] - unx * x[2] + v1 * x[3];
+    z[3] = C + a * B;
   };
   float Lam[4];
   if (ROE) {
@@ -228,7 +231,8 @@ __device__ __forceinline__ FFlx ftecno(const BParams& k, const FRec& L, const FR
 #pragma unroll
   for (int i = 0; i < 4; ++i) q[i] = Lam[i] * fjump<RECON>(d[i], RECON != RECON_FIRST ? sl[i] : 0.0f,
                                                              RECON != RECON_FIRST ? sr[i] : 0.0f);
-  q[0] *= S0; q[1] *= S1; q[2] *= S2; q[3] *= S0;
+  const float s01 = rho * k.inv_gamma;
+  q[0] *= 0.5f * s01; q[1] *= (k.gamma - 1.0f) * s01; q[2] *= p; q[3] *= 0.5f * s01;
   const float sum = q[0] + q[1] + q[3], dif = q[3] - q[0];
   F.m -= 0.5f * sum;
   F.x -= 0.5f * (vx * sum + a * unx * dif + uny * q[2]);
@@ -242,8 +246,8 @@ __device__ __forceinline__ FFlx fflux(const BParams& k, const FRec& L, const FRe
                                       float dy, const float* gL, const float* gR) {
   if (FLUX == FLUX_TECNO_ROE) return ftecno<1, RECON>(k, L, R, unx, uny, dx, dy, gL, gR);
   if (FLUX == FLUX_TECNO_RUSANOV) return ftecno<0, RECON>(k, L, R, unx, uny, dx, dy, gL, gR);
-  float r, b;
-  return fkepec(k, L, R, unx, uny, r, b);
+  float r, b, p;
+  return fkepec(k, L, R, unx, uny, r, b, p);
 }
 
 // ------------------------------------------------- FP32 boundaries, viscous
