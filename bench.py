@@ -85,7 +85,8 @@ def parse():
     ap.add_argument("--seed", type=int, default=0)
     ap.add_argument("--e2e-steps", type=int, default=20)
     ap.add_argument("--no-cpu-baseline", action="store_true")
-    ap.add_argument("--workload", default="single", choices=["single", "mc", "cylinder", "partitioned"])
+    ap.add_argument("--workload", default="single",
+                    choices=["single", "mc", "cylinder", "cylinder-rse", "cylinder2", "multilevel", "partitioned"])
     ap.add_argument("--samples", type=int, default=None,
                     help="ensemble size (--workload mc: 4096, --workload cylinder: 1024)")
     ap.add_argument("--final-time", type=float, default=2.0, help="cylinder: run length of every sample")
@@ -96,6 +97,8 @@ def parse():
     ap.add_argument("--no-mc", action="store_true", help="skip the Monte Carlo object of the default line")
     ap.add_argument("--parts", default="1,2,4", help="partitioned: partition counts")
     ap.add_argument("--throughput-only", action="store_true", help="mc: the ensemble's stepping alone")
+    ap.add_argument("--mc-cap", type=float, default=120.0,
+                    help="mc: wall-clock cap of the plain FP64 arm of the measured time to 1%% RSE")
     a = ap.parse_args()
     a.flux_list = [(f, r) for f, r in FLUXES if f in a.fluxes.split(",")]
     return a
@@ -410,9 +413,9 @@ def run_ours(args):
     if rank == 0 and world == 1 and not args.no_mc:
         solvers.clear()          # release the single-solve handles before the ensemble
         s_e2e = None
-        mc = mc_line(257, 4096, 20, 3, args.seed)
+        mc = mc_line(257, 4096, 20, 3, args.seed, mc_cap=args.mc_cap)
         mc = {k: mc[k] for k in ("metric", "value", "unit", "ms_per_step", "config", "autotune", "fp64_per_sample",
-                                 "roofline", "qoi", "time_to_rse", "cv", "clocks")}
+                                 "roofline", "qoi", "time_to_rse_measured", "time_to_rse", "cv", "clocks")}
         mc["command"] = "python bench.py --workload mc --steps 20 --warmup 3"
 
     if dist:
@@ -434,7 +437,7 @@ def run_ours(args):
 MC_BYTES_PER_VSS = 187.0   # FP32 batched compulsory bytes per vertex-sample-stage (state, U_old, gradients)
 
 
-def mc_line(n, S, K, W, seed, throughput_only=False):
+def mc_line(n, S, K, W, seed, throughput_only=False, mc_cap=120.0):
     """Batched FP32 ensemble throughput and time to QoI error (one GPU): the JSON object
     (throughput_only: the graph-replayed steps alone, e.g. for a profiler)."""
     import torch
@@ -530,6 +533,10 @@ def mc_line(n, S, K, W, seed, throughput_only=False):
         ttr[f"rse_{rse:g}"] = dict(t, samples_plain=n_plain, samples_cv=n_cv,
                                    speedup_batched_vs_plain_fp64=t["plain_fp64_mc_s"] / t["batched_fp32_mc_s"],
                                    speedup_cv_vs_plain_fp64=t["plain_fp64_mc_s"] / t["batched_fp32_cv_s"])
+    # measured: each arm sampled until the mean and variance of every QoI reach 1 % RSE
+    from tensum_b200 import mcrse
+    measured = mcrse.measure(g, m, dict(base, final_time=t_q), lambda i: cases.kh_rnd_row(seed * 1000003 + i),
+                             rse=0.01, cap_s=mc_cap, seed=seed)
     line = {"metric": "vertex-sample-stage updates/s (FP32 ensemble); time to 1% RSE of the mean QoI vs plain FP64 MC",
             "value": value, "unit": "vertex-sample-stage updates/s", "n_gpus": 1, "steps": K, "warmup": W,
             "ms_per_step": ms / K, "higher_is_better": True, "scaling": "weak", "vs_baseline": None,
@@ -546,11 +553,14 @@ def mc_line(n, S, K, W, seed, throughput_only=False):
             "qoi": {"time": t_q, "names": ["0.5 rho v^2", "0.5 rho u^2", "-rho s/(gamma-1)"],
                     "fp32_vs_fp64_rel_err_max": [float(x) for x in qerr.max(0)], "fp64_subset": n_sub,
                     "batched_steps_issued": float(info[0]), "fp64_steps_mean": float(np.mean(steps64))},
+            "time_to_rse_measured": dict(measured, qoi_time=t_q,
+                                         qois=["0.5 rho v^2", "0.5 rho u^2", "-rho s/(gamma-1)"]),
             "time_to_rse": dict(ttr, qoi="0.5 rho v^2 (mean)", n_train=n_train, train_s=t_train,
                                 surrogate_evals=1 << 20, surrogate_eval_s=t_surr,
                                 fp64_sample_s=t_fp64_sample, batched_sample_s=t_batch_sample,
-                                note="sample counts from the ensemble's variance and control-variate residual "
-                                     "variance; FP64 per-sample time measured on a 32-sample subset"),
+                                note="model: sample counts from the ensemble's variance and control-variate "
+                                     "residual variance times per-sample costs (FP64 on a 32-sample subset); "
+                                     "time_to_rse_measured holds the measured runs"),
             "cv": {"gain": [float(x) for x in r["gain"]], "used": [bool(x) for x in r["used"]],
                    "mean": [float(x) for x in r["mean"]], "plain_mean": [float(x) for x in r["plain_mean"]],
                    "se_mean": [float(x) for x in r["se_mean"]]},
@@ -563,7 +573,7 @@ def mc_line(n, S, K, W, seed, throughput_only=False):
 
 def run_mc(args):
     n = args.n if args.n != 1025 else 257
-    print(json.dumps(mc_line(n, args.samples or 4096, args.steps, max(3, args.warmup), args.seed,
+    print(json.dumps(mc_line(n, args.samples or 4096, args.steps, max(3, args.warmup), args.seed, mc_cap=args.mc_cap,
                              throughput_only=args.throughput_only)))
     return 0
 
@@ -659,6 +669,222 @@ def run_cylinder(args):
     return 0
 
 
+def cylinder2_line(n_steps, n_out, fp32_samples, seed, n_r=256, n_t=512, mach=0.2, reynolds=100.0):
+    """The Navier-Stokes cylinder of the single-solve configuration (256 x 512 O-mesh, Mach 0.2,
+    Re 100, adiabatic wall, characteristic far field) for n_steps SSP-RK3 steps in FP64 and, as an
+    FP32 batch of identical members, over the same output times: the JSON object."""
+    import torch
+    from tensum_b200 import abi, batch, cases, cylinder, gpu, preproc, qoi
+    torch.cuda.set_device(0)
+    m = cases.cylinder_mesh(n_r, n_t, seed)
+    g = preproc.preprocess(m)
+    V = g.n_vertex
+    ic = cases.cylinder_ic(m.coords, mach, 0.0)
+    # the run length: n_steps steps at the time step the flow settles to (measured over a
+    # first stretch), cut into n_out equal output intervals that both precisions stop at
+    probe = gpu.Solver(abi.Problem(g, cases.cylinder_config(mach, reynolds, 0.0, 1.0e9, 1)))
+    probe.set_state(ic)
+    probe.step(1000)
+    t1 = probe.step(1000)[0]
+    ms64 = probe.time_phase("step", 200)      # device time of a step (final time far away)
+    probe.close()
+    T = float(n_steps * (t1 / 2000.0))
+    cfg = cases.cylinder_config(mach, reynolds, 0.0, T, n_out)
+    s = gpu.Solver(abi.Problem(g, cfg))
+    s.set_state(ic)
+    hist64 = [s.forces(cylinder.FORCES)[0]]
+    with ClockSampler(0) as clk64:
+        t0 = time.perf_counter()
+        for i in range(1, n_out + 1):
+            info = s.advance(i)
+            hist64.append(s.forces(cylinder.FORCES)[0])
+        wall64 = time.perf_counter() - t0
+    steps64 = int(info[3])
+    s.close()
+    hist64 = np.array(hist64)
+    times = np.linspace(0.0, T, n_out + 1)
+    t_start = 0.5 * T
+    cd64, cl64 = qoi.force_coefficients(hist64, mach, 0.0)
+    q64 = qoi.cylinder_qoi(times, cd64, cl64, mach, t_start)
+    # FP32 members: fp32_samples copies of the same configuration in one batch
+    b = batch.Batch([(abi.Problem(g, cfg), fp32_samples)])
+    rec = cases.cylinder_ic(m.coords[:1], mach, 0.0)
+    b.set_uniform(0, np.repeat(rec, fp32_samples, axis=0))
+    hist32 = [b.forces(0, cylinder.FORCES)[:, 0]]
+    with ClockSampler(0) as clk32:
+        t0 = time.perf_counter()
+        for i in range(1, n_out + 1):
+            b.advance(i)
+            hist32.append(b.forces(0, cylinder.FORCES)[:, 0])
+        wall32 = time.perf_counter() - t0
+    _, _, bad = b.clock(0)
+    hist32 = np.stack(hist32, axis=1)[0]
+    cd32, cl32 = qoi.force_coefficients(hist32, mach, 0.0)
+    q32 = qoi.cylinder_qoi(times, cd32, cl32, mach, t_start)
+    sel = times >= t_start
+    fl = cl64[sel] - cl64[sel].mean()
+    # periodic shedding behind a circular cylinder at Re 100 carries a lift amplitude of
+    # order 0.3 (RMS about 0.2); lift crossings at a far smaller amplitude are not shedding
+    shed = bool(np.isfinite(q64[2]) and q64[1] > 0.01)
+    err = np.abs(q32 - q64) / np.maximum(np.abs(q64), 1e-300)
+    line = {"metric": "vertex-stage updates/s (navier-stokes cylinder, fp64) and the cylinder QoIs",
+            "value": V * 3 * steps64 / wall64, "unit": UNIT, "n_gpus": 1, "steps": steps64, "warmup": 0,
+            "ms_per_step": ms64, "higher_is_better": True, "scaling": "weak", "vs_baseline": None, "dtype": "f64",
+            "data": "synthetic (seeded O-mesh, uniform free stream start)",
+            "config": {"workload": f"navier-stokes cylinder {n_r}x{n_t} O-mesh (r 0.5..20, first spacing 2e-3, "
+                                   f"ratio 1.02), mach {mach}, re {reynolds}, pr 0.72, adiabatic no-slip wall, "
+                                   f"characteristic far field, kepes_tecno_roe(minmod), ssprk3 cfl 0.8, "
+                                   f"{n_steps} steps to t = {T:.4g}, forces at {n_out} outputs",
+                       "mesh_vertices": V, "final_time": T, "outputs": n_out, "qoi_window": [t_start, T]},
+            "qoi": {"names": ["mean drag coefficient", "lift coefficient RMS", "strouhal number"],
+                    "fp64": [float(x) for x in q64], "fp32": [float(x) for x in q32],
+                    "fp32_vs_fp64_rel_err": [float(x) for x in err],
+                    "shedding": shed,
+                    "lift_upward_zero_crossings_in_window": int(np.count_nonzero((fl[:-1] < 0) & (fl[1:] >= 0))),
+                    "lift_history_last_quarter": [float(x) for x in cl64[-(n_out // 4):][::max(1, n_out // 200)]],
+                    "note": ("shedding measured in the window" if shed else
+                             f"measured: no vortex shedding by t = {T:.4g} from the uniform start (lift RMS "
+                             f"{q64[1]:.2g} against about 0.2 for a shedding cylinder at Re 100); the Strouhal "
+                             "entry is that of the small lift oscillation, not of shedding")},
+            "fp64": {"wall_s": wall64, "steps": steps64, "device_ms_per_step": ms64,
+                     "device_value": V * 3 / (ms64 / 1e3), "clocks": clk64.summary()},
+            "fp32": {"wall_s": wall32, "samples": fp32_samples, "bad_samples": int(bad.sum()),
+                     "value": V * 3 * fp32_samples * steps64 / wall32, "clocks": clk32.summary()},
+            "gpu_launches": None, "impl": "ours", "roofline": None, "clocks": clk64.summary(),
+            "command": f"python bench.py --workload cylinder2 --steps {n_steps} --outputs {n_out}"}
+    return line
+
+
+def run_cylinder2(args):
+    print(json.dumps(cylinder2_line(args.steps if args.steps != 200 else 200000, args.outputs if args.outputs != 40
+                                    else 2000, args.samples or 32, args.seed)))
+    return 0
+
+
+def multilevel_line(levels, n_steps, n_fp64, seed):
+    """The multilevel Monte Carlo configuration: Kelvin-Helmholtz ensembles on several meshes
+    ((n, samples) per level) in one fused FP32 batch, all to the time the finest mesh reaches in
+    n_steps steps; the pointwise mean and standard-deviation fields of the first n_fp64 samples of
+    every level against FP64 solves of the same samples.  The JSON object."""
+    import torch
+    from tensum_b200 import abi, batch, cases, gpu, preproc
+    torch.cuda.set_device(0)
+    base = dict(flux="kepes_tecno_rusanov", reconstruct="minmod", boundary={t: ("periodic", {}) for t in (1, 2, 3, 4)},
+                cfl=0.8)
+    meshes = [cases.kh_mesh(n, seed + i) for i, (n, _) in enumerate(levels)]
+    geoms = [preproc.preprocess(m) for m in meshes]
+    rows = [np.stack([cases.kh_rnd_row(seed * 1000003 + 7919 * i + s) for s in range(S)])
+            for i, (_, S) in enumerate(levels)]
+    # common final time: n_steps of the finest level's first time step
+    fine = int(np.argmax([g.n_vertex for g in geoms]))
+    probe = gpu.Solver(abi.Problem(geoms[fine], dict(base, final_time=1.0e9, time_stamps=1)))
+    probe.set_state(cases.kh_ic_rnd(meshes[fine].coords, rows[fine][0]))
+    T = float(n_steps * probe.step(1)[1])
+    probe.close()
+    probs = [abi.Problem(g, dict(base, final_time=T, time_stamps=1)) for g in geoms]
+    b = batch.Batch([(P, S) for P, (_, S) in zip(probs, levels)])
+    for i, r in enumerate(rows):
+        b.set_kh(i, r)
+    shape, _ = b.tune(3)
+    for i, r in enumerate(rows):
+        b.set_kh(i, r)
+    ms_step = b.time_steps(10)        # device time of a step of every level (graph replays)
+    for i, r in enumerate(rows):
+        b.set_kh(i, r)
+    with ClockSampler(0) as clk:
+        torch.cuda.synchronize()
+        t0 = time.perf_counter()
+        info = b.advance(1)
+        torch.cuda.synchronize()
+        wall = time.perf_counter() - t0
+    launches_steps = int(info[0])
+    per_level, work = [], 0
+    for i, ((n, S), g, m, P) in enumerate(zip(levels, geoms, meshes, probs)):
+        el, cnt, bad = b.clock(i)
+        # FP64 solves of the first n_fp64 samples of the level, to the same time
+        k = min(n_fp64, S)
+        s64 = gpu.Solver(P)
+        x64, x32, steps64 = [], [], []
+        for j in range(k):
+            s64.set_state(cases.kh_ic_rnd(m.coords, rows[i][j]))
+            inf = s64.advance(1)
+            steps64.append(int(inf[3]))
+            x64.append(s64.get_state())
+            x32.append(b.get_state(i, j))
+        s64.close()
+        x64, x32 = np.stack(x64), np.stack(x32)
+        cols = [0, 1, 2, 3]                      # T, p, u, v
+        m64, m32 = x64.mean(0)[:, cols], x32.mean(0)[:, cols]
+        sd64, sd32 = x64.std(0, ddof=1)[:, cols], x32.std(0, ddof=1)[:, cols]
+        scale = np.abs(m64).max(0)
+        scale[2] = scale[3] = max(scale[2], scale[3])
+        work += g.n_vertex * S * 3 * int(np.mean(steps64))
+        per_level.append({"n": n, "vertices": g.n_vertex, "samples": S, "steps": int(np.mean(steps64)),
+                          "bad_samples": int(bad.sum()), "reached": bool(np.all(cnt >= 2)),
+                          "fp64_subset": k,
+                          "mean_field_rel_err": (np.abs(m32 - m64).max(0) / scale).tolist(),
+                          "std_field_rel_err": (np.abs(sd32 - sd64).max(0) / (sd64.max(0) + 1e-300)).tolist()})
+    line = {"metric": "vertex-sample-stage updates/s (multilevel FP32 ensemble, one fused batch)",
+            "value": work / wall, "unit": "vertex-sample-stage updates/s", "n_gpus": 1, "steps": launches_steps,
+            "warmup": 0, "ms_per_step": ms_step, "higher_is_better": True, "scaling": "weak", "vs_baseline": None,
+            "dtype": "f32 members, f64 geometry / log-mean series / clocks", "data": "synthetic (seeded rnd rows)",
+            "config": {"workload": "kelvin-helmholtz multilevel ensemble " +
+                                   ", ".join(f"{S} x {n}^2" for n, S in levels) +
+                                   f", one fused batch, kepes_tecno_rusanov(minmod), ssprk3 cfl 0.8, to t = {T:.4g} "
+                                   f"({n_steps} steps of the finest mesh)", "shape": shape, "final_time": T},
+            "levels": per_level,
+            "fields": "pointwise mean and sample standard deviation of T, p, u, v over the FP64 subset, "
+                      "FP32 members against FP64 solves of the same samples; errors relative to each field's "
+                      "maximum (velocities: the larger velocity scale)",
+            "wall_s": wall, "gpu_launches": int(b.query("kernels_per_step")) * launches_steps,
+            "clocks": clk.summary(), "impl": "ours", "roofline": None,
+            "command": "python bench.py --workload multilevel"}
+    return line
+
+
+def run_multilevel(args):
+    levels = [(129, 2048), (257, 512), (513, 128)]
+    if args.samples:
+        levels = [(n, max(32, (S * args.samples // 4096) // 32 * 32)) for n, S in levels]
+    print(json.dumps(multilevel_line(levels, args.steps if args.steps != 200 else 1000, args.fp64_samples, args.seed)))
+    return 0
+
+
+def cylinder_rse_line(T, n_out, t_start, seed, cap_plain, cap_batched, cap_cv, n_r=128, n_t=256):
+    """Measured time to 1 % RSE of the mean and variance of the cylinder QoIs for plain FP64 MC,
+    batched FP32 MC and batched FP32 with the surrogate control variate: the JSON object."""
+    import torch
+    from tensum_b200 import cases, mcrse, preproc
+    torch.cuda.set_device(0)
+    m = cases.cylinder_mesh(n_r, n_t, seed)
+    g = preproc.preprocess(m)
+    with ClockSampler(0) as clk:
+        r = mcrse.measure_cylinder(g, m.coords, T, n_out, t_start, rse=0.01, seed=seed, cap_plain_s=cap_plain,
+                                   cap_batched_s=cap_batched, cap_cv_s=cap_cv)
+    return {"metric": "wall time to 1% RSE of the mean and variance of the cylinder QoIs, vs plain FP64 MC",
+            "value": r["speedup_cv_vs_plain_fp64"], "unit": "x (plain FP64 MC time / batched FP32 + CV time)",
+            "higher_is_better": True, "n_gpus": 1, "dtype": "f32 members, f64 geometry / forces; fp64 plain arm",
+            "data": "synthetic (seeded uncertain inputs, seeded O-mesh)",
+            "config": {"workload": f"navier-stokes cylinder {n_r}x{n_t} O-mesh, mach U[0.15,0.25], re U[80,120], "
+                                   f"angle U[-2,2] deg, kepes_tecno_roe(minmod), ssprk3 cfl 0.8, t = 0 .. {T}, "
+                                   f"forces at {n_out} outputs, QoI window t >= {t_start}",
+                       "qois": list(cylinder_names()), "caps_s": {"plain": cap_plain, "batched": cap_batched,
+                                                                 "cv": cap_cv}},
+            "time_to_rse_measured": r, "clocks": clk.summary(), "impl": "ours",
+            "command": "python bench.py --workload cylinder-rse"}
+
+
+def cylinder_names():
+    from tensum_b200 import cylinder
+    return cylinder.NAMES
+
+
+def run_cylinder_rse(args):
+    print(json.dumps(cylinder_rse_line(args.final_time, args.outputs, args.t_start, args.seed, args.mc_cap,
+                                       args.mc_cap, 900.0)))
+    return 0
+
+
 def run_partitioned(args):
     """The domain-decomposed solve (all partitions on this GPU) against the one-partition step."""
     import torch
@@ -719,6 +945,25 @@ def main():
                               "groups run one sample after another (see the single-solve reference arm)"}))
             return 0
         return run_mc(args)
+    if args.workload == "cylinder-rse":
+        if args.impl == "reference":
+            print(json.dumps({"impl": "reference", "unavailable": "the reference has no batched ensemble path; its MC "
+                              "groups run one sample after another (see the single-solve reference arm)"}))
+            return 0
+        return run_cylinder_rse(args)
+    if args.workload == "multilevel":
+        if args.impl == "reference":
+            print(json.dumps({"impl": "reference", "unavailable": "the reference has no batched ensemble path; its MC "
+                              "groups run one sample after another (see the single-solve reference arm)"}))
+            return 0
+        return run_multilevel(args)
+    if args.workload == "cylinder2":
+        if args.impl == "reference":
+            print(json.dumps({"impl": "reference", "unavailable": "200k steps of the 131k-vertex Navier-Stokes "
+                              "cylinder take about a day on one host core; the single-solve reference arm times "
+                              "the reference's own code"}))
+            return 0
+        return run_cylinder2(args)
     if args.workload == "cylinder":
         if args.impl == "reference":
             print(json.dumps({"impl": "reference", "unavailable": "the reference has no batched ensemble path; its MC "

@@ -58,6 +58,17 @@ def kh_rnd_row(seed: int, n_modes: int = 10) -> np.ndarray:
     return rng.uniform(0.0, 1.0, 2 * n_modes)
 
 
+def kh_expressions(n_modes: int = 10) -> dict:
+    """The Kelvin-Helmholtz initial condition as the parameter file's
+    expressions: the layer and the seeded perturbation through pert(4, ...)
+    over the sample's rnd-file row (src/perturb.cc:196-208), equal to
+    kh_ic_rnd."""
+    terms = " + ".join(f"pert(4,x,y,{k})*sin(2*pi*{k}*x+2*pi*pert(4,x,y,{n_modes + k}))"
+                       for k in range(1, n_modes + 1))
+    return {"temperature": "2.5/(1+(abs(y-0.5)<0.25))", "xvelocity": "(abs(y-0.5)<0.25)-0.5",
+            "yvelocity": f"0.01*({terms})", "zvelocity": "0.0", "pressure": "2.5"}
+
+
 def kh_ic_rnd(coords: np.ndarray, row: np.ndarray, gas_const: float = 1.0) -> np.ndarray:
     """The Kelvin-Helmholtz initial state of one Monte Carlo sample from its
     random-number row.  It is the value of the parameter-file initial condition

@@ -100,3 +100,34 @@ def samples_for_rse_var(y, g=None, rse: float = 0.01) -> np.ndarray:
     gz = (g - g.mean(0)) ** 2
     _, _, _, _, beta = _cv(z, gz, gz)
     return np.ceil((z - beta * gz).var(0, ddof=1) / target)
+
+
+def rse_now(y, g=None, g_extra=None) -> tuple[np.ndarray, np.ndarray]:
+    """Current relative standard errors of the mean and of the variance estimate
+    of each QoI column, from the N samples in hand (the stopping rule of a
+    sequential Monte Carlo run).
+
+    Plain MC (g None): se(mean) = sqrt(Var Y / N), se(var) = sqrt(Var Z / N)
+    with Z = (Y - mean Y)^2.  With the surrogate (g at the same inputs, g_extra
+    at M fresh ones) the mean gets the control-variate standard error of
+    `estimate` and Z gets (g - mean g_extra)^2 as its control, each with the
+    surrogate's own sampling term beta^2 Var / M; where the control does not
+    reduce the error, the plain one is used, as `estimate` falls back."""
+    y = np.asarray(y, np.float64)
+    if y.ndim == 1:
+        y = y[:, None]
+    N = y.shape[0]
+    mu, var = y.mean(0), y.var(0, ddof=1)
+    z = (y - mu) ** 2
+    se_m, se_v = np.sqrt(var / N), np.sqrt(z.var(0, ddof=1) / N)
+    if g is not None:
+        g = np.asarray(g, np.float64).reshape(y.shape)
+        ge = np.asarray(g_extra, np.float64)
+        ge = ge.reshape(ge.shape[0], -1)
+        _, var_cv, _, _, _ = _cv(y, g, ge)
+        gem = ge.mean(0)
+        gz, gze = (g - gem) ** 2, (ge - gem) ** 2
+        _, var_cvz, _, _, _ = _cv(z, gz, gze)
+        se_m = np.minimum(se_m, np.sqrt(var_cv))
+        se_v = np.minimum(se_v, np.sqrt(var_cvz))
+    return se_m / np.abs(mu), se_v / var

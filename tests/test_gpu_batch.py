@@ -151,3 +151,35 @@ def test_rejects_unsupported_setups():
     with pytest.raises(gpu.TensumError) as e:
         b.set_parameters(0, mu_ref=np.zeros(32))       # periodic Euler: nothing per sample
     assert abi.STATUS[e.value.status] == "TG_NOT_SUPPORTED"
+
+
+def test_multilevel_moment_fields_against_fp64_ensembles():
+    """Three meshes in one fused batch (the multilevel configuration at small
+    sizes), advanced to one output time: each level's FP64 moment fields
+    (reduce_moments' recurrence, src/reduce_moments.cc:14-221, in sample order)
+    against FP64 per-sample Monte Carlo of the same samples on the device."""
+    levels = [(17, 64), (33, 32), (65, 32)]
+    probs, meshes, rows = [], [], []
+    for i, (n, S) in enumerate(levels):
+        m, P = _problem(n, seed=i, final_time=0.03, stamps=1)
+        meshes.append(m); probs.append(P); rows.append(_rows(S, 1000 * i))
+    b = batch.Batch([(P, S) for P, (_, S) in zip(probs, levels)])
+    for i, r in enumerate(rows):
+        b.set_kh(i, r)
+    b.advance(1)
+    for i, ((n, S), m, P) in enumerate(zip(levels, meshes, probs)):
+        el, cnt, bad = b.clock(i)
+        assert np.all(cnt == 2) and not bad.any() and np.allclose(el, 0.03, rtol=0, atol=1e-15)
+        fm, sm, m2 = b.moments(i, extras=1 | 2 | 4)
+        s64 = gpu.Solver(P)
+        mc.run_group(s64, [cases.kh_ic_rnd(m.coords, r) for r in rows[i]], 2, 1 | 2 | 4)
+        f64, _, m264 = s64.moments_get(1)
+        scale = np.abs(f64).max(axis=0)
+        scale[2] = scale[3] = max(scale[2], scale[3])
+        scale[4] = 1.0
+        # FP32 members, pointwise over every vertex: the finest level takes the most steps
+        assert np.all(np.abs(fm - f64) <= 1e-5 * scale), n
+        sd = np.sqrt(m264 / (S - 1))
+        got_sd = np.sqrt(np.maximum(m2, 0.0) / (S - 1))
+        cols = [0, 1, 2, 3, 5, 6, 7]
+        assert np.all(np.abs(got_sd - sd)[:, cols] <= 1e-3 * (sd.max(axis=0) + 1e-30)[cols] + 1e-5 * scale[cols]), n
