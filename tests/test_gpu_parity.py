@@ -112,7 +112,7 @@ def test_vortex_cfg0_mesh_1000_steps_matches_oracle():
     assert rel_l2(s.get_state(), o.get_prim()) <= TOL_STATE_LONG
 
 
-@pytest.mark.parametrize("recon", ["first", "second", "van_albada", "tvb_minmod", "eno2"])
+@pytest.mark.parametrize("recon", ["first", "second", "second_muscl", "van_albada", "tvb_minmod", "eno2"])
 def test_cylinder_ns_multistep_matches_oracle(recon):
     m = M.annulus(16, 32, 0.5, 20.0, 0.05, seed=2)
     prim0 = cases.cylinder_ic(m.coords)
@@ -123,11 +123,13 @@ def test_cylinder_ns_multistep_matches_oracle(recon):
                                           "zvelocity": 0.0, "pressure": 1 / 1.4})},
                final_time=100.0, time_stamps=1, cfl=0.8)
     s, o = _run_pair(m, cfg, prim0, 25)
-    # ENO2 (minabs) and TVB minmod switch discontinuously (|a| vs |b|, |c| vs M h^2):
-    # a last-ulp difference can pick the other branch at a near-tie and the
-    # difference then propagates.  Their per-stage parity is checked at 1e-12
-    # against the reference fixtures; over many steps they get a looser bound.
-    tol = 1e-5 if recon in ("eno2", "tvb_minmod") else TOL_STATE_LONG
+    # ENO2's minabs takes the other slope at an exact tie |a| = |b| when the last
+    # bit of a rounded product differs, which fused multiply-adds change: the
+    # reference's own arithmetic moves by 1e-9 in one step under that change
+    # (tests/test_oracle_eno2_ties.py), the device's by about 2e-7, without growth
+    # (measured: at most 3e-7 over the 25 steps).  Every other reconstruction,
+    # TVB minmod included, stays at 1e-15.
+    tol = 1e-6 if recon == "eno2" else TOL_STATE_LONG
     assert rel_l2(s.get_state(), o.get_prim()) <= tol
 
 
