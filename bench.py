@@ -249,6 +249,9 @@ def run_reference(args):
             "warmup": warm, "ms_per_step": 1e3 * r["seconds"] / steps, "higher_is_better": True,
             "scaling": "weak", "vs_baseline": None, "dtype": "f64", "data": "synthetic (seeded mesh and field)",
             "config": config_dict(args, m, ne), "impl": "reference", "per_flux": r["per_flux"],
+            "steps_note": f"{steps} timed step(s) per flux (about {r['seconds'] / max(1, len(args.flux_list)) / steps:.1f} "
+                          "s each on one core), fewer than the GPU arm's, which times --steps; the metric is a "
+                          "rate, so the counts need not match",
             "cpu_baseline": {k: r[k] for k in ("value", "unit", "cores", "kind", "sample")},
             "e2e": {"value": r["value"], "unit": UNIT, "h2d_bytes_per_step": 0, "d2h_bytes_per_step": 0}}
     print(json.dumps(line))
@@ -373,32 +376,37 @@ def run_ours(args):
             el = float(t.item())
         return V * 3 * ne2e * world / el
 
-    def e2e_pipelined():
+    def e2e_pipelined(s):
+        """Seconds for ne2e steps of solver s with its state in and out of host memory each step."""
         ins, outs = (pin_in, pin_in2), (pin_out, pin_out2)
         torch.cuda.synchronize()
         if dist:
             dist.barrier()
         t0 = time.perf_counter()
-        s_e2e.set_state_async(ins[0])
+        s.set_state_async(ins[0])
         for i in range(ne2e):
             if i + 1 < ne2e:
-                s_e2e.set_state_async(ins[(i + 1) % 2])   # the next step's input streams in now
-            s_e2e.step(1)                                 # takes this step's input, steps
-            s_e2e.output_begin(outs[i % 2])               # the result streams out during the next step
-        s_e2e.output_wait()
+                s.set_state_async(ins[(i + 1) % 2])   # the next step's input streams in now
+            s.step(1)                                 # takes this step's input, steps
+            s.output_begin(outs[i % 2])               # the result streams out during the next step
+        s.output_wait()
         el = time.perf_counter() - t0
         if dist:
             t = torch.tensor([el], device="cuda", dtype=torch.float64)
             dist.all_reduce(t, op=dist.ReduceOp.MAX)
             el = float(t.item())
-        return V * 3 * ne2e * world / el
+        return el
 
+    # the same four solves as `value`: every flux ne2e steps, total updates over total time
     e2e_run(pin_in, pin_out)   # first touch of the staging paths
-    e2e_pipelined()
-    e2e = {"value": e2e_pipelined(), "unit": UNIT, "h2d_bytes_per_step": 40 * V,
-           "d2h_bytes_per_step": 40 * V, "steps": ne2e, "flux": dom_flux,
-           "path": "per step: tg_set_state_async(pinned host PrimVar[V]) of the next step's input, tg_step(1), "
-                   "tg_output_begin(pinned host PrimVar[V]) of its result; copies overlap the steps",
+    e2e_pipelined(s_e2e)
+    e2e_s = {f: e2e_pipelined(s) for f, s, _ in solvers}
+    e2e = {"value": V * 3 * ne2e * world * len(e2e_s) / sum(e2e_s.values()), "unit": UNIT,
+           "h2d_bytes_per_step": 40 * V * len(e2e_s), "d2h_bytes_per_step": 40 * V * len(e2e_s), "steps": ne2e,
+           "fluxes": list(e2e_s), "per_flux": {f: V * 3 * ne2e * world / t for f, t in e2e_s.items()},
+           "path": "per step and flux: tg_set_state_async(pinned host PrimVar[V]) of the next step's input, "
+                   "tg_step(1), tg_output_begin(pinned host PrimVar[V]) of its result; copies overlap the steps",
+           "blocking_flux": dom_flux,
            "blocking_value": e2e_run(pin_in, pin_out),
            "blocking_path": "tg_set_state(pinned) + tg_step(1) + tg_get_state(pinned) per step",
            "pageable_value": e2e_run(np.ascontiguousarray(prim0), page_out)}

@@ -705,6 +705,7 @@ static tg_status create_handle(const tg_mesh* mesh, const tg_material* mat, cons
   k.sqrt_gm1 = std::sqrt(mat->gamma - 1.0);
   k.inv_gamma = 1.0 / mat->gamma;
   k.inv_gm1 = 1.0 / (mat->gamma - 1.0);
+  k.gp1_gm1 = (mat->gamma + 1.0) / (mat->gamma - 1.0);
   k.prandtl = mat->prandtl; k.mu_ref = mat->mu_ref; k.T0 = mat->T_0; k.Tref = mat->T_ref; k.omega = mat->omega;
   k.ev_alpha = mat->ev_mod_alpha; k.ev_beta = mat->ev_mod_beta; k.tvbM = mat->tvb_minmod_coef; k.cfl = opt->cfl;
   k.model = mat->model; k.flux = mat->flux_scheme; k.mu_model = mat->mu_model; k.recon = mat->reconstruct_scheme;
@@ -1211,6 +1212,7 @@ tg_status tg_update_parameters(tg_handle* h, const tg_material* mat, const tg_bc
   k.sqrt_gm1 = std::sqrt(mat->gamma - 1.0);
   k.inv_gamma = 1.0 / mat->gamma;
   k.inv_gm1 = 1.0 / (mat->gamma - 1.0);
+  k.gp1_gm1 = (mat->gamma + 1.0) / (mat->gamma - 1.0);
   k.prandtl = mat->prandtl; k.mu_ref = mat->mu_ref; k.T0 = mat->T_0; k.Tref = mat->T_ref; k.omega = mat->omega;
   k.ev_alpha = mat->ev_mod_alpha; k.ev_beta = mat->ev_mod_beta; k.tvbM = mat->tvb_minmod_coef;
   k.nd = mat->nd_active; k.visc = mat->visc_active; k.heat = mat->heat_active;

@@ -29,6 +29,7 @@ enum : int { BC_NONE = 0, BC_SLIP = 1, BC_NOSLIP = 2, BC_FARFIELD = 3, BC_INLET 
 struct Params {
   double gamma, R, Cp, prandtl;
   double sqrt_gm1, inv_gamma, inv_gm1;   // sqrt(gamma - 1), 1/gamma, 1/(gamma - 1)
+  double gp1_gm1;                        // (gamma + 1)/(gamma - 1)
   double mu_ref, T0, Tref, omega;
   double ev_alpha, ev_beta, tvbM;
   double cfl;
@@ -290,9 +291,9 @@ __device__ __forceinline__ Flx kepec_flux(const Params& k, const VRec& L, const 
 }
 
 __device__ __forceinline__ Flx kep_flux(const Params& k, const VRec& L, const VRec& R, double unx, double uny) {
-  // src/kep.cc:10-38 (pow(a, 2.0) is the square a*a)
-  double Hl = L.a * L.a / (k.gamma - 1.0) + 0.5 * (L.u * L.u + L.v * L.v);
-  double Hr = R.a * R.a / (k.gamma - 1.0) + 0.5 * (R.u * R.u + R.v * R.v);
+  // src/kep.cc:10-38 (pow(a, 2.0) is the square a*a; a^2 / (gamma - 1) as a^2 times 1/(gamma - 1))
+  double Hl = L.a * L.a * k.inv_gm1 + 0.5 * (L.u * L.u + L.v * L.v);
+  double Hr = R.a * R.a * k.inv_gm1 + 0.5 * (R.u * R.u + R.v * R.v);
   double p = 0.5 * (L.p + R.p);
   double rho = 0.5 * (L.rho + R.rho);
   double H = 0.5 * (Hl + Hr);
@@ -307,22 +308,28 @@ __device__ __forceinline__ Flx kep_flux(const Params& k, const VRec& L, const VR
 }
 
 __device__ __forceinline__ Flx roe_ec_flux(const Params& k, const VRec& L, const VRec& R, double unx, double uny) {
-  // src/roe_ec.cc:10-44
+  // src/roe_ec.cc:10-44.  The reference divides nine times per edge; here the
+  // reciprocal of z1b = (b_l + b_r)/2 serves its log-mean ratio, 1/z1_ln = F_1 / z1b and
+  // the three divisions by z1b, the reciprocal of the z5 sum its ratio, and
+  // (gamma + 1)/(gamma - 1) is a constant: two reciprocals and one division.
   double pl = L.p, pr = R.p;
   double bl = L.b, br = R.b;
   double z1b = 0.5 * (bl + br);
   double zx = L.u * (0.5 * bl) + R.u * (0.5 * br);
   double zy = L.v * (0.5 * bl) + R.v * (0.5 * br);
-  double z5b = 0.5 * (bl * pl + br * pr);
+  double z5l_ = bl * pl, z5r_ = br * pr;
+  double z5b = 0.5 * (z5l_ + z5r_);
   double zn = zx * unx + zy * uny;
-  double z1l = logavg(bl, br);
-  double z5l = logavg(bl * pl, br * pr);
+  const double i1b = 1.0 / z1b, i5s = 1.0 / (z5l_ + z5r_);
+  const double F1 = logavg_F_of((br - bl) * (0.5 * i1b), bl, br);    // z1_ln = z1b / F1
+  const double F5 = logavg_F_of((z5r_ - z5l_) * i5s, z5l_, z5r_);
+  double z5l = z5b / F5;
   Flx F;
   F.m = z5l * zn;
-  double c1 = z5b / z1b, c2 = F.m / z1b;
+  double c1 = z5b * i1b, c2 = F.m * i1b;
   F.x = unx * c1 + zx * c2;
   F.y = uny * c1 + zy * c2;
-  F.e = 0.5 * ((k.gamma + 1.0) / (k.gamma - 1.0) * F.m / z1l + (F.x * zx + F.y * zy)) / z1b;
+  F.e = 0.5 * (k.gp1_gm1 * F.m * (F1 * i1b) + (F.x * zx + F.y * zy)) * i1b;
   return F;
 }
 
