@@ -397,6 +397,14 @@ tg_status tg_batch_create(const tg_batch_level* levels, int n_levels, const tg_m
       return st;
     }
   }
+  // the kernels index a launch's warps in 32 bits
+  for (int kind : {IT_VERTEX, IT_EDGE, IT_BSLOT, IT_UNIT}) {
+    Batch tmp = b->B;
+    if (layout_warps<16>(tmp, kind) >= (1LL << 31) || layout_warps<32>(tmp, kind) >= (1LL << 31)) {
+      tg_batch_destroy(b);
+      return bfail(nullptr, TG_INVALID_ARG, "batch too large: a launch exceeds 2^31 warps");
+    }
+  }
   BParams& k = b->prm;
   k.gamma = (float)mat->gamma; k.R = (float)mat->gas_const;
   k.inv_gm1 = (float)(1.0 / (mat->gamma - 1.0)); k.inv_gamma = (float)(1.0 / mat->gamma);

@@ -428,22 +428,25 @@ __host__ __device__ __forceinline__ int item_count(const LevelMesh& m, int kind)
   return kind == IT_VERTEX ? m.nv : kind == IT_EDGE ? m.ne : kind == IT_BSLOT ? 2 * m.nb : m.nvu;
 }
 
+// The warp index of a launch fits 32 bits (tg_batch_create refuses larger
+// batches), so the split into sample tile and item warp is a 32-bit division.
 template <int ST, int KIND = IT_VERTEX>
-__device__ __forceinline__ Item item_of(const Batch& B, long long w, int lane) {
-  constexpr int VPW = 32 / ST;
+__device__ __forceinline__ Item item_of(const Batch& B, unsigned w, int lane) {
+  constexpr unsigned VPW = 32 / ST;
   Item it{0, 0, 0, false};
-  if (w >= B.work) return it;
+  if ((long long)w >= B.work) return it;
   int l = 0;
 #pragma unroll
   for (int i = 1; i < kMaxLevels; ++i)
-    if (i < B.nlev && w >= B.lev[i].w_begin) l = i;
-  const long long r = w - B.lev[l].w_begin;
-  const int n = item_count(B.lev[l].m, KIND);
-  const int nvw = (n + VPW - 1) / VPW;
+    if (i < B.nlev && (long long)w >= B.lev[i].w_begin) l = i;
+  const unsigned r = w - (unsigned)B.lev[l].w_begin;
+  const unsigned n = (unsigned)item_count(B.lev[l].m, KIND);
+  const unsigned nvw = (n + VPW - 1) / VPW;
+  const unsigned tile = r / nvw;
   it.l = l;
-  it.s = (int)(r / nvw) * ST + (lane % ST);
-  it.v = (int)(r % nvw) * VPW + lane / ST;
-  it.ok = it.v < n;
+  it.s = (int)(tile * ST) + (lane % ST);
+  it.v = (int)((r - tile * nvw) * VPW) + lane / ST;
+  it.ok = it.v < (int)n;
   return it;
 }
 
@@ -558,7 +561,7 @@ __global__ void kb_dt_final(Batch B, BParams k) {
 // (src/fv.cc:926-966).  every != 0: all samples, held ones included (forces).
 template <int ST, bool BND>
 __global__ void kb_grad(Batch B, BParams k, int r, int every) {
-  const long long w = (blockIdx.x * (long long)blockDim.x + threadIdx.x) >> 5;
+  const unsigned w = blockIdx.x * (blockDim.x >> 5) + (threadIdx.x >> 5);
   const Item it = item_of<ST>(B, w, threadIdx.x & 31);
   if (!it.ok) return;
   const Level& L = B.lev[it.l];
@@ -624,7 +627,7 @@ __global__ void kb_grad(Batch B, BParams k, int r, int every) {
 // b right) times |n|, stored for the gather.  Held samples skip.
 template <int FLUX, int RECON, int ST, int BS>
 __global__ void __launch_bounds__(BS) kb_edge_flux(Batch B, BParams k, int r) {
-  const long long w = (blockIdx.x * (long long)blockDim.x + threadIdx.x) >> 5;
+  const unsigned w = blockIdx.x * (blockDim.x >> 5) + (threadIdx.x >> 5);
   const Item it = item_of<ST, IT_EDGE>(B, w, threadIdx.x & 31);
   if (!it.ok) return;
   const Level& L = B.lev[it.l];
@@ -656,7 +659,7 @@ __global__ void __launch_bounds__(BS) kb_edge_flux(Batch B, BParams k, int r) {
 // order (the reference passes zero gradients); otherwise inviscid_bflux.
 template <int FLUX, int ST, int BS>
 __global__ void __launch_bounds__(BS) kb_bflux(Batch B, BParams k, int r) {
-  const long long w = (blockIdx.x * (long long)blockDim.x + threadIdx.x) >> 5;
+  const unsigned w = blockIdx.x * (blockDim.x >> 5) + (threadIdx.x >> 5);
   const Item it = item_of<ST, IT_BSLOT>(B, w, threadIdx.x & 31);
   if (!it.ok) return;
   const Level& L = B.lev[it.l];
@@ -697,7 +700,7 @@ __global__ void __launch_bounds__(BS) kb_bflux(Batch B, BParams k, int r) {
 // the adiabatic heat-flux correction.  One (unit, sample) per thread.
 template <int ST, int BS>
 __global__ void __launch_bounds__(BS) kb_viscous(Batch B, BParams k, int r) {
-  const long long w = (blockIdx.x * (long long)blockDim.x + threadIdx.x) >> 5;
+  const unsigned w = blockIdx.x * (blockDim.x >> 5) + (threadIdx.x >> 5);
   const Item it = item_of<ST, IT_UNIT>(B, w, threadIdx.x & 31);
   if (!it.ok) return;
   const Level& L = B.lev[it.l];
@@ -787,7 +790,7 @@ __global__ void __launch_bounds__(BS) kb_viscous(Batch B, BParams k, int r) {
 // samples copy their state through.
 template <int ST, int BS, bool BND>
 __global__ void __launch_bounds__(BS) kb_gather_update(Batch B, BParams k, int r) {
-  const long long w = (blockIdx.x * (long long)blockDim.x + threadIdx.x) >> 5;
+  const unsigned w = blockIdx.x * (blockDim.x >> 5) + (threadIdx.x >> 5);
   const Item it = item_of<ST>(B, w, threadIdx.x & 31);
   if (!it.ok) return;
   const Level& L = B.lev[it.l];
