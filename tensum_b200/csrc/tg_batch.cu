@@ -119,6 +119,22 @@ long long layout_warps(Batch& B, int kind) {
 
 long long layout(Batch& B, int st, int kind) { return st == 32 ? layout_warps<32>(B, kind) : layout_warps<16>(B, kind); }
 
+// The same for the paired kernels (two samples per lane).
+template <int ST>
+long long layout_warps_pair(Batch& B, int kind) {
+  long long w = 0;
+  for (int l = 0; l < B.nlev; ++l) {
+    B.lev[l].w_begin = w;
+    w += level_warps_pair<ST>(item_count(B.lev[l].m, kind), B.lev[l].S);
+  }
+  B.work = w;
+  return w;
+}
+
+long long layout_pair(Batch& B, int st, int kind) {
+  return st == 32 ? layout_warps_pair<32>(B, kind) : layout_warps_pair<16>(B, kind);
+}
+
 typedef void (*FluxK)(Batch, BParams, int);
 
 template <int F, int R>
@@ -206,8 +222,8 @@ unsigned blocks_of(const Batch& B, int bs) { return (unsigned)((B.work * 32 + bs
 void enqueue_step(tg_batch* b) {
   const Shape sh = kShapes[b->shape];
   Batch B = b->B, BE = b->B, BB = b->B, BU = b->B;
-  layout(B, sh.st, IT_VERTEX);
-  layout(BE, sh.st, IT_EDGE);
+  layout_pair(B, sh.st, IT_VERTEX);
+  layout_pair(BE, sh.st, IT_EDGE);
   layout(BB, sh.st, IT_BSLOT);
   layout(BU, sh.st, IT_UNIT);
   const dim3 gs((max_samples(b) + 255) / 256, b->nlev);
@@ -587,7 +603,7 @@ tg_status tg_batch_forces(tg_batch* b, int level, int n_forces, const int* n_tag
   // the viscous force reads the vertex gradients of the current state (src/force.cc:123)
   const Shape sh = kShapes[0];
   Batch B = b->B;
-  layout(B, sh.st, IT_VERTEX);
+  layout_pair(B, sh.st, IT_VERTEX);
   if (b->prm.model == 1) grad_kernel(sh.st, true)<<<blocks_of(B, sh.bs), sh.bs, 0, b->stream>>>(B, b->prm, 0, 1);
   int* drec = nullptr;
   int* doff = nullptr;

@@ -408,6 +408,184 @@ __device__ __forceinline__ void fviscous_apply(const FViscK& K, float nx, float 
   fe = -(K.a4 * nx + K.b4 * ny) * K.e4;
 }
 
+// ------------------------------------------------------------ paired samples
+// The three per-stage kernels over vertices and edges (gradients, edge fluxes,
+// gather + RK stage) hold two neighbouring samples per thread: one 8-byte load
+// per stored pair, the index and address work shared by the pair, and the FP32
+// arithmetic issued as paired instructions (__fadd2_rn, __fmul2_rn, __ffma2_rn:
+// each component rounds as the scalar _rn operation does).  What has no paired
+// form runs per component: reciprocals and square roots of the flux (the
+// approximate forms, at most 1 ulp and 2^-23 relative, as __fdividef), the
+// logarithms, the FP64 near-equal branch of the log mean and the limiter's
+// selects.  A sample's arithmetic is the same whichever sample it is paired
+// with and whatever the launch shape.
+typedef float2 f2;
+__device__ __forceinline__ f2 sp(float a) { return make_float2(a, a); }
+__device__ __forceinline__ f2 neg2(f2 a) { return make_float2(-a.x, -a.y); }
+__device__ __forceinline__ f2 add2(f2 a, f2 b) { return __fadd2_rn(a, b); }
+__device__ __forceinline__ f2 sub2(f2 a, f2 b) { return __fadd2_rn(a, neg2(b)); }
+__device__ __forceinline__ f2 mul2(f2 a, f2 b) { return __fmul2_rn(a, b); }
+__device__ __forceinline__ f2 fma2(f2 a, f2 b, f2 c) { return __ffma2_rn(a, b, c); }
+__device__ __forceinline__ f2 abs2(f2 a) { return make_float2(fabsf(a.x), fabsf(a.y)); }
+__device__ __forceinline__ float rcp_apx(float x) {
+  float r;
+  asm("rcp.approx.ftz.f32 %0, %1;" : "=f"(r) : "f"(x));
+  return r;
+}
+__device__ __forceinline__ float sqrt_apx(float x) {
+  float r;
+  asm("sqrt.approx.ftz.f32 %0, %1;" : "=f"(r) : "f"(x));
+  return r;
+}
+__device__ __forceinline__ f2 rcp2(f2 a) { return make_float2(rcp_apx(a.x), rcp_apx(a.y)); }
+__device__ __forceinline__ f2 sqrt2(f2 a) { return make_float2(sqrt_apx(a.x), sqrt_apx(a.y)); }
+__device__ __forceinline__ f2 ld2(const float* p) { return __ldg(reinterpret_cast<const float2*>(p)); }
+__device__ __forceinline__ void st2(float* p, f2 v) { *reinterpret_cast<float2*>(p) = v; }
+
+// F of the Ismail-Roe log mean of one component (src/material.h:24-42), the
+// near-equal series in FP64; 1 / (a + b) from the approximate FP32 reciprocal
+// refined by one Newton-Raphson step in FP64 (relative error about 2^-46).
+__device__ __forceinline__ float logF1(float a, float b) {
+  const double da = a, db = b;
+  const double d = db + da;                      // exact in FP64, as is db - da
+  const double y0 = (double)rcp_apx((float)d);
+  const double f = (db - da) * (y0 * ::fma(-d, y0, 2.0));
+  const double u = f * f;
+  if (u < 1.0e-2) {
+    const double u2 = u * u;
+    return (float)::fma(u2 * u, 1.0 / 7.0, ::fma(u2, 1.0 / 5.0, ::fma(u, 1.0 / 3.0, 1.0)));
+  }
+  return logf(b / a) / (2.0f * (float)f);
+}
+
+// minmod (src/limiter.h:14-27) of one component
+__device__ __forceinline__ float minmod1(float a, float b) {
+  const float m = fminf(fabsf(a), fabsf(b));
+  return ((a > 0.0f && b > 0.0f) || (a < 0.0f && b < 0.0f)) ? copysignf(m, a) : 0.0f;
+}
+
+struct PRec { f2 rho, u, v, p, beta, V1; };
+struct PFlx { f2 m, x, y, e; };
+struct PAvg { f2 rho, ibeta, p, vx, vy, vn; };
+
+// Flux record from a stored pair (u, v, p, V1, V5 with V5 = -2 beta, rho = 2 beta p).
+__device__ __forceinline__ PRec prec(f2 u, f2 v, f2 p, f2 V1, f2 V5) {
+  PRec r;
+  const f2 nV5 = neg2(V5);
+  r.u = u; r.v = v; r.p = p; r.V1 = V1;
+  r.beta = mul2(sp(0.5f), nV5);
+  r.rho = mul2(nV5, p);
+  return r;
+}
+
+// KEPEC central flux (src/kepec.cc:10-38) on a unit normal, with its averages.
+__device__ __forceinline__ PFlx kepec2(const BParams& k, const PRec& L, const PRec& R, float unx, float uny, PAvg& A) {
+  const f2 sr = add2(L.rho, R.rho), sb = add2(L.beta, R.beta);
+  const f2 Fr = make_float2(logF1(L.rho.x, R.rho.x), logF1(L.rho.y, R.rho.y));
+  const f2 Fb = make_float2(logF1(L.beta.x, R.beta.x), logF1(L.beta.y, R.beta.y));
+  const f2 hs = mul2(sp(0.5f), sr);
+  const f2 isb = rcp2(sb);
+  A.rho = mul2(hs, rcp2(Fr));          // (rho_l + rho_r) / 2 / F_rho
+  A.p = mul2(hs, isb);                 // (rho_l + rho_r) / (2 (beta_l + beta_r))
+  A.ibeta = mul2(add2(Fb, Fb), isb);   // F_beta / ((beta_l + beta_r) / 2)
+  A.vx = mul2(sp(0.5f), add2(L.u, R.u));
+  A.vy = mul2(sp(0.5f), add2(L.v, R.v));
+  A.vn = fma2(A.vy, sp(uny), mul2(A.vx, sp(unx)));
+  const f2 vel2 = mul2(sp(0.5f), add2(fma2(L.v, L.v, mul2(L.u, L.u)), fma2(R.v, R.v, mul2(R.u, R.u))));
+  PFlx F;
+  F.m = mul2(A.rho, A.vn);
+  F.x = fma2(A.vx, F.m, mul2(sp(unx), A.p));
+  F.y = fma2(A.vy, F.m, mul2(sp(uny), A.p));
+  const f2 h = mul2(sp(0.5f), fma2(A.ibeta, sp(k.inv_gm1), neg2(vel2)));
+  F.e = fma2(h, F.m, fma2(F.y, A.vy, mul2(F.x, A.vx)));
+  return F;
+}
+
+// KEPES-TeCNO (src/kepes_tecno_roe.cc:11-173, src/kepes_tecno_rusanov.cc:11-164)
+// in the unscaled form of ftecno: S^2 (Lambda jump(R0^T V)), first order or minmod.
+template <int ROE, int RECON>
+__device__ __forceinline__ PFlx tecno2(const BParams& k, const PRec& L, const PRec& R, float unx, float uny, float dx,
+                                       float dy, const f2* gL, const f2* gR) {
+  static_assert(RECON == RECON_FIRST || RECON == RECON_TVD_MINMOD, "ensembles run first order or minmod");
+  PAvg A;
+  PFlx F = kepec2(k, L, R, unx, uny, A);
+  const f2 U = sp(unx), W = sp(uny);
+  const f2 aa = mul2(sp(0.5f * k.gamma), A.ibeta);   // a^2
+  const f2 a = sqrt2(aa);
+  const f2 hv = mul2(sp(0.5f), fma2(A.vy, A.vy, mul2(A.vx, A.vx)));
+  const f2 H = fma2(aa, sp(k.inv_gm1), hv);
+  const f2 v1 = fma2(A.vx, W, mul2(A.vy, sp(-unx)));
+  auto RT = [&](const f2* x, f2* z) {
+    const f2 Aq = fma2(A.vy, x[2], fma2(A.vx, x[1], x[0]));
+    const f2 Bq = fma2(A.vn, x[3], fma2(W, x[2], mul2(U, x[1])));
+    const f2 Cq = fma2(H, x[3], Aq);
+    z[0] = fma2(neg2(a), Bq, Cq);
+    z[1] = fma2(hv, x[3], Aq);
+    z[2] = fma2(v1, x[3], fma2(W, x[1], mul2(sp(-unx), x[2])));
+    z[3] = fma2(a, Bq, Cq);
+  };
+  f2 Lam[4];
+  if (ROE) {
+    const f2 gr = sp(k.gamma);
+    const f2 al = sqrt2(mul2(mul2(gr, L.p), rcp2(L.rho))), ar = sqrt2(mul2(mul2(gr, R.p), rcp2(R.rho)));
+    const f2 vnl = fma2(L.v, W, mul2(L.u, U)), vnr = fma2(R.v, W, mul2(R.u, U));
+    const f2 b1 = sp(1.0f + k.ev_beta), al1 = sp(k.ev_alpha);
+    Lam[0] = fma2(b1, abs2(sub2(A.vn, a)), mul2(al1, abs2(sub2(sub2(vnl, al), sub2(vnr, ar)))));
+    Lam[1] = Lam[2] = abs2(A.vn);
+    Lam[3] = fma2(b1, abs2(add2(A.vn, a)), mul2(al1, abs2(sub2(add2(vnl, al), add2(vnr, ar)))));
+  } else {
+    Lam[0] = Lam[1] = Lam[2] = Lam[3] = add2(abs2(A.vn), a);
+  }
+  // V = (V1, 2 beta u, 2 beta v, -2 beta)
+  f2 dV[4];
+  dV[0] = sub2(R.V1, L.V1);
+  dV[1] = mul2(sp(2.0f), fma2(R.u, R.beta, neg2(mul2(L.u, L.beta))));
+  dV[2] = mul2(sp(2.0f), fma2(R.v, R.beta, neg2(mul2(L.v, L.beta))));
+  dV[3] = mul2(sp(-2.0f), sub2(R.beta, L.beta));
+  f2 q[4];
+  RT(dV, q);
+  if (RECON != RECON_FIRST) {
+    f2 gl[4], gr[4], sl[4], sr[4];
+#pragma unroll
+    for (int i = 0; i < 4; ++i) {
+      gl[i] = fma2(gL[2 * i + 1], sp(dy), mul2(gL[2 * i], sp(dx)));
+      gr[i] = fma2(gR[2 * i + 1], sp(dy), mul2(gR[2 * i], sp(dx)));
+    }
+    RT(gl, sl);
+    RT(gr, sr);
+#pragma unroll
+    for (int i = 0; i < 4; ++i) {   // Z_ji - Z_ij = d - minmod(2 s_r - d, d) / 2 - minmod(2 s_l - d, d) / 2
+      const f2 d = q[i], nd = neg2(d);
+      const f2 xr = fma2(sp(2.0f), sr[i], nd), xl = fma2(sp(2.0f), sl[i], nd);
+      const f2 mr = make_float2(minmod1(xr.x, d.x), minmod1(xr.y, d.y));
+      const f2 ml = make_float2(minmod1(xl.x, d.x), minmod1(xl.y, d.y));
+      q[i] = fma2(sp(-0.5f), ml, fma2(sp(-0.5f), mr, d));
+    }
+  }
+  const f2 s01 = mul2(A.rho, sp(k.inv_gamma));
+  const f2 hs01 = mul2(sp(0.5f), s01);
+  q[0] = mul2(mul2(Lam[0], q[0]), hs01);
+  q[1] = mul2(mul2(Lam[1], q[1]), mul2(sp(k.gamma - 1.0f), s01));
+  q[2] = mul2(mul2(Lam[2], q[2]), A.p);
+  q[3] = mul2(mul2(Lam[3], q[3]), hs01);
+  const f2 sum = add2(add2(q[0], q[1]), q[3]), dif = sub2(q[3], q[0]);
+  const f2 adif = mul2(a, dif), mh = sp(-0.5f);
+  F.m = fma2(mh, sum, F.m);
+  F.x = fma2(mh, fma2(W, q[2], fma2(adif, U, mul2(A.vx, sum))), F.x);
+  F.y = fma2(mh, fma2(sp(-unx), q[2], fma2(adif, W, mul2(A.vy, sum))), F.y);
+  F.e = fma2(mh, fma2(v1, q[2], fma2(hv, q[1], fma2(adif, A.vn, mul2(H, add2(q[0], q[3]))))), F.e);
+  return F;
+}
+
+template <int FLUX, int RECON>
+__device__ __forceinline__ PFlx pflux(const BParams& k, const PRec& L, const PRec& R, float unx, float uny, float dx,
+                                      float dy, const f2* gL, const f2* gR) {
+  if (FLUX == FLUX_TECNO_ROE) return tecno2<1, RECON>(k, L, R, unx, uny, dx, dy, gL, gR);
+  if (FLUX == FLUX_TECNO_RUSANOV) return tecno2<0, RECON>(k, L, R, unx, uny, dx, dy, gL, gR);
+  PAvg A;
+  return kepec2(k, L, R, unx, uny, A);
+}
+
 // ------------------------------------------------------------------ indexing
 // A warp covers 32/ST vertices x ST samples (the sample tile ST is 32 or 16);
 // warps are ordered sample-group-major, so consecutive warps walk neighbouring
@@ -446,6 +624,35 @@ __device__ __forceinline__ Item item_of(const Batch& B, unsigned w, int lane) {
   it.l = l;
   it.s = (int)(tile * ST) + (lane % ST);
   it.v = (int)((r - tile * nvw) * VPW) + lane / ST;
+  it.ok = it.v < (int)n;
+  return it;
+}
+
+// Paired kernels (gradients, edge fluxes, gather + update): ST/2 lanes per
+// item, each lane holding two neighbouring samples, so a warp covers 64/ST
+// items x ST samples.
+template <int ST>
+__host__ __device__ __forceinline__ long long level_warps_pair(int nv, int S) {
+  constexpr int IPW = 64 / ST;
+  return (long long)((nv + IPW - 1) / IPW) * (S / ST);
+}
+
+template <int ST, int KIND = IT_VERTEX>
+__device__ __forceinline__ Item item_of_pair(const Batch& B, unsigned w, int lane) {
+  constexpr unsigned LPI = ST / 2, IPW = 64 / ST;
+  Item it{0, 0, 0, false};
+  if ((long long)w >= B.work) return it;
+  int l = 0;
+#pragma unroll
+  for (int i = 1; i < kMaxLevels; ++i)
+    if (i < B.nlev && (long long)w >= B.lev[i].w_begin) l = i;
+  const unsigned r = w - (unsigned)B.lev[l].w_begin;
+  const unsigned n = (unsigned)item_count(B.lev[l].m, KIND);
+  const unsigned nvw = (n + IPW - 1) / IPW;
+  const unsigned tile = r / nvw;
+  it.l = l;
+  it.s = (int)(tile * ST) + 2 * (int)(lane % LPI);
+  it.v = (int)((r - tile * nvw) * IPW) + (int)(lane / LPI);
   it.ok = it.v < (int)n;
   return it;
 }
@@ -556,40 +763,45 @@ __global__ void kb_dt_final(Batch B, BParams k) {
 }
 
 // Gradients of the entropy variables (src/fv.cc:699-1059 in the edge form
-// grad_v = sum_e g_{v,e} (W_o - W_v) / (6 mcarea)), one (vertex, sample) per
-// thread.  BND adds the boundary-face corrections n_b (W_b0 + W_b1 - W_0 - W_1) / 2
-// (src/fv.cc:926-966).  every != 0: all samples, held ones included (forces).
+// grad_v = sum_e g_{v,e} (W_o - W_v) / (6 mcarea)), one vertex and a pair of
+// samples per thread.  BND adds the boundary-face corrections
+// n_b (W_b0 + W_b1 - W_0 - W_1) / 2 (src/fv.cc:926-966).  every != 0: all
+// samples, held ones included (forces); otherwise a pair whose two samples
+// are both held skips.
 template <int ST, bool BND>
 __global__ void kb_grad(Batch B, BParams k, int r, int every) {
   const unsigned w = blockIdx.x * (blockDim.x >> 5) + (threadIdx.x >> 5);
-  const Item it = item_of<ST>(B, w, threadIdx.x & 31);
+  const Item it = item_of_pair<ST>(B, w, threadIdx.x & 31);
   if (!it.ok) return;
   const Level& L = B.lev[it.l];
-  if (!every && !L.c.active[it.s]) return;
   const int v = it.v, s = it.s;
+  if (!every) {
+    const int2 act = *reinterpret_cast<const int2*>(L.c.active + s);
+    if (!act.x && !act.y) return;
+  }
   const int S = L.P;   // row pitch
   const float* Q = L.Q[r] + s;
-  auto W = [&](int x, float* o) {
+  auto W = [&](int x, f2* o) {   // V2 = 2 beta u = -V5 u
     const float* q = Q + rows(x, kQ, S);
-    const float u = q[0], vv = q[S], V5 = q[4 * S];
-    o[0] = q[3 * S]; o[1] = -V5 * u; o[2] = -V5 * vv; o[3] = V5;   // V2 = 2 beta u = -V5 u
+    const f2 V5 = ld2(q + 4 * S), nV5 = neg2(V5);
+    o[0] = ld2(q + 3 * S); o[1] = mul2(nV5, ld2(q)); o[2] = mul2(nV5, ld2(q + S)); o[3] = V5;
   };
-  float ws[4];
+  f2 ws[4];
   W(v, ws);
-  float acc[kG];
+  f2 acc[kG];
 #pragma unroll
-  for (int c = 0; c < kG; ++c) acc[c] = 0.0f;
+  for (int c = 0; c < kG; ++c) acc[c] = sp(0.0f);
   for (int j = L.m.ce_off[v]; j < L.m.ce_off[v + 1]; ++j) {
     const int ent = L.m.ce_ent[j], e = ent >> 1, side = ent & 1;
     const int o = side ? L.m.e_a[e] : L.m.e_b[e];
-    const float gx = side ? L.m.g1x[e] : L.m.g0x[e], gy = side ? L.m.g1y[e] : L.m.g0y[e];
-    float wo[4];
+    const f2 gx = sp(side ? L.m.g1x[e] : L.m.g0x[e]), gy = sp(side ? L.m.g1y[e] : L.m.g0y[e]);
+    f2 wo[4];
     W(o, wo);
 #pragma unroll
     for (int c = 0; c < 4; ++c) {
-      const float d = wo[c] - ws[c];
-      acc[2 * c] += gx * d;
-      acc[2 * c + 1] += gy * d;
+      const f2 d = sub2(wo[c], ws[c]);
+      acc[2 * c] = fma2(gx, d, acc[2 * c]);
+      acc[2 * c + 1] = fma2(gy, d, acc[2 * c + 1]);
     }
   }
   if (BND) {
@@ -602,56 +814,67 @@ __global__ void kb_grad(Batch B, BParams k, int r, int every) {
       const float* val = L.bval + rows(d, 10, S) + s;
       const float* q0 = Q + rows(L.m.b_v0[d], kQ, S);
       const float* q1 = Q + rows(L.m.b_v1[d], kQ, S);
-      const FEnt e0 = fbc_ent(k, kind, ad, val, S, nx, ny, q0);
-      const FEnt e1 = fbc_ent(k, kind, ad, val + 5 * S, S, nx, ny, q1);
-      float w0[4], w1[4];
+      FEnt e0[2], e1[2];
+#pragma unroll
+      for (int h = 0; h < 2; ++h) {
+        e0[h] = fbc_ent(k, kind, ad, val + h, S, nx, ny, q0 + h);
+        e1[h] = fbc_ent(k, kind, ad, val + 5 * S + h, S, nx, ny, q1 + h);
+      }
+      const f2 eb[4] = {add2(make_float2(e0[0].f, e0[1].f), make_float2(e1[0].f, e1[1].f)),
+                        add2(make_float2(e0[0].vx, e0[1].vx), make_float2(e1[0].vx, e1[1].vx)),
+                        add2(make_float2(e0[0].vy, e0[1].vy), make_float2(e1[0].vy, e1[1].vy)),
+                        add2(make_float2(e0[0].l, e0[1].l), make_float2(e1[0].l, e1[1].l))};
+      f2 w0[4], w1[4];
       W(L.m.b_v0[d], w0);
       W(L.m.b_v1[d], w1);
-      const float dW[4] = {(e0.f + e1.f - w0[0] - w1[0]) * 0.5f, (e0.vx + e1.vx - w0[1] - w1[1]) * 0.5f,
-                           (e0.vy + e1.vy - w0[2] - w1[2]) * 0.5f, (e0.l + e1.l - w0[3] - w1[3]) * 0.5f};
 #pragma unroll
       for (int c = 0; c < 4; ++c) {
-        acc[2 * c] += nx * dW[c];
-        acc[2 * c + 1] += ny * dW[c];
+        const f2 dW = mul2(sub2(sub2(eb[c], w0[c]), w1[c]), sp(0.5f));
+        acc[2 * c] = fma2(sp(nx), dW, acc[2 * c]);
+        acc[2 * c + 1] = fma2(sp(ny), dW, acc[2 * c + 1]);
       }
     }
   }
-  const float f = L.m.inv6mc[v];
+  const f2 f = sp(L.m.inv6mc[v]);
   float* G = L.G + rows(v, kG, S) + s;
 #pragma unroll
-  for (int c = 0; c < kG; ++c) G[c * S] = acc[c] * f;
+  for (int c = 0; c < kG; ++c) st2(G + c * S, mul2(acc[c], f));
 }
 
 // Edge fluxes of one stage (src/fv.cc:1066-1192, src/material.cc:27-74): one
-// (edge, sample) per thread, the flux of the edge's own orientation (a left,
-// b right) times |n|, stored for the gather.  Held samples skip.
+// edge and a pair of samples per thread, the flux of the edge's own
+// orientation (a left, b right) times |n|, stored for the gather.  A pair
+// whose two samples are both held skips.
 template <int FLUX, int RECON, int ST, int BS>
 __global__ void __launch_bounds__(BS) kb_edge_flux(Batch B, BParams k, int r) {
   const unsigned w = blockIdx.x * (blockDim.x >> 5) + (threadIdx.x >> 5);
-  const Item it = item_of<ST, IT_EDGE>(B, w, threadIdx.x & 31);
+  const Item it = item_of_pair<ST, IT_EDGE>(B, w, threadIdx.x & 31);
   if (!it.ok) return;
   const Level& L = B.lev[it.l];
   const int e = it.v, s = it.s;
-  if (!L.c.active[s]) return;
-  constexpr bool kA = (FLUX == FLUX_TECNO_ROE);
+  const int2 act = *reinterpret_cast<const int2*>(L.c.active + s);
+  if (!act.x && !act.y) return;
   constexpr bool kGr = (RECON != RECON_FIRST) && (FLUX == FLUX_TECNO_ROE || FLUX == FLUX_TECNO_RUSANOV);
   const int S = L.P;   // row pitch
   const int ia = L.m.e_a[e], ib = L.m.e_b[e];
   const float* qa = L.Q[r] + rows(ia, kQ, S) + s;
   const float* qb = L.Q[r] + rows(ib, kQ, S) + s;
-  const FRec A = frec(k, qa[0], qa[S], qa[2 * S], qa[3 * S], qa[4 * S], kA);
-  const FRec Bv = frec(k, qb[0], qb[S], qb[2 * S], qb[3 * S], qb[4 * S], kA);
-  float ga[kG], gb[kG];
+  const PRec A = prec(ld2(qa), ld2(qa + S), ld2(qa + 2 * S), ld2(qa + 3 * S), ld2(qa + 4 * S));
+  const PRec Bv = prec(ld2(qb), ld2(qb + S), ld2(qb + 2 * S), ld2(qb + 3 * S), ld2(qb + 4 * S));
+  f2 ga[kG], gb[kG];
   if (kGr) {
     const float* Ga = L.G + rows(ia, kG, S) + s;
     const float* Gb = L.G + rows(ib, kG, S) + s;
 #pragma unroll
-    for (int c = 0; c < kG; ++c) { ga[c] = Ga[c * S]; gb[c] = Gb[c * S]; }
+    for (int c = 0; c < kG; ++c) { ga[c] = ld2(Ga + c * S); gb[c] = ld2(Gb + c * S); }
+  } else {
+#pragma unroll
+    for (int c = 0; c < kG; ++c) ga[c] = gb[c] = sp(0.0f);
   }
-  const FFlx F = fflux<FLUX, RECON>(k, A, Bv, L.m.ux[e], L.m.uy[e], L.m.dx[e], L.m.dy[e], ga, gb);
-  const float ar = L.m.ar[e];
+  const PFlx F = pflux<FLUX, RECON>(k, A, Bv, L.m.ux[e], L.m.uy[e], L.m.dx[e], L.m.dy[e], ga, gb);
+  const f2 ar = sp(L.m.ar[e]);
   float* Fo = L.F + rows(e, 4, S) + s;
-  Fo[0] = F.m * ar; Fo[S] = F.x * ar; Fo[2 * S] = F.y * ar; Fo[3 * S] = F.e * ar;
+  st2(Fo, mul2(F.m, ar)); st2(Fo + S, mul2(F.x, ar)); st2(Fo + 2 * S, mul2(F.y, ar)); st2(Fo + 3 * S, mul2(F.e, ar));
 }
 
 // Boundary-face fluxes (src/fv.cc:1100-1188): one (face vertex, sample) per
@@ -786,12 +1009,13 @@ __global__ void __launch_bounds__(BS) kb_viscous(Batch B, BParams k, int r) {
 }
 
 // Residual gather in the fixed per-vertex edge order and the SSP-RK3 stage
-// update (src/fv.cc:1635-1658), state r -> state (r+1) % 3.  Held or finished
-// samples copy their state through.
+// update (src/fv.cc:1635-1658), state r -> state (r+1) % 3, one vertex and a
+// pair of samples per thread.  Held or finished samples copy their state
+// through.
 template <int ST, int BS, bool BND>
 __global__ void __launch_bounds__(BS) kb_gather_update(Batch B, BParams k, int r) {
   const unsigned w = blockIdx.x * (blockDim.x >> 5) + (threadIdx.x >> 5);
-  const Item it = item_of<ST>(B, w, threadIdx.x & 31);
+  const Item it = item_of_pair<ST>(B, w, threadIdx.x & 31);
   if (!it.ok) return;
   const Level& L = B.lev[it.l];
   const int v = it.v, s = it.s;
@@ -799,19 +1023,21 @@ __global__ void __launch_bounds__(BS) kb_gather_update(Batch B, BParams k, int r
   const size_t ov = rows(v, kQ, S) + s;
   const float* Q = L.Q[r] + ov;
   float* Qn = L.Q[(r + 1) % 3] + ov;
-  if (!L.c.active[s]) {
+  const int2 act = *reinterpret_cast<const int2*>(L.c.active + s);
+  if (!act.x && !act.y) {
 #pragma unroll
-    for (int c = 0; c < kQ; ++c) Qn[c * S] = Q[c * S];
+    for (int c = 0; c < kQ; ++c) st2(Qn + c * S, ld2(Q + c * S));
     return;
   }
-  float r0 = 0.0f, r1 = 0.0f, r2 = 0.0f, r3 = 0.0f;
+  f2 r0 = sp(0.0f), r1 = sp(0.0f), r2 = sp(0.0f), r3 = sp(0.0f);
   const int j0 = L.m.ce_off[v], j1 = L.m.ce_off[v + 1];
 #pragma unroll 4
   for (int j = j0; j < j1; ++j) {
     const int ent = L.m.ce_ent[j];
     const float* Fe = L.F + rows(ent >> 1, 4, S) + s;
-    const float sg = (ent & 1) ? -1.0f : 1.0f;
-    r0 += Fe[0] * sg; r1 += Fe[S] * sg; r2 += Fe[2 * S] * sg; r3 += Fe[3 * S] * sg;
+    const f2 sg = sp((ent & 1) ? -1.0f : 1.0f);
+    r0 = fma2(ld2(Fe), sg, r0); r1 = fma2(ld2(Fe + S), sg, r1);
+    r2 = fma2(ld2(Fe + 2 * S), sg, r2); r3 = fma2(ld2(Fe + 3 * S), sg, r3);
   }
   if (BND) {   // boundary and viscous contributions in list order (src/fv.cc:1100-1188, 1197-1320)
     for (int j = L.m.cb_off[v]; j < L.m.cb_off[v + 1]; ++j) {
@@ -819,40 +1045,49 @@ __global__ void __launch_bounds__(BS) kb_gather_update(Batch B, BParams k, int r
       const int type = ent & 3, idx = ent >> 2;
       if (type == 0) {
         const float* Fe = L.Fb + rows(idx, 4, S) + s;
-        r0 += Fe[0] * 0.5f; r1 += Fe[S] * 0.5f; r2 += Fe[2 * S] * 0.5f; r3 += Fe[3 * S] * 0.5f;
-      } else if (type == 2 && k.model == 1) {
-        const float* Fe = L.Fv + rows(idx, 3, S) + s;
-        r1 += Fe[0] * -0.5f; r2 += Fe[S] * -0.5f; r3 += Fe[2 * S] * -0.5f;
-      } else if (type == 3 && k.model == 1) {
-        const float* Fe = L.Fvb + rows(idx, 3, S) + s;
-        r1 += Fe[0] * 0.5f; r2 += Fe[S] * 0.5f; r3 += Fe[2 * S] * 0.5f;
+        const f2 h = sp(0.5f);
+        r0 = fma2(ld2(Fe), h, r0); r1 = fma2(ld2(Fe + S), h, r1);
+        r2 = fma2(ld2(Fe + 2 * S), h, r2); r3 = fma2(ld2(Fe + 3 * S), h, r3);
+      } else if ((type == 2 || type == 3) && k.model == 1) {
+        const float* Fe = (type == 2 ? L.Fv : L.Fvb) + rows(idx, 3, S) + s;
+        const f2 h = sp(type == 2 ? -0.5f : 0.5f);
+        r1 = fma2(ld2(Fe), h, r1); r2 = fma2(ld2(Fe + S), h, r2); r3 = fma2(ld2(Fe + 2 * S), h, r3);
       }
     }
   }
-  const float u0 = Q[0], v0 = Q[S], p0 = Q[2 * S], V50 = Q[4 * S];
-  const float rho0 = -V50 * p0;
+  const f2 u0 = ld2(Q), v0 = ld2(Q + S), p0 = ld2(Q + 2 * S), V50 = ld2(Q + 4 * S);
+  const f2 rho0 = mul2(neg2(V50), p0);
   // Shu-Osher SSP-RK3 stage (src/constants.h:4-6)
-  const float a_rk = r == 0 ? 0.0f : (r == 1 ? 0.75f : 1.0f / 3.0f);
-  const float b_rk = r == 0 ? 1.0f : (r == 1 ? 0.25f : 2.0f / 3.0f);
-  const float factor = (float)L.c.dt[s] / L.m.area[v];
-  const float c2 = -factor * b_rk;
+  const f2 a_rk = sp(r == 0 ? 0.0f : (r == 1 ? 0.75f : 1.0f / 3.0f));
+  const f2 b_rk = sp(r == 0 ? 1.0f : (r == 1 ? 0.25f : 2.0f / 3.0f));
+  const float area = L.m.area[v];
+  const f2 c2 = mul2(make_float2((float)L.c.dt[s] / area, (float)L.c.dt[s + 1] / area), neg2(b_rk));
   const float* Uo = L.Uold + rows(v, 4, S) + s;
-  const float cr = rho0 * b_rk + Uo[0] * a_rk + r0 * c2;
-  const float cx = rho0 * u0 * b_rk + Uo[S] * a_rk + r1 * c2;
-  const float cy = rho0 * v0 * b_rk + Uo[2 * S] * a_rk + r2 * c2;
-  const float cE = (p0 * k.inv_gm1 + 0.5f * (u0 * u0 + v0 * v0) * rho0) * b_rk + Uo[3 * S] * a_rk + r3 * c2;
-  const float ir = 1.0f / cr;
-  const float u = cx * ir, vv = cy * ir;
-  const float p = (k.gamma - 1.0f) * (cE - 0.5f * (cx * u + cy * vv));
-  const float beta = 0.5f * cr / p;
-  const float sent = logf(p) - k.gamma * logf(cr);
-  const float V1 = (k.gamma - sent) * k.inv_gm1 - (u * u + vv * vv) * beta;
-  Qn[0] = u;
-  Qn[S] = vv;
-  Qn[2 * S] = p;
-  Qn[3 * S] = V1;
-  Qn[4 * S] = -2.0f * beta;
-  if (!(p > 0.0f) || !(cr > 0.0f) || !isfinite(u) || !isfinite(vv) || !isfinite(p)) L.c.bad[s] = 1;
+  const f2 cr = fma2(r0, c2, fma2(ld2(Uo), a_rk, mul2(rho0, b_rk)));
+  const f2 cx = fma2(r1, c2, fma2(ld2(Uo + S), a_rk, mul2(mul2(rho0, u0), b_rk)));
+  const f2 cy = fma2(r2, c2, fma2(ld2(Uo + 2 * S), a_rk, mul2(mul2(rho0, v0), b_rk)));
+  const f2 E0 = fma2(p0, sp(k.inv_gm1), mul2(mul2(sp(0.5f), fma2(v0, v0, mul2(u0, u0))), rho0));
+  const f2 cE = fma2(r3, c2, fma2(ld2(Uo + 3 * S), a_rk, mul2(E0, b_rk)));
+  const f2 ir = make_float2(1.0f / cr.x, 1.0f / cr.y);
+  const f2 u = mul2(cx, ir), vv = mul2(cy, ir);
+  const f2 p = mul2(sp(k.gamma - 1.0f), fma2(sp(-0.5f), fma2(cy, vv, mul2(cx, u)), cE));
+  const f2 hc = mul2(sp(0.5f), cr);
+  const f2 beta = make_float2(hc.x / p.x, hc.y / p.y);
+  const f2 sent = make_float2(__fmaf_rn(-k.gamma, logf(cr.x), logf(p.x)), __fmaf_rn(-k.gamma, logf(cr.y), logf(p.y)));
+  const f2 V1 = fma2(sub2(sp(k.gamma), sent), sp(k.inv_gm1), neg2(mul2(fma2(vv, vv, mul2(u, u)), beta)));
+  f2 o[kQ] = {u, vv, p, V1, mul2(sp(-2.0f), beta)};
+  if (!act.x || !act.y) {   // the held sample of the pair keeps its state
+#pragma unroll
+    for (int c = 0; c < kQ; ++c) {
+      const f2 old = ld2(Q + c * S);
+      if (!act.x) o[c].x = old.x;
+      if (!act.y) o[c].y = old.y;
+    }
+  }
+#pragma unroll
+  for (int c = 0; c < kQ; ++c) st2(Qn + c * S, o[c]);
+  if (act.x && (!(p.x > 0.0f) || !(cr.x > 0.0f) || !isfinite(u.x) || !isfinite(vv.x) || !isfinite(p.x))) L.c.bad[s] = 1;
+  if (act.y && (!(p.y > 0.0f) || !(cr.y > 0.0f) || !isfinite(u.y) || !isfinite(vv.y) || !isfinite(p.y))) L.c.bad[s + 1] = 1;
 }
 
 // Per-sample step end (src/fv.cc:2307-2336).
