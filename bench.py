@@ -33,7 +33,9 @@ U[-2, 2] degrees): S batched FP32 solves to time T with the wall force at K
 output times, FP64 solves of a subset (several handles at once), a surrogate
 trained on the first --train solves, and the time to a 1 % relative standard
 error of the mean and of the variance of each QoI for plain FP64 MC, batched
-FP32 MC and batched FP32 with the control variate.
+FP32 MC and batched FP32 with the control variate.  With --throughput-only
+either Monte Carlo workload times the ensemble's graph-replayed steps alone
+(a short command for a profiler).
 
     python bench.py --workload partitioned [--parts 1,2,4] [--steps K]
 
@@ -96,7 +98,7 @@ def parse():
     ap.add_argument("--train", type=int, default=256, help="cylinder: solver runs the surrogate is trained on")
     ap.add_argument("--no-mc", action="store_true", help="skip the Monte Carlo object of the default line")
     ap.add_argument("--parts", default="1,2,4", help="partitioned: partition counts")
-    ap.add_argument("--throughput-only", action="store_true", help="mc: the ensemble's stepping alone")
+    ap.add_argument("--throughput-only", action="store_true", help="mc, cylinder: the ensemble's stepping alone")
     ap.add_argument("--mc-cap", type=float, default=120.0,
                     help="mc: wall-clock cap of the plain FP64 arm of the measured time to 1%% RSE")
     a = ap.parse_args()
@@ -586,8 +588,9 @@ def run_mc(args):
     return 0
 
 
-def cylinder_line(S, T, n_out, t_start, n_fp64, n_train, K, seed, n_r=128, n_t=256):
-    """Surrogate control-variate MC on the Navier-Stokes cylinder (one GPU): the JSON object."""
+def cylinder_line(S, T, n_out, t_start, n_fp64, n_train, K, seed, n_r=128, n_t=256, throughput_only=False):
+    """Surrogate control-variate MC on the Navier-Stokes cylinder (one GPU): the JSON object
+    (throughput_only: the ensemble's graph-replayed steps alone, e.g. for a profiler)."""
     import torch
     from tensum_b200 import cases, cv, cylinder, mlp, preproc
     torch.cuda.set_device(0)
@@ -595,6 +598,15 @@ def cylinder_line(S, T, n_out, t_start, n_fp64, n_train, K, seed, n_r=128, n_t=2
     V = m.n_vertex
     g = preproc.preprocess(m)
     X = cylinder.draw_inputs(S, seed)
+    if throughput_only:
+        with ClockSampler(0) as clk:
+            rb = cylinder.run_batched(g, m.coords, X, 0.01, 1, 0.0, time_steps=K)
+        return {"metric": "vertex-sample-stage updates/s (FP32 ensemble)", "value": V * S * 3 / (rb["ms_per_step"] / 1e3),
+                "unit": "vertex-sample-stage updates/s", "ms_per_step": rb["ms_per_step"], "steps": K,
+                "gpu_launches": rb["kernels_per_step"] * K,
+                "config": {"workload": f"navier-stokes cylinder {n_r}x{n_t} O-mesh ensemble of {S} samples, "
+                                       "kepes_tecno_roe(minmod), ssprk3, fp32 members", "shape": rb["shape"]},
+                "clocks": clk.summary()}
     with ClockSampler(0) as clk:
         rb = cylinder.run_batched(g, m.coords, X, T, n_out, t_start, time_steps=K)
     y = rb["y"]
@@ -673,7 +685,8 @@ def cylinder_line(S, T, n_out, t_start, n_fp64, n_train, K, seed, n_r=128, n_t=2
 
 def run_cylinder(args):
     print(json.dumps(cylinder_line(args.samples or 1024, args.final_time, args.outputs, args.t_start, args.fp64_samples,
-                                   args.train, max(5, min(args.steps, 50)), args.seed)))
+                                   args.train, max(5, min(args.steps, 50)), args.seed,
+                                   throughput_only=args.throughput_only)))
     return 0
 
 

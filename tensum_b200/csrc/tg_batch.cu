@@ -119,20 +119,23 @@ long long layout_warps(Batch& B, int kind) {
 
 long long layout(Batch& B, int st, int kind) { return st == 32 ? layout_warps<32>(B, kind) : layout_warps<16>(B, kind); }
 
-// The same for the paired kernels (two samples per lane).
-template <int ST>
+// The same for the paired kernels (H pairs of samples per lane).
+template <int ST, int H>
 long long layout_warps_pair(Batch& B, int kind) {
   long long w = 0;
   for (int l = 0; l < B.nlev; ++l) {
     B.lev[l].w_begin = w;
-    w += level_warps_pair<ST>(item_count(B.lev[l].m, kind), B.lev[l].S);
+    w += level_warps_pair<ST, H>(item_count(B.lev[l].m, kind), B.lev[l].S);
   }
   B.work = w;
   return w;
 }
 
-long long layout_pair(Batch& B, int st, int kind) {
-  return st == 32 ? layout_warps_pair<32>(B, kind) : layout_warps_pair<16>(B, kind);
+// h pairs of samples per lane (edges and viscous units 1; the vertex kernels kLanePairs,
+// the gradients of meshes with boundaries 1).
+long long layout_pair(Batch& B, int st, int kind, int h) {
+  if (h == 1) return st == 32 ? layout_warps_pair<32, 1>(B, kind) : layout_warps_pair<16, 1>(B, kind);
+  return st == 32 ? layout_warps_pair<32, kLanePairs>(B, kind) : layout_warps_pair<16, kLanePairs>(B, kind);
 }
 
 typedef void (*FluxK)(Batch, BParams, int);
@@ -221,11 +224,12 @@ unsigned blocks_of(const Batch& B, int bs) { return (unsigned)((B.work * 32 + bs
 // One full step of every level on b->stream.
 void enqueue_step(tg_batch* b) {
   const Shape sh = kShapes[b->shape];
-  Batch B = b->B, BE = b->B, BB = b->B, BU = b->B;
-  layout_pair(B, sh.st, IT_VERTEX);
-  layout_pair(BE, sh.st, IT_EDGE);
+  Batch B = b->B, BG = b->B, BE = b->B, BB = b->B, BU = b->B;
+  layout_pair(B, sh.st, IT_VERTEX, kLanePairs);
+  layout_pair(BG, sh.st, IT_VERTEX, b->bnd ? 1 : kLanePairs);   // as kb_grad's default
+  layout_pair(BE, sh.st, IT_EDGE, 1);
   layout(BB, sh.st, IT_BSLOT);
-  layout(BU, sh.st, IT_UNIT);
+  layout_pair(BU, sh.st, IT_UNIT, 1);
   const dim3 gs((max_samples(b) + 255) / 256, b->nlev);
   kb_step_begin<<<gs, 256, 0, b->stream>>>(B, b->prm);
   long long dt_blocks = 0;
@@ -237,7 +241,7 @@ void enqueue_step(tg_batch* b) {
   FluxK gk = gather_kernel(b->shape, b->bnd);
   GradK rk = grad_kernel(sh.st, b->bnd);
   for (int r = 0; r < 3; ++r) {
-    if (needs_grad(b)) rk<<<blocks_of(B, sh.bs), sh.bs, 0, b->stream>>>(B, b->prm, r, 0);
+    if (needs_grad(b)) rk<<<blocks_of(BG, sh.bs), sh.bs, 0, b->stream>>>(BG, b->prm, r, 0);
     if (b->bnd && BB.work > 0) bflux_kernel(b->prm.flux, b->shape)<<<blocks_of(BB, sh.bs), sh.bs, 0, b->stream>>>(BB, b->prm, r);
     if (b->prm.model == 1) viscous_kernel(b->shape)<<<blocks_of(BU, sh.bs), sh.bs, 0, b->stream>>>(BU, b->prm, r);
     fk<<<blocks_of(BE, sh.bs), sh.bs, 0, b->stream>>>(BE, b->prm, r);
@@ -366,8 +370,14 @@ tg_status tg_batch_create(const tg_batch_level* levels, int n_levels, const tg_m
     LevelMesh& m = V.m;
     m.nv = L.nv; m.ne = L.ne;
     // geometry formed in FP64, stored in FP32
-    std::vector<double> ux(L.ne), uy(L.ne), ar(L.ne), aw(L.nv);
+    std::vector<double> ux(L.ne), uy(L.ne), ar(L.ne), aw(L.nv), visw(L.nv, 0.0);
     for (int v = 0; v < L.nv; ++v) aw[v] = L.dcarea[v] * L.pweight[v];
+    for (int v = 0; v < L.nv; ++v)
+      for (int j = L.ce_off[v]; j < L.ce_off[v + 1]; ++j) {
+        const int e = L.ce_ent[j] >> 1;
+        visw[v] += std::sqrt(L.e_nx[e] * L.e_nx[e] + L.e_ny[e] * L.e_ny[e]) /
+                   std::sqrt(L.e_dx[e] * L.e_dx[e] + L.e_dy[e] * L.e_dy[e]);
+      }
     for (int e = 0; e < L.ne; ++e) {
       const double a = std::sqrt(L.e_nx[e] * L.e_nx[e] + L.e_ny[e] * L.e_ny[e]);
       const double ia = a > 0.0 ? 1.0 / a : 0.0;   // gradient-only edges carry no flux
@@ -377,7 +387,7 @@ tg_status tg_batch_create(const tg_batch_level* levels, int n_levels, const tg_m
     if ((st = bupload(b, vec, &m.field)) != TG_OK) { tg_batch_destroy(b); return st; }
     BU(L.e_a, e_a) BU(L.e_b, e_b) BU(ux, ux) BU(uy, uy) BU(ar, ar) BU(L.e_nx, nx) BU(L.e_ny, ny)
     BU(L.e_dx, dx) BU(L.e_dy, dy) BU(L.e_g0x, g0x) BU(L.e_g0y, g0y) BU(L.e_g1x, g1x) BU(L.e_g1y, g1y)
-    BU(L.ce_off, ce_off) BU(L.ce_ent, ce_ent) BU(L.dcarea, area) BU(L.inv6mc, inv6mc) BU(L.x, x) BU(L.y, y) BU(aw, aw)
+    BU(L.ce_off, ce_off) BU(L.ce_ent, ce_ent) BU(L.dcarea, area) BU(L.inv6mc, inv6mc) BU(visw, visw) BU(L.x, x) BU(L.y, y) BU(aw, aw)
     m.nb = L.nb; m.nvu = L.nvu; m.nic = L.n_int_cells;
     BU(L.b_v0, b_v0) BU(L.b_v1, b_v1) BU(L.b_kind, b_kind) BU(L.b_adiab, b_adiab) BU(L.b_nx, b_nx) BU(L.b_ny, b_ny)
     BU(L.cb_off, cb_off) BU(L.cb_ent, cb_ent)
@@ -603,7 +613,7 @@ tg_status tg_batch_forces(tg_batch* b, int level, int n_forces, const int* n_tag
   // the viscous force reads the vertex gradients of the current state (src/force.cc:123)
   const Shape sh = kShapes[0];
   Batch B = b->B;
-  layout_pair(B, sh.st, IT_VERTEX);
+  layout_pair(B, sh.st, IT_VERTEX, 1);   // kb_grad<*, true> takes one pair per lane
   if (b->prm.model == 1) grad_kernel(sh.st, true)<<<blocks_of(B, sh.bs), sh.bs, 0, b->stream>>>(B, b->prm, 0, 1);
   int* drec = nullptr;
   int* doff = nullptr;

@@ -45,6 +45,7 @@ struct LevelMesh {
   const float *g0x, *g0y, *g1x, *g1y;   // P1 gradient weights of the a / b side
   const int *ce_off, *ce_ent;      // per-vertex gather: (edge << 1) | side
   const float *area, *inv6mc;      // dual area, 1 / (6 median area)
+  const float* visw;               // sum over the vertex's edges of |n| / |x_b - x_a| (viscous time step)
   const double* aw;                // dual area x periodic-copy weight (integrals)
   const double *x, *y;             // coordinates (initial conditions)
   // non-periodic boundary faces and the per-vertex boundary / viscous gather
@@ -628,18 +629,19 @@ __device__ __forceinline__ Item item_of(const Batch& B, unsigned w, int lane) {
   return it;
 }
 
-// Paired kernels (gradients, edge fluxes, gather + update): ST/2 lanes per
-// item, each lane holding two neighbouring samples, so a warp covers 64/ST
-// items x ST samples.
-template <int ST>
+// Paired kernels (gradients, edge fluxes, gather + update): each lane holds H
+// pairs of neighbouring samples, ST / (2 H) lanes per item, so a warp covers
+// 64 H / ST items x ST samples.
+template <int ST, int H = 1>
 __host__ __device__ __forceinline__ long long level_warps_pair(int nv, int S) {
-  constexpr int IPW = 64 / ST;
+  constexpr int IPW = 64 * H / ST;
   return (long long)((nv + IPW - 1) / IPW) * (S / ST);
 }
 
-template <int ST, int KIND = IT_VERTEX>
+template <int ST, int KIND = IT_VERTEX, int H = 1>
 __device__ __forceinline__ Item item_of_pair(const Batch& B, unsigned w, int lane) {
-  constexpr unsigned LPI = ST / 2, IPW = 64 / ST;
+  constexpr unsigned LPI = ST / (2 * H), IPW = 64 * H / ST;
+  static_assert(LPI >= 1, "sample tile too small for the pairs per lane");
   Item it{0, 0, 0, false};
   if ((long long)w >= B.work) return it;
   int l = 0;
@@ -651,11 +653,17 @@ __device__ __forceinline__ Item item_of_pair(const Batch& B, unsigned w, int lan
   const unsigned nvw = (n + IPW - 1) / IPW;
   const unsigned tile = r / nvw;
   it.l = l;
-  it.s = (int)(tile * ST) + 2 * (int)(lane % LPI);
+  it.s = (int)(tile * ST) + 2 * H * (int)(lane % LPI);
   it.v = (int)((r - tile * nvw) * IPW) + (int)(lane / LPI);
   it.ok = it.v < (int)n;
   return it;
 }
+
+// Pairs per lane of the gradient and gather passes.
+#ifndef TG_BATCH_LANE_PAIRS
+#define TG_BATCH_LANE_PAIRS 2
+#endif
+constexpr int kLanePairs = TG_BATCH_LANE_PAIRS;
 
 // Row block of item i in a [item][C][sample] array (add the sample, then c * S).
 __device__ __forceinline__ size_t rows(int i, int C, int S) { return (size_t)i * C * S; }
@@ -718,14 +726,9 @@ __global__ void __launch_bounds__(32 * VT) kb_dt(Batch B, BParams k, int chunks)
           const float nx = L.m.b_nx[d], ny = L.m.b_ny[d];
           lam += 0.5f * (fabsf(u * nx + w * ny) + c * sqrtf(nx * nx + ny * ny));
         }
-        if (k.model == 1) {
-          const float mu = L.mu[s];
-          for (int j = L.m.ce_off[v]; j < L.m.ce_off[v + 1]; ++j) {
-            const int e = L.m.ce_ent[j] >> 1;
-            const float dx = L.m.dx[e], dy = L.m.dy[e];
-            lam += mu * L.m.ar[e] / sqrtf(dx * dx + dy * dy) / rho;
-          }
-        }
+        // the viscous terms mu |n_e| / |d_e| / rho summed over the vertex's edges, the
+        // geometric sum formed once per mesh
+        if (k.model == 1) lam += L.mu[s] * L.m.visw[v] / rho;
       }
       const float dtv = k.cfl * L.m.area[v] / lam;
       m = fminf(m, dtv > 0.0f ? dtv : __int_as_float(0x7f800000));
@@ -763,46 +766,59 @@ __global__ void kb_dt_final(Batch B, BParams k) {
 }
 
 // Gradients of the entropy variables (src/fv.cc:699-1059 in the edge form
-// grad_v = sum_e g_{v,e} (W_o - W_v) / (6 mcarea)), one vertex and a pair of
+// grad_v = sum_e g_{v,e} (W_o - W_v) / (6 mcarea)), one vertex and H pairs of
 // samples per thread.  BND adds the boundary-face corrections
 // n_b (W_b0 + W_b1 - W_0 - W_1) / 2 (src/fv.cc:926-966).  every != 0: all
-// samples, held ones included (forces); otherwise a pair whose two samples
-// are both held skips.
-template <int ST, bool BND>
+// samples, held ones included (forces); otherwise a thread whose samples are
+// all held skips.
+template <int ST, bool BND, int H = BND ? 1 : kLanePairs>
 __global__ void kb_grad(Batch B, BParams k, int r, int every) {
   const unsigned w = blockIdx.x * (blockDim.x >> 5) + (threadIdx.x >> 5);
-  const Item it = item_of_pair<ST>(B, w, threadIdx.x & 31);
+  const Item it = item_of_pair<ST, IT_VERTEX, H>(B, w, threadIdx.x & 31);
   if (!it.ok) return;
   const Level& L = B.lev[it.l];
   const int v = it.v, s = it.s;
   if (!every) {
-    const int2 act = *reinterpret_cast<const int2*>(L.c.active + s);
-    if (!act.x && !act.y) return;
+    bool any = false;
+#pragma unroll
+    for (int h = 0; h < H; ++h) {
+      const int2 act = *reinterpret_cast<const int2*>(L.c.active + s + 2 * h);
+      any = any || act.x || act.y;
+    }
+    if (!any) return;
   }
   const int S = L.P;   // row pitch
   const float* Q = L.Q[r] + s;
-  auto W = [&](int x, f2* o) {   // V2 = 2 beta u = -V5 u
+  auto W = [&](int x, f2 (*o)[4]) {   // V2 = 2 beta u = -V5 u
     const float* q = Q + rows(x, kQ, S);
-    const f2 V5 = ld2(q + 4 * S), nV5 = neg2(V5);
-    o[0] = ld2(q + 3 * S); o[1] = mul2(nV5, ld2(q)); o[2] = mul2(nV5, ld2(q + S)); o[3] = V5;
-  };
-  f2 ws[4];
-  W(v, ws);
-  f2 acc[kG];
 #pragma unroll
-  for (int c = 0; c < kG; ++c) acc[c] = sp(0.0f);
+    for (int h = 0; h < H; ++h) {
+      const f2 V5 = ld2(q + 4 * S + 2 * h), nV5 = neg2(V5);
+      o[h][0] = ld2(q + 3 * S + 2 * h); o[h][1] = mul2(nV5, ld2(q + 2 * h)); o[h][2] = mul2(nV5, ld2(q + S + 2 * h));
+      o[h][3] = V5;
+    }
+  };
+  f2 ws[H][4];
+  W(v, ws);
+  f2 acc[H][kG];
+#pragma unroll
+  for (int h = 0; h < H; ++h)
+#pragma unroll
+    for (int c = 0; c < kG; ++c) acc[h][c] = sp(0.0f);
   for (int j = L.m.ce_off[v]; j < L.m.ce_off[v + 1]; ++j) {
     const int ent = L.m.ce_ent[j], e = ent >> 1, side = ent & 1;
     const int o = side ? L.m.e_a[e] : L.m.e_b[e];
     const f2 gx = sp(side ? L.m.g1x[e] : L.m.g0x[e]), gy = sp(side ? L.m.g1y[e] : L.m.g0y[e]);
-    f2 wo[4];
+    f2 wo[H][4];
     W(o, wo);
 #pragma unroll
-    for (int c = 0; c < 4; ++c) {
-      const f2 d = sub2(wo[c], ws[c]);
-      acc[2 * c] = fma2(gx, d, acc[2 * c]);
-      acc[2 * c + 1] = fma2(gy, d, acc[2 * c + 1]);
-    }
+    for (int h = 0; h < H; ++h)
+#pragma unroll
+      for (int c = 0; c < 4; ++c) {
+        const f2 d = sub2(wo[h][c], ws[h][c]);
+        acc[h][2 * c] = fma2(gx, d, acc[h][2 * c]);
+        acc[h][2 * c + 1] = fma2(gy, d, acc[h][2 * c + 1]);
+      }
   }
   if (BND) {
     for (int j = L.m.cb_off[v]; j < L.m.cb_off[v + 1]; ++j) {
@@ -814,39 +830,54 @@ __global__ void kb_grad(Batch B, BParams k, int r, int every) {
       const float* val = L.bval + rows(d, 10, S) + s;
       const float* q0 = Q + rows(L.m.b_v0[d], kQ, S);
       const float* q1 = Q + rows(L.m.b_v1[d], kQ, S);
-      FEnt e0[2], e1[2];
-#pragma unroll
-      for (int h = 0; h < 2; ++h) {
-        e0[h] = fbc_ent(k, kind, ad, val + h, S, nx, ny, q0 + h);
-        e1[h] = fbc_ent(k, kind, ad, val + 5 * S + h, S, nx, ny, q1 + h);
-      }
-      const f2 eb[4] = {add2(make_float2(e0[0].f, e0[1].f), make_float2(e1[0].f, e1[1].f)),
-                        add2(make_float2(e0[0].vx, e0[1].vx), make_float2(e1[0].vx, e1[1].vx)),
-                        add2(make_float2(e0[0].vy, e0[1].vy), make_float2(e1[0].vy, e1[1].vy)),
-                        add2(make_float2(e0[0].l, e0[1].l), make_float2(e1[0].l, e1[1].l))};
-      f2 w0[4], w1[4];
+      f2 w0[H][4], w1[H][4];
       W(L.m.b_v0[d], w0);
       W(L.m.b_v1[d], w1);
 #pragma unroll
-      for (int c = 0; c < 4; ++c) {
-        const f2 dW = mul2(sub2(sub2(eb[c], w0[c]), w1[c]), sp(0.5f));
-        acc[2 * c] = fma2(sp(nx), dW, acc[2 * c]);
-        acc[2 * c + 1] = fma2(sp(ny), dW, acc[2 * c + 1]);
+      for (int h = 0; h < H; ++h) {
+        FEnt e0[2], e1[2];
+#pragma unroll
+        for (int c = 0; c < 2; ++c) {
+          const int o = 2 * h + c;
+          e0[c] = fbc_ent(k, kind, ad, val + o, S, nx, ny, q0 + o);
+          e1[c] = fbc_ent(k, kind, ad, val + 5 * S + o, S, nx, ny, q1 + o);
+        }
+        const f2 eb[4] = {add2(make_float2(e0[0].f, e0[1].f), make_float2(e1[0].f, e1[1].f)),
+                          add2(make_float2(e0[0].vx, e0[1].vx), make_float2(e1[0].vx, e1[1].vx)),
+                          add2(make_float2(e0[0].vy, e0[1].vy), make_float2(e1[0].vy, e1[1].vy)),
+                          add2(make_float2(e0[0].l, e0[1].l), make_float2(e1[0].l, e1[1].l))};
+#pragma unroll
+        for (int c = 0; c < 4; ++c) {
+          const f2 dW = mul2(sub2(sub2(eb[c], w0[h][c]), w1[h][c]), sp(0.5f));
+          acc[h][2 * c] = fma2(sp(nx), dW, acc[h][2 * c]);
+          acc[h][2 * c + 1] = fma2(sp(ny), dW, acc[h][2 * c + 1]);
+        }
       }
     }
   }
   const f2 f = sp(L.m.inv6mc[v]);
   float* G = L.G + rows(v, kG, S) + s;
 #pragma unroll
-  for (int c = 0; c < kG; ++c) st2(G + c * S, mul2(acc[c], f));
+  for (int h = 0; h < H; ++h)
+#pragma unroll
+    for (int c = 0; c < kG; ++c) st2(G + c * S + 2 * h, mul2(acc[h][c], f));
 }
 
 // Edge fluxes of one stage (src/fv.cc:1066-1192, src/material.cc:27-74): one
 // edge and a pair of samples per thread, the flux of the edge's own
 // orientation (a left, b right) times |n|, stored for the gather.  A pair
 // whose two samples are both held skips.
+// Resident threads per SM the edge pass is compiled for (0: the compiler's choice).
+#ifndef TG_BATCH_EDGE_THREADS
+#define TG_BATCH_EDGE_THREADS 896
+#endif
+#if TG_BATCH_EDGE_THREADS > 0
+#define TG_EDGE_BOUNDS(BS) __launch_bounds__(BS, TG_BATCH_EDGE_THREADS / (BS))
+#else
+#define TG_EDGE_BOUNDS(BS) __launch_bounds__(BS)
+#endif
 template <int FLUX, int RECON, int ST, int BS>
-__global__ void __launch_bounds__(BS) kb_edge_flux(Batch B, BParams k, int r) {
+__global__ void TG_EDGE_BOUNDS(BS) kb_edge_flux(Batch B, BParams k, int r) {
   const unsigned w = blockIdx.x * (blockDim.x >> 5) + (threadIdx.x >> 5);
   const Item it = item_of_pair<ST, IT_EDGE>(B, w, threadIdx.x & 31);
   if (!it.ok) return;
@@ -920,32 +951,78 @@ __global__ void __launch_bounds__(BS) kb_bflux(Batch B, BParams k, int r) {
 // state (interior cells: the three vertices; boundary cells: the boundary
 // states of the cell's boundary-face vertices), and the viscous flux through
 // each vertex's P1 normal; a boundary unit adds the face's viscous flux with
-// the adiabatic heat-flux correction.  One (unit, sample) per thread.
+// the adiabatic heat-flux correction.  One unit and a pair of samples per
+// thread; boundary states per component (fbc_ent), the rest paired.
+struct PViscK { f2 a1, a2, a4, b1, b2, b4, e4, c2; };
+
+// Viscous matrices K dV (src/material.cc:158-230) for a pair, as fviscous_K.
+__device__ __forceinline__ PViscK pviscous_K(const BParams& k, f2 mu, f2 vx, f2 vy, f2 l, const f2* dE) {
+  f2 kk = mul2(mu, sp(k.cp_over_pr));
+  if (!k.visc) mu = sp(0.0f);
+  if (!k.heat) kk = sp(0.0f);
+  const f2 e4 = make_float2(1.0f / l.x, 1.0f / l.y);
+  const f2 e1 = mul2(vx, e4), e2 = mul2(vy, e4);
+  const f2 c1 = make_float2(4.0f * mu.x / 3.0f, 4.0f * mu.y / 3.0f);
+  const f2 c2 = make_float2(kk.x / k.R, kk.y / k.R);
+  const f2 c3 = make_float2(2.0f * mu.x / 3.0f, 2.0f * mu.y / 3.0f);
+  const f2 d1x = dE[2], d1y = dE[3], d2x = dE[4], d2y = dE[5], d4x = dE[6], d4y = dE[7];
+  const f2 c1e1 = mul2(c1, e1), c1e2 = mul2(c1, e2), mue1 = mul2(mu, e1), mue2 = mul2(mu, e2);
+  const f2 mmc = mul2(mul2(sub2(mu, c3), e1), e2);            // (mu - c3) e1 e2
+  const f2 c2e4 = mul2(c2, e4);
+  const f2 K11_1 = mul2(c1, fma2(e1, d4x, neg2(d1x)));
+  const f2 K11_2 = mul2(mu, fma2(e2, d4x, neg2(d2x)));
+  const f2 K11_4 = fma2(add2(sub2(neg2(mul2(c1e1, e1)), mul2(mu, mul2(e2, e2))), c2e4), d4x,
+                        add2(mul2(c1e1, d1x), mul2(mu, mul2(e2, d2x))));
+  const f2 K12_1 = mul2(c3, fma2(neg2(e2), d4y, d2y));
+  const f2 K12_2 = mul2(mu, fma2(e1, d4y, neg2(d1y)));
+  const f2 K12_4 = sub2(sub2(mul2(mue2, d1y), mul2(mul2(c3, e1), d2y)), mul2(mmc, d4y));
+  const f2 K21_2 = mul2(c3, fma2(neg2(e1), d4x, d1x));
+  const f2 K21_4 = sub2(add2(neg2(mul2(mul2(c3, e2), d1x)), mul2(mue1, d2x)), mul2(mmc, d4x));
+  const f2 K22_2 = mul2(c1, fma2(e2, d4y, neg2(d2y)));
+  const f2 K22_4 = fma2(add2(sub2(neg2(mul2(mu, mul2(e1, e1))), mul2(c1e2, e2)), c2e4), d4y,
+                        add2(mul2(mu, mul2(e1, d1y)), mul2(c1e2, d2y)));
+  PViscK r;
+  r.a1 = add2(K11_1, K12_1); r.a2 = add2(K11_2, K12_2); r.a4 = add2(K11_4, K12_4);
+  r.b1 = add2(K11_2, K12_2);                                  // K21_1 = K11_2, K22_1 = K12_2
+  r.b2 = add2(K21_2, K22_2); r.b4 = add2(K21_4, K22_4);
+  r.e4 = e4;
+  r.c2 = c2;
+  return r;
+}
+
+__device__ __forceinline__ void pviscous_apply(const PViscK& K, float nx, float ny, f2& fx, f2& fy, f2& fe) {
+  const f2 me4 = neg2(K.e4), X = sp(nx), Y = sp(ny);
+  fx = mul2(fma2(K.b1, Y, mul2(K.a1, X)), me4);
+  fy = mul2(fma2(K.b2, Y, mul2(K.a2, X)), me4);
+  fe = mul2(fma2(K.b4, Y, mul2(K.a4, X)), me4);
+}
+
 template <int ST, int BS>
 __global__ void __launch_bounds__(BS) kb_viscous(Batch B, BParams k, int r) {
   const unsigned w = blockIdx.x * (blockDim.x >> 5) + (threadIdx.x >> 5);
-  const Item it = item_of<ST, IT_UNIT>(B, w, threadIdx.x & 31);
+  const Item it = item_of_pair<ST, IT_UNIT>(B, w, threadIdx.x & 31);
   if (!it.ok) return;
   const Level& L = B.lev[it.l];
   const int u = it.v, s = it.s;
-  if (!L.c.active[s]) return;
+  const int2 act = *reinterpret_cast<const int2*>(L.c.active + s);
+  if (!act.x && !act.y) return;
   const int S = L.P;   // row pitch
   const float* Q = L.Q[r] + s;
+  auto W = [&](int x, f2* o) {   // V2 = 2 beta u = -V5 u
+    const float* q = Q + rows(x, kQ, S);
+    const f2 V5 = ld2(q + 4 * S), nV5 = neg2(V5);
+    o[0] = ld2(q + 3 * S); o[1] = mul2(nV5, ld2(q)); o[2] = mul2(nV5, ld2(q + S)); o[3] = V5;
+  };
   const int c = L.m.u_cell[u];
-  const int cv[3] = {L.m.c_v[3 * c], L.m.c_v[3 * c + 1], L.m.c_v[3 * c + 2]};
   const float* n = L.m.c_n + 6 * (size_t)c;
-  float wv[3][4];
+  f2 wv[3][4];
 #pragma unroll
-  for (int i = 0; i < 3; ++i) {
-    const float* q = Q + rows(cv[i], kQ, S);
-    const float V5 = q[4 * S];
-    wv[i][0] = q[3 * S]; wv[i][1] = -V5 * q[0]; wv[i][2] = -V5 * q[S]; wv[i][3] = V5;
-  }
-  float dE[kG];
+  for (int i = 0; i < 3; ++i) W(L.m.c_v[3 * c + i], wv[i]);
+  f2 dE[kG];
 #pragma unroll
   for (int i = 0; i < 4; ++i) {
-    dE[2 * i] = n[0] * wv[0][i] + n[2] * wv[1][i] + n[4] * wv[2][i];
-    dE[2 * i + 1] = n[1] * wv[0][i] + n[3] * wv[1][i] + n[5] * wv[2][i];
+    dE[2 * i] = fma2(sp(n[4]), wv[2][i], fma2(sp(n[2]), wv[1][i], mul2(sp(n[0]), wv[0][i])));
+    dE[2 * i + 1] = fma2(sp(n[5]), wv[2][i], fma2(sp(n[3]), wv[1][i], mul2(sp(n[1]), wv[0][i])));
   }
   for (int j = L.m.c_bf_off[c]; j < L.m.c_bf_off[c + 1]; ++j) {
     const int d = L.m.c_bf[j];
@@ -954,30 +1031,36 @@ __global__ void __launch_bounds__(BS) kb_viscous(Batch B, BParams k, int r) {
     const float* val = L.bval + rows(d, 10, S) + s;
     const float* q0 = Q + rows(L.m.b_v0[d], kQ, S);
     const float* q1 = Q + rows(L.m.b_v1[d], kQ, S);
-    const FEnt e0 = fbc_ent(k, kind, ad, val, S, nx, ny, q0);
-    const FEnt e1 = fbc_ent(k, kind, ad, val + 5 * S, S, nx, ny, q1);
-    const float dW[4] = {(e0.f + e1.f - q0[3 * S] - q1[3 * S]) * 0.5f,
-                         (e0.vx + e1.vx - (-q0[4 * S] * q0[0]) - (-q1[4 * S] * q1[0])) * 0.5f,
-                         (e0.vy + e1.vy - (-q0[4 * S] * q0[S]) - (-q1[4 * S] * q1[S])) * 0.5f,
-                         (e0.l + e1.l - q0[4 * S] - q1[4 * S]) * 0.5f};
+    FEnt e0[2], e1[2];
+#pragma unroll
+    for (int h = 0; h < 2; ++h) {
+      e0[h] = fbc_ent(k, kind, ad, val + h, S, nx, ny, q0 + h);
+      e1[h] = fbc_ent(k, kind, ad, val + 5 * S + h, S, nx, ny, q1 + h);
+    }
+    f2 w0[4], w1[4];
+    W(L.m.b_v0[d], w0);
+    W(L.m.b_v1[d], w1);
+    const f2 eb[4] = {add2(make_float2(e0[0].f, e0[1].f), make_float2(e1[0].f, e1[1].f)),
+                      add2(make_float2(e0[0].vx, e0[1].vx), make_float2(e1[0].vx, e1[1].vx)),
+                      add2(make_float2(e0[0].vy, e0[1].vy), make_float2(e1[0].vy, e1[1].vy)),
+                      add2(make_float2(e0[0].l, e0[1].l), make_float2(e1[0].l, e1[1].l))};
 #pragma unroll
     for (int i = 0; i < 4; ++i) {
-      dE[2 * i] += nx * dW[i];
-      dE[2 * i + 1] += ny * dW[i];
+      const f2 dW = mul2(sub2(sub2(eb[i], w0[i]), w1[i]), sp(0.5f));
+      dE[2 * i] = fma2(sp(nx), dW, dE[2 * i]);
+      dE[2 * i + 1] = fma2(sp(ny), dW, dE[2 * i + 1]);
     }
   }
-  const float f = L.m.c_inv2a[c];
+  const f2 f = sp(L.m.c_inv2a[c]);
 #pragma unroll
-  for (int i = 0; i < kG; ++i) dE[i] *= f;
-  FEnt avg;
+  for (int i = 0; i < kG; ++i) dE[i] = mul2(dE[i], f);
+  f2 avg[4];
   if (u < L.m.nic) {
-    const float t3 = 1.0f / 3.0f;
-    avg.f = wv[0][0] * t3 + wv[1][0] * t3 + wv[2][0] * t3;
-    avg.vx = wv[0][1] * t3 + wv[1][1] * t3 + wv[2][1] * t3;
-    avg.vy = wv[0][2] * t3 + wv[1][2] * t3 + wv[2][2] * t3;
-    avg.l = wv[0][3] * t3 + wv[1][3] * t3 + wv[2][3] * t3;
+    const f2 t3 = sp(1.0f / 3.0f);
+#pragma unroll
+    for (int i = 0; i < 4; ++i) avg[i] = fma2(wv[2][i], t3, fma2(wv[1][i], t3, mul2(wv[0][i], t3)));
   } else {
-    avg.f = avg.vx = avg.vy = avg.l = 0.0f;
+    float a[2][4] = {{0.0f, 0.0f, 0.0f, 0.0f}, {0.0f, 0.0f, 0.0f, 0.0f}};
     const int cnt = L.m.c_nbr_off[c + 1] - L.m.c_nbr_off[c];
     for (int j = L.m.c_nbr_off[c]; j < L.m.c_nbr_off[c + 1]; ++j) {
       const int d = L.m.c_nbr[j];
@@ -985,37 +1068,48 @@ __global__ void __launch_bounds__(BS) kb_viscous(Batch B, BParams k, int r) {
       for (int q = 0; q < 2; ++q) {
         const int vb = q ? L.m.bf_v1[d] : L.m.bf_v0[d];
         const float* val = L.bval + rows(d, 10, S) + (vb == L.m.b_v0[d] ? 0 : 5) * S + s;
-        const FEnt e = fbc_ent(k, L.m.b_kind[d], L.m.b_adiab[d], val, S, L.m.bf_nx[d], L.m.bf_ny[d],
-                               Q + rows(vb, kQ, S));
-        avg.f += e.f; avg.vx += e.vx; avg.vy += e.vy; avg.l += e.l;
+#pragma unroll
+        for (int h = 0; h < 2; ++h) {
+          const FEnt e = fbc_ent(k, L.m.b_kind[d], L.m.b_adiab[d], val + h, S, L.m.bf_nx[d], L.m.bf_ny[d],
+                                 Q + rows(vb, kQ, S) + h);
+          a[h][0] += e.f; a[h][1] += e.vx; a[h][2] += e.vy; a[h][3] += e.l;
+        }
       }
     }
-    const float sc = 0.5f / (float)cnt;
-    avg.f *= sc; avg.vx *= sc; avg.vy *= sc; avg.l *= sc;
+    const f2 sc = sp(0.5f / (float)cnt);
+#pragma unroll
+    for (int i = 0; i < 4; ++i) avg[i] = mul2(make_float2(a[0][i], a[1][i]), sc);
   }
-  const FViscK K = fviscous_K(k, L.mu[s], avg, dE);
+  const PViscK K = pviscous_K(k, make_float2(L.mu[s], L.mu[s + 1]), avg[1], avg[2], avg[3], dE);
   float* Fo = L.Fv + rows(u, 9, S) + s;
 #pragma unroll
-  for (int q = 0; q < 3; ++q) fviscous_apply(K, n[2 * q], n[2 * q + 1], Fo[(3 * q) * S], Fo[(3 * q + 1) * S], Fo[(3 * q + 2) * S]);
+  for (int q = 0; q < 3; ++q) {
+    f2 fx, fy, fe;
+    pviscous_apply(K, n[2 * q], n[2 * q + 1], fx, fy, fe);
+    st2(Fo + (3 * q) * S, fx); st2(Fo + (3 * q + 1) * S, fy); st2(Fo + (3 * q + 2) * S, fe);
+  }
   if (u >= L.m.nic) {
     const int d = u - L.m.nic;
     const float nbx = L.m.b_nx[d], nby = L.m.b_ny[d];
-    const float cor = L.m.b_adiab[d] ? -(K.c2 * K.e4 * K.e4 * (dE[6] * nbx + dE[7] * nby)) : 0.0f;
-    float fx, fy, fe;
-    fviscous_apply(K, nbx, nby, fx, fy, fe);
+    f2 fx, fy, fe;
+    pviscous_apply(K, nbx, nby, fx, fy, fe);
+    if (L.m.b_adiab[d]) {   // fe - cor with cor = -(c2 e4^2 (dT/dn)) (the adiabatic wall's heat flux)
+      const f2 dn = fma2(dE[7], sp(nby), mul2(dE[6], sp(nbx)));
+      fe = fma2(mul2(mul2(K.c2, K.e4), K.e4), dn, fe);
+    }
     float* Fb = L.Fvb + rows(d, 3, S) + s;
-    Fb[0] = fx; Fb[S] = fy; Fb[2 * S] = fe - cor;
+    st2(Fb, fx); st2(Fb + S, fy); st2(Fb + 2 * S, fe);
   }
 }
 
 // Residual gather in the fixed per-vertex edge order and the SSP-RK3 stage
-// update (src/fv.cc:1635-1658), state r -> state (r+1) % 3, one vertex and a
-// pair of samples per thread.  Held or finished samples copy their state
+// update (src/fv.cc:1635-1658), state r -> state (r+1) % 3, one vertex and H
+// pairs of samples per thread.  Held or finished samples copy their state
 // through.
-template <int ST, int BS, bool BND>
+template <int ST, int BS, bool BND, int H = kLanePairs>
 __global__ void __launch_bounds__(BS) kb_gather_update(Batch B, BParams k, int r) {
   const unsigned w = blockIdx.x * (blockDim.x >> 5) + (threadIdx.x >> 5);
-  const Item it = item_of_pair<ST>(B, w, threadIdx.x & 31);
+  const Item it = item_of_pair<ST, IT_VERTEX, H>(B, w, threadIdx.x & 31);
   if (!it.ok) return;
   const Level& L = B.lev[it.l];
   const int v = it.v, s = it.s;
@@ -1023,21 +1117,34 @@ __global__ void __launch_bounds__(BS) kb_gather_update(Batch B, BParams k, int r
   const size_t ov = rows(v, kQ, S) + s;
   const float* Q = L.Q[r] + ov;
   float* Qn = L.Q[(r + 1) % 3] + ov;
-  const int2 act = *reinterpret_cast<const int2*>(L.c.active + s);
-  if (!act.x && !act.y) {
+  int2 act[H];
+  bool any = false;
 #pragma unroll
-    for (int c = 0; c < kQ; ++c) st2(Qn + c * S, ld2(Q + c * S));
+  for (int h = 0; h < H; ++h) {
+    act[h] = *reinterpret_cast<const int2*>(L.c.active + s + 2 * h);
+    any = any || act[h].x || act[h].y;
+  }
+  if (!any) {
+#pragma unroll
+    for (int h = 0; h < H; ++h)
+#pragma unroll
+      for (int c = 0; c < kQ; ++c) st2(Qn + c * S + 2 * h, ld2(Q + c * S + 2 * h));
     return;
   }
-  f2 r0 = sp(0.0f), r1 = sp(0.0f), r2 = sp(0.0f), r3 = sp(0.0f);
+  f2 r0[H], r1[H], r2[H], r3[H];
+#pragma unroll
+  for (int h = 0; h < H; ++h) r0[h] = r1[h] = r2[h] = r3[h] = sp(0.0f);
   const int j0 = L.m.ce_off[v], j1 = L.m.ce_off[v + 1];
 #pragma unroll 4
   for (int j = j0; j < j1; ++j) {
     const int ent = L.m.ce_ent[j];
     const float* Fe = L.F + rows(ent >> 1, 4, S) + s;
     const f2 sg = sp((ent & 1) ? -1.0f : 1.0f);
-    r0 = fma2(ld2(Fe), sg, r0); r1 = fma2(ld2(Fe + S), sg, r1);
-    r2 = fma2(ld2(Fe + 2 * S), sg, r2); r3 = fma2(ld2(Fe + 3 * S), sg, r3);
+#pragma unroll
+    for (int h = 0; h < H; ++h) {
+      r0[h] = fma2(ld2(Fe + 2 * h), sg, r0[h]); r1[h] = fma2(ld2(Fe + S + 2 * h), sg, r1[h]);
+      r2[h] = fma2(ld2(Fe + 2 * S + 2 * h), sg, r2[h]); r3[h] = fma2(ld2(Fe + 3 * S + 2 * h), sg, r3[h]);
+    }
   }
   if (BND) {   // boundary and viscous contributions in list order (src/fv.cc:1100-1188, 1197-1320)
     for (int j = L.m.cb_off[v]; j < L.m.cb_off[v + 1]; ++j) {
@@ -1045,49 +1152,62 @@ __global__ void __launch_bounds__(BS) kb_gather_update(Batch B, BParams k, int r
       const int type = ent & 3, idx = ent >> 2;
       if (type == 0) {
         const float* Fe = L.Fb + rows(idx, 4, S) + s;
-        const f2 h = sp(0.5f);
-        r0 = fma2(ld2(Fe), h, r0); r1 = fma2(ld2(Fe + S), h, r1);
-        r2 = fma2(ld2(Fe + 2 * S), h, r2); r3 = fma2(ld2(Fe + 3 * S), h, r3);
+        const f2 hf = sp(0.5f);
+#pragma unroll
+        for (int h = 0; h < H; ++h) {
+          r0[h] = fma2(ld2(Fe + 2 * h), hf, r0[h]); r1[h] = fma2(ld2(Fe + S + 2 * h), hf, r1[h]);
+          r2[h] = fma2(ld2(Fe + 2 * S + 2 * h), hf, r2[h]); r3[h] = fma2(ld2(Fe + 3 * S + 2 * h), hf, r3[h]);
+        }
       } else if ((type == 2 || type == 3) && k.model == 1) {
         const float* Fe = (type == 2 ? L.Fv : L.Fvb) + rows(idx, 3, S) + s;
-        const f2 h = sp(type == 2 ? -0.5f : 0.5f);
-        r1 = fma2(ld2(Fe), h, r1); r2 = fma2(ld2(Fe + S), h, r2); r3 = fma2(ld2(Fe + 2 * S), h, r3);
+        const f2 hf = sp(type == 2 ? -0.5f : 0.5f);
+#pragma unroll
+        for (int h = 0; h < H; ++h) {
+          r1[h] = fma2(ld2(Fe + 2 * h), hf, r1[h]); r2[h] = fma2(ld2(Fe + S + 2 * h), hf, r2[h]);
+          r3[h] = fma2(ld2(Fe + 2 * S + 2 * h), hf, r3[h]);
+        }
       }
     }
   }
-  const f2 u0 = ld2(Q), v0 = ld2(Q + S), p0 = ld2(Q + 2 * S), V50 = ld2(Q + 4 * S);
-  const f2 rho0 = mul2(neg2(V50), p0);
   // Shu-Osher SSP-RK3 stage (src/constants.h:4-6)
   const f2 a_rk = sp(r == 0 ? 0.0f : (r == 1 ? 0.75f : 1.0f / 3.0f));
   const f2 b_rk = sp(r == 0 ? 1.0f : (r == 1 ? 0.25f : 2.0f / 3.0f));
   const float area = L.m.area[v];
-  const f2 c2 = mul2(make_float2((float)L.c.dt[s] / area, (float)L.c.dt[s + 1] / area), neg2(b_rk));
   const float* Uo = L.Uold + rows(v, 4, S) + s;
-  const f2 cr = fma2(r0, c2, fma2(ld2(Uo), a_rk, mul2(rho0, b_rk)));
-  const f2 cx = fma2(r1, c2, fma2(ld2(Uo + S), a_rk, mul2(mul2(rho0, u0), b_rk)));
-  const f2 cy = fma2(r2, c2, fma2(ld2(Uo + 2 * S), a_rk, mul2(mul2(rho0, v0), b_rk)));
-  const f2 E0 = fma2(p0, sp(k.inv_gm1), mul2(mul2(sp(0.5f), fma2(v0, v0, mul2(u0, u0))), rho0));
-  const f2 cE = fma2(r3, c2, fma2(ld2(Uo + 3 * S), a_rk, mul2(E0, b_rk)));
-  const f2 ir = make_float2(1.0f / cr.x, 1.0f / cr.y);
-  const f2 u = mul2(cx, ir), vv = mul2(cy, ir);
-  const f2 p = mul2(sp(k.gamma - 1.0f), fma2(sp(-0.5f), fma2(cy, vv, mul2(cx, u)), cE));
-  const f2 hc = mul2(sp(0.5f), cr);
-  const f2 beta = make_float2(hc.x / p.x, hc.y / p.y);
-  const f2 sent = make_float2(__fmaf_rn(-k.gamma, logf(cr.x), logf(p.x)), __fmaf_rn(-k.gamma, logf(cr.y), logf(p.y)));
-  const f2 V1 = fma2(sub2(sp(k.gamma), sent), sp(k.inv_gm1), neg2(mul2(fma2(vv, vv, mul2(u, u)), beta)));
-  f2 o[kQ] = {u, vv, p, V1, mul2(sp(-2.0f), beta)};
-  if (!act.x || !act.y) {   // the held sample of the pair keeps its state
 #pragma unroll
-    for (int c = 0; c < kQ; ++c) {
-      const f2 old = ld2(Q + c * S);
-      if (!act.x) o[c].x = old.x;
-      if (!act.y) o[c].y = old.y;
+  for (int h = 0; h < H; ++h) {
+    const int o = 2 * h;
+    const f2 u0 = ld2(Q + o), v0 = ld2(Q + S + o), p0 = ld2(Q + 2 * S + o), V50 = ld2(Q + 4 * S + o);
+    const f2 rho0 = mul2(neg2(V50), p0);
+    const f2 c2 = mul2(make_float2((float)L.c.dt[s + o] / area, (float)L.c.dt[s + o + 1] / area), neg2(b_rk));
+    const f2 cr = fma2(r0[h], c2, fma2(ld2(Uo + o), a_rk, mul2(rho0, b_rk)));
+    const f2 cx = fma2(r1[h], c2, fma2(ld2(Uo + S + o), a_rk, mul2(mul2(rho0, u0), b_rk)));
+    const f2 cy = fma2(r2[h], c2, fma2(ld2(Uo + 2 * S + o), a_rk, mul2(mul2(rho0, v0), b_rk)));
+    const f2 E0 = fma2(p0, sp(k.inv_gm1), mul2(mul2(sp(0.5f), fma2(v0, v0, mul2(u0, u0))), rho0));
+    const f2 cE = fma2(r3[h], c2, fma2(ld2(Uo + 3 * S + o), a_rk, mul2(E0, b_rk)));
+    const f2 ir = make_float2(1.0f / cr.x, 1.0f / cr.y);
+    const f2 u = mul2(cx, ir), vv = mul2(cy, ir);
+    const f2 p = mul2(sp(k.gamma - 1.0f), fma2(sp(-0.5f), fma2(cy, vv, mul2(cx, u)), cE));
+    const f2 hc = mul2(sp(0.5f), cr);
+    const f2 beta = make_float2(hc.x / p.x, hc.y / p.y);
+    const f2 sent = make_float2(__fmaf_rn(-k.gamma, logf(cr.x), logf(p.x)), __fmaf_rn(-k.gamma, logf(cr.y), logf(p.y)));
+    const f2 V1 = fma2(sub2(sp(k.gamma), sent), sp(k.inv_gm1), neg2(mul2(fma2(vv, vv, mul2(u, u)), beta)));
+    f2 out[kQ] = {u, vv, p, V1, mul2(sp(-2.0f), beta)};
+    if (!act[h].x || !act[h].y) {   // a held sample keeps its state
+#pragma unroll
+      for (int c = 0; c < kQ; ++c) {
+        const f2 old = ld2(Q + c * S + o);
+        if (!act[h].x) out[c].x = old.x;
+        if (!act[h].y) out[c].y = old.y;
+      }
     }
-  }
 #pragma unroll
-  for (int c = 0; c < kQ; ++c) st2(Qn + c * S, o[c]);
-  if (act.x && (!(p.x > 0.0f) || !(cr.x > 0.0f) || !isfinite(u.x) || !isfinite(vv.x) || !isfinite(p.x))) L.c.bad[s] = 1;
-  if (act.y && (!(p.y > 0.0f) || !(cr.y > 0.0f) || !isfinite(u.y) || !isfinite(vv.y) || !isfinite(p.y))) L.c.bad[s + 1] = 1;
+    for (int c = 0; c < kQ; ++c) st2(Qn + c * S + o, out[c]);
+    if (act[h].x && (!(p.x > 0.0f) || !(cr.x > 0.0f) || !isfinite(u.x) || !isfinite(vv.x) || !isfinite(p.x)))
+      L.c.bad[s + o] = 1;
+    if (act[h].y && (!(p.y > 0.0f) || !(cr.y > 0.0f) || !isfinite(u.y) || !isfinite(vv.y) || !isfinite(p.y)))
+      L.c.bad[s + o + 1] = 1;
+  }
 }
 
 // Per-sample step end (src/fv.cc:2307-2336).
