@@ -233,7 +233,7 @@ void enqueue_step(tg_batch* b) {
   const dim3 gs((max_samples(b) + 255) / 256, b->nlev);
   kb_step_begin<<<gs, 256, 0, b->stream>>>(B, b->prm);
   long long dt_blocks = 0;
-  for (int l = 0; l < b->nlev; ++l) dt_blocks += (long long)(B.lev[l].S >> 5) * b->dt_chunks;
+  for (int l = 0; l < b->nlev; ++l) dt_blocks += (long long)dt_groups(B.lev[l].S) * b->dt_chunks;
   if (b->bnd) kb_dt<8, true><<<(unsigned)dt_blocks, 256, 0, b->stream>>>(B, b->prm, b->dt_chunks);
   else kb_dt<8, false><<<(unsigned)dt_blocks, 256, 0, b->stream>>>(B, b->prm, b->dt_chunks);
   kb_dt_final<<<gs, 256, 0, b->stream>>>(B, b->prm);
@@ -456,7 +456,7 @@ tg_status tg_batch_create(const tg_batch_level* levels, int n_levels, const tg_m
   cudaMemcpy(b->stop, &inf, sizeof(int), cudaMemcpyHostToDevice);
   // dt kernel: about four blocks per SM over all sample groups
   long long groups = 0;
-  for (int l = 0; l < n_levels; ++l) groups += b->B.lev[l].S >> 5;
+  for (int l = 0; l < n_levels; ++l) groups += dt_groups(b->B.lev[l].S);
   int sms = 148;
   cudaDeviceGetAttribute(&sms, cudaDevAttrMultiProcessorCount, b->device);
   b->dt_chunks = (int)std::max<long long>(1, (4LL * sms + groups - 1) / groups);

@@ -682,10 +682,14 @@ __global__ void kb_step_begin(Batch B, BParams k) {
 }
 
 // Local time step (src/fv.cc:1499-1580) of every vertex and the running
-// per-sample minimum; U_old (src/fv.cc:1626-1630).  Each thread keeps one
-// sample and walks a strided set of vertices, so one atomic per block and
-// sample remains.  BND adds the boundary-face terms and, for Navier-Stokes,
-// the viscous ones, in the reference's order.
+// per-sample minimum; U_old (src/fv.cc:1626-1630).  Each lane keeps a pair of
+// samples (a group of 64; the last group of a level whose sample count is an
+// odd multiple of 32 leaves its upper half-warp idle) and walks a strided set of
+// vertices, so one atomic per block and sample remains.  BND adds the
+// boundary-face terms and, for Navier-Stokes, the viscous ones, in the
+// reference's order.
+__host__ __device__ __forceinline__ int dt_groups(int S) { return (S + 63) / 64; }
+
 template <int VT, bool BND>
 __global__ void __launch_bounds__(32 * VT) kb_dt(Batch B, BParams k, int chunks) {
   const int lane = threadIdx.x & 31, vg = threadIdx.x >> 5;
@@ -694,29 +698,33 @@ __global__ void __launch_bounds__(32 * VT) kb_dt(Batch B, BParams k, int chunks)
   int l = 0;
   long long base = 0;
   for (int i = 0; i < B.nlev; ++i) {
-    const long long nb = (long long)(B.lev[i].S >> 5) * chunks;
+    const long long nb = (long long)dt_groups(B.lev[i].S) * chunks;
     if (bid < base + nb) { l = i; break; }
     base += nb;
   }
   const Level& L = B.lev[l];
-  const long long r = bid - base;
-  const int sg = (int)(r / chunks), ch = (int)(r % chunks);
-  const int s = sg * 32 + lane;
-  const bool act = L.c.active[s];
-  float m = __int_as_float(0x7f800000);
-  if (act) {
+  const int r = (int)(bid - base);
+  const int sg = r / chunks, ch = r - sg * chunks;
+  const int s = sg * 64 + 2 * lane;
+  const int2 act = s < L.S ? *reinterpret_cast<const int2*>(L.c.active + s) : make_int2(0, 0);
+  const float inf = __int_as_float(0x7f800000);
+  f2 m = sp(inf);
+  if (act.x || act.y) {
+    const int P = L.P;
     const int per = (L.m.nv + chunks - 1) / chunks;
     const int v0 = ch * per, v1 = min(L.m.nv, v0 + per);
+    const f2 mu = BND && k.model == 1 ? make_float2(L.mu[s], L.mu[s + 1]) : sp(0.0f);
     for (int v = v0 + vg; v < v1; v += VT) {
-      const float* q = L.Q[0] + rows(v, kQ, L.P) + s;
-      const float u = q[0], w = q[L.P], p = q[2 * L.P], V5 = q[4 * L.P];
-      const float rho = -V5 * p;
-      const float c = sqrtf(k.gamma * p / rho);
-      float lam = 0.0f;
+      const float* q = L.Q[0] + rows(v, kQ, P) + s;
+      const f2 u = ld2(q), w = ld2(q + P), p = ld2(q + 2 * P), V5 = ld2(q + 4 * P);
+      const f2 rho = mul2(neg2(V5), p);
+      const f2 gp = mul2(sp(k.gamma), p);
+      const f2 c = make_float2(sqrtf(gp.x / rho.x), sqrtf(gp.y / rho.y));
+      f2 lam = sp(0.0f);
       for (int j = L.m.ce_off[v]; j < L.m.ce_off[v + 1]; ++j) {
         const int e = L.m.ce_ent[j] >> 1;
-        const float nx = L.m.nx[e], ny = L.m.ny[e];
-        lam += fabsf(u * nx + w * ny) + c * L.m.ar[e];
+        const f2 vn = fma2(w, sp(L.m.ny[e]), mul2(u, sp(L.m.nx[e])));
+        lam = add2(lam, fma2(c, sp(L.m.ar[e]), abs2(vn)));
       }
       if (BND) {
         for (int j = L.m.cb_off[v]; j < L.m.cb_off[v + 1]; ++j) {
@@ -724,28 +732,35 @@ __global__ void __launch_bounds__(32 * VT) kb_dt(Batch B, BParams k, int chunks)
           if ((ent & 3) != 0) continue;
           const int d = ent >> 3;           // entry (2 d + vertex slot) << 2
           const float nx = L.m.b_nx[d], ny = L.m.b_ny[d];
-          lam += 0.5f * (fabsf(u * nx + w * ny) + c * sqrtf(nx * nx + ny * ny));
+          const f2 vn = fma2(w, sp(ny), mul2(u, sp(nx)));
+          lam = fma2(sp(0.5f), fma2(c, sp(sqrtf(nx * nx + ny * ny)), abs2(vn)), lam);
         }
         // the viscous terms mu |n_e| / |d_e| / rho summed over the vertex's edges, the
         // geometric sum formed once per mesh
-        if (k.model == 1) lam += L.mu[s] * L.m.visw[v] / rho;
+        if (k.model == 1) lam = fma2(make_float2(mu.x / rho.x, mu.y / rho.y), sp(L.m.visw[v]), lam);
       }
-      const float dtv = k.cfl * L.m.area[v] / lam;
-      m = fminf(m, dtv > 0.0f ? dtv : __int_as_float(0x7f800000));
+      const float ca = k.cfl * L.m.area[v];
+      const f2 dtv = make_float2(ca / lam.x, ca / lam.y);
+      m.x = fminf(m.x, dtv.x > 0.0f ? dtv.x : inf);
+      m.y = fminf(m.y, dtv.y > 0.0f ? dtv.y : inf);
       // U_old
-      float* uo = L.Uold + rows(v, 4, L.P) + s;
-      uo[0] = rho;
-      uo[L.P] = rho * u;
-      uo[2 * L.P] = rho * w;
-      uo[3 * L.P] = p * k.inv_gm1 + 0.5f * (u * u + w * w) * rho;
+      float* uo = L.Uold + rows(v, 4, P) + s;
+      st2(uo, rho);
+      st2(uo + P, mul2(rho, u));
+      st2(uo + 2 * P, mul2(rho, w));
+      st2(uo + 3 * P, fma2(p, sp(k.inv_gm1), mul2(mul2(sp(0.5f), fma2(w, w, mul2(u, u))), rho)));
     }
   }
-  __shared__ float red[VT][32];
+  __shared__ float2 red[VT][32];
   red[vg][lane] = m;
   __syncthreads();
   if (vg == 0) {
-    for (int i = 1; i < VT; ++i) m = fminf(m, red[i][lane]);
-    if (act) atomicMin(&L.c.dtmin_bits[s], __float_as_uint(m));
+    for (int i = 1; i < VT; ++i) {
+      m.x = fminf(m.x, red[i][lane].x);
+      m.y = fminf(m.y, red[i][lane].y);
+    }
+    if (act.x) atomicMin(&L.c.dtmin_bits[s], __float_as_uint(m.x));
+    if (act.y) atomicMin(&L.c.dtmin_bits[s + 1], __float_as_uint(m.y));
   }
 }
 
