@@ -100,7 +100,10 @@ def parse():
     ap.add_argument("--parts", default="1,2,4", help="partitioned: partition counts")
     ap.add_argument("--throughput-only", action="store_true", help="mc, cylinder: the ensemble's stepping alone")
     ap.add_argument("--mc-cap", type=float, default=120.0,
-                    help="mc: wall-clock cap of the plain FP64 arm of the measured time to 1%% RSE")
+                    help="mc: wall-clock cap of the plain FP64 arm of the measured time to 1%% RSE "
+                         "(cylinder-rse: of the plain and the batched arms)")
+    ap.add_argument("--cv-cap", type=float, default=900.0,
+                    help="cylinder-rse: wall-clock cap of the control-variate arm")
     a = ap.parse_args()
     a.flux_list = [(f, r) for f, r in FLUXES if f in a.fluxes.split(",")]
     return a
@@ -902,7 +905,7 @@ def cylinder_names():
 
 def run_cylinder_rse(args):
     print(json.dumps(cylinder_rse_line(args.final_time, args.outputs, args.t_start, args.seed, args.mc_cap,
-                                       args.mc_cap, 900.0)))
+                                       args.mc_cap, args.cv_cap)))
     return 0
 
 

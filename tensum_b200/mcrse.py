@@ -18,7 +18,11 @@ evaluations.  Handle and batch creation are set-up and stay outside.
 
 An arm may have a wall-clock cap; an arm that hits it reports the errors it
 reached and the time the 1/sqrt(N) law gives for the target from its measured
-rate, marked as extrapolated.
+rate, marked as extrapolated.  Because a capped plain arm may hold few samples
+(the error of a variance estimate is itself noisy there), the summary adds a
+second plain time: the sample count the plain estimator needs, judged on all
+the control-variate arm's solver samples, times the plain arm's measured wall
+time per sample.
 
 Two workloads: Kelvin-Helmholtz samples (rnd-file rows; QoIs 0.5 rho v^2,
 0.5 rho u^2 and -rho s/(gamma-1) integrated over the mesh at the output time)
@@ -139,19 +143,33 @@ def cv_arm(run_batch, draw_extra, rse, n_train, batch_n, train_batch=None, n_ext
             break
     wall = time.perf_counter() - t0
     est = cv.estimate(np.concatenate(Y), np.concatenate(G), g_extra)
+    # the plain estimator's errors on every solver sample this arm drew (training ones included)
+    pm, pv = cv.rse_now(np.concatenate([Ytr] + Y))
     out = dict(wall_s=wall, train_s=t_train, samples=n_train + len(Y) * batch_n, train_samples=n_train,
                eval_samples=len(Y) * batch_n, surrogate_evals=n_extra, reached=reached,
                rse_mean=rm.tolist(), rse_var=rv.tolist(), gain=[float(x) for x in est["gain"]],
-               used=[bool(x) for x in est["used"]])
+               used=[bool(x) for x in est["used"]], plain_rse_mean_same_samples=pm.tolist(),
+               plain_rse_var_same_samples=pv.tolist())
     return out if reached else _capped(out, rm, rv, rse, cap_s)
 
 
 def _summary(rse, pl, bt, cvr):
     def t(a):
         return a["wall_s"] if a["reached"] else a["extrapolated_wall_s"]
+    # A second plain-MC time that does not lean on the capped arm's few samples: the plain
+    # estimator's errors over the control-variate arm's (many more) solver samples give the
+    # sample count it needs, times the plain arm's measured wall time per sample.
+    worst = max(max(m, v) for m, v in zip(cvr["plain_rse_mean_same_samples"], cvr["plain_rse_var_same_samples"]))
+    need = cvr["samples"] * (worst / rse) ** 2
+    per = pl["wall_s"] / max(pl["samples"], 1)
+    by_count = {"samples_needed": need, "wall_s_per_sample": per, "wall_s": need * per,
+                "from": f"plain estimator errors over the {cvr['samples']} solver samples of the control-variate arm"}
     return {"rse": rse, "targets": "mean and variance of every QoI", "plain_fp64": pl, "batched_fp32": bt,
             "batched_fp32_cv": cvr, "speedup_batched_vs_plain_fp64": t(pl) / t(bt),
             "speedup_cv_vs_plain_fp64": t(pl) / t(cvr),
+            "plain_fp64_by_sample_count": by_count,
+            "speedup_cv_vs_plain_fp64_by_sample_count": by_count["wall_s"] / t(cvr),
+            "speedup_batched_vs_plain_fp64_by_sample_count": by_count["wall_s"] / t(bt),
             "time_kind": {k: ("measured" if a["reached"] else "extrapolated from a capped run")
                           for k, a in (("plain_fp64", pl), ("batched_fp32", bt), ("batched_fp32_cv", cvr))}}
 
